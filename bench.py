@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the mesh signed-distance query path (one JSON line on rank 0).
+
+Workload (default): the level-8 displaced icosphere (1,310,720 triangles, Morton-built 4-wide BVH)
+queried on the 512^3 cell-centre grid over [-1.25,1.25]^3 (134,217,728 points) plus 16,777,216
+points within +-1e-3 of the surface: 150,994,944 queries per step, FP32 traversal with the FP64
+near-surface band.  A step is one pass of the query path over all of them.  Inputs are seeded
+synthetic data of that shape (no dataset).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+--impl ours (default): device-resident timing (``value``, CUDA events around K steps, max over
+ranks), end-to-end timing through the host entry point with pinned buffers (``e2e``), the roofline
+of the traversal kernel from per-phase CUDA events recorded on the launching stream during the timed
+steps, nvidia-smi clock samples during the timed region, and (rank 0, N=1) the reference CPU
+implementation timed on a bounded sample of the same points (``cpu_baseline``).
+--impl reference: the reference's own CPU implementation (compiled from its headers into
+oracle/_ref) on all host threads, each step a bounded sample of the same workload.
+Multi-GPU (torchrun): each rank runs the full workload on its own GPU (weak scaling, replicas with
+no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SDF queries/s on 1 B200: learned-seeded vs plain GPU BVH at equal accuracy"
+UNIT = "queries/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--level", type=int, default=8)
+    ap.add_argument("--grid", type=int, default=512)
+    ap.add_argument("--band-points", type=int, default=16 * 1024 * 1024)
+    ap.add_argument("--build", default="Morton")
+    ap.add_argument("--leaf", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    return ap.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def workload(args):
+    from ebgeometry_b200 import workloads as W
+    v, f = W.displaced_icosphere(args.level, 1)
+    grid = W.grid_points(args.grid, -1.25, 1.25)
+    band = W.band_points(v, f, args.band_points, 2, 1e-3)
+    pts = np.concatenate([grid, band])
+    return v, f, pts
+
+
+def sample_indices(n_grid, n_band, n, seed=17):
+    """Seeded stratified sample of the workload: grid and band points in their workload proportion."""
+    rng = np.random.default_rng(seed)
+    ng = int(round(n * n_grid / (n_grid + n_band)))
+    gi = rng.choice(n_grid, size=min(ng, n_grid), replace=False)
+    bi = n_grid + rng.choice(n_band, size=min(n - ng, n_band), replace=False)
+    return np.sort(np.concatenate([gi, bi]))
+
+
+# --- reference CPU implementation -----------------------------------------------------------------
+def reference_mesh(v, f):
+    import oracle
+    R = oracle.ref()
+    t0 = time.time()
+    m = R.mesh(v, f, kind=0, build=1, max_leaf_groups=4)  # TriMeshSDF<double,short,4,4>, Morton
+    return R, m, time.time() - t0
+
+
+def time_reference(m, pts, threads=0):
+    p = pts.astype(np.float64)
+    t0 = time.perf_counter()
+    m.sdf(p, threads=threads)
+    return time.perf_counter() - t0
+
+
+def calibrated_sample(m, pts, n_grid, n_band, target_s):
+    """Sizes a stratified sample so the reference spends about target_s seconds on it."""
+    n0 = 16384
+    idx = sample_indices(n_grid, n_band, n0, seed=5)
+    dt = time_reference(m, pts[idx])
+    qps = n0 / max(dt, 1e-6)
+    n = int(min(max(qps * target_s, 16384), 8_000_000))
+    return sample_indices(n_grid, n_band, n), qps
+
+
+def cpu_info():
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return model
+
+
+# --- clocks sampler -------------------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def l2_read_bandwidth(torch, dev):
+    """Read bandwidth of a 64 MB L2-resident buffer (torch.sum; for the roofline's L2 roof)."""
+    x = torch.ones(16 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(5):
+        x.sum()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    it = 200
+    for _ in range(it):
+        x.sum()
+    e1.record()
+    torch.cuda.synchronize()
+    return x.numel() * 4 * it / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
+# --- arms -------------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle library not built (oracle/_ref)"}))
+        return 0
+    v, f, pts = workload(args)
+    n_grid, n_band = args.grid ** 3, args.band_points
+    R, m, tbuild = reference_mesh(v, f)
+    # each step: a fresh stratified sample sized for ~4 s of CPU work
+    _, qps0 = calibrated_sample(m, pts, n_grid, n_band, 1.0)
+    n = int(min(max(qps0 * 4.0, 16384), 4_000_000))
+    for s in range(args.warmup):
+        time_reference(m, pts[sample_indices(n_grid, n_band, n, seed=100 + s)])
+    times = []
+    for s in range(args.steps):
+        times.append(time_reference(m, pts[sample_indices(n_grid, n_band, n, seed=200 + s)]))
+    tot = sum(times)
+    qps = n * args.steps / tot
+    cores = R.max_threads()
+    sample = (f"{n} points per step: a seeded stratified sample of the {n_grid + n_band} workload points "
+              f"({n_grid} grid + {n_band} band in proportion)")
+    line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"mesh SDF, displaced icosphere level {args.level} ({f.shape[0]} triangles), "
+                                   f"{args.grid}^3 grid + {n_band} band points",
+                       "implementation": "reference TriMeshSDF<double,short,4,4> (Morton build), value() per "
+                                         "point in an OpenMP parallel-for", "build_s": tbuild,
+                       "cpu": cpu_info()},
+            "cpu_baseline": {"value": qps, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": qps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from ebgeometry_b200 import TriMeshSDF, _capi
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    v, f, pts = workload(args)
+    n = pts.shape[0]
+    n_grid, n_band = args.grid ** 3, args.band_points
+    t0 = time.time()
+    mesh = TriMeshSDF(v, f, build=args.build, leaf_size=args.leaf, device=local_rank)
+    t_build = time.time() - t0
+    log(f"[rank {rank}] mesh {f.shape[0]} tris built in {t_build:.2f}s: {mesh.info}")
+
+    pd = torch.from_numpy(pts).to(dev)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # traversal counters (untimed): per-query visits of the plain traversal, for the roofline
+    _, st = mesh.stats(pd)
+    log(f"[rank {rank}] stats {st}")
+
+    for _ in range(args.warmup):
+        mesh.signed_distance(pd, out=out)
+    torch.cuda.synchronize(dev)
+    mesh.check_status()
+
+    clocks = Clocks(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    tms = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        tm = _capi.PhaseTimings()
+        mesh.signed_distance(pd, out=out, timings=tm)
+        tms.append((tm.order_ms, tm.traverse_ms, tm.band_ms, tm.total_ms))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    mesh.check_status()
+    ms_step = ms / args.steps
+    value = n * world / (ms_step * 1e-3)
+    tms = np.array(tms)
+
+    # end to end through the host entry point: pinned input, H2D + query + D2H every step
+    e2e_steps = args.e2e_steps or max(2, min(args.steps, 3))
+    ph = torch.from_numpy(pts).pin_memory()
+    oh = torch.empty(n, dtype=torch.float32).pin_memory()
+    import ctypes as C
+    opts = _capi.QueryOpts()
+
+    def host_call():
+        _capi.check(_capi.lib.ebg_mesh_signed_distance_host(
+            mesh.handle, C.c_void_p(ph.data_ptr()), n, C.c_void_p(oh.data_ptr()), None, C.byref(opts),
+            C.c_void_p(stream.cuda_stream)))
+
+    host_call()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    for _ in range(e2e_steps):
+        host_call()
+    h1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = h0.elapsed_time(h1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    # the host path must give the device path's numbers
+    same = bool(torch.equal(oh, out.cpu()))
+
+    if rank != 0:
+        return 0
+
+    # roofline of the traversal kernel
+    hbm_peak, peak_kind = measured_peaks()
+    l2_gbs = l2_read_bandwidth(torch, dev)
+    node_b, tri_b = 128, 48
+    nq = float(n)
+    bq = 12 + 4 + st["nodes_visited"] / nq * node_b + st["triangles_tested"] / nq * tri_b
+    trav_ms = float(tms[:, 1].mean())
+    achieved = nq * bq / (trav_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            tj = json.load(fh)
+        key = f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}"
+        traffic = tj.get(key)
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            R, m, tb = reference_mesh(v, f)
+            # bounded sample: probe the reference's rate, then size the sample to ~cpu_seconds
+            sidx, qps_probe = calibrated_sample(m, pts, n_grid, n_band, args.cpu_seconds)
+            ns = len(sidx)
+            dt = time_reference(m, pts[sidx])
+            # parity on that sample while it is at hand (reported, not asserted)
+            d_ref = m.sdf(pts[sidx].astype(np.float64))
+            d_gpu = out.index_select(0, torch.from_numpy(sidx).to(dev)).cpu().numpy().astype(np.float64)
+            err = np.abs(d_gpu - d_ref)
+            bandm = np.abs(d_ref) > 1e-4 * mesh.diagonal
+            cpu = {"value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
+                   "sample": f"{ns} seeded stratified points of the workload ({n_grid} grid : {n_band} band), "
+                             f"reference TriMeshSDF<double,short,4,4> Morton build ({tb:.1f}s), OpenMP over "
+                             f"value(); host CPU: {cpu_info()}",
+                   "parity_on_sample": {"max_abs_err": float(err.max()), "tol": 1e-6 * mesh.diagonal,
+                                        "sign_mismatch_outside_band": int(np.sum(np.sign(d_gpu[bandm]) !=
+                                                                                 np.sign(d_ref[bandm])))}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"mesh SDF: displaced icosphere level {args.level} ({f.shape[0]} triangles, "
+                               f"{args.build} 4-wide BVH, leaf {args.leaf}), {args.grid}^3 grid over [-1.25,1.25]^3 "
+                               f"+ {n_band} points within 1e-3 of the surface = {n} queries/step; FP32 traversal, "
+                               f"FP64 band |d| <= 1e-4 diag",
+                   "seed": "none (plain traversal)", "queries_per_step": n, "l2": "inputs larger than L2 "
+                   f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
+                   "phase_ms_mean": {"order": float(tms[:, 0].mean()), "traverse": trav_ms,
+                                     "band64": float(tms[:, 2].mean()), "total": float(tms[:, 3].mean())},
+                   "per_query": {"nodes": st["nodes_visited"] / nq, "leaves": st["leaves_visited"] / nq,
+                                 "triangles": st["triangles_tested"] / nq, "band_fraction": st["band_queries"] / nq}},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "kMeshSdf32 (FP32 packet traversal)",
+                     "bytes_per_query": bq, "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
+        "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
+                "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},
+        "gpu_launches": 3 * args.steps,
+        "gpu_launches_note": "per step: Morton-key kernel, FP32 traversal, FP64 band pass (plus the CUB radix-sort "
+                             "passes of the point ordering)",
+        "clocks": ck,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            return run_reference(args, rank, world)
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,161 @@
+"""ebgeometry_b200 -- B200-native (sm_100a) mesh signed distance, nearest neighbours and CSG union.
+
+Python mirror of the reference's (rmrsk/EBGeometry) C++ query objects on top of the C ABI in
+``include/ebgeometry_b200.h``.  Class and method names follow the reference:
+
+* :class:`TriMeshSDF` -- ``TriMeshSDF(mesh, build, maxLeafGroups)`` (MeshDistanceFunctions.hpp:
+  309-489) with ``value(point)`` / ``signedDistance(point)`` for one point (ImplicitFunction.hpp:
+  51-60) and a batched ``signed_distance(points)`` over CUDA tensors or numpy arrays.
+
+There is no CPU fallback: every query runs in the CUDA kernels of ``libebgb200.so``, and importing
+this package fails if that library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import EbgError, check, lib
+
+__all__ = ["TriMeshSDF", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
+
+BUILD_SAH = 0
+BUILD_MORTON = 1
+
+
+def version() -> str:
+    return lib.ebg_version().decode()
+
+
+def device_count() -> int:
+    return int(lib.ebg_device_count())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class TriMeshSDF:
+    """Signed distance to a watertight triangle mesh (the reference's TriMeshSDF).
+
+    ``vertices``: (V,3) float64; ``triangles``: (T,3) int32 corner indices, counter-clockwise seen
+    from outside.  Pseudonormals are computed the way the reference's DCEL computes them unless
+    ``vertex_normals`` (per corner, (T,3,3)) and ``edge_normals`` ((T,3,3), edge i from corner i to
+    i+1) are given.  ``build``: "SAH" or "Morton"; ``leaf_size``: max triangles per leaf.
+    """
+
+    def __init__(self, vertices, triangles, build="SAH", leaf_size=8, device=-1,
+                 vertex_normals=None, edge_normals=None):
+        v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        f = np.ascontiguousarray(triangles, dtype=np.int32).reshape(-1, 3)
+        b = {"SAH": BUILD_SAH, "MORTON": BUILD_MORTON}[str(build).upper()] if isinstance(build, str) else int(build)
+        opts = _capi.BuildOpts(b, int(leaf_size), int(device), 0)
+        h = C.c_void_p()
+        if vertex_normals is not None or edge_normals is not None:
+            vn = np.ascontiguousarray(vertex_normals, dtype=np.float64).reshape(-1, 9)
+            en = np.ascontiguousarray(edge_normals, dtype=np.float64).reshape(-1, 9)
+            if vn.shape[0] != f.shape[0] or en.shape[0] != f.shape[0]:
+                raise ValueError("one row of 9 normal components per triangle expected")
+            check(lib.ebg_mesh_create_with_normals(_ptr(v), v.shape[0], _ptr(f), f.shape[0], _ptr(vn),
+                                                   _ptr(en), C.byref(opts), C.byref(h)))
+        else:
+            check(lib.ebg_mesh_create(_ptr(v), v.shape[0], _ptr(f), f.shape[0], C.byref(opts),
+                                      C.byref(h)))
+        self._h = h
+        self.num_triangles = f.shape[0]
+        inf = _capi.MeshInfo()
+        check(lib.ebg_mesh_get_info(self._h, C.byref(inf)))
+        self.info = {k: (list(getattr(inf, k)) if k in ("lo", "hi") else getattr(inf, k))
+                     for k, _ in _capi.MeshInfo._fields_}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_mesh_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def diagonal(self) -> float:
+        return float(self.info["diagonal"])
+
+    def normals(self):
+        """(face (T,3), corner vertex (T,3,3), edge (T,3,3)) pseudonormals as float64."""
+        t = self.num_triangles
+        fn, vn, en = np.empty((t, 3)), np.empty((t, 3, 3)), np.empty((t, 3, 3))
+        check(lib.ebg_mesh_get_normals(self._h, _ptr(fn), _ptr(vn), _ptr(en)))
+        return fn, vn, en
+
+    @staticmethod
+    def _opts(band, sort, fp64_band, warps_per_block, timings=None):
+        return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1, None,
+                               int(warps_per_block or 0), 0,
+                               C.pointer(timings) if timings is not None else None)
+
+    # --- ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance -----------------
+    def value(self, point) -> float:
+        out = C.c_double()
+        check(lib.ebg_mesh_value(self._h, float(point[0]), float(point[1]), float(point[2]),
+                                 C.byref(out)))
+        return out.value
+
+    signedDistance = value
+    __call__ = value
+
+    # --- batched ----------------------------------------------------------------------------------
+    def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
+                        fp64_band=True, warps_per_block=None, stream=None, timings=None):
+        """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
+        on ``stream``, default the current torch stream); numpy arrays go through the host entry
+        point (synchronous).  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
+        times (the call then synchronises)."""
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings)
+        if isinstance(points, np.ndarray):
+            p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            n = p.shape[0]
+            d = out if out is not None else np.empty(n, np.float32)
+            t = closest_tri
+            check(lib.ebg_mesh_signed_distance_host(self._h, _ptr(p), n, _ptr(d),
+                                                    _ptr(t) if t is not None else None,
+                                                    C.byref(opts), None))
+            return (d, t) if t is not None else d
+        import torch
+        p = points
+        if not (p.is_cuda and p.dtype == torch.float32 and p.is_contiguous()):
+            raise ValueError("points must be a contiguous float32 CUDA tensor of shape (n,3)")
+        n = p.numel() // 3
+        d = out if out is not None else torch.empty(n, dtype=torch.float32, device=p.device)
+        check(lib.ebg_mesh_signed_distance(self._h, C.c_void_p(p.data_ptr()), n,
+                                           C.c_void_p(d.data_ptr()),
+                                           C.c_void_p(closest_tri.data_ptr()) if closest_tri is not None else None,
+                                           C.byref(opts), _stream_ptr(stream)))
+        return (d, closest_tri) if closest_tri is not None else d
+
+    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None):
+        """Traversal counters summed over the points (synchronous; CUDA tensor input)."""
+        import torch
+        n = points.numel() // 3
+        d = torch.empty(n, dtype=torch.float32, device=points.device)
+        st = _capi.QueryStats()
+        opts = self._opts(band, sort, fp64_band, None)
+        check(lib.ebg_mesh_signed_distance_stats(self._h, C.c_void_p(points.data_ptr()), n,
+                                                 C.c_void_p(d.data_ptr()), C.byref(opts),
+                                                 C.byref(st), _stream_ptr(stream)))
+        return d, {k: getattr(st, k) for k, _ in _capi.QueryStats._fields_}
+
+    def check_status(self, stream=None):
+        check(lib.ebg_check_status(self._h, _stream_ptr(stream)))

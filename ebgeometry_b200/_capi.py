@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI declared in include/ebgeometry_b200.h.
+
+The shared library ``libebgb200.so`` is built in-tree (``ebgeometry_b200/csrc/Makefile``).  There
+is no CPU fallback: if the library cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libebgb200.so")
+
+
+class BuildOpts(C.Structure):
+    _fields_ = [("build", C.c_int32), ("leaf_size", C.c_int32), ("device", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class PhaseTimings(C.Structure):
+    _fields_ = [("order_ms", C.c_float), ("traverse_ms", C.c_float), ("band_ms", C.c_float),
+                ("total_ms", C.c_float)]
+
+
+class QueryOpts(C.Structure):
+    _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
+                ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("reserved", C.c_int32),
+                ("timings", C.POINTER(PhaseTimings))]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("num_triangles", C.c_int64), ("num_vertices", C.c_int64),
+                ("num_nodes", C.c_int64), ("num_leaves", C.c_int64), ("depth", C.c_int32),
+                ("leaf_size", C.c_int32), ("lo", C.c_double * 3), ("hi", C.c_double * 3),
+                ("diagonal", C.c_double), ("device_bytes", C.c_int64)]
+
+
+class QueryStats(C.Structure):
+    _fields_ = [("nodes_visited", C.c_int64), ("leaves_visited", C.c_int64),
+                ("triangles_tested", C.c_int64), ("band_queries", C.c_int64),
+                ("seed_fallbacks", C.c_int64)]
+
+
+EBG_OK = 0
+STATUS_NAMES = {0: "EBG_OK", 1: "EBG_ERR_INVALID", 2: "EBG_ERR_CUDA", 3: "EBG_ERR_NO_MEMORY",
+                4: "EBG_ERR_TRAVERSAL", 5: "EBG_ERR_NOT_FOUND", 6: "EBG_ERR_TOO_LARGE"}
+
+_P = C.c_void_p
+_I64 = C.c_int64
+_I32 = C.c_int32
+_D = C.c_double
+
+# name -> (restype, argtypes); every symbol the header declares
+SIGNATURES = {
+    "ebg_last_error": (C.c_char_p, []),
+    "ebg_version": (C.c_char_p, []),
+    "ebg_device_count": (C.c_int, []),
+    "ebg_mesh_create": (C.c_int, [_P, _I64, _P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "ebg_mesh_create_with_normals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, C.POINTER(BuildOpts),
+                                               C.POINTER(_P)]),
+    "ebg_compute_pseudonormals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _P]),
+    "ebg_mesh_destroy": (C.c_int, [_P]),
+    "ebg_mesh_get_info": (C.c_int, [_P, C.POINTER(MeshInfo)]),
+    "ebg_mesh_get_normals": (C.c_int, [_P, _P, _P, _P]),
+    "ebg_mesh_signed_distance": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_mesh_signed_distance_host": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_mesh_signed_distance_stats": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts),
+                                                 C.POINTER(QueryStats), _P]),
+    "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),
+    "ebg_check_status": (C.c_int, [_P, _P]),
+}
+
+
+class EbgError(RuntimeError):
+    """A C ABI call returned a non-zero ebg_status."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C ebgeometry_b200/csrc` (or "
+            "__graft_entry__.build()); there is no CPU fallback")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != EBG_OK:
+        raise EbgError(status, lib.ebg_last_error().decode())

@@ -1,0 +1,39 @@
+// Library-wide C ABI entry points (errors, version, devices).
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "capi_common.h"
+#include "ebgeometry_b200.h"
+
+namespace ebg {
+
+namespace {
+thread_local std::string g_lastError;
+}
+
+ebg_status setError(ebg_status code, const std::string& msg)
+{
+  g_lastError = msg;
+  return code;
+}
+
+} // namespace ebg
+
+extern "C" {
+
+const char* ebg_last_error(void) { return ebg::g_lastError.c_str(); }
+
+const char* ebg_version(void) { return "ebgeometry_b200 0.1.0 (sm_100a)"; }
+
+int ebg_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+} // extern "C"

@@ -1,0 +1,648 @@
+// C ABI of the mesh path: handle lifetime, host build + upload, and the query pipeline
+//   Morton keys -> radix sort (query coherence) -> FP32 packet traversal -> FP64 band pass.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include "capi_common.h"
+#include "ebgeometry_b200.h"
+#include "mesh_host.h"
+#include "mesh_kernels.h"
+
+using namespace ebg;
+
+struct ebg_mesh
+{
+  int           device = 0;
+  int           numSms = 148;
+  EbgMeshView   view{};
+  ebg_mesh_info info{};
+  // device allocations
+  void*         dNodes = nullptr;
+  void*         dHot   = nullptr;
+  void*         dSign  = nullptr;
+  void*         dTri64 = nullptr;
+  void*         dTriId = nullptr;
+  int*          dStatus = nullptr;
+  // host copies of the pseudonormals (soup order)
+  std::vector<double> triN, cornerVN, edgeN;
+};
+
+namespace {
+
+ebg_status buildMesh(const double*         V,
+                     int64_t               nv,
+                     const int32_t*        F,
+                     int64_t               nt,
+                     const double*         givenVN,
+                     const double*         givenEN,
+                     const ebg_build_opts* opts,
+                     ebg_mesh**            out)
+{
+  if (out == nullptr) {
+    return setError(EBG_ERR_INVALID, "out handle pointer is null");
+  }
+  *out = nullptr;
+  if (V == nullptr || F == nullptr || nv <= 0 || nt <= 0) {
+    return setError(EBG_ERR_INVALID, "mesh needs at least one vertex and one triangle");
+  }
+  if (nt >= int64_t(EBG_LEAF_BIT) || nv > int64_t(INT32_MAX)) {
+    return setError(EBG_ERR_TOO_LARGE, "mesh too large (triangles < 2^31, vertices < 2^31)");
+  }
+  for (int64_t i = 0; i < 3 * nt; i++) {
+    if (F[i] < 0 || F[i] >= nv) {
+      return setError(EBG_ERR_INVALID, "triangle corner index out of range");
+    }
+  }
+  for (int64_t i = 0; i < 3 * nv; i++) {
+    if (!std::isfinite(V[i])) {
+      return setError(EBG_ERR_INVALID, "non-finite vertex coordinate");
+    }
+  }
+  const int build    = opts ? opts->build : EBG_BUILD_SAH;
+  const int leafSize = (opts && opts->leaf_size > 0) ? opts->leaf_size : 8;
+  int       device   = (opts && opts->device >= 0) ? opts->device : -1;
+  if (build != EBG_BUILD_SAH && build != EBG_BUILD_MORTON) {
+    return setError(EBG_ERR_INVALID, "unknown build method");
+  }
+  DeviceGuard guard;
+  if (device >= 0) {
+    if (cudaSetDevice(device) != cudaSuccess) {
+      return setError(EBG_ERR_NOT_FOUND, "cannot select CUDA device " + std::to_string(device));
+    }
+  }
+  else if (cudaGetDevice(&device) != cudaSuccess) {
+    return setError(EBG_ERR_NOT_FOUND, "no CUDA device");
+  }
+
+  // Keep freed stream-ordered allocations in the device's default pool: every query call takes its
+  // workspace from it, and returning the memory to the driver at each synchronisation would make
+  // the next call map it again.
+  {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
+  auto* m   = new ebg_mesh;
+  m->device = device;
+  cudaDeviceGetAttribute(&m->numSms, cudaDevAttrMultiProcessorCount, device);
+
+  std::string msg;
+  if (givenVN != nullptr && givenEN != nullptr) {
+    m->cornerVN.assign(givenVN, givenVN + 9 * nt);
+    m->edgeN.assign(givenEN, givenEN + 9 * nt);
+    m->triN.resize(3 * nt);
+    for (int64_t f = 0; f < nt; f++) {
+      const double* a = V + 3 * int64_t(F[3 * f]);
+      const double* b = V + 3 * int64_t(F[3 * f + 1]);
+      const double* c = V + 3 * int64_t(F[3 * f + 2]);
+      const double  u[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+      const double  w[3] = {c[0] - b[0], c[1] - b[1], c[2] - b[2]};
+      const double  x[3] = {u[1] * w[2] - u[2] * w[1], u[2] * w[0] - u[0] * w[2], u[0] * w[1] - u[1] * w[0]};
+      const double  l    = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+      if (!(l > 0.0)) {
+        delete m;
+        return setError(EBG_ERR_INVALID, "degenerate (zero-area) triangle in the soup");
+      }
+      const double is = 1.0 / l;
+      for (int k = 0; k < 3; k++) {
+        m->triN[3 * f + k] = is * x[k];
+      }
+    }
+  }
+  else if (!computePseudonormals(V, nv, F, nt, m->triN, m->cornerVN, m->edgeN, msg)) {
+    delete m;
+    return setError(EBG_ERR_INVALID, msg);
+  }
+
+  // primitive boxes / centroids
+  std::vector<double> lo(3 * nt), hi(3 * nt), cen(3 * nt);
+#pragma omp parallel for schedule(static)
+  for (int64_t f = 0; f < nt; f++) {
+    for (int a = 0; a < 3; a++) {
+      const double x0 = V[3 * int64_t(F[3 * f]) + a], x1 = V[3 * int64_t(F[3 * f + 1]) + a],
+                   x2 = V[3 * int64_t(F[3 * f + 2]) + a];
+      lo[3 * f + a]  = std::min(x0, std::min(x1, x2));
+      hi[3 * f + a]  = std::max(x0, std::max(x1, x2));
+      cen[3 * f + a] = (x0 + x1 + x2) / 3.0;
+    }
+  }
+  Bvh4 bvh;
+  if (!buildBvh4(lo, hi, cen, build, leafSize, bvh, msg)) {
+    delete m;
+    return setError(EBG_ERR_INVALID, msg);
+  }
+
+  // leaf-ordered triangle records
+  const size_t            N = size_t(nt);
+  std::vector<EbgTriHot>  hot(N);
+  std::vector<EbgTriSign> sign(N);
+  std::vector<double>     tri64(30 * N);
+  std::vector<int32_t>    triId(N);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < int64_t(N); i++) {
+    const int64_t f = bvh.order[i];
+    triId[i]        = int32_t(f);
+    const double* a = V + 3 * int64_t(F[3 * f]);
+    const double* b = V + 3 * int64_t(F[3 * f + 1]);
+    const double* c = V + 3 * int64_t(F[3 * f + 2]);
+    const double  ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double  ac[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    EbgTriHot&    h     = hot[i];
+    h.v0x = float(a[0]);
+    h.v0y = float(a[1]);
+    h.v0z = float(a[2]);
+    h.abx = float(ab[0]);
+    h.aby = float(ab[1]);
+    h.abz = float(ab[2]);
+    h.acx = float(ac[0]);
+    h.acy = float(ac[1]);
+    h.acz = float(ac[2]);
+    h.ab2  = float(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
+    h.abac = float(ab[0] * ac[0] + ab[1] * ac[1] + ab[2] * ac[2]);
+    h.ac2  = float(ac[0] * ac[0] + ac[1] * ac[1] + ac[2] * ac[2]);
+    EbgTriSign& s = sign[i];
+    s.nx          = float(m->triN[3 * f]);
+    s.ny          = float(m->triN[3 * f + 1]);
+    s.nz          = float(m->triN[3 * f + 2]);
+    s.pad0 = s.pad1 = s.pad2 = 0.f;
+    for (int k = 0; k < 9; k++) {
+      s.vn[k] = float(m->cornerVN[9 * f + k]);
+      s.en[k] = float(m->edgeN[9 * f + k]);
+    }
+    double* t = &tri64[30 * size_t(i)];
+    for (int k = 0; k < 3; k++) {
+      t[k]     = a[k];
+      t[3 + k] = b[k];
+      t[6 + k] = c[k];
+      t[9 + k] = m->triN[3 * f + k];
+    }
+    for (int k = 0; k < 9; k++) {
+      t[12 + k] = m->cornerVN[9 * f + k];
+      t[21 + k] = m->edgeN[9 * f + k];
+    }
+  }
+
+  // upload
+  auto up = [&](void** dst, const void* src, size_t bytes) -> bool {
+    if (cudaMalloc(dst, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+      return false;
+    }
+    return bytes == 0 || cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  };
+  const size_t nodeBytes = bvh.nodes.size() * sizeof(EbgNode4);
+  if (!up(&m->dNodes, bvh.nodes.data(), nodeBytes) || !up(&m->dHot, hot.data(), N * sizeof(EbgTriHot)) ||
+      !up(&m->dSign, sign.data(), N * sizeof(EbgTriSign)) || !up(&m->dTri64, tri64.data(), 30 * N * sizeof(double)) ||
+      !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
+      cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
+      cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    ebg_mesh_destroy(m);
+    return setError(EBG_ERR_NO_MEMORY, "device allocation or upload failed for the mesh");
+  }
+
+  EbgMeshView& v = m->view;
+  v.nodes        = static_cast<const EbgNode4*>(m->dNodes);
+  v.hot          = static_cast<const EbgTriHot*>(m->dHot);
+  v.sign         = static_cast<const EbgTriSign*>(m->dSign);
+  v.tri64        = static_cast<const double*>(m->dTri64);
+  v.tri_id       = static_cast<const int32_t*>(m->dTriId);
+  for (int a = 0; a < 3; a++) {
+    v.root_lo[a] = roundDown(bvh.lo[a]);
+    v.root_hi[a] = roundUp(bvh.hi[a]);
+    // Morton domain for query ordering: the mesh box grown to twice its extent about its centre
+    const double c   = 0.5 * (bvh.lo[a] + bvh.hi[a]);
+    const double ext = std::max(bvh.hi[a] - bvh.lo[a], 1e-30);
+    v.morton_lo[a]   = float(c - ext);
+    v.morton_scale[a] = float(1024.0 / (2.0 * ext));
+  }
+  v.root_ref   = bvh.rootRef;
+  v.root_count = bvh.rootCount;
+
+  ebg_mesh_info& inf = m->info;
+  inf.num_triangles  = nt;
+  inf.num_vertices   = nv;
+  inf.num_nodes      = int64_t(bvh.nodes.size());
+  inf.num_leaves     = bvh.numLeaves;
+  inf.depth          = bvh.depth;
+  inf.leaf_size      = leafSize;
+  double d2          = 0;
+  for (int a = 0; a < 3; a++) {
+    inf.lo[a] = bvh.lo[a];
+    inf.hi[a] = bvh.hi[a];
+    d2 += (bvh.hi[a] - bvh.lo[a]) * (bvh.hi[a] - bvh.lo[a]);
+  }
+  inf.diagonal     = std::sqrt(d2);
+  inf.device_bytes = int64_t(nodeBytes + N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 30 * sizeof(double) + 4));
+  *out             = m;
+  return EBG_OK;
+}
+
+struct Workspace
+{
+  cudaStream_t      s;
+  std::vector<void*> ptrs;
+  bool              ok = true;
+  explicit Workspace(cudaStream_t st) : s(st) {}
+  template <class T>
+  T* get(size_t count)
+  {
+    void* p = nullptr;
+    if (ok && cudaMallocAsync(&p, std::max<size_t>(count * sizeof(T), 16), s) == cudaSuccess) {
+      ptrs.push_back(p);
+      return static_cast<T*>(p);
+    }
+    ok = false;
+    return nullptr;
+  }
+  ~Workspace()
+  {
+    for (void* p : ptrs) {
+      cudaFreeAsync(p, s);
+    }
+  }
+};
+
+ebg_status runQuery(const ebg_mesh*       m,
+                    const float*          pts,
+                    int64_t               n,
+                    float*                outD,
+                    int32_t*              outTri,
+                    const ebg_query_opts* opts,
+                    unsigned long long*   statsDev,
+                    cudaStream_t          s)
+{
+  if (n > int64_t(INT32_MAX)) {
+    return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
+  }
+  const bool sort   = !(opts && opts->no_sort);
+  const bool band64 = !(opts && opts->no_fp64_band);
+  const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block : 4;
+  double     band   = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
+  const float* seedR = nullptr;
+  if (opts && opts->seed) {
+    return setError(EBG_ERR_INVALID, "seeded queries go through ebg_seed_signed_distance");
+  }
+
+  // optional per-phase events (ev[0] start, [1] after ordering, [2] after traversal, [3] end)
+  ebg_phase_timings* tm = opts ? opts->timings : nullptr;
+  cudaEvent_t        ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (tm) {
+    for (auto& e : ev) {
+      cudaEventCreate(&e);
+    }
+    cudaEventRecord(ev[0], s);
+  }
+  struct EventGuard
+  {
+    cudaEvent_t* ev;
+    ~EventGuard()
+    {
+      for (int i = 0; i < 4; i++) {
+        if (ev[i]) {
+          cudaEventDestroy(ev[i]);
+        }
+      }
+    }
+  } evGuard{ev};
+
+  Workspace ws(s);
+  uint32_t* order = nullptr;
+  if (sort) {
+    uint32_t* keysIn  = ws.get<uint32_t>(n);
+    uint32_t* keysOut = ws.get<uint32_t>(n);
+    uint32_t* idsIn   = ws.get<uint32_t>(n);
+    order             = ws.get<uint32_t>(n);
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "query workspace allocation failed");
+    }
+    launchQueryKeys(pts, n, m->view.morton_lo, m->view.morton_scale, keysIn, idsIn, s);
+    size_t tempBytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keysIn, keysOut, idsIn, order, int(n), 0, 30, s);
+    void* temp = ws.get<char>(tempBytes);
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "sort workspace allocation failed");
+    }
+    if (cub::DeviceRadixSort::SortPairs(temp, tempBytes, keysIn, keysOut, idsIn, order, int(n), 0, 30, s) !=
+        cudaSuccess) {
+      return setError(EBG_ERR_CUDA, "query sort failed");
+    }
+  }
+  unsigned long long* counters = ws.get<unsigned long long>(2); // [0] packets, [1] band count (u32)
+  uint32_t*           bandList = band64 ? ws.get<uint32_t>(n) : nullptr;
+  float*              bandD    = band64 ? ws.get<float>(n) : nullptr;
+  if (!ws.ok) {
+    return setError(EBG_ERR_NO_MEMORY, "query workspace allocation failed");
+  }
+  cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
+  if (tm) {
+    cudaEventRecord(ev[1], s);
+  }
+
+  MeshQueryArgs a{};
+  a.mesh       = m->view;
+  a.points     = pts;
+  a.order      = order;
+  a.seed_r     = seedR;
+  a.n          = n;
+  a.out_d      = outD;
+  a.out_tri    = outTri;
+  a.band       = float(band);
+  a.band_list  = bandList;
+  a.band_count = reinterpret_cast<uint32_t*>(counters + 1);
+  a.band_d32   = bandD;
+  a.work       = counters;
+  a.status     = m->dStatus;
+  a.stats      = statsDev;
+  if (launchMeshSdf32(a, wpb, m->numSms, s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  if (tm) {
+    cudaEventRecord(ev[2], s);
+  }
+  if (band64) {
+    // delta bounds the FP32 distance error (relative 1e-6 of the box diagonal)
+    const float delta = float(2e-6 * m->info.diagonal) + 1e-30f;
+    if (launchMeshBand64(a, delta, m->numSms, s) != cudaSuccess) {
+      return setError(EBG_ERR_CUDA, "band launch failed");
+    }
+    if (statsDev) {
+      cudaMemcpyAsync(statsDev + 3, counters + 1, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s);
+    }
+  }
+  if (tm) {
+    cudaEventRecord(ev[3], s);
+    if (cudaEventSynchronize(ev[3]) != cudaSuccess) {
+      return setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+    }
+    cudaEventElapsedTime(&tm->order_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&tm->traverse_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&tm->band_ms, ev[2], ev[3]);
+    cudaEventElapsedTime(&tm->total_ms, ev[0], ev[3]);
+  }
+  return EBG_OK;
+}
+
+bool checkPoints(const float* p, int64_t n)
+{
+  for (int64_t i = 0; i < 3 * n; i++) {
+    if (!std::isfinite(p[i])) {
+      return false;
+    }
+  }
+  return true;
+}
+
+} // namespace
+
+extern "C" {
+
+ebg_status ebg_mesh_create(const double*         vertices,
+                           int64_t               num_vertices,
+                           const int32_t*        triangles,
+                           int64_t               num_triangles,
+                           const ebg_build_opts* opts,
+                           ebg_mesh**            out)
+{
+  return buildMesh(vertices, num_vertices, triangles, num_triangles, nullptr, nullptr, opts, out);
+}
+
+ebg_status ebg_mesh_create_with_normals(const double*         vertices,
+                                        int64_t               num_vertices,
+                                        const int32_t*        triangles,
+                                        int64_t               num_triangles,
+                                        const double*         corner_vertex_normals,
+                                        const double*         edge_normals,
+                                        const ebg_build_opts* opts,
+                                        ebg_mesh**            out)
+{
+  if (corner_vertex_normals == nullptr || edge_normals == nullptr) {
+    return setError(EBG_ERR_INVALID, "normal arrays are null");
+  }
+  return buildMesh(vertices, num_vertices, triangles, num_triangles, corner_vertex_normals, edge_normals, opts, out);
+}
+
+ebg_status ebg_compute_pseudonormals(const double*  vertices,
+                                     int64_t        num_vertices,
+                                     const int32_t* triangles,
+                                     int64_t        num_triangles,
+                                     double*        face_normals,
+                                     double*        corner_vertex_normals,
+                                     double*        edge_normals)
+{
+  if (vertices == nullptr || triangles == nullptr || num_vertices <= 0 || num_triangles <= 0 ||
+      face_normals == nullptr || corner_vertex_normals == nullptr || edge_normals == nullptr) {
+    return setError(EBG_ERR_INVALID, "null buffer or empty mesh");
+  }
+  for (int64_t i = 0; i < 3 * num_triangles; i++) {
+    if (triangles[i] < 0 || triangles[i] >= num_vertices) {
+      return setError(EBG_ERR_INVALID, "triangle corner index out of range");
+    }
+  }
+  std::vector<double> tn, vn, en;
+  std::string         msg;
+  if (!computePseudonormals(vertices, num_vertices, triangles, num_triangles, tn, vn, en, msg)) {
+    return setError(EBG_ERR_INVALID, msg);
+  }
+  std::memcpy(face_normals, tn.data(), tn.size() * sizeof(double));
+  std::memcpy(corner_vertex_normals, vn.data(), vn.size() * sizeof(double));
+  std::memcpy(edge_normals, en.data(), en.size() * sizeof(double));
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_destroy(ebg_mesh* m)
+{
+  if (m == nullptr) {
+    return EBG_OK;
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  cudaFree(m->dNodes);
+  cudaFree(m->dHot);
+  cudaFree(m->dSign);
+  cudaFree(m->dTri64);
+  cudaFree(m->dTriId);
+  cudaFree(m->dStatus);
+  delete m;
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_get_info(const ebg_mesh* m, ebg_mesh_info* info)
+{
+  if (m == nullptr || info == nullptr) {
+    return setError(EBG_ERR_INVALID, "null argument");
+  }
+  *info = m->info;
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_get_normals(const ebg_mesh* m, double* fn, double* vn, double* en)
+{
+  if (m == nullptr) {
+    return setError(EBG_ERR_INVALID, "null mesh");
+  }
+  if (fn) {
+    std::memcpy(fn, m->triN.data(), m->triN.size() * sizeof(double));
+  }
+  if (vn) {
+    std::memcpy(vn, m->cornerVN.data(), m->cornerVN.size() * sizeof(double));
+  }
+  if (en) {
+    std::memcpy(en, m->edgeN.data(), m->edgeN.size() * sizeof(double));
+  }
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_signed_distance(const ebg_mesh*       m,
+                                    const float*          points_dev,
+                                    int64_t               n,
+                                    float*                dist_dev,
+                                    int32_t*              closest_tri_dev,
+                                    const ebg_query_opts* opts,
+                                    void*                 stream)
+{
+  if (m == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  return runQuery(m, points_dev, n, dist_dev, closest_tri_dev, opts, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
+                                         const float*          points_host,
+                                         int64_t               n,
+                                         float*                dist_host,
+                                         int32_t*              closest_tri_host,
+                                         const ebg_query_opts* opts,
+                                         void*                 stream)
+{
+  if (m == nullptr || n < 0 || (n > 0 && (points_host == nullptr || dist_host == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  if (!checkPoints(points_host, n)) {
+    return setError(EBG_ERR_INVALID, "non-finite query coordinate");
+  }
+  DeviceGuard  guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(m->dStatus, 0, sizeof(int), s);
+  ebg_status rc;
+  {
+    Workspace ws(s);
+    float*    dp = ws.get<float>(3 * n);
+    float*    dd = ws.get<float>(n);
+    int32_t*  dt = closest_tri_host ? ws.get<int32_t>(n) : nullptr;
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "device buffers for the host call");
+    }
+    cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s);
+    rc = runQuery(m, dp, n, dd, dt, opts, nullptr, s);
+    if (rc == EBG_OK) {
+      cudaMemcpyAsync(dist_host, dd, n * sizeof(float), cudaMemcpyDeviceToHost, s);
+      if (dt) {
+        cudaMemcpyAsync(closest_tri_host, dt, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      }
+    }
+  }
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  return ebg_check_status(m, stream);
+}
+
+ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
+                                          const float*          points_dev,
+                                          int64_t               n,
+                                          float*                dist_dev,
+                                          const ebg_query_opts* opts,
+                                          ebg_query_stats*      stats,
+                                          void*                 stream)
+{
+  if (m == nullptr || stats == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null argument or negative count");
+  }
+  std::memset(stats, 0, sizeof(*stats));
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard  guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ebg_status   rc;
+  unsigned long long host[5] = {0, 0, 0, 0, 0};
+  {
+    Workspace           ws(s);
+    unsigned long long* dev = ws.get<unsigned long long>(5);
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "stats buffer");
+    }
+    cudaMemsetAsync(dev, 0, 5 * sizeof(unsigned long long), s);
+    rc = runQuery(m, points_dev, n, dist_dev, nullptr, opts, dev, s);
+    if (rc == EBG_OK) {
+      cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, s);
+    }
+  }
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  }
+  stats->nodes_visited    = int64_t(host[0]);
+  stats->leaves_visited   = int64_t(host[1]);
+  stats->triangles_tested = int64_t(host[2]);
+  stats->band_queries     = int64_t(host[3] & 0xffffffffull);
+  stats->seed_fallbacks   = int64_t(host[4]);
+  return ebg_check_status(m, stream);
+}
+
+ebg_status ebg_mesh_value(const ebg_mesh* m, double x, double y, double z, double* value)
+{
+  if (m == nullptr || value == nullptr) {
+    return setError(EBG_ERR_INVALID, "null argument");
+  }
+  const float p[3] = {float(x), float(y), float(z)};
+  float       d    = 0.f;
+  ebg_query_opts o{};
+  o.no_sort = 1;
+  const ebg_status rc = ebg_mesh_signed_distance_host(m, p, 1, &d, nullptr, &o, nullptr);
+  *value              = double(d);
+  return rc;
+}
+
+ebg_status ebg_check_status(const ebg_mesh* m, void* stream)
+{
+  if (m == nullptr) {
+    return setError(EBG_ERR_INVALID, "null mesh");
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int          st = 0;
+  if (cudaMemcpyAsync(&st, m->dStatus, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  }
+  if (st != 0) {
+    cudaMemsetAsync(m->dStatus, 0, sizeof(int), s);
+    return setError(EBG_ERR_TRAVERSAL, "traversal stopped early (status " + std::to_string(st) + ")");
+  }
+  return EBG_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,58 @@
+// Device helpers shared by the mesh kernels.
+#ifndef EBG_DEVICE_CUH
+#define EBG_DEVICE_CUH
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ebg_layout.h"
+
+namespace ebg {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// Device-side status word values (host reads them after the call).
+constexpr int ST_STACK = 1;  // traversal stack would overflow (never for trees the builder accepts)
+constexpr int ST_ITERS = 2;  // iteration cap reached
+
+// Iteration cap per packet traversal: far above any real traversal (a packet visits at most
+// every node and leaf once per pass), so hitting it means corrupt input; the kernel then stops,
+// records ST_ITERS and returns instead of spinning.
+constexpr uint32_t MAX_ITERS = 1u << 26;
+
+// Squared distance from p to an axis-aligned box, the reference's AABBT::getDistance2
+// (BoundingVolumesImplem.hpp:480-496): sum over axes of max(0, lo - p, p - hi)^2.
+__device__ __forceinline__ float boxDist2(float lx, float ly, float lz, float hx, float hy, float hz, float px,
+                                          float py, float pz)
+{
+  const float dx = fmaxf(0.f, fmaxf(lx - px, px - hx));
+  const float dy = fmaxf(0.f, fmaxf(ly - py, py - hy));
+  const float dz = fmaxf(0.f, fmaxf(lz - pz, pz - hz));
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+
+// 10 bits per axis -> 30-bit Morton code.
+__device__ __forceinline__ uint32_t spread10(uint32_t x)
+{
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+__device__ __forceinline__ float warpSum(float v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(FULL, v, o);
+  }
+  return v;
+}
+
+} // namespace ebg
+
+#endif

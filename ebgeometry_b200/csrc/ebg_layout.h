@@ -1,0 +1,78 @@
+// Device data layout shared by the host builder (C++) and the CUDA kernels.
+//
+// HBM layout of one triangle mesh (all arrays 16-byte aligned, leaf order = the order the BVH
+// leaves reference triangles in):
+//
+//   Node4   nodes[num_nodes]      128 B each = one L2 line: the boxes of the node's four children
+//                                 in structure-of-arrays form (lo.x[4] lo.y[4] lo.z[4] hi.x[4]
+//                                 hi.y[4] hi.z[4], FP32, rounded outward from the FP64 boxes so
+//                                 that pruning with them never drops a primitive the FP64 boxes
+//                                 would keep), then child[4] and count[4].
+//   TriHot  tri_hot[num_tris]     48 B: v0 and the two edge vectors ab, ac in FP32 with |ab|^2,
+//                                 ab.ac, |ac|^2 in the .w slots -- everything the FP32
+//                                 point-triangle distance test reads.
+//   TriSign tri_sign[num_tris]    96 B: FP32 face normal, 3 vertex and 3 edge pseudonormals; read
+//                                 once per query, for the winning triangle's sign.
+//   double  tri64[num_tris][30]   240 B: FP64 vertices, face normal, vertex and edge
+//                                 pseudonormals for the near-surface re-evaluation (the
+//                                 reference's TriangleSoA lane data, TriangleSoAImplem.hpp:28-70).
+//   int32   tri_id[num_tris]      leaf position -> triangle index in the caller's soup.
+//
+// child[k] of an interior slot is a node index; of a leaf slot, the first triangle (leaf order)
+// with EBG_LEAF_BIT set, count[k] its triangle count.  An empty slot has count 0 and an empty box
+// (lo = +inf, hi = -inf), whose point distance is +inf, so no bound ever admits it.
+#ifndef EBG_LAYOUT_H
+#define EBG_LAYOUT_H
+
+#include <stdint.h>
+
+#define EBG_LEAF_BIT 0x80000000u
+#define EBG_MAX_LEAF 32
+
+// Traversal stack depth (entries per warp).  The builder rejects trees whose depth would need
+// more (a 4-wide node pushes at most 3 siblings per level besides the one it descends into).
+#define EBG_STACK_DEPTH 96
+
+struct alignas(128) EbgNode4
+{
+  float    lox[4], loy[4], loz[4];
+  float    hix[4], hiy[4], hiz[4];
+  uint32_t child[4];
+  uint32_t count[4];
+};
+
+struct alignas(16) EbgTriHot
+{
+  float v0x, v0y, v0z, ab2;
+  float abx, aby, abz, abac;
+  float acx, acy, acz, ac2;
+};
+
+struct alignas(16) EbgTriSign
+{
+  float nx, ny, nz, pad0;
+  float vn[9];
+  float en[9];
+  float pad1, pad2;
+};
+
+static_assert(sizeof(EbgNode4) == 128, "node must be one 128-byte line");
+static_assert(sizeof(EbgTriHot) == 48, "hot triangle record must be 48 bytes");
+static_assert(sizeof(EbgTriSign) == 96, "sign record must be 96 bytes");
+
+// Device view of one mesh (passed by value to kernels).
+struct EbgMeshView
+{
+  const EbgNode4*   nodes;
+  const EbgTriHot*  hot;
+  const EbgTriSign* sign;
+  const double*     tri64;
+  const int32_t*    tri_id;
+  float             root_lo[3], root_hi[3]; // root box (FP32, outward)
+  uint32_t          root_ref;               // node index 0, or a leaf reference for tiny meshes
+  uint32_t          root_count;             // leaf count when root_ref is a leaf
+  float             morton_lo[3];           // Morton quantisation box for query ordering
+  float             morton_scale[3];
+};
+
+#endif

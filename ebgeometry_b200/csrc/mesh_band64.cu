@@ -1,0 +1,202 @@
+// FP64 near-surface re-evaluation (sm_100a).  Compiled with -fmad=false: the point-triangle
+// arithmetic below keeps the reference's separate multiplies and adds in the reference's order.
+//
+// Queries whose FP32 distance fell inside the band |d| <= band (default 1e-4 x the mesh's bounding
+// box diagonal, where the sign is ill-conditioned) are re-evaluated here with the reference's own
+// FP64 triangle test -- a lane-by-lane restatement of the AVX W=4 double path of
+// TriangleSoAT::signedDistance (TriangleSoAImplem.hpp:1029-1180) -- over every triangle whose FP32
+// (outward-rounded) box lies within |d32| + delta of the point, keeping the value of smallest
+// magnitude with strict < (MeshDistanceFunctionsImplem.hpp:492-502).  delta covers the FP32
+// distance error, so the FP64 winner is never pruned.  Packets of 32 band queries share one
+// traversal stack exactly as in the FP32 kernel.
+#include <cfloat>
+
+#include "ebg_device.cuh"
+#include "mesh_kernels.h"
+
+namespace ebg {
+
+namespace {
+
+struct D3
+{
+  double x, y, z;
+};
+__device__ __forceinline__ D3 ld3(const double* p) { return {p[0], p[1], p[2]}; }
+__device__ __forceinline__ D3 sub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b)
+{
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ D3 scl(double s, D3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ double sgnb(double x) { return signbit(x) ? -1.0 : 1.0; }
+
+// tri: v0 v1 v2 n vn0 vn1 vn2 en0 en1 en2 (30 doubles)
+__device__ double triSd64(const double* __restrict__ tri, D3 P)
+{
+  const D3 v0 = ld3(tri), v1 = ld3(tri + 3), v2 = ld3(tri + 6), n = ld3(tri + 9);
+  const D3 v21 = sub(v1, v0), v32 = sub(v2, v1), v13 = sub(v0, v2);
+  const D3 p1 = sub(P, v0), p2 = sub(P, v1), p3 = sub(P, v2);
+  const double s0 = sgnb(dot(cross(v21, n), p1));
+  const double s1 = sgnb(dot(cross(v32, n), p2));
+  const double s2 = sgnb(dot(cross(v13, n), p3));
+  if (fabs((s0 + s1) + s2) >= 2.0) {
+    return dot(n, p1);
+  }
+  const double t1 = dot(p1, v21) / dot(v21, v21);
+  const double t2 = dot(p2, v32) / dot(v32, v32);
+  const double t3 = dot(p3, v13) / dot(v13, v13);
+  const D3     y1 = sub(p1, scl(t1, v21)), y2 = sub(p2, scl(t2, v32)), y3 = sub(p3, scl(t3, v13));
+
+  double bd2 = dot(p1, p1);
+  double bs  = sgnb(dot(ld3(tri + 12), p1));
+  const double p2d2 = dot(p2, p2), p3d2 = dot(p3, p3);
+  if (p2d2 < bd2) {
+    bd2 = p2d2;
+    bs  = sgnb(dot(ld3(tri + 15), p2));
+  }
+  if (p3d2 < bd2) {
+    bd2 = p3d2;
+    bs  = sgnb(dot(ld3(tri + 18), p3));
+  }
+  const double y1d2 = dot(y1, y1), y2d2 = dot(y2, y2), y3d2 = dot(y3, y3);
+  if (t1 > 0.0 && t1 < 1.0 && y1d2 < bd2) {
+    bd2 = y1d2;
+    bs  = sgnb(dot(ld3(tri + 21), y1));
+  }
+  if (t2 > 0.0 && t2 < 1.0 && y2d2 < bd2) {
+    bd2 = y2d2;
+    bs  = sgnb(dot(ld3(tri + 24), y2));
+  }
+  if (t3 > 0.0 && t3 < 1.0 && y3d2 < bd2) {
+    bd2 = y3d2;
+    bs  = sgnb(dot(ld3(tri + 27), y3));
+  }
+  return bs * sqrt(bd2);
+}
+
+__global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float delta)
+{
+  __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
+  const int          lane  = threadIdx.x & 31;
+  float4*            stk   = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
+  const EbgMeshView& m     = a.mesh;
+  const uint32_t     count = *a.band_count;
+  const uint32_t     numPk = (count + 31) / 32;
+  const uint32_t     warpId = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t     nWarps = (gridDim.x * blockDim.x) >> 5;
+
+  for (uint32_t pk = warpId; pk < numPk; pk += nWarps) {
+    const uint32_t j     = pk * 32 + lane;
+    const bool     valid = j < count;
+    const uint32_t jj    = valid ? j : count - 1;
+    const uint32_t pos   = a.band_list[jj];
+    const uint32_t id    = a.order ? a.order[pos] : pos;
+    const D3       P     = {double(a.points[3 * size_t(id)]), double(a.points[3 * size_t(id) + 1]),
+                    double(a.points[3 * size_t(id) + 2])};
+    const float    px = float(P.x), py = float(P.y), pz = float(P.z);
+    const float    d32 = a.band_d32[jj];
+    float          r   = (fabsf(d32) + delta) * 1.000001f;
+    float          bound = r * r;
+    double         best  = DBL_MAX;
+    int            bt    = -1;
+    uint32_t       iters = 0;
+    int            err   = 0;
+
+    int sp = 1;
+    if (lane == 0) {
+      stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
+      stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+    }
+    __syncwarp();
+    while (sp > 0) {
+      if (++iters > MAX_ITERS) {
+        err |= ST_ITERS;
+        break;
+      }
+      --sp;
+      const float4 A = stk[2 * sp], B = stk[2 * sp + 1];
+      const float  d2 = boxDist2(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
+      if (!__any_sync(FULL, d2 <= bound)) {
+        continue;
+      }
+      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
+      if (ref & EBG_LEAF_BIT) {
+        const uint32_t t0 = ref & ~EBG_LEAF_BIT;
+        for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
+          const double d = triSd64(m.tri64 + 30 * size_t(tt), P);
+          if (fabs(d) < fabs(best)) {
+            best = d;
+            bt   = int(tt);
+            // shrink the bound to the FP64 winner (with the same relative margin)
+            const float rb = float(fabs(d)) * 1.000001f + 1e-30f;
+            bound          = fminf(bound, rb * rb);
+          }
+        }
+      }
+      else {
+        const EbgNode4& nd = m.nodes[ref];
+        int             o[4], np = 0;
+        float           key[4];
+        for (int k = 0; k < 4; k++) {
+          const float dk = boxDist2(nd.lox[k], nd.loy[k], nd.loz[k], nd.hix[k], nd.hiy[k], nd.hiz[k], px, py, pz);
+          if (__any_sync(FULL, dk <= bound)) {
+            o[np]   = k;
+            key[np] = dk;
+            np++;
+          }
+        }
+        // per-lane keys differ, so order by lane 0's distance (any fixed order is correct)
+        for (int i = 0; i < np; i++) {
+          key[i] = __shfl_sync(FULL, key[i], 0);
+        }
+        for (int i = 1; i < np; i++) {
+          for (int q = i; q > 0 && key[q - 1] < key[q]; q--) {
+            const float tk = key[q];
+            key[q]         = key[q - 1];
+            key[q - 1]     = tk;
+            const int to   = o[q];
+            o[q]           = o[q - 1];
+            o[q - 1]       = to;
+          }
+        }
+        for (int i = 0; i < np; i++) {
+          if (sp >= EBG_STACK_DEPTH) {
+            err |= ST_STACK;
+            break;
+          }
+          const int k = o[i];
+          if (lane == 0) {
+            stk[2 * sp]     = make_float4(nd.lox[k], nd.loy[k], nd.loz[k], __uint_as_float(nd.child[k]));
+            stk[2 * sp + 1] = make_float4(nd.hix[k], nd.hiy[k], nd.hiz[k], __uint_as_float(nd.count[k]));
+          }
+          sp++;
+        }
+        __syncwarp();
+        if (err) {
+          break;
+        }
+      }
+    }
+    if (err && lane == 0) {
+      atomicOr(a.status, err);
+    }
+    if (valid && bt >= 0) {
+      a.out_d[id] = float(best);
+      if (a.out_tri) {
+        a.out_tri[id] = m.tri_id[bt];
+      }
+    }
+  }
+}
+
+} // namespace
+
+cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s)
+{
+  kMeshBand64<<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+  return cudaGetLastError();
+}
+
+} // namespace ebg

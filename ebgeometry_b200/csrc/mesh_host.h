@@ -1,0 +1,53 @@
+// Host-side (C++) preprocessing of the mesh path: pseudonormals and the 4-wide BVH build.
+#ifndef EBG_MESH_HOST_H
+#define EBG_MESH_HOST_H
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "ebg_layout.h"
+
+namespace ebg {
+
+// Face, edge and angle-weighted vertex pseudonormals of a triangle soup, as the reference's DCEL
+// computes them (see mesh_host.cpp).  Outputs per triangle: triN (3), cornerVN (9), edgeN (9).
+// Returns false (with msg) on a non-manifold edge shared by more than two triangles or a
+// degenerate triangle.
+bool computePseudonormals(const double*        V,
+                          int64_t              nv,
+                          const int32_t*       F,
+                          int64_t              nt,
+                          std::vector<double>& triN,
+                          std::vector<double>& cornerVN,
+                          std::vector<double>& edgeN,
+                          std::string&         msg);
+
+struct Bvh4
+{
+  std::vector<EbgNode4> nodes;
+  std::vector<uint32_t> order; // leaf position -> primitive index
+  uint32_t              rootRef   = 0;
+  uint32_t              rootCount = 0;
+  int                   depth     = 0;
+  int64_t               numLeaves = 0;
+  double                lo[3], hi[3];
+};
+
+// Builds a 4-wide BVH over primitives given by FP64 boxes (lo/hi, 3 per primitive) and
+// centroids.  build: 0 = binned SAH, 1 = Morton.  leafSize: max primitives per leaf.
+bool buildBvh4(const std::vector<double>& boxLo,
+               const std::vector<double>& boxHi,
+               const std::vector<double>& centroid,
+               int                        build,
+               int                        leafSize,
+               Bvh4&                      out,
+               std::string&               msg);
+
+// Outward rounding of FP64 box bounds to FP32.
+float roundDown(double x);
+float roundUp(double x);
+
+} // namespace ebg
+
+#endif

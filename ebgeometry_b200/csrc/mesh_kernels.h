@@ -1,0 +1,42 @@
+// Launch wrappers of the mesh kernels (called from the C ABI layer).
+#ifndef EBG_MESH_KERNELS_H
+#define EBG_MESH_KERNELS_H
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ebg_layout.h"
+
+namespace ebg {
+
+struct MeshQueryArgs
+{
+  EbgMeshView        mesh;
+  const float*       points;     // caller's xyz (n x 3)
+  const uint32_t*    order;      // sorted position -> caller index (nullptr = identity)
+  const float*       seed_r;     // per sorted position: predicted pruning radius (nullptr = none)
+  int64_t            n;
+  float*             out_d;      // caller order
+  int32_t*           out_tri;    // caller order (nullable)
+  float              band;       // |d| <= band -> FP64 re-evaluation list
+  uint32_t*          band_list;  // sorted positions needing FP64 (nullable = no band pass)
+  uint32_t*          band_count;
+  float*             band_d32;   // FP32 distance of each band entry
+  unsigned long long* work;      // packet counter (zeroed before the launch)
+  int*               status;     // device status word (ST_* bits)
+  unsigned long long* stats;     // 5 counters (nullable)
+};
+
+// Morton keys of the query points (30 bits) and the identity permutation.
+void launchQueryKeys(const float* points, int64_t n, const float* lo, const float* scale, uint32_t* keys,
+                     uint32_t* ids, cudaStream_t s);
+
+// FP32 packet traversal.  warpsPerBlock in {1,2,4,8}.
+cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int warpsPerBlock, int numSms, cudaStream_t s);
+
+// FP64 re-evaluation of the band list (reads band_count on the device).
+cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s);
+
+} // namespace ebg
+
+#endif

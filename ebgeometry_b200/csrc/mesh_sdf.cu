@@ -1,0 +1,385 @@
+// FP32 mesh signed-distance traversal (sm_100a).
+//
+// The reference evaluates one point at a time with a stack-based branch-and-bound DFS over a
+// K-wide packed BVH (PackedBVH::pruneTraverse, BVHImplem.hpp:1098-1606): pop {node, d2}; skip if
+// d2 > bound; leaf -> evaluate its triangles, keeping the signed distance of smallest magnitude
+// (strict <, MeshDistanceFunctionsImplem.hpp:480-509); interior -> box distances of the K
+// children, sorted far-to-near, pushed if d2 <= bound.
+//
+// Here one warp traverses a PACKET of 32 queries that were sorted along a Morton curve, so they
+// are spatial neighbours:
+//  - the warp shares one stack in shared memory (entries carry the child box, so a popped entry is
+//    re-tested against every lane's current bound without touching global memory);
+//  - every node and triangle is read once per packet with a warp-uniform (broadcast) 16-byte load
+//    and tested by all 32 lanes, so control flow never diverges;
+//  - a child is pushed when __any_sync says some lane's bound admits it; children are ordered
+//    near-first by their distance to the packet centroid;
+//  - each lane keeps its own bound (its best squared distance so far), exactly the reference's
+//    prune bound for that point;
+//  - the leaf test computes only the unsigned squared distance (closest point by Voronoi region);
+//    the winning triangle's sign is taken once at the end from the pseudonormal of its closest
+//    feature, which is what the reference's per-triangle signed test yields for the minimum;
+//  - queries with |d| inside the near-surface band are appended to a list for the FP64
+//    re-evaluation (mesh_band64.cu).
+// Packets are handed out by an atomic counter, so a warp that drew cheap exterior packets keeps
+// working while others finish interior ("blind spot") packets.
+#include <cfloat>
+#include <cub/device/device_radix_sort.cuh>
+
+#include "ebg_device.cuh"
+#include "mesh_kernels.h"
+
+namespace ebg {
+
+namespace {
+
+// Closest point of triangle (v0, v0+ab, v0+ac) to p by Voronoi region (the standard barycentric
+// region tests).  Returns the squared distance; s, t are the barycentric weights of ab and ac of
+// the closest point and region is 0 face, 1..3 vertex 0..2, 4 edge 0-1, 5 edge 1-2, 6 edge 2-0.
+// Equivalent to the reference's triangle test (TriangleSoAImplem.hpp:1199-1293): its "inside"
+// test (all three (e_i x n).p_i of one sign) is the face region, and outside it the minimum over
+// vertices and interior edge points is the closest boundary point.
+template <bool WANT_REGION>
+__device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, const float4 h2, float px, float py,
+                                          float pz, float& s, float& t, int& region)
+{
+  const float apx = px - h0.x, apy = py - h0.y, apz = pz - h0.z;
+  const float ab2 = h0.w, abac = h1.w, ac2 = h2.w;
+  const float d1 = fmaf(h1.x, apx, fmaf(h1.y, apy, h1.z * apz));
+  const float d2 = fmaf(h2.x, apx, fmaf(h2.y, apy, h2.z * apz));
+  const float d3 = d1 - ab2, d4 = d2 - abac;
+  const float d5 = d1 - abac, d6 = d2 - ac2;
+  const float vc = fmaf(d1, d4, -d3 * d2);
+  const float vb = fmaf(d5, d2, -d1 * d6);
+  const float va = fmaf(d3, d6, -d5 * d4);
+
+  // face region by default; each test below overrides, the highest-priority region last
+  float sn = vb, tn = vc, den = va + vb + vc;
+  int   r  = 0;
+  const float bc1 = d4 - d3, bc2 = d5 - d6;
+  if (va <= 0.f && bc1 >= 0.f && bc2 >= 0.f) { // edge 1-2
+    sn = bc2;
+    tn = bc1;
+    den = bc1 + bc2;
+    r   = 5;
+  }
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) { // edge 2-0 (along ac)
+    sn  = 0.f;
+    tn  = d2;
+    den = d2 - d6;
+    r   = 6;
+  }
+  if (d6 >= 0.f && d5 <= d6) { // vertex 2
+    sn  = 0.f;
+    tn  = 1.f;
+    den = 1.f;
+    r   = 3;
+  }
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) { // edge 0-1 (along ab)
+    sn  = d1;
+    tn  = 0.f;
+    den = d1 - d3;
+    r   = 4;
+  }
+  if (d3 >= 0.f && d4 <= d3) { // vertex 1
+    sn  = 1.f;
+    tn  = 0.f;
+    den = 1.f;
+    r   = 2;
+  }
+  if (d1 <= 0.f && d2 <= 0.f) { // vertex 0
+    sn  = 0.f;
+    tn  = 0.f;
+    den = 1.f;
+    r   = 1;
+  }
+  const float inv = __fdividef(1.f, den);
+  s               = sn * inv;
+  t               = tn * inv;
+  const float dx  = fmaf(-t, h2.x, fmaf(-s, h1.x, apx));
+  const float dy  = fmaf(-t, h2.y, fmaf(-s, h1.y, apy));
+  const float dz  = fmaf(-t, h2.z, fmaf(-s, h1.z, apz));
+  if (WANT_REGION) {
+    region = r;
+  }
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+__device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
+
+// Signed distance of p to triangle `tri` (leaf order), sign from the pseudonormal of the closest
+// feature (the reference's sign-bit convention, TriangleSoAImplem.hpp:1076-1082: +0 -> +1).
+__device__ float signedFromWinner(const EbgMeshView& m, uint32_t tri, float px, float py, float pz)
+{
+  const float4* h = reinterpret_cast<const float4*>(m.hot + tri);
+  const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+  float         s, t;
+  int           region;
+  const float   d2 = triDist2<true>(h0, h1, h2, px, py, pz, s, t, region);
+  const float*  sg = reinterpret_cast<const float*>(m.sign + tri);
+  const float   apx = px - h0.x, apy = py - h0.y, apz = pz - h0.z;
+  if (region == 0) {
+    // face: the reference returns n . (p - v0) itself
+    return fmaf(__ldg(sg + 0), apx, fmaf(__ldg(sg + 1), apy, __ldg(sg + 2) * apz));
+  }
+  const float dx = fmaf(-t, h2.x, fmaf(-s, h1.x, apx));
+  const float dy = fmaf(-t, h2.y, fmaf(-s, h1.y, apy));
+  const float dz = fmaf(-t, h2.z, fmaf(-s, h1.z, apz));
+  // vertex i -> vn[3i..], edge j -> en[3j..]: sign record = n(3) pad vn(9) en(9)
+  const int   o  = (region <= 3) ? (4 + 3 * (region - 1)) : (13 + 3 * (region - 4));
+  const float sd = fmaf(__ldg(sg + o), dx, fmaf(__ldg(sg + o + 1), dy, __ldg(sg + o + 2) * dz));
+  return signOf(sd) * sqrtf(d2);
+}
+
+template <bool STATS, bool SEEDED>
+__global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
+{
+  extern __shared__ float4 smem[];
+  const int     lane = threadIdx.x & 31;
+  float4*       stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
+  const EbgMeshView& m = a.mesh;
+  const uint64_t numPackets = (uint64_t(a.n) + 31) / 32;
+
+  while (true) {
+    unsigned long long pk = 0;
+    if (lane == 0) {
+      pk = atomicAdd(a.work, 1ull);
+    }
+    pk = __shfl_sync(FULL, pk, 0);
+    if (pk >= numPackets) {
+      break;
+    }
+    const int64_t  pos   = int64_t(pk) * 32 + lane;
+    const bool     valid = pos < a.n;
+    const int64_t  src   = valid ? pos : a.n - 1;
+    const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
+    const float    px = __ldg(a.points + 3 * size_t(id)), py = __ldg(a.points + 3 * size_t(id) + 1),
+                pz = __ldg(a.points + 3 * size_t(id) + 2);
+    const float cx = warpSum(px) * (1.f / 32.f), cy = warpSum(py) * (1.f / 32.f), cz = warpSum(pz) * (1.f / 32.f);
+
+    float best    = FLT_MAX;
+    int   besttri = -1;
+    if (SEEDED) {
+      const float r = __ldg(a.seed_r + src);
+      best          = (r > 0.f && r < 1e18f) ? r * r : FLT_MAX;
+    }
+    uint32_t iters = 0;
+    int      err   = 0;
+    uint32_t cNode = 0, cLeaf = 0, cTri = 0, cFall = 0;
+
+#pragma unroll 1
+    for (int pass = 0; pass < (SEEDED ? 2 : 1); pass++) {
+      if (pass == 1) {
+        const bool fail = besttri < 0;
+        if (!__any_sync(FULL, fail)) {
+          break;
+        }
+        if (fail) {
+          best = FLT_MAX;
+          cFall++;
+        }
+      }
+      int sp = 1;
+      if (lane == 0) {
+        stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
+        stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+      }
+      __syncwarp();
+#pragma unroll 1
+      while (sp > 0) {
+        if (++iters > MAX_ITERS) {
+          err |= ST_ITERS;
+          break;
+        }
+        --sp;
+        const float4 A    = stk[2 * sp];
+        const float4 B    = stk[2 * sp + 1];
+        const float  d2   = boxDist2(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
+        const bool   need = d2 <= best;
+        if (!__any_sync(FULL, need)) {
+          continue;
+        }
+        const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
+        if (ref & EBG_LEAF_BIT) {
+          const uint32_t t0 = ref & ~EBG_LEAF_BIT;
+          if (STATS && need) {
+            cLeaf++;
+            cTri += cnt;
+          }
+#pragma unroll 1
+          for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
+            const float4* h = reinterpret_cast<const float4*>(m.hot + tt);
+            const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+            float         s, t;
+            int           r;
+            const float   dd = triDist2<false>(h0, h1, h2, px, py, pz, s, t, r);
+            if (dd < best) {
+              best    = dd;
+              besttri = int(tt);
+            }
+          }
+        }
+        else {
+          if (STATS && need) {
+            cNode++;
+          }
+          const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
+          const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+          const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+          const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
+          const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+          const float   clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
+                      clz[4] = {lz.x, lz.y, lz.z, lz.w};
+          const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
+                      chz[4] = {hz.x, hz.y, hz.z, hz.w};
+          const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
+          float          key[4];
+          int            o[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
+            const bool  nk = __any_sync(FULL, dk <= best);
+            // uniform ordering key; children nobody needs get -1 and are not pushed
+            key[k] = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
+            o[k]   = k;
+          }
+          // sort slots by key, descending (far first) -- a 5-comparator network
+#define EBG_CSWAP(i, j)                                                                                               \
+  if (key[o[i]] < key[o[j]]) {                                                                                        \
+    const int tmp = o[i];                                                                                             \
+    o[i]          = o[j];                                                                                             \
+    o[j]          = tmp;                                                                                              \
+  }
+          EBG_CSWAP(0, 1);
+          EBG_CSWAP(2, 3);
+          EBG_CSWAP(0, 2);
+          EBG_CSWAP(1, 3);
+          EBG_CSWAP(1, 2);
+#undef EBG_CSWAP
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const int k = o[j];
+            if (key[k] >= 0.f) {
+              if (sp >= EBG_STACK_DEPTH) {
+                err |= ST_STACK;
+                break;
+              }
+              if (lane == 0) {
+                stk[2 * sp]     = make_float4(clx[k], cly[k], clz[k], __uint_as_float(cref[k]));
+                stk[2 * sp + 1] = make_float4(chx[k], chy[k], chz[k], __uint_as_float(ccnt[k]));
+              }
+              sp++;
+            }
+          }
+          __syncwarp();
+          if (err) {
+            break;
+          }
+        }
+      }
+      if (err) {
+        break;
+      }
+    }
+
+    if (err && lane == 0) {
+      atomicOr(a.status, err);
+    }
+    float dist = FLT_MAX;
+    if (besttri >= 0) {
+      dist = signedFromWinner(m, uint32_t(besttri), px, py, pz);
+    }
+    if (valid) {
+      a.out_d[id] = dist;
+      if (a.out_tri) {
+        a.out_tri[id] = besttri >= 0 ? __ldg(m.tri_id + besttri) : -1;
+      }
+    }
+    if (a.band_list) {
+      const bool     inb  = valid && besttri >= 0 && fabsf(dist) <= a.band;
+      const unsigned mask = __ballot_sync(FULL, inb);
+      if (mask) {
+        uint32_t base = 0;
+        if (lane == 0) {
+          base = atomicAdd(a.band_count, uint32_t(__popc(mask)));
+        }
+        base = __shfl_sync(FULL, base, 0);
+        if (inb) {
+          const uint32_t r = base + __popc(mask & ((1u << lane) - 1u));
+          a.band_list[r]   = uint32_t(pos);
+          a.band_d32[r]    = dist;
+        }
+      }
+    }
+    if (STATS) {
+      if (!valid) {
+        cNode = cLeaf = cTri = cFall = 0;
+      }
+      atomicAdd(a.stats + 0, (unsigned long long)cNode);
+      atomicAdd(a.stats + 1, (unsigned long long)cLeaf);
+      atomicAdd(a.stats + 2, (unsigned long long)cTri);
+      atomicAdd(a.stats + 4, (unsigned long long)cFall);
+    }
+  }
+}
+
+__global__ void kQueryKeys(const float* __restrict__ pts, int64_t n, float lx, float ly, float lz, float sx, float sy,
+                           float sz, uint32_t* __restrict__ keys, uint32_t* __restrict__ ids)
+{
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  const float x = pts[3 * i], y = pts[3 * i + 1], z = pts[3 * i + 2];
+  const float fx = fminf(fmaxf((x - lx) * sx, 0.f), 1023.f);
+  const float fy = fminf(fmaxf((y - ly) * sy, 0.f), 1023.f);
+  const float fz = fminf(fmaxf((z - lz) * sz, 0.f), 1023.f);
+  // NaN coordinates quantise to 0 (fmaxf drops NaN); they are rejected on the host before launch
+  keys[i] = (spread10(uint32_t(fx)) << 2) | (spread10(uint32_t(fy)) << 1) | spread10(uint32_t(fz));
+  ids[i]  = uint32_t(i);
+}
+
+template <bool STATS, bool SEEDED>
+cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
+{
+  const int    threads = 32 * wpb;
+  const size_t smem    = size_t(wpb) * 2 * EBG_STACK_DEPTH * sizeof(float4);
+  int          perSm   = 0;
+  cudaError_t  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEEDED>, threads, smem);
+  if (e != cudaSuccess) {
+    return e;
+  }
+  perSm               = perSm < 1 ? 1 : perSm;
+  const int64_t need  = ((int64_t(a.n) + 31) / 32 + wpb - 1) / wpb;
+  int64_t       grid  = int64_t(numSms) * perSm;
+  grid                = grid < need ? grid : need;
+  grid                = grid < 1 ? 1 : grid;
+  kMeshSdf32<STATS, SEEDED><<<unsigned(grid), threads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+} // namespace
+
+void launchQueryKeys(const float* points, int64_t n, const float* lo, const float* scale, uint32_t* keys,
+                     uint32_t* ids, cudaStream_t s)
+{
+  const int     threads = 256;
+  const int64_t blocks  = (n + threads - 1) / threads;
+  kQueryKeys<<<unsigned(blocks), threads, 0, s>>>(points, n, lo[0], lo[1], lo[2], scale[0], scale[1], scale[2], keys,
+                                                  ids);
+}
+
+cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
+{
+  if (wpb != 1 && wpb != 2 && wpb != 4 && wpb != 8) {
+    wpb = 4;
+  }
+  const bool stats  = a.stats != nullptr;
+  const bool seeded = a.seed_r != nullptr;
+  if (stats) {
+    return seeded ? launchOne<true, true>(a, wpb, numSms, s) : launchOne<true, false>(a, wpb, numSms, s);
+  }
+  return seeded ? launchOne<false, true>(a, wpb, numSms, s) : launchOne<false, false>(a, wpb, numSms, s);
+}
+
+} // namespace ebg

@@ -1,0 +1,201 @@
+/*
+ * ebgeometry_b200 -- C ABI of the B200-native mesh signed-distance / nearest-neighbour /
+ * CSG-union query path (sm_100a CUDA kernels behind plain C entry points).
+ *
+ * The reference (rmrsk/EBGeometry) is a header-only C++ library with no C ABI: its interface is
+ * the virtual ImplicitFunction<T>::value(point) (Source/EBGeometry_ImplicitFunction.hpp:51-60)
+ * called once per point.  Each entry point below names the reference interface it replaces.
+ * The C++ drop-in classes in ebgeometry_b200/include/EBGeometry_B200.hpp wrap this ABI behind the
+ * reference's class names and value(point) signature.
+ *
+ * Conventions
+ *  - Every function returns an ebg_status (0 = EBG_OK).  On failure, ebg_last_error() returns a
+ *    thread-local message describing the last error on the calling thread.
+ *  - Handles are opaque and owned by the caller (create / destroy).
+ *  - "_dev" pointers are CUDA device pointers on the handle's device; "_host" entry points take
+ *    host pointers and do the host<->device copies themselves.
+ *  - stream is a cudaStream_t passed as void* (NULL = the legacy default stream).  Device entry
+ *    points are asynchronous on that stream unless stated otherwise; status codes that depend on
+ *    device-side checks are reported by the next synchronising call (ebg_check_status).
+ *  - Points are float32 xyz triples (interleaved, 12 bytes per point).
+ */
+#ifndef EBGEOMETRY_B200_H
+#define EBGEOMETRY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ebg_status
+{
+  EBG_OK             = 0,
+  EBG_ERR_INVALID    = 1, /* bad argument (null pointer, negative size, k out of range, ...) */
+  EBG_ERR_CUDA       = 2, /* a CUDA runtime call failed */
+  EBG_ERR_NO_MEMORY  = 3, /* device or host allocation failed */
+  EBG_ERR_TRAVERSAL  = 4, /* a kernel hit its stack-depth or iteration bound and stopped early */
+  EBG_ERR_NOT_FOUND  = 5, /* the library or a device could not be found */
+  EBG_ERR_TOO_LARGE  = 6  /* input exceeds a documented limit */
+} ebg_status;
+
+/* Tree builders, mirroring BVH::Build (Source/EBGeometry_BVH.hpp:47-55). */
+typedef enum ebg_build
+{
+  EBG_BUILD_SAH    = 0, /* binned SAH, top-down (BinnedSAHPartitioner, BVH.hpp:715-734) */
+  EBG_BUILD_MORTON = 1  /* bottom-up along a Morton curve (bottomUpSortAndPartition, BVHImplem.hpp:207-312) */
+} ebg_build;
+
+typedef struct ebg_build_opts
+{
+  int32_t build;     /* ebg_build */
+  int32_t leaf_size; /* max primitives per leaf (the reference's maxLeafGroups * W); 0 = default 8 */
+  int32_t device;    /* CUDA device ordinal; -1 = current device */
+  int32_t reserved;
+} ebg_build_opts;
+
+typedef struct ebg_mesh  ebg_mesh;
+typedef struct ebg_cloud ebg_cloud;
+typedef struct ebg_scene ebg_scene;
+typedef struct ebg_seed  ebg_seed;
+
+/* Device time of each phase of one query call, from CUDA events recorded on the call's stream. */
+typedef struct ebg_phase_timings
+{
+  float order_ms;    /* Morton keys + radix sort of the points */
+  float traverse_ms; /* FP32 packet traversal (+ seed inference when seeded) */
+  float band_ms;     /* FP64 near-surface re-evaluation */
+  float total_ms;
+} ebg_phase_timings;
+
+/* Per-call options of the mesh signed-distance query.  Zero-initialised = defaults. */
+typedef struct ebg_query_opts
+{
+  double             band;            /* |d| below which the FP64 re-evaluation runs; <= 0 -> 1e-4 * diag */
+  int32_t            no_sort;         /* 1: keep the caller's point order (no Morton reordering) */
+  int32_t            no_fp64_band;    /* 1: skip the FP64 near-surface re-evaluation */
+  const ebg_seed*    seed;            /* learned pruning-radius model (NULL = plain traversal) */
+  int32_t            warps_per_block; /* 0 = tuned default */
+  int32_t            reserved;
+  ebg_phase_timings* timings;         /* non-NULL: record events per phase; the call then
+                                         synchronises the stream and fills this struct */
+} ebg_query_opts;
+
+/* Mesh summary. */
+typedef struct ebg_mesh_info
+{
+  int64_t num_triangles;
+  int64_t num_vertices;
+  int64_t num_nodes;   /* 4-wide BVH nodes */
+  int64_t num_leaves;
+  int32_t depth;       /* node levels on the deepest root-to-leaf path */
+  int32_t leaf_size;
+  double  lo[3], hi[3];
+  double  diagonal;    /* |hi - lo| of the vertex bounding box */
+  int64_t device_bytes;
+} ebg_mesh_info;
+
+/* Counters of one query call (for the roofline and the seed statistics).  Filled when the call
+ * is made through a *_stats entry point; all counts are summed over the queries of the call. */
+typedef struct ebg_query_stats
+{
+  int64_t nodes_visited;     /* interior nodes whose child boxes were loaded, per query */
+  int64_t leaves_visited;    /* leaves whose triangles were tested, per query */
+  int64_t triangles_tested;  /* point-triangle tests, per query */
+  int64_t band_queries;      /* queries re-evaluated in FP64 */
+  int64_t seed_fallbacks;    /* seeded queries whose predicted radius held no triangle */
+} ebg_query_stats;
+
+const char* ebg_last_error(void);
+const char* ebg_version(void);
+int         ebg_device_count(void);
+
+/* ---- triangle meshes: TriMeshSDF (MeshDistanceFunctions.hpp:309-489) -------------------------
+ *
+ * ebg_mesh_create replaces TriMeshSDF(mesh, build, maxLeafGroups) after Soup::soupToDCEL
+ * (MeshDistanceFunctionsImplem.hpp:417-460, SoupImplem.hpp:149-227): it takes a vertex/triangle
+ * soup (double xyz, int32 corner indices, counter-clockwise = outward), computes the face, edge
+ * and angle-weighted vertex pseudonormals the way the reference's DCEL does, builds the 4-wide BVH
+ * on the host and uploads it.  Vertices are not merged (as in soupToDCEL). */
+ebg_status ebg_mesh_create(const double*         vertices,
+                           int64_t               num_vertices,
+                           const int32_t*        triangles,
+                           int64_t               num_triangles,
+                           const ebg_build_opts* opts,
+                           ebg_mesh**            out);
+
+/* Same with caller-given pseudonormals instead of computed ones (the reference's
+ * Triangle::setVertexNormals / setEdgeNormals, TriangleImplem.hpp:60-88): per triangle, 3 vertex
+ * normals and 3 edge normals (edge i runs from corner i to corner i+1), 9 doubles each. */
+ebg_status ebg_mesh_create_with_normals(const double*         vertices,
+                                        int64_t               num_vertices,
+                                        const int32_t*        triangles,
+                                        int64_t               num_triangles,
+                                        const double*         corner_vertex_normals,
+                                        const double*         edge_normals,
+                                        const ebg_build_opts* opts,
+                                        ebg_mesh**            out);
+
+/* Host-only: the pseudonormals ebg_mesh_create computes (no device needed).  Per triangle: the
+ * face normal (3 doubles; Triangle::computeNormal, TriangleImplem.hpp:94-106), the vertex
+ * pseudonormal at each corner (9; angle-weighted, DCEL_VertexImplem.hpp:190-~290) and the
+ * pseudonormal of each edge (9; edge i from corner i to i+1, DCEL_EdgeImplem.hpp:128-165). */
+ebg_status ebg_compute_pseudonormals(const double*  vertices,
+                                     int64_t        num_vertices,
+                                     const int32_t* triangles,
+                                     int64_t        num_triangles,
+                                     double*        face_normals,
+                                     double*        corner_vertex_normals,
+                                     double*        edge_normals);
+
+ebg_status ebg_mesh_destroy(ebg_mesh* mesh);
+ebg_status ebg_mesh_get_info(const ebg_mesh* mesh, ebg_mesh_info* info);
+
+/* Pseudonormals the handle computed (per triangle: face normal 3, vertex normals 9, edge normals 9
+ * doubles), for checking against the reference's DCEL. */
+ebg_status ebg_mesh_get_normals(const ebg_mesh* mesh, double* face_normals, double* corner_vertex_normals,
+                                double* edge_normals);
+
+/* Batched TriMeshSDF::signedDistance (MeshDistanceFunctionsImplem.hpp:480-509) over n points:
+ * dist_dev[i] = signed distance of points_dev[3i..3i+2]; closest_tri_dev (nullable) receives the
+ * index of the winning triangle in the input soup (getClosestTriangle's metadata,
+ * MeshDistanceFunctionsImplem.hpp:511-549).  Asynchronous on stream. */
+ebg_status ebg_mesh_signed_distance(const ebg_mesh*       mesh,
+                                    const float*          points_dev,
+                                    int64_t               n,
+                                    float*                dist_dev,
+                                    int32_t*              closest_tri_dev,
+                                    const ebg_query_opts* opts,
+                                    void*                 stream);
+
+/* The same with host buffers: copies points in, evaluates, copies distances out, synchronises. */
+ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       mesh,
+                                         const float*          points_host,
+                                         int64_t               n,
+                                         float*                dist_host,
+                                         int32_t*              closest_tri_host,
+                                         const ebg_query_opts* opts,
+                                         void*                 stream);
+
+/* Synchronous variant that also returns traversal counters (slower: counts with atomics). */
+ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       mesh,
+                                          const float*          points_dev,
+                                          int64_t               n,
+                                          float*                dist_dev,
+                                          const ebg_query_opts* opts,
+                                          ebg_query_stats*      stats,
+                                          void*                 stream);
+
+/* ImplicitFunction<T>::value(point) for one point (ImplicitFunction.hpp:51-52): the drop-in
+ * single-point call.  Synchronous; each call is one tiny launch, so batch where you can. */
+ebg_status ebg_mesh_value(const ebg_mesh* mesh, double x, double y, double z, double* value);
+
+/* Blocks until the stream's work for this mesh is done and reports any device-side error
+ * (EBG_ERR_TRAVERSAL) recorded by earlier asynchronous calls. */
+ebg_status ebg_check_status(const ebg_mesh* mesh, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EBGEOMETRY_B200_H */
