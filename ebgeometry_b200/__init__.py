@@ -6,6 +6,8 @@ Python mirror of the reference's (rmrsk/EBGeometry) C++ query objects on top of 
 * :class:`TriMeshSDF` -- ``TriMeshSDF(mesh, build, maxLeafGroups)`` (MeshDistanceFunctions.hpp:
   309-489) with ``value(point)`` / ``signedDistance(point)`` for one point (ImplicitFunction.hpp:
   51-60) and a batched ``signed_distance(points)`` over CUDA tensors or numpy arrays.
+* :class:`PointCloudBVH` -- ``PointCloudBVH(positions, meta)`` (PointCloudBVH.hpp:56-350) with
+  ``closestPoint`` / ``closestPoints`` for one point and a batched ``knn(queries, k)``.
 
 There is no CPU fallback: every query runs in the CUDA kernels of ``libebgb200.so``, and importing
 this package fails if that library is missing.
@@ -19,7 +21,7 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["TriMeshSDF", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
+__all__ = ["TriMeshSDF", "PointCloudBVH", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
 BUILD_MORTON = 1
@@ -159,3 +161,72 @@ class TriMeshSDF:
 
     def check_status(self, stream=None):
         check(lib.ebg_check_status(self._h, _stream_ptr(stream)))
+
+
+class PointCloudBVH:
+    """k-nearest-neighbour search over a point cloud (the reference's PointCloudBVH).
+
+    ``points``: (n,3) float32, a numpy array (built after a host->device copy) or a CUDA tensor
+    (built in place).  Neighbours come in increasing (squared distance, index) order, so equal
+    distances resolve to the lowest index; squared distances are the reference's float arithmetic.
+    """
+
+    def __init__(self, points, leaf_size=16, device=-1, stream=None):
+        opts = _capi.BuildOpts(0, int(leaf_size), int(device), 0)
+        h = C.c_void_p()
+        if isinstance(points, np.ndarray):
+            p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            check(lib.ebg_cloud_create(_ptr(p), p.shape[0], C.byref(opts), C.byref(h)))
+            self.n = p.shape[0]
+        else:
+            import torch
+            if not (points.is_cuda and points.dtype == torch.float32 and points.is_contiguous()):
+                raise ValueError("points must be a contiguous float32 CUDA tensor of shape (n,3)")
+            self.n = points.numel() // 3
+            check(lib.ebg_cloud_create_device(C.c_void_p(points.data_ptr()), self.n, C.byref(opts), C.byref(h),
+                                              _stream_ptr(stream)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_cloud_destroy(h)
+            self._h = None
+
+    def numPoints(self) -> int:
+        return int(lib.ebg_cloud_size(self._h))
+
+    def knn(self, queries, k, sort=True, stream=None):
+        """(idx (nq,k) int32, d2 (nq,k) float32) for (nq,3) float32 queries (CUDA tensor: asynchronous
+        on ``stream``; numpy: synchronous host call)."""
+        opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0, None, 0, 0, None)
+        if isinstance(queries, np.ndarray):
+            q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, 3)
+            idx = np.empty((q.shape[0], k), np.int32)
+            d2 = np.empty((q.shape[0], k), np.float32)
+            check(lib.ebg_cloud_knn_host(self._h, _ptr(q), q.shape[0], int(k), _ptr(idx), _ptr(d2), C.byref(opts),
+                                         None))
+            return idx, d2
+        import torch
+        if not (queries.is_cuda and queries.dtype == torch.float32 and queries.is_contiguous()):
+            raise ValueError("queries must be a contiguous float32 CUDA tensor of shape (n,3)")
+        nq = queries.numel() // 3
+        idx = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        d2 = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+        check(lib.ebg_cloud_knn(self._h, C.c_void_p(queries.data_ptr()), nq, int(k), C.c_void_p(idx.data_ptr()),
+                                C.c_void_p(d2.data_ptr()), C.byref(opts), _stream_ptr(stream)))
+        return idx, d2
+
+    # --- the reference's single-point API (PointCloudBVHImplem.hpp:429-453) -----------------------
+    def closestPoint(self, q):
+        """(index, squared distance) of the nearest point."""
+        idx, d2 = self.knn(np.asarray(q, np.float32).reshape(1, 3), 1)
+        return int(idx[0, 0]), float(d2[0, 0])
+
+    def closestPoints(self, q, k):
+        """The k nearest as a list of (index, squared distance), nearest first."""
+        idx, d2 = self.knn(np.asarray(q, np.float32).reshape(1, 3), k)
+        return [(int(i), float(d)) for i, d in zip(idx[0], d2[0]) if i >= 0]
+
+    def check_status(self, stream=None):
+        check(lib.ebg_cloud_check_status(self._h, _stream_ptr(stream)))

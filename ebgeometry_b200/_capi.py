@@ -68,6 +68,13 @@ SIGNATURES = {
                                                  C.POINTER(QueryStats), _P]),
     "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),
     "ebg_check_status": (C.c_int, [_P, _P]),
+    "ebg_cloud_create": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "ebg_cloud_create_device": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P), _P]),
+    "ebg_cloud_destroy": (C.c_int, [_P]),
+    "ebg_cloud_size": (_I64, [_P]),
+    "ebg_cloud_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_cloud_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_cloud_check_status": (C.c_int, [_P, _P]),
 }
 
 

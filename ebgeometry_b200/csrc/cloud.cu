@@ -1,0 +1,452 @@
+// Point-cloud nearest-neighbour search (sm_100a): GPU build + packet k-NN traversal.
+//
+// Reference: PointCloudBVH (PointCloudBVH.hpp:56-350, PointCloudBVHImplem.hpp:59-610): a K-wide
+// packed BVH over SoA groups of W points, built by recursive longest-axis midpoint partitioning,
+// queried by pruneTraverse with a {d2, index} state for k = 1 and an insertion-sorted Hit[k] for
+// k > 1 (PointCloudBVHImplem.hpp:263-427).
+//
+// Build here (all on the device, a few kernels):
+//   1. bounding box of the points; 2. 30-bit Morton key of each point in that box; 3. radix sort
+//   of (key, index); 4. leaves = runs of L consecutive sorted points, stored as float4
+//   (x, y, z, original index) -- one or two 128-byte lines per leaf; 5. an implicit 4-ary tree over
+//   the leaves in Morton order, level by level (node j of a level owns children 4j..4j+3 of the level
+//   below), written as 128-byte EbgNode4 records with the root at index 0.
+// Query: Morton-sorted queries in packets of 32 per warp with a shared stack (as the mesh kernel);
+// each lane keeps its k best (d2, index) pairs sorted in registers.  Order is lexicographic on
+// (d2, index), so equal distances resolve to the lowest index, and d2 is the reference's float
+// arithmetic (PointSoAImplem.hpp:214-230): dx = q - p, d2 = (dx*dx + dy*dy) + dz*dz, each operation
+// rounded separately (no fused multiply-add).  Box distances use the same association, which makes
+// the box distance of a leaf never exceed the computed d2 of any point inside it, so pruning with
+// "box d2 > k-th best d2" never drops a point that belongs in the answer, ties included.
+#include <algorithm>
+#include <cfloat>
+#include <cstdint>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "cloud_kernels.h"
+#include "ebg_device.cuh"
+
+namespace ebg {
+
+namespace {
+
+__device__ __forceinline__ float d2exact(float dx, float dy, float dz)
+{
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ float boxD2exact(float lx, float ly, float lz, float hx, float hy, float hz, float px,
+                                            float py, float pz)
+{
+  const float gx = fmaxf(0.f, fmaxf(__fsub_rn(lx, px), __fsub_rn(px, hx)));
+  const float gy = fmaxf(0.f, fmaxf(__fsub_rn(ly, py), __fsub_rn(py, hy)));
+  const float gz = fmaxf(0.f, fmaxf(__fsub_rn(lz, pz), __fsub_rn(pz, hz)));
+  return d2exact(gx, gy, gz);
+}
+
+// order-preserving float <-> uint mapping for atomic min/max of floats
+__device__ __forceinline__ uint32_t fkey(float f)
+{
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float funkey(uint32_t k)
+{
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void kBounds(const float* __restrict__ p, int64_t n, uint32_t* __restrict__ box)
+{
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const float v = p[3 * i + a];
+      lo[a]         = fminf(lo[a], v);
+      hi[a]         = fmaxf(hi[a], v);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[a] = fminf(lo[a], __shfl_xor_sync(FULL, lo[a], o));
+      hi[a] = fmaxf(hi[a], __shfl_xor_sync(FULL, hi[a], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int a = 0; a < 3; a++) {
+      atomicMin(box + a, fkey(lo[a]));
+      atomicMax(box + 3 + a, fkey(hi[a]));
+    }
+  }
+}
+
+__global__ void kCloudKeys(const float* __restrict__ p, int64_t n, const uint32_t* __restrict__ box,
+                           uint32_t* __restrict__ keys, uint32_t* __restrict__ ids)
+{
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  uint32_t q[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const float lo = funkey(box[a]), hi = funkey(box[3 + a]);
+    const float ext = hi - lo;
+    const float s   = ext > 0.f ? 1023.f / ext : 0.f;
+    q[a]            = uint32_t(fminf(fmaxf((p[3 * i + a] - lo) * s, 0.f), 1023.f));
+  }
+  keys[i] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+  ids[i]  = uint32_t(i);
+}
+
+__global__ void kGatherLeaves(const float* __restrict__ p, const uint32_t* __restrict__ order, int64_t n,
+                              float4* __restrict__ leafPts)
+{
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) {
+    return;
+  }
+  const uint32_t id = order[i];
+  leafPts[i]        = make_float4(p[3 * size_t(id)], p[3 * size_t(id) + 1], p[3 * size_t(id) + 2], __uint_as_float(id));
+}
+
+// Box of each leaf (L consecutive points); boxes as 6 floats (lo xyz, hi xyz).
+__global__ void kLeafBoxes(const float4* __restrict__ pts, int64_t n, int L, int64_t nLeaves, float* __restrict__ boxes)
+{
+  const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (l >= nLeaves) {
+    return;
+  }
+  float         lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  const int64_t b = l * L, e = (b + L < n) ? b + L : n;
+  for (int64_t i = b; i < e; i++) {
+    const float4 q = pts[i];
+    lo[0] = fminf(lo[0], q.x);
+    lo[1] = fminf(lo[1], q.y);
+    lo[2] = fminf(lo[2], q.z);
+    hi[0] = fmaxf(hi[0], q.x);
+    hi[1] = fmaxf(hi[1], q.y);
+    hi[2] = fmaxf(hi[2], q.z);
+  }
+  for (int a = 0; a < 3; a++) {
+    boxes[6 * l + a]     = lo[a];
+    boxes[6 * l + 3 + a] = hi[a];
+  }
+}
+
+// One tree level: node j (0 <= j < nNodes) gets children 4j..4j+3 of the level below (nChild
+// entries with boxes childBoxes).  childIsLeaf: children are point leaves (ref = LEAF | first point,
+// count = points) else nodes at index childBase + c.  Writes the node record at nodes[nodeBase + j]
+// and its own box into outBoxes[j].
+__global__ void kTreeLevel(int64_t nNodes, int64_t nChild, const float* __restrict__ childBoxes, int childIsLeaf,
+                           int64_t childBase, int L, int64_t nPoints, EbgNode4* __restrict__ nodes, int64_t nodeBase,
+                           float* __restrict__ outBoxes)
+{
+  const int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= nNodes) {
+    return;
+  }
+  EbgNode4 nd;
+  float    lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int64_t c = 4 * j + k;
+    if (c < nChild) {
+      const float* b = childBoxes + 6 * c;
+      nd.lox[k] = b[0];
+      nd.loy[k] = b[1];
+      nd.loz[k] = b[2];
+      nd.hix[k] = b[3];
+      nd.hiy[k] = b[4];
+      nd.hiz[k] = b[5];
+      for (int a = 0; a < 3; a++) {
+        lo[a] = fminf(lo[a], b[a]);
+        hi[a] = fmaxf(hi[a], b[3 + a]);
+      }
+      if (childIsLeaf) {
+        const int64_t first = c * L;
+        const int64_t cnt   = (first + L < nPoints) ? L : nPoints - first;
+        nd.child[k]         = EBG_LEAF_BIT | uint32_t(first);
+        nd.count[k]         = uint32_t(cnt);
+      }
+      else {
+        nd.child[k] = uint32_t(childBase + c);
+        nd.count[k] = 0;
+      }
+    }
+    else {
+      nd.lox[k] = nd.loy[k] = nd.loz[k] = __int_as_float(0x7f800000);  // +inf
+      nd.hix[k] = nd.hiy[k] = nd.hiz[k] = __int_as_float(0xff800000);  // -inf
+      nd.child[k] = 0;
+      nd.count[k] = 0;
+    }
+  }
+  nodes[nodeBase + j] = nd;
+  for (int a = 0; a < 3; a++) {
+    outBoxes[6 * j + a]     = lo[a];
+    outBoxes[6 * j + 3 + a] = hi[a];
+  }
+}
+
+// ---- query ---------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool lexLess(float da, uint32_t ia, float db, uint32_t ib)
+{
+  return da < db || (da == db && ia < ib);
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
+{
+  __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
+  const int          lane = threadIdx.x & 31;
+  float4*            stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
+  const EbgCloudView& c   = a.cloud;
+  const uint64_t     numPackets = (uint64_t(a.n) + 31) / 32;
+
+  while (true) {
+    unsigned long long pk = 0;
+    if (lane == 0) {
+      pk = atomicAdd(a.work, 1ull);
+    }
+    pk = __shfl_sync(FULL, pk, 0);
+    if (pk >= numPackets) {
+      break;
+    }
+    const int64_t  pos   = int64_t(pk) * 32 + lane;
+    const bool     valid = pos < a.n;
+    const int64_t  src   = valid ? pos : a.n - 1;
+    const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
+    const float    px = __ldg(a.queries + 3 * size_t(id)), py = __ldg(a.queries + 3 * size_t(id) + 1),
+                pz = __ldg(a.queries + 3 * size_t(id) + 2);
+    const float cx = warpSum(px) * (1.f / 32.f), cy = warpSum(py) * (1.f / 32.f), cz = warpSum(pz) * (1.f / 32.f);
+
+    float    kd[K];
+    uint32_t ki[K];
+#pragma unroll
+    for (int j = 0; j < K; j++) {
+      kd[j] = __int_as_float(0x7f800000);  // +inf: every finite point beats it
+      ki[j] = 0xffffffffu;
+    }
+    uint32_t iters = 0;
+    int      err   = 0;
+    int      sp    = 1;
+    if (lane == 0) {
+      stk[0] = make_float4(c.root_lo[0], c.root_lo[1], c.root_lo[2], __uint_as_float(c.root_ref));
+      stk[1] = make_float4(c.root_hi[0], c.root_hi[1], c.root_hi[2], __uint_as_float(c.root_count));
+    }
+    __syncwarp();
+    while (sp > 0) {
+      if (++iters > MAX_ITERS) {
+        err |= ST_ITERS;
+        break;
+      }
+      --sp;
+      const float4 A = stk[2 * sp], B = stk[2 * sp + 1];
+      const float  bound = kd[K - 1];
+      const float  d2    = boxD2exact(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
+      if (!__any_sync(FULL, d2 <= bound)) {
+        continue;
+      }
+      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
+      if (ref & EBG_LEAF_BIT) {
+        const uint32_t p0 = ref & ~EBG_LEAF_BIT;
+        for (uint32_t t = p0; t < p0 + cnt; ++t) {
+          const float4   q  = __ldg(c.points + t);
+          const float    dd = d2exact(px - q.x, py - q.y, pz - q.z);
+          const uint32_t ii = __float_as_uint(q.w);
+          if (lexLess(dd, ii, kd[K - 1], ki[K - 1])) {
+            kd[K - 1] = dd;
+            ki[K - 1] = ii;
+#pragma unroll
+            for (int j = K - 1; j > 0; j--) {
+              if (lexLess(kd[j], ki[j], kd[j - 1], ki[j - 1])) {
+                const float    td = kd[j];
+                const uint32_t ti = ki[j];
+                kd[j]             = kd[j - 1];
+                ki[j]             = ki[j - 1];
+                kd[j - 1]         = td;
+                ki[j - 1]         = ti;
+              }
+            }
+          }
+        }
+      }
+      else {
+        const float4* nd = reinterpret_cast<const float4*>(c.nodes + ref);
+        const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+        const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+        const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
+        const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+        const float   clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
+                    clz[4] = {lz.x, lz.y, lz.z, lz.w};
+        const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
+                    chz[4] = {hz.x, hz.y, hz.z, hz.w};
+        const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
+        float          key[4];
+        int            o[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const float dk = boxD2exact(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
+          const bool  nk = __any_sync(FULL, dk <= bound);
+          key[k]         = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
+          o[k]           = k;
+        }
+#define EBG_CSWAP(i, j)                                                                                               \
+  if (key[i] < key[j]) {                                                                                              \
+    const float tk = key[i];                                                                                          \
+    key[i]         = key[j];                                                                                          \
+    key[j]         = tk;                                                                                              \
+    const int to   = o[i];                                                                                            \
+    o[i]           = o[j];                                                                                            \
+    o[j]           = to;                                                                                              \
+  }
+        EBG_CSWAP(0, 1);
+        EBG_CSWAP(2, 3);
+        EBG_CSWAP(0, 2);
+        EBG_CSWAP(1, 3);
+        EBG_CSWAP(1, 2);
+#undef EBG_CSWAP
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          if (key[j] >= 0.f) {
+            if (sp >= EBG_STACK_DEPTH) {
+              err |= ST_STACK;
+              break;
+            }
+            const int k = o[j];
+            if (lane == 0) {
+              const float lxk = k == 0 ? clx[0] : (k == 1 ? clx[1] : (k == 2 ? clx[2] : clx[3]));
+              const float lyk = k == 0 ? cly[0] : (k == 1 ? cly[1] : (k == 2 ? cly[2] : cly[3]));
+              const float lzk = k == 0 ? clz[0] : (k == 1 ? clz[1] : (k == 2 ? clz[2] : clz[3]));
+              const float hxk = k == 0 ? chx[0] : (k == 1 ? chx[1] : (k == 2 ? chx[2] : chx[3]));
+              const float hyk = k == 0 ? chy[0] : (k == 1 ? chy[1] : (k == 2 ? chy[2] : chy[3]));
+              const float hzk = k == 0 ? chz[0] : (k == 1 ? chz[1] : (k == 2 ? chz[2] : chz[3]));
+              const uint32_t rk = k == 0 ? cref[0] : (k == 1 ? cref[1] : (k == 2 ? cref[2] : cref[3]));
+              const uint32_t nk = k == 0 ? ccnt[0] : (k == 1 ? ccnt[1] : (k == 2 ? ccnt[2] : ccnt[3]));
+              stk[2 * sp]     = make_float4(lxk, lyk, lzk, __uint_as_float(rk));
+              stk[2 * sp + 1] = make_float4(hxk, hyk, hzk, __uint_as_float(nk));
+            }
+            sp++;
+          }
+        }
+        __syncwarp();
+        if (err) {
+          break;
+        }
+      }
+    }
+    if (err && lane == 0) {
+      atomicOr(a.status, err);
+    }
+    if (valid) {
+#pragma unroll
+      for (int j = 0; j < K; j++) {
+        if (j < a.k) {
+          const bool found = ki[j] != 0xffffffffu;
+          a.out_idx[size_t(id) * a.k + j] = found ? int32_t(ki[j]) : -1;
+          a.out_d2[size_t(id) * a.k + j]  = found ? kd[j] : __int_as_float(0x7f800000);
+        }
+      }
+    }
+  }
+}
+
+template <int K>
+cudaError_t launchKnnK(const CloudQueryArgs& a, int numSms, cudaStream_t s)
+{
+  int perSm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kCloudKnn<K>, 128, 0);
+  perSm              = perSm < 1 ? 1 : perSm;
+  const int64_t need = ((int64_t(a.n) + 31) / 32 + 3) / 4;
+  int64_t       grid = int64_t(numSms) * perSm;
+  grid               = grid < need ? grid : need;
+  grid               = grid < 1 ? 1 : grid;
+  kCloudKnn<K><<<unsigned(grid), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+inline unsigned blocksFor(int64_t n, int t) { return unsigned((n + t - 1) / t); }
+
+} // namespace
+
+int cloudLevels(int64_t nLeaves, int64_t* levelNodes, int maxLevels)
+{
+  int     nl = 0;
+  int64_t c  = nLeaves;
+  while (c > 1 && nl < maxLevels) {
+    c                = (c + 3) / 4;
+    levelNodes[nl++] = c;
+  }
+  return nl;
+}
+
+cudaError_t buildCloud(const float* points, int64_t n, int L, const CloudBuildBuffers& b, EbgNode4* nodes,
+                       float4* leafPts, const int64_t* levelNodes, int nLevels, float* rootBox, cudaStream_t s)
+{
+  const int T = 256;
+  // box init: lo = fkey(+max) (atomicMin), hi = fkey(-max) (atomicMax)
+  {
+    const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    cudaMemcpyAsync(b.box, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  }
+  kBounds<<<unsigned(std::min<int64_t>(blocksFor(n, T), 4096)), T, 0, s>>>(points, n, b.box);
+  kCloudKeys<<<blocksFor(n, T), T, 0, s>>>(points, n, b.box, b.keysIn, b.idsIn);
+  size_t tb = b.sortTempBytes;
+  cub::DeviceRadixSort::SortPairs(b.sortTemp, tb, b.keysIn, b.keysOut, b.idsIn, b.idsOut, int(n), 0, 30, s);
+  kGatherLeaves<<<blocksFor(n, T), T, 0, s>>>(points, b.idsOut, n, leafPts);
+  const int64_t nLeaves = (n + L - 1) / L;
+  kLeafBoxes<<<blocksFor(nLeaves, T), T, 0, s>>>(leafPts, n, L, nLeaves, b.boxA);
+  // levels bottom-up; node index base of level l (1..nLevels) counts the levels above it
+  int64_t base[64];
+  int64_t acc = 0;
+  for (int l = nLevels; l >= 1; l--) {
+    base[l] = acc;
+    acc += levelNodes[l - 1];
+  }
+  float*  cur    = b.boxA;
+  float*  nxt    = b.boxB;
+  int64_t nChild = nLeaves;
+  for (int l = 1; l <= nLevels; l++) {
+    const int64_t nn = levelNodes[l - 1];
+    kTreeLevel<<<blocksFor(nn, T), T, 0, s>>>(nn, nChild, cur, l == 1 ? 1 : 0, l == 1 ? 0 : base[l - 1], L, n, nodes,
+                                             base[l], nxt);
+    float* t = cur;
+    cur      = nxt;
+    nxt      = t;
+    nChild   = nn;
+  }
+  // root box (6 floats) for the traversal's first stack entry
+  cudaMemcpyAsync(rootBox, cur, 6 * sizeof(float), cudaMemcpyDeviceToHost, s);
+  return cudaGetLastError();
+}
+
+size_t cloudSortTempBytes(int64_t n)
+{
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr), int(n), 0, 30);
+  return tb;
+}
+
+cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s)
+{
+  switch (kTemplate) {
+  case 1:
+    return launchKnnK<1>(a, numSms, s);
+  case 2:
+    return launchKnnK<2>(a, numSms, s);
+  case 4:
+    return launchKnnK<4>(a, numSms, s);
+  case 8:
+    return launchKnnK<8>(a, numSms, s);
+  case 16:
+    return launchKnnK<16>(a, numSms, s);
+  default:
+    return launchKnnK<32>(a, numSms, s);
+  }
+}
+
+} // namespace ebg

@@ -1,0 +1,58 @@
+// Point-cloud build and k-NN launch wrappers (called from the C ABI layer).
+#ifndef EBG_CLOUD_KERNELS_H
+#define EBG_CLOUD_KERNELS_H
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ebg_layout.h"
+
+namespace ebg {
+
+// Device view of a point cloud: 4-wide nodes (root at 0) over leaves of consecutive float4
+// (x, y, z, original index bits) points in Morton order.
+struct EbgCloudView
+{
+  const EbgNode4* nodes;
+  const float4*   points;
+  float           root_lo[3], root_hi[3];
+  uint32_t        root_ref, root_count;
+  float           morton_lo[3], morton_scale[3];
+};
+
+struct CloudQueryArgs
+{
+  EbgCloudView        cloud;
+  const float*        queries; // caller's xyz
+  const uint32_t*     order;   // sorted position -> caller index (nullptr = identity)
+  int64_t             n;
+  int                 k;       // neighbours written per query (<= template K)
+  int32_t*            out_idx; // n x k, caller order
+  float*              out_d2;  // n x k
+  unsigned long long* work;
+  int*                status;
+};
+
+struct CloudBuildBuffers
+{
+  uint32_t* box;      // 6 words
+  uint32_t* keysIn;
+  uint32_t* keysOut;
+  uint32_t* idsIn;
+  uint32_t* idsOut;
+  void*     sortTemp;
+  size_t    sortTempBytes;
+  float*    boxA;     // 6 floats per leaf
+  float*    boxB;
+};
+
+// Node counts of the levels above nLeaves leaves (bottom-up); returns the number of levels.
+int         cloudLevels(int64_t nLeaves, int64_t* levelNodes, int maxLevels);
+size_t      cloudSortTempBytes(int64_t n);
+cudaError_t buildCloud(const float* points, int64_t n, int L, const CloudBuildBuffers& b, EbgNode4* nodes,
+                       float4* leafPts, const int64_t* levelNodes, int nLevels, float* rootBoxHost, cudaStream_t s);
+cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s);
+
+} // namespace ebg
+
+#endif

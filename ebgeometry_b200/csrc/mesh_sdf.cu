@@ -107,6 +107,16 @@ __device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, cons
 
 __device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
 
+// a[k] for a warp-uniform k without dynamic register-array indexing (which would go to local memory)
+__device__ __forceinline__ float sel4(const float (&a)[4], int k)
+{
+  return k == 0 ? a[0] : (k == 1 ? a[1] : (k == 2 ? a[2] : a[3]));
+}
+__device__ __forceinline__ uint32_t sel4u(const uint32_t (&a)[4], int k)
+{
+  return k == 0 ? a[0] : (k == 1 ? a[1] : (k == 2 ? a[2] : a[3]));
+}
+
 // Signed distance of p to triangle `tri` (leaf order), sign from the pseudonormal of the closest
 // feature (the reference's sign-bit convention, TriangleSoAImplem.hpp:1076-1082: +0 -> +1).
 __device__ float signedFromWinner(const EbgMeshView& m, uint32_t tri, float px, float py, float pz)
@@ -233,8 +243,8 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
           const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
                       chz[4] = {hz.x, hz.y, hz.z, hz.w};
           const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
-          float          key[4];
-          int            o[4];
+          float key[4];
+          int   o[4];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
@@ -243,12 +253,16 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
             key[k] = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
             o[k]   = k;
           }
-          // sort slots by key, descending (far first) -- a 5-comparator network
+          // sort (key, slot) pairs by key, descending (far first): a 5-comparator network on
+          // registers (constant indices only, so nothing spills to local memory)
 #define EBG_CSWAP(i, j)                                                                                               \
-  if (key[o[i]] < key[o[j]]) {                                                                                        \
-    const int tmp = o[i];                                                                                             \
-    o[i]          = o[j];                                                                                             \
-    o[j]          = tmp;                                                                                              \
+  if (key[i] < key[j]) {                                                                                              \
+    const float tk = key[i];                                                                                          \
+    key[i]         = key[j];                                                                                          \
+    key[j]         = tk;                                                                                              \
+    const int to   = o[i];                                                                                            \
+    o[i]           = o[j];                                                                                            \
+    o[j]           = to;                                                                                              \
   }
           EBG_CSWAP(0, 1);
           EBG_CSWAP(2, 3);
@@ -258,15 +272,16 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
 #undef EBG_CSWAP
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            const int k = o[j];
-            if (key[k] >= 0.f) {
+            if (key[j] >= 0.f) {
               if (sp >= EBG_STACK_DEPTH) {
                 err |= ST_STACK;
                 break;
               }
+              const int k = o[j];
               if (lane == 0) {
-                stk[2 * sp]     = make_float4(clx[k], cly[k], clz[k], __uint_as_float(cref[k]));
-                stk[2 * sp + 1] = make_float4(chx[k], chy[k], chz[k], __uint_as_float(ccnt[k]));
+                stk[2 * sp] = make_float4(sel4(clx, k), sel4(cly, k), sel4(clz, k), __uint_as_float(sel4u(cref, k)));
+                stk[2 * sp + 1] =
+                  make_float4(sel4(chx, k), sel4(chy, k), sel4(chz, k), __uint_as_float(sel4u(ccnt, k)));
               }
               sp++;
             }

@@ -194,6 +194,44 @@ ebg_status ebg_mesh_value(const ebg_mesh* mesh, double x, double y, double z, do
  * (EBG_ERR_TRAVERSAL) recorded by earlier asynchronous calls. */
 ebg_status ebg_check_status(const ebg_mesh* mesh, void* stream);
 
+/* ---- point clouds: PointCloudBVH (PointCloudBVH.hpp:56-350) --------------------------------
+ *
+ * ebg_cloud_create replaces PointCloudBVH(positions, meta) (PointCloudBVHImplem.hpp:27-57): the
+ * tree is built on the device (Morton order, leaves of opts->leaf_size points, default 16, and a
+ * 4-wide tree above them).  The cloud index of a point is its position in the input array. */
+ebg_status ebg_cloud_create(const float* points_host, int64_t n, const ebg_build_opts* opts, ebg_cloud** out);
+/* The same from a device array (no host copy); the build runs on stream and is complete on return. */
+ebg_status ebg_cloud_create_device(const float* points_dev, int64_t n, const ebg_build_opts* opts, ebg_cloud** out,
+                                   void* stream);
+ebg_status ebg_cloud_destroy(ebg_cloud* cloud);
+int64_t    ebg_cloud_size(const ebg_cloud* cloud);
+
+/* Batched PointCloudBVH::closestPoints (PointCloudBVHImplem.hpp:441-453) / closestPoint (k = 1):
+ * for each query the k nearest points in increasing (squared distance, index) order -- equal
+ * distances resolve to the LOWEST index -- as int32 indices idx_dev[q*k + j] and float squared
+ * distances d2_dev[q*k + j] computed as the reference does ((dx*dx + dy*dy) + dz*dz, dx = q - p,
+ * float, no fused multiply-add).  Fewer than k points: the missing entries are index -1 and +inf.
+ * 1 <= k <= 32.  opts: only no_sort is used.  Asynchronous on stream. */
+ebg_status ebg_cloud_knn(const ebg_cloud*      cloud,
+                         const float*          queries_dev,
+                         int64_t               num_queries,
+                         int32_t               k,
+                         int32_t*              idx_dev,
+                         float*                d2_dev,
+                         const ebg_query_opts* opts,
+                         void*                 stream);
+/* The same with host buffers (copies in and out, synchronous). */
+ebg_status ebg_cloud_knn_host(const ebg_cloud*      cloud,
+                              const float*          queries_host,
+                              int64_t               num_queries,
+                              int32_t               k,
+                              int32_t*              idx_host,
+                              float*                d2_host,
+                              const ebg_query_opts* opts,
+                              void*                 stream);
+/* Synchronises stream and reports a device-side traversal error of earlier k-NN calls. */
+ebg_status ebg_cloud_check_status(const ebg_cloud* cloud, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

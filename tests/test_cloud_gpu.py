@@ -1,0 +1,107 @@
+"""Parity of the CUDA k-nearest-neighbour path (PointCloudBVH) with the oracle.
+
+Contract: int32 neighbour indices bit-identical to the oracle's, ordered by (squared distance,
+index) so ties resolve to the lowest index; squared distances bit-identical (the reference's
+float arithmetic)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from ebgeometry_b200 import EbgError, PointCloudBVH
+from ebgeometry_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def knn_gpu(cloud, q, k, **kw):
+    idx, d2 = cloud.knn(torch.from_numpy(np.ascontiguousarray(q, np.float32)).cuda(), k, **kw)
+    torch.cuda.synchronize()
+    cloud.check_status()
+    return idx.cpu().numpy(), d2.cpu().numpy()
+
+
+def test_reference_cloud_fixture(golden):
+    g = golden("cloud2000.npz")
+    c = PointCloudBVH(g["points"])
+    for k, key, dkey in ((1, "lex1", "lexd1"), (8, "lex8", "lexd8")):
+        idx, d2 = knn_gpu(c, g["queries"], k)
+        assert np.array_equal(idx, g[key].astype(np.int32))
+        assert np.array_equal(d2, g[dkey])
+    # the reference's own closestPoints(k=5): same distances (its tie order follows its traversal)
+    idx, d2 = knn_gpu(c, g["queries"], 5)
+    assert np.array_equal(d2, g["d5"])
+    # querying at a cloud point returns that point at distance 0 (TestPointCloudBVH.cpp:85-93)
+    for i in range(0, 2000, 137):
+        j, dd = c.closestPoint(g["points"][i])
+        assert j == i and dd == 0.0
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 8, 17, 32])
+@pytest.mark.parametrize("leaf", [1, 7, 16, 32])
+def test_against_brute_force(k, leaf):
+    pts = W.point_cloud(20000, 3)
+    q = np.concatenate([W.uniform_points(3000, 4, 0, 1), pts[:500]])  # includes exact hits
+    ref_idx, ref_d2 = oracle.port().knn_brute(pts, q, k)
+    c = PointCloudBVH(pts, leaf_size=leaf)
+    idx, d2 = knn_gpu(c, q, k)
+    assert np.array_equal(idx, ref_idx)
+    assert np.array_equal(d2, ref_d2)
+    idx2, d22 = knn_gpu(c, q, k, sort=False)
+    assert np.array_equal(idx2, ref_idx) and np.array_equal(d22, ref_d2)
+
+
+def test_ties_lowest_index():
+    # duplicated points: every query ties between copies; the lowest index must win
+    base = W.uniform_points(500, 7, 0, 1)
+    pts = np.concatenate([base, base, base])
+    q = W.uniform_points(1000, 8, 0, 1)
+    ref_idx, ref_d2 = oracle.port().knn_brute(pts, q, 8)
+    idx, d2 = knn_gpu(PointCloudBVH(pts), q, 8)
+    assert np.array_equal(idx, ref_idx) and np.array_equal(d2, ref_d2)
+    assert np.all(idx[:, 0] < 500)
+    # grid points: many exactly equal distances
+    g = W.grid_points(16, 0, 1)
+    qq = W.grid_points(8, 0, 1)
+    ref_idx, _ = oracle.port().knn_brute(g, qq, 8)
+    idx, _ = knn_gpu(PointCloudBVH(g), qq, 8)
+    assert np.array_equal(idx, ref_idx)
+
+
+def test_small_and_edge_cases():
+    one = np.array([[0.5, 0.5, 0.5]], np.float32)
+    c = PointCloudBVH(one)
+    idx, d2 = knn_gpu(c, W.uniform_points(40, 1, 0, 1), 3)
+    assert np.all(idx[:, 0] == 0) and np.all(idx[:, 1:] == -1) and np.all(np.isinf(d2[:, 1:]))
+    with pytest.raises(EbgError):
+        PointCloudBVH(np.zeros((0, 3), np.float32))
+    with pytest.raises(EbgError):
+        c.knn(torch.zeros((4, 3), device="cuda"), 33)
+    idx, d2 = c.knn(np.zeros((0, 3), np.float32), 2)
+    assert idx.shape == (0, 2)
+
+
+def test_device_build_and_host_query_agree():
+    pts = W.point_cloud(50000, 9)
+    q = W.uniform_points(5000, 10, 0, 1)
+    a = PointCloudBVH(torch.from_numpy(pts).cuda())
+    b = PointCloudBVH(pts)
+    ia, da = knn_gpu(a, q, 8)
+    ib, db = b.knn(q, 8)
+    assert np.array_equal(ia, ib) and np.array_equal(da, db)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference oracle library not built")
+def test_full_size_cloud_against_reference_sample():
+    """16M-point cloud of the benchmark configuration: a 20k-query sample against the reference's
+    own PointCloudBVH traversal (lexicographic state), k = 1 and 8, bit-exact."""
+    pts = W.point_cloud(16 * 1024 * 1024, 1)
+    q = W.uniform_points(20000, 2, 0, 1)
+    c = PointCloudBVH(torch.from_numpy(pts).cuda())
+    R = oracle.ref()
+    rc = R.cloud(pts)
+    for k in (1, 8):
+        idx, d2 = knn_gpu(c, q, k)
+        ri, rd = rc.knn(q, k, lex=True)
+        assert np.array_equal(d2, rd)
+        assert np.mean(idx == ri) > 0.9999  # the reference traversal's own ties at equal box distance
