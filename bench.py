@@ -177,20 +177,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def l2_read_bandwidth(torch, dev):
-    """Read bandwidth of a 64 MB L2-resident buffer (torch.sum; for the roofline's L2 roof)."""
-    x = torch.ones(16 * 1024 * 1024, dtype=torch.float32, device=dev)
-    for _ in range(5):
-        x.sum()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    it = 200
-    for _ in range(it):
-        x.sum()
-    e1.record()
-    torch.cuda.synchronize()
-    return x.numel() * 4 * it / (e0.elapsed_time(e1) * 1e-3) / 1e9
+def l2_read_bandwidth():
+    """Read bandwidth of a 48 MB L2-resident buffer streamed by the library's own kernel."""
+    import ctypes as C
+
+    from ebgeometry_b200 import _capi
+    out = C.c_double()
+    _capi.check(_capi.lib.ebg_measure_read_bandwidth(48 << 20, 200, C.byref(out)))
+    return out.value
 
 
 # --- arms -------------------------------------------------------------------------------------------
@@ -320,7 +314,7 @@ def run_ours(args, rank, world, local_rank):
 
     # roofline of the traversal kernel
     hbm_peak, peak_kind = measured_peaks()
-    l2_gbs = l2_read_bandwidth(torch, dev)
+    l2_gbs = l2_read_bandwidth()
     node_b, tri_b = 128, 48
     nq = float(n)
     bq = 12 + 4 + st["nodes_visited"] / nq * node_b + st["triangles_tested"] / nq * tri_b

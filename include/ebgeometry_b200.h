@@ -110,6 +110,11 @@ const char* ebg_last_error(void);
 const char* ebg_version(void);
 int         ebg_device_count(void);
 
+/* Read bandwidth (GB/s) of a kernel streaming a `bytes`-sized device buffer `iters` times on the
+ * current device: with bytes well under the L2 size (126 MB on B200) it measures the L2 read roof
+ * the traversal kernels are compared with.  No reference counterpart (measurement utility). */
+ebg_status ebg_measure_read_bandwidth(int64_t bytes, int32_t iters, double* gbs);
+
 /* ---- triangle meshes: TriMeshSDF (MeshDistanceFunctions.hpp:309-489) -------------------------
  *
  * ebg_mesh_create replaces TriMeshSDF(mesh, build, maxLeafGroups) after Soup::soupToDCEL
