@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-seed", action="store_true", help="time the plain traversal only")
+    ap.add_argument("--seed-samples", type=int, default=1 << 25)
+    ap.add_argument("--seed-steps", type=int, default=2000)
+    ap.add_argument("--seed-batch", type=int, default=1 << 18)
     return ap.parse_args()
 
 
@@ -183,7 +187,7 @@ def l2_read_bandwidth():
 
     from ebgeometry_b200 import _capi
     out = C.c_double()
-    _capi.check(_capi.lib.ebg_measure_read_bandwidth(48 << 20, 200, C.byref(out)))
+    _capi.check(_capi.lib.ebg_measure_read_bandwidth(48 << 20, 20, C.byref(out)))
     return out.value
 
 
@@ -225,11 +229,41 @@ def run_reference(args, rank, world):
     return 0
 
 
+def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, dist, local_rank):
+    """K steps bracketed by barrier + synchronize, CUDA events on the launching stream, clocks
+    sampled meanwhile; per-phase events recorded inside each call.  Returns (ms/step max over
+    ranks, phase array, clocks)."""
+    clocks = Clocks(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    tms = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        tm = _capi.PhaseTimings()
+        mesh.signed_distance(pd, out=out, timings=tm, seed=seed)
+        tms.append((tm.order_ms, tm.traverse_ms, tm.band_ms, tm.total_ms))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    mesh.check_status()
+    return ms / steps, np.array(tms), ck
+
+
 def run_ours(args, rank, world, local_rank):
+    import ctypes as C
+
     import torch
     import torch.distributed as dist
 
-    from ebgeometry_b200 import TriMeshSDF, _capi
+    from ebgeometry_b200 import SeedModel, TriMeshSDF, _capi
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -244,47 +278,48 @@ def run_ours(args, rank, world, local_rank):
     pd = torch.from_numpy(pts).to(dev)
     out = torch.empty(n, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    tsteps = (mesh, pd, out, args.steps)
+    tctx = (dev, world, stream, _capi, torch, dist, local_rank)
 
-    # traversal counters (untimed): per-query visits of the plain traversal, for the roofline
+    # plain traversal: counters (untimed; the roofline's per-query work unit), warm-up, timed steps
     _, st = mesh.stats(pd)
-    log(f"[rank {rank}] stats {st}")
-
+    log(f"[rank {rank}] plain stats {st}")
     for _ in range(args.warmup):
         mesh.signed_distance(pd, out=out)
     torch.cuda.synchronize(dev)
-    mesh.check_status()
+    ms_plain, tms_plain, ck_plain = timed_steps(*tsteps, None, *tctx)
+    plain_ref = out.clone() if not args.no_seed else None
+    log(f"[rank {rank}] plain {ms_plain:.1f} ms/step")
 
-    clocks = Clocks(local_rank)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    clocks.start()
-    tms = []
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        tm = _capi.PhaseTimings()
-        mesh.signed_distance(pd, out=out, timings=tm)
-        tms.append((tm.order_ms, tm.traverse_ms, tm.band_ms, tm.total_ms))
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    mesh.check_status()
-    ms_step = ms / args.steps
+    seed, rep, st_seed = None, None, None
+    if not args.no_seed:
+        t0 = time.time()
+        seed = SeedModel.train(mesh, num_samples=args.seed_samples, steps=args.seed_steps, batch=args.seed_batch,
+                               rng_seed=7, lo=[-1.25] * 3, hi=[1.25] * 3)
+        rep = seed.report()
+        rep["wall_s"] = time.time() - t0
+        log(f"[rank {rank}] seed trained: {rep}")
+        _, st_seed = mesh.stats(pd, seed=seed)
+        log(f"[rank {rank}] seeded stats {st_seed}")
+        for _ in range(args.warmup):
+            mesh.signed_distance(pd, out=out, seed=seed)
+        torch.cuda.synchronize(dev)
+        ms_seed, tms_seed, ck_seed = timed_steps(*tsteps, seed, *tctx)
+        log(f"[rank {rank}] seeded {ms_seed:.1f} ms/step")
+        diff = (out - plain_ref).abs()
+        same_frac = float((out == plain_ref).float().mean().item())
+        max_diff = float(diff.max().item())
+    ms_step, tms, ck = (ms_seed, tms_seed, ck_seed) if seed is not None else (ms_plain, tms_plain, ck_plain)
     value = n * world / (ms_step * 1e-3)
-    tms = np.array(tms)
+    plain_value = n * world / (ms_plain * 1e-3)
 
     # end to end through the host entry point: pinned input, H2D + query + D2H every step
     e2e_steps = args.e2e_steps or max(2, min(args.steps, 3))
     ph = torch.from_numpy(pts).pin_memory()
     oh = torch.empty(n, dtype=torch.float32).pin_memory()
-    import ctypes as C
     opts = _capi.QueryOpts()
+    if seed is not None:
+        opts.seed = seed.handle
 
     def host_call():
         _capi.check(_capi.lib.ebg_mesh_signed_distance_host(
@@ -306,13 +341,13 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    # the host path must give the device path's numbers
     same = bool(torch.equal(oh, out.cpu()))
 
     if rank != 0:
         return 0
 
-    # roofline of the traversal kernel
+    # roofline of the traversal kernel: per-query algorithmic bytes of the PLAIN traversal (the
+    # equal work unit for both runs) over the traversal phase's event-timed duration
     hbm_peak, peak_kind = measured_peaks()
     l2_gbs = l2_read_bandwidth()
     node_b, tri_b = 128, 48
@@ -325,8 +360,7 @@ def run_ours(args, rank, world, local_rank):
     if os.path.exists(tpath):
         with open(tpath) as fh:
             tj = json.load(fh)
-        key = f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}"
-        traffic = tj.get(key)
+        traffic = tj.get(f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}")
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -350,6 +384,14 @@ def run_ours(args, rank, world, local_rank):
                                         "sign_mismatch_outside_band": int(np.sum(np.sign(d_gpu[bandm]) !=
                                                                                  np.sign(d_ref[bandm])))}}
 
+    def per_query(s):
+        return None if s is None else {"nodes": s["nodes_visited"] / nq, "leaves": s["leaves_visited"] / nq,
+                                       "triangles": s["triangles_tested"] / nq,
+                                       "band_fraction": s["band_queries"] / nq,
+                                       "seed_fallback_fraction": s["seed_fallbacks"] / nq}
+
+    phases = lambda t: {"order": float(t[:, 0].mean()), "traverse": float(t[:, 1].mean()),
+                        "band64": float(t[:, 2].mean()), "total": float(t[:, 3].mean())}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -358,21 +400,27 @@ def run_ours(args, rank, world, local_rank):
                                f"{args.build} 4-wide BVH, leaf {args.leaf}), {args.grid}^3 grid over [-1.25,1.25]^3 "
                                f"+ {n_band} points within 1e-3 of the surface = {n} queries/step; FP32 traversal, "
                                f"FP64 band |d| <= 1e-4 diag",
-                   "seed": "none (plain traversal)", "queries_per_step": n, "l2": "inputs larger than L2 "
+                   "seed": ("learned pruning radius (16-level hash grid + 3x64 BF16 MLP, trained on the GPU)"
+                            if seed is not None else "none (plain traversal)"),
+                   "queries_per_step": n, "l2": "inputs larger than L2 "
                    f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
-                   "phase_ms_mean": {"order": float(tms[:, 0].mean()), "traverse": trav_ms,
-                                     "band64": float(tms[:, 2].mean()), "total": float(tms[:, 3].mean())},
-                   "per_query": {"nodes": st["nodes_visited"] / nq, "leaves": st["leaves_visited"] / nq,
-                                 "triangles": st["triangles_tested"] / nq, "band_fraction": st["band_queries"] / nq}},
+                   "plain": {"value": plain_value, "ms_per_step": ms_plain, "phase_ms_mean": phases(tms_plain),
+                             "per_query": per_query(st), "clocks": ck_plain},
+                   "seeded": None if seed is None else {
+                       "value": value, "ms_per_step": ms_seed, "speedup_vs_plain": value / plain_value,
+                       "phase_ms_mean": phases(tms_seed), "per_query": per_query(st_seed),
+                       "equal_to_plain_fraction": same_frac, "max_abs_diff_vs_plain": max_diff,
+                       "training": rep}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "kMeshSdf32 (FP32 packet traversal)",
-                     "bytes_per_query": bq, "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
+                     "kernel": "kMeshSdf32 (FP32 packet traversal" + (", seeded)" if seed is not None else ")"),
+                     "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit)",
+                     "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
         "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                 "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},
-        "gpu_launches": 3 * args.steps,
-        "gpu_launches_note": "per step: Morton-key kernel, FP32 traversal, FP64 band pass (plus the CUB radix-sort "
-                             "passes of the point ordering)",
+        "gpu_launches": (4 if seed is not None else 3) * args.steps,
+        "gpu_launches_note": "per step: Morton-key kernel, " + ("seed inference, " if seed is not None else "") +
+                             "FP32 traversal, FP64 band pass (plus the CUB radix-sort passes of the point ordering)",
         "clocks": ck,
         "cpu_baseline": cpu,
     }

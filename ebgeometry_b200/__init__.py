@@ -21,7 +21,7 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["TriMeshSDF", "PointCloudBVH", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
+__all__ = ["TriMeshSDF", "PointCloudBVH", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
 BUILD_MORTON = 1
@@ -103,8 +103,9 @@ class TriMeshSDF:
         return fn, vn, en
 
     @staticmethod
-    def _opts(band, sort, fp64_band, warps_per_block, timings=None):
-        return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1, None,
+    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None):
+        return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
+                               seed.handle if seed is not None else None,
                                int(warps_per_block or 0), 0,
                                C.pointer(timings) if timings is not None else None)
 
@@ -120,12 +121,13 @@ class TriMeshSDF:
 
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
-                        fp64_band=True, warps_per_block=None, stream=None, timings=None):
+                        fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
-        times (the call then synchronises)."""
-        opts = self._opts(band, sort, fp64_band, warps_per_block, timings)
+        times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
+        radius seeds the traversal's pruning bound (results stay exact)."""
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed)
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
             n = p.shape[0]
@@ -147,13 +149,13 @@ class TriMeshSDF:
                                            C.byref(opts), _stream_ptr(stream)))
         return (d, closest_tri) if closest_tri is not None else d
 
-    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None):
+    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None, seed=None):
         """Traversal counters summed over the points (synchronous; CUDA tensor input)."""
         import torch
         n = points.numel() // 3
         d = torch.empty(n, dtype=torch.float32, device=points.device)
         st = _capi.QueryStats()
-        opts = self._opts(band, sort, fp64_band, None)
+        opts = self._opts(band, sort, fp64_band, None, None, seed)
         check(lib.ebg_mesh_signed_distance_stats(self._h, C.c_void_p(points.data_ptr()), n,
                                                  C.c_void_p(d.data_ptr()), C.byref(opts),
                                                  C.byref(st), _stream_ptr(stream)))
@@ -230,3 +232,100 @@ class PointCloudBVH:
 
     def check_status(self, stream=None):
         check(lib.ebg_cloud_check_status(self._h, _stream_ptr(stream)))
+
+
+class SeedModel:
+    """Learned pruning radius for :class:`TriMeshSDF` queries (no counterpart in the reference).
+
+    A 16-level hash-grid encoding with a 3-layer, 64-wide BF16 ReLU MLP, trained on the GPU by the
+    library's own kernels on exact signed distances the mesh path generates.  Use
+    ``mesh.signed_distance(points, seed=model)``.
+    """
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @staticmethod
+    def _opts(**kw):
+        o = _capi.SeedOpts()
+        for k, v in kw.items():
+            if k in ("lo", "hi"):
+                getattr(o, k)[:] = [float(x) for x in v]
+            elif v is not None:
+                setattr(o, k, v)
+        return o
+
+    @classmethod
+    def train(cls, mesh, stream=None, **kw):
+        """Trains on ``mesh`` (see ebg_seed_opts for the keyword options)."""
+        o = cls._opts(**kw)
+        h = C.c_void_p()
+        rep = _capi.SeedReport()
+        check(lib.ebg_seed_train(mesh.handle, C.byref(o), C.byref(h), C.byref(rep),
+                                 _stream_ptr(stream) if stream is not None else None))
+        return cls(h)
+
+    @classmethod
+    def create(cls, **kw):
+        """Untrained model (random parameters) over the domain lo..hi."""
+        o = cls._opts(**kw)
+        h = C.c_void_p()
+        check(lib.ebg_seed_create(C.byref(o), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, path, device=-1):
+        h = C.c_void_p()
+        check(lib.ebg_seed_load(str(path).encode(), int(device), C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_seed_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def report(self):
+        r = _capi.SeedReport()
+        check(lib.ebg_seed_get_report(self._h, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in _capi.SeedReport._fields_}
+
+    def save(self, path):
+        check(lib.ebg_seed_save(self._h, str(path).encode()))
+
+    def predict(self, points, stream=None):
+        """Raw predicted signed distance at (n,3) float32 CUDA points."""
+        import torch
+        n = points.numel() // 3
+        out = torch.empty(n, dtype=torch.float32, device=points.device)
+        check(lib.ebg_seed_predict(self._h, C.c_void_p(points.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                   _stream_ptr(stream)))
+        return out
+
+    def get_params(self, table_size):
+        table = np.empty(table_size, np.float32)
+        params = np.empty(10497, np.float32)
+        check(lib.ebg_seed_get_params(self._h, _ptr(table), _ptr(params)))
+        return table, params
+
+    def set_params(self, table=None, params=None):
+        t = np.ascontiguousarray(table, np.float32) if table is not None else None
+        p = np.ascontiguousarray(params, np.float32) if params is not None else None
+        check(lib.ebg_seed_set_params(self._h, _ptr(t) if t is not None else None,
+                                      _ptr(p) if p is not None else None))
+
+    def gradients(self, points, targets, eps, table_size):
+        """(loss, grad_table, grad_params) of one batch, parameters unchanged."""
+        import torch
+        pt = torch.from_numpy(np.ascontiguousarray(points, np.float32)).cuda()
+        tt = torch.from_numpy(np.ascontiguousarray(targets, np.float32)).cuda()
+        loss = C.c_float()
+        gt = np.empty(table_size, np.float32)
+        gp = np.empty(10497, np.float32)
+        check(lib.ebg_seed_gradients(self._h, C.c_void_p(pt.data_ptr()), C.c_void_p(tt.data_ptr()),
+                                     pt.shape[0], float(eps), C.byref(loss), _ptr(gt), _ptr(gp)))
+        return loss.value, gt, gp

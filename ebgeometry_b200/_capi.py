@@ -28,6 +28,20 @@ class QueryOpts(C.Structure):
                 ("timings", C.POINTER(PhaseTimings))]
 
 
+class SeedOpts(C.Structure):
+    _fields_ = [("num_samples", C.c_int64), ("steps", C.c_int32), ("batch", C.c_int32),
+                ("log2_table", C.c_int32), ("base_resolution", C.c_int32), ("max_resolution", C.c_int32),
+                ("learning_rate", C.c_float), ("surface_band", C.c_float), ("coverage", C.c_float),
+                ("rng_seed", C.c_uint64), ("lo", C.c_double * 3), ("hi", C.c_double * 3)]
+
+
+class SeedReport(C.Structure):
+    _fields_ = [("train_seconds", C.c_float), ("final_loss", C.c_float), ("alpha", C.c_float),
+                ("beta", C.c_float), ("coverage", C.c_float), ("mean_abs_err", C.c_float),
+                ("far_tau", C.c_float), ("max_abs_err_far", C.c_float),
+                ("validation_samples", C.c_int64), ("train_samples", C.c_int64)]
+
+
 class MeshInfo(C.Structure):
     _fields_ = [("num_triangles", C.c_int64), ("num_vertices", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_leaves", C.c_int64), ("depth", C.c_int32),
@@ -76,6 +90,16 @@ SIGNATURES = {
     "ebg_cloud_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_check_status": (C.c_int, [_P, _P]),
+    "ebg_seed_create": (C.c_int, [C.POINTER(SeedOpts), C.POINTER(_P)]),
+    "ebg_seed_train": (C.c_int, [_P, C.POINTER(SeedOpts), C.POINTER(_P), C.POINTER(SeedReport), _P]),
+    "ebg_seed_destroy": (C.c_int, [_P]),
+    "ebg_seed_get_report": (C.c_int, [_P, C.POINTER(SeedReport)]),
+    "ebg_seed_predict": (C.c_int, [_P, _P, _I64, _P, _P]),
+    "ebg_seed_save": (C.c_int, [_P, C.c_char_p]),
+    "ebg_seed_load": (C.c_int, [C.c_char_p, _I32, C.POINTER(_P)]),
+    "ebg_seed_get_params": (C.c_int, [_P, _P, _P]),
+    "ebg_seed_set_params": (C.c_int, [_P, _P, _P]),
+    "ebg_seed_gradients": (C.c_int, [_P, _P, _P, _I32, C.c_float, C.POINTER(C.c_float), _P, _P]),
 }
 
 

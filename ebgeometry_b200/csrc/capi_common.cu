@@ -22,19 +22,21 @@ namespace {
 
 // Streams float4 loads over a buffer (grid-stride, 4 independent loads in flight per thread) and
 // folds them into one word per block, so the loads cannot be removed.
-__global__ void kReadBandwidth(const float4* __restrict__ buf, int64_t n4, float* __restrict__ sink)
+__global__ void kReadBandwidth(const float4* __restrict__ buf, int64_t n4, int reps, float* __restrict__ sink)
 {
   float         acc  = 0.f;
   const int64_t step = int64_t(gridDim.x) * blockDim.x;
-  int64_t       i    = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (; i + 3 * step < n4; i += 4 * step) {
-    const float4 a = __ldcg(buf + i), b = __ldcg(buf + i + step), c = __ldcg(buf + i + 2 * step),
-                 d = __ldcg(buf + i + 3 * step);
-    acc += (a.x + b.y) + (c.z + d.w);
-  }
-  for (; i < n4; i += step) {
-    const float4 a = __ldcg(buf + i);
-    acc += a.x;
+  for (int r = 0; r < reps; r++) {
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (; i + 3 * step < n4; i += 4 * step) {
+      const float4 a = __ldcg(buf + i), b = __ldcg(buf + i + step), c = __ldcg(buf + i + 2 * step),
+                   d = __ldcg(buf + i + 3 * step);
+      acc += (a.x + b.y) + (c.z + d.w);
+    }
+    for (; i < n4; i += step) {
+      const float4 a = __ldcg(buf + i);
+      acc += a.x;
+    }
   }
   if (acc == 12345.678f) {
     sink[blockIdx.x] = acc;
@@ -68,12 +70,14 @@ ebg_status ebg_measure_read_bandwidth(int64_t bytes, int32_t iters, double* gbs)
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // each launch streams the buffer `reps` times so launch overhead is negligible
+  const int reps = 32;
   for (int w = 0; w < 3; w++) {
-    ebg::kReadBandwidth<<<blocks, 256>>>(buf, n4, sink);
+    ebg::kReadBandwidth<<<blocks, 256>>>(buf, n4, reps, sink);
   }
   cudaEventRecord(e0);
   for (int it = 0; it < iters; it++) {
-    ebg::kReadBandwidth<<<blocks, 256>>>(buf, n4, sink);
+    ebg::kReadBandwidth<<<blocks, 256>>>(buf, n4, reps, sink);
   }
   cudaEventRecord(e1);
   cudaEventSynchronize(e1);
@@ -86,7 +90,7 @@ ebg_status ebg_measure_read_bandwidth(int64_t bytes, int32_t iters, double* gbs)
   if (cudaGetLastError() != cudaSuccess || ms <= 0.f) {
     return ebg::setError(EBG_ERR_CUDA, "bandwidth kernel failed");
   }
-  *gbs = double(n4) * 16.0 * iters / (double(ms) * 1e-3) / 1e9;
+  *gbs = double(n4) * 16.0 * iters * reps / (double(ms) * 1e-3) / 1e9;
   return EBG_OK;
 }
 

@@ -1,0 +1,65 @@
+// Internal handle layouts shared by the C ABI translation units.
+#ifndef EBG_CAPI_INTERNAL_H
+#define EBG_CAPI_INTERNAL_H
+
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "ebg_layout.h"
+#include "ebgeometry_b200.h"
+#include "seed_kernels.h"
+
+struct ebg_mesh
+{
+  int           device = 0;
+  int           numSms = 148;
+  EbgMeshView   view{};
+  ebg_mesh_info info{};
+  // device allocations
+  void* dNodes  = nullptr;
+  void* dHot    = nullptr;
+  void* dSign   = nullptr;
+  void* dTri64  = nullptr;
+  void* dTriId  = nullptr;
+  int*  dStatus = nullptr;
+  // host copies of the pseudonormals (soup order) and the cumulative triangle area (leaf order)
+  std::vector<double> triN, cornerVN, edgeN;
+  std::vector<double> areaCdf;
+};
+
+struct ebg_seed
+{
+  int            device = 0;
+  int            numSms = 148;
+  ebg::SeedView  view{};
+  int64_t        tableSize = 0; // L * T * 2 features
+  float*         tableF32  = nullptr;
+  __nv_bfloat16* tableBf16 = nullptr;
+  float*         tableGrad = nullptr;
+  float*         tableM    = nullptr;
+  float*         tableV    = nullptr;
+  float*         params    = nullptr;
+  float*         paramGrad = nullptr;
+  float*         paramM    = nullptr;
+  float*         paramV    = nullptr;
+  ebg_seed_report report{};
+};
+
+namespace ebg {
+
+// The mesh query pipeline (ordering, optional seed inference, FP32 traversal, FP64 band pass) on
+// device buffers, asynchronous on s.
+ebg_status meshQuery(const ebg_mesh*       m,
+                     const float*          pts,
+                     int64_t               n,
+                     float*                outD,
+                     int32_t*              outTri,
+                     const ebg_query_opts* opts,
+                     unsigned long long*   statsDev,
+                     cudaStream_t          s);
+
+} // namespace ebg
+
+#endif

@@ -11,28 +11,13 @@
 #include <cuda_runtime.h>
 
 #include "capi_common.h"
+#include "capi_internal.h"
 #include "ebgeometry_b200.h"
 #include "mesh_host.h"
 #include "mesh_kernels.h"
+#include "seed_kernels.h"
 
 using namespace ebg;
-
-struct ebg_mesh
-{
-  int           device = 0;
-  int           numSms = 148;
-  EbgMeshView   view{};
-  ebg_mesh_info info{};
-  // device allocations
-  void*         dNodes = nullptr;
-  void*         dHot   = nullptr;
-  void*         dSign  = nullptr;
-  void*         dTri64 = nullptr;
-  void*         dTriId = nullptr;
-  int*          dStatus = nullptr;
-  // host copies of the pseudonormals (soup order)
-  std::vector<double> triN, cornerVN, edgeN;
-};
 
 namespace {
 
@@ -147,6 +132,7 @@ ebg_status buildMesh(const double*         V,
   std::vector<EbgTriSign> sign(N);
   std::vector<double>     tri64(30 * N);
   std::vector<int32_t>    triId(N);
+  m->areaCdf.resize(N);
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < int64_t(N); i++) {
     const int64_t f = bvh.order[i];
@@ -166,6 +152,11 @@ ebg_status buildMesh(const double*         V,
     h.acx = float(ac[0]);
     h.acy = float(ac[1]);
     h.acz = float(ac[2]);
+    {
+      const double cx = ab[1] * ac[2] - ab[2] * ac[1], cy = ab[2] * ac[0] - ab[0] * ac[2],
+                   cz = ab[0] * ac[1] - ab[1] * ac[0];
+      m->areaCdf[i] = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+    }
     h.ab2  = float(ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2]);
     h.abac = float(ab[0] * ac[0] + ab[1] * ac[1] + ab[2] * ac[2]);
     h.ac2  = float(ac[0] * ac[0] + ac[1] * ac[1] + ac[2] * ac[2]);
@@ -191,6 +182,9 @@ ebg_status buildMesh(const double*         V,
     }
   }
 
+  for (size_t i = 1; i < N; i++) {
+    m->areaCdf[i] += m->areaCdf[i - 1];
+  }
   // upload
   auto up = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (cudaMalloc(dst, std::max<size_t>(bytes, 16)) != cudaSuccess) {
@@ -271,14 +265,16 @@ struct Workspace
   }
 };
 
-ebg_status runQuery(const ebg_mesh*       m,
-                    const float*          pts,
-                    int64_t               n,
-                    float*                outD,
-                    int32_t*              outTri,
-                    const ebg_query_opts* opts,
-                    unsigned long long*   statsDev,
-                    cudaStream_t          s)
+} // namespace
+
+ebg_status ebg::meshQuery(const ebg_mesh*       m,
+                          const float*          pts,
+                          int64_t               n,
+                          float*                outD,
+                          int32_t*              outTri,
+                          const ebg_query_opts* opts,
+                          unsigned long long*   statsDev,
+                          cudaStream_t          s)
 {
   if (n > int64_t(INT32_MAX)) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
@@ -287,9 +283,9 @@ ebg_status runQuery(const ebg_mesh*       m,
   const bool band64 = !(opts && opts->no_fp64_band);
   const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block : 4;
   double     band   = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
-  const float* seedR = nullptr;
-  if (opts && opts->seed) {
-    return setError(EBG_ERR_INVALID, "seeded queries go through ebg_seed_signed_distance");
+  const ebg_seed* seed = opts ? opts->seed : nullptr;
+  if (seed && seed->device != m->device) {
+    return setError(EBG_ERR_INVALID, "seed model lives on another device than the mesh");
   }
 
   // optional per-phase events (ev[0] start, [1] after ordering, [2] after traversal, [3] end)
@@ -336,6 +332,15 @@ ebg_status runQuery(const ebg_mesh*       m,
       return setError(EBG_ERR_CUDA, "query sort failed");
     }
   }
+  // learned pruning radius per packet of 32 sorted queries (the traversal widens it per lane by the
+  // distance to the packet centroid, which keeps it an upper bound wherever it holds at the centroid)
+  float* seedR = nullptr;
+  if (seed) {
+    seedR = ws.get<float>((n + 31) / 32);
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "seed workspace allocation failed");
+    }
+  }
   unsigned long long* counters = ws.get<unsigned long long>(2); // [0] packets, [1] band count (u32)
   uint32_t*           bandList = band64 ? ws.get<uint32_t>(n) : nullptr;
   float*              bandD    = band64 ? ws.get<float>(n) : nullptr;
@@ -345,6 +350,9 @@ ebg_status runQuery(const ebg_mesh*       m,
   cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
   if (tm) {
     cudaEventRecord(ev[1], s);
+  }
+  if (seed && launchSeedPackets(seed->view, pts, order, n, seedR, m->numSms, s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, "seed inference launch failed");
   }
 
   MeshQueryArgs a{};
@@ -390,6 +398,8 @@ ebg_status runQuery(const ebg_mesh*       m,
   }
   return EBG_OK;
 }
+
+namespace {
 
 bool checkPoints(const float* p, int64_t n)
 {
@@ -517,7 +527,7 @@ ebg_status ebg_mesh_signed_distance(const ebg_mesh*       m,
   }
   DeviceGuard guard;
   cudaSetDevice(m->device);
-  return runQuery(m, points_dev, n, dist_dev, closest_tri_dev, opts, nullptr, static_cast<cudaStream_t>(stream));
+  return meshQuery(m, points_dev, n, dist_dev, closest_tri_dev, opts, nullptr, static_cast<cudaStream_t>(stream));
 }
 
 ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
@@ -551,7 +561,7 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
       return setError(EBG_ERR_NO_MEMORY, "device buffers for the host call");
     }
     cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s);
-    rc = runQuery(m, dp, n, dd, dt, opts, nullptr, s);
+    rc = meshQuery(m, dp, n, dd, dt, opts, nullptr, s);
     if (rc == EBG_OK) {
       cudaMemcpyAsync(dist_host, dd, n * sizeof(float), cudaMemcpyDeviceToHost, s);
       if (dt) {
@@ -592,7 +602,7 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
       return setError(EBG_ERR_NO_MEMORY, "stats buffer");
     }
     cudaMemsetAsync(dev, 0, 5 * sizeof(unsigned long long), s);
-    rc = runQuery(m, points_dev, n, dist_dev, nullptr, opts, dev, s);
+    rc = meshQuery(m, points_dev, n, dist_dev, nullptr, opts, dev, s);
     if (rc == EBG_OK) {
       cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, s);
     }

@@ -170,8 +170,12 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
     float best    = FLT_MAX;
     int   besttri = -1;
     if (SEEDED) {
-      const float r = __ldg(a.seed_r + src);
-      best          = (r > 0.f && r < 1e18f) ? r * r : FLT_MAX;
+      // packet radius at the centroid, widened by this lane's distance to the centroid (the SDF is
+      // 1-Lipschitz), squared and rounded up so FP32 rounding never makes the bound too tight
+      const float rp = __ldg(a.seed_r + pk);
+      const float ex = px - cx, ey = py - cy, ez = pz - cz;
+      const float r  = rp + sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+      best           = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
     }
     uint32_t iters = 0;
     int      err   = 0;

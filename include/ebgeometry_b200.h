@@ -237,6 +237,69 @@ ebg_status ebg_cloud_knn_host(const ebg_cloud*      cloud,
 /* Synchronises stream and reports a device-side traversal error of earlier k-NN calls. */
 ebg_status ebg_cloud_check_status(const ebg_cloud* cloud, void* stream);
 
+/* ---- learned pruning radius (no counterpart in the reference) --------------------------------
+ *
+ * A multiresolution hash-grid encoding (16 levels x 2 BF16 features, 2^log2_table entries per
+ * level) feeding a 3-hidden-layer, 64-wide ReLU MLP (BF16 weights, FP32 accumulation on the tensor
+ * cores) that predicts the signed distance.  Passed as ebg_query_opts.seed, it seeds each packet of
+ * 32 sorted queries with the pruning radius (1 + alpha) |prediction at the packet centroid| + beta,
+ * widened per query by its distance to the centroid.  Distances stay exact: the radius only prunes,
+ * and a query whose radius holds no triangle is traversed again without it. */
+typedef struct ebg_seed_opts
+{
+  int64_t  num_samples;     /* exact training samples: half uniform in the domain, half within
+                               +-surface_band of the surface; 0 = 2^25 */
+  int32_t  steps;           /* Adam steps; 0 = 2000 */
+  int32_t  batch;           /* samples per step; 0 = 2^18 */
+  int32_t  log2_table;      /* hash-table entries per level = 2^log2_table; 0 = 19 */
+  int32_t  base_resolution; /* grid resolution of the coarsest level; 0 = 16 */
+  int32_t  max_resolution;  /* of the finest level; 0 = 1024 */
+  float    learning_rate;   /* initial Adam step (decays 10x over the run); 0 = 1e-2 */
+  float    surface_band;    /* half-width of the near-surface sample band; 0 = 0.02 */
+  float    coverage;        /* fraction of validation points whose radius must hold |d|; 0 = 0.995 */
+  uint64_t rng_seed;
+  double   lo[3], hi[3];    /* sample / encoding domain; lo == hi -> the mesh box grown 1.25x */
+} ebg_seed_opts;
+
+typedef struct ebg_seed_report
+{
+  float   train_seconds;
+  float   final_loss;         /* weighted MSE of the last step */
+  float   alpha, beta;        /* radius = (1 + alpha) |prediction| + beta */
+  float   coverage;           /* validation fraction with radius >= |d| */
+  float   mean_abs_err;       /* |prediction - d| over the validation samples */
+  float   far_tau;            /* far-field threshold (0.05) */
+  float   max_abs_err_far;    /* max |prediction - d| where |d| > far_tau (the optional surrogate's error) */
+  int64_t validation_samples;
+  int64_t train_samples;
+} ebg_seed_report;
+
+/* Untrained model (random initial parameters) over a domain; used by ebg_seed_train and by
+ * gradient checks. */
+ebg_status ebg_seed_create(const ebg_seed_opts* opts, ebg_seed** out);
+/* Generates num_samples exact signed distances with the mesh path, trains the model on the device
+ * with the library's own forward/backward/Adam kernels, calibrates alpha and beta on fresh
+ * validation samples and returns the model.  report (nullable) receives the training summary. */
+ebg_status ebg_seed_train(const ebg_mesh* mesh, const ebg_seed_opts* opts, ebg_seed** out, ebg_seed_report* report,
+                          void* stream);
+ebg_status ebg_seed_destroy(ebg_seed* seed);
+ebg_status ebg_seed_get_report(const ebg_seed* seed, ebg_seed_report* report);
+/* Raw predicted signed distance at n device points (the optional far-field surrogate). */
+ebg_status ebg_seed_predict(const ebg_seed* seed, const float* points_dev, int64_t n, float* out_dev, void* stream);
+/* Checkpoint of the model (configuration, FP32 tables and MLP parameters, calibration). */
+ebg_status ebg_seed_save(const ebg_seed* seed, const char* path);
+ebg_status ebg_seed_load(const char* path, int32_t device, ebg_seed** out);
+/* Parameter access: table = 16 * 2^log2_table * 2 floats (level-major, [level][entry][feature]),
+ * params = the 10,497 MLP floats (W1[64][32], b1, W2[64][64], b2, W3[64][64], b3, w4[64], b4).
+ * Either pointer may be null. */
+ebg_status ebg_seed_get_params(const ebg_seed* seed, float* table, float* params);
+ebg_status ebg_seed_set_params(ebg_seed* seed, const float* table, const float* params);
+/* Loss and gradients of one training batch (device samples) with the current parameters, without
+ * updating them: loss = sum_i w_i (y_i - d_i)^2 / n, w_i = 1 / (|d_i| + eps)^2.  Outputs are host
+ * arrays (grad_table nullable). */
+ebg_status ebg_seed_gradients(ebg_seed* seed, const float* points_dev, const float* target_dev, int32_t n, float eps,
+                              float* loss, float* grad_table, float* grad_params);
+
 #ifdef __cplusplus
 }
 #endif
