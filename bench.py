@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--seed-samples", type=int, default=1 << 25)
     ap.add_argument("--seed-steps", type=int, default=2000)
     ap.add_argument("--seed-batch", type=int, default=1 << 18)
+    ap.add_argument("--seed-save", default=None, help="write the trained model to this path")
+    ap.add_argument("--seed-load", default=None, help="load a trained model instead of training one")
     return ap.parse_args()
 
 
@@ -294,10 +296,16 @@ def run_ours(args, rank, world, local_rank):
     seed, rep, st_seed = None, None, None
     if not args.no_seed:
         t0 = time.time()
-        seed = SeedModel.train(mesh, num_samples=args.seed_samples, steps=args.seed_steps, batch=args.seed_batch,
-                               rng_seed=7, lo=[-1.25] * 3, hi=[1.25] * 3)
+        if args.seed_load:
+            seed = SeedModel.load(args.seed_load, device=local_rank)
+        else:
+            seed = SeedModel.train(mesh, num_samples=args.seed_samples, steps=args.seed_steps,
+                                   batch=args.seed_batch, rng_seed=7, lo=[-1.25] * 3, hi=[1.25] * 3)
         rep = seed.report()
         rep["wall_s"] = time.time() - t0
+        rep["loaded_from"] = args.seed_load
+        if args.seed_save:
+            seed.save(args.seed_save)
         log(f"[rank {rank}] seed trained: {rep}")
         _, st_seed = mesh.stats(pd, seed=seed)
         log(f"[rank {rank}] seeded stats {st_seed}")

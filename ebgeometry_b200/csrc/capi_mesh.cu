@@ -1,6 +1,7 @@
 // C ABI of the mesh path: handle lifetime, host build + upload, and the query pipeline
 //   Morton keys -> radix sort (query coherence) -> FP32 packet traversal -> FP64 band pass.
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -20,6 +21,122 @@
 using namespace ebg;
 
 namespace {
+
+// Oriented box of each leaf (see EbgLeafObb): n = area-weighted mean face normal (the smallest
+// extent axis of the leaf's AABB if the normals cancel), u = principal in-plane direction of the
+// leaf's vertices, extents from the vertex projections, padded by `pad` so FP32 evaluation of the
+// box distance never exceeds the FP64 distance to a triangle inside.
+void computeLeafObbs(const double* V, const int32_t* F, const Bvh4& bvh, std::vector<EbgLeafObb>& out)
+{
+  const size_t nl = bvh.leafFirst.size();
+  out.resize(nl);
+  double scale = 0;
+  for (int a = 0; a < 3; a++) {
+    scale = std::max(scale, std::max(std::fabs(bvh.lo[a]), std::fabs(bvh.hi[a])));
+  }
+  const double pad = 2e-6 * std::max(scale, 1e-30);
+#pragma omp parallel for schedule(static)
+  for (int64_t l = 0; l < int64_t(nl); l++) {
+    const uint32_t b = bvh.leafFirst[l], c = bvh.leafCount[l];
+    double         n[3] = {0, 0, 0}, area = 0, lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    std::vector<std::array<double, 3>> pts;
+    pts.reserve(3 * c);
+    for (uint32_t i = b; i < b + c; i++) {
+      const int64_t f = bvh.order[i];
+      const double* p0 = V + 3 * int64_t(F[3 * f]);
+      const double* p1 = V + 3 * int64_t(F[3 * f + 1]);
+      const double* p2 = V + 3 * int64_t(F[3 * f + 2]);
+      const double  e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+      const double  e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+      const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      for (int a = 0; a < 3; a++) {
+        n[a] += cr[a];
+      }
+      area += std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      for (const double* p : {p0, p1, p2}) {
+        pts.push_back({p[0], p[1], p[2]});
+        for (int a = 0; a < 3; a++) {
+          lo[a] = std::min(lo[a], p[a]);
+          hi[a] = std::max(hi[a], p[a]);
+        }
+      }
+    }
+    double ln = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (!(ln > 0.5 * area) || !(ln > 0)) {
+      int ax = 0;
+      for (int a = 1; a < 3; a++) {
+        if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
+          ax = a;
+        }
+      }
+      n[0] = n[1] = n[2] = 0;
+      n[ax] = 1;
+      ln    = 1;
+    }
+    for (int a = 0; a < 3; a++) {
+      n[a] /= ln;
+    }
+    // a first in-plane axis t1 (any perpendicular), then the principal direction in that plane
+    double t1[3];
+    if (std::fabs(n[0]) < 0.9) {
+      t1[0] = 0;
+      t1[1] = n[2];
+      t1[2] = -n[1];
+    }
+    else {
+      t1[0] = -n[2];
+      t1[1] = 0;
+      t1[2] = n[0];
+    }
+    double l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    for (int a = 0; a < 3; a++) {
+      t1[a] /= l1;
+    }
+    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
+    double       mx = 0, my = 0;
+    for (const auto& p : pts) {
+      mx += p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2];
+      my += p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2];
+    }
+    mx /= double(pts.size());
+    my /= double(pts.size());
+    double sxx = 0, syy = 0, sxy = 0;
+    for (const auto& p : pts) {
+      const double x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - mx;
+      const double y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - my;
+      sxx += x * x;
+      syy += y * y;
+      sxy += x * y;
+    }
+    const double th = 0.5 * std::atan2(2 * sxy, sxx - syy);
+    const double u[3] = {std::cos(th) * t1[0] + std::sin(th) * t2[0], std::cos(th) * t1[1] + std::sin(th) * t2[1],
+                         std::cos(th) * t1[2] + std::sin(th) * t2[2]};
+    const double w[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2], n[0] * u[1] - n[1] * u[0]};
+    double       mn[3] = {1e300, 1e300, 1e300}, mxx[3] = {-1e300, -1e300, -1e300};
+    for (const auto& p : pts) {
+      const double pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
+                            p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
+      for (int a = 0; a < 3; a++) {
+        mn[a]  = std::min(mn[a], pr[a]);
+        mxx[a] = std::max(mxx[a], pr[a]);
+      }
+    }
+    const double cn = 0.5 * (mn[0] + mxx[0]), cu = 0.5 * (mn[1] + mxx[1]), cw = 0.5 * (mn[2] + mxx[2]);
+    EbgLeafObb&  o  = out[l];
+    o.cx = float(cn * n[0] + cu * u[0] + cw * w[0]);
+    o.cy = float(cn * n[1] + cu * u[1] + cw * w[1]);
+    o.cz = float(cn * n[2] + cu * u[2] + cw * w[2]);
+    o.nx = float(n[0]);
+    o.ny = float(n[1]);
+    o.nz = float(n[2]);
+    o.ux = float(u[0]);
+    o.uy = float(u[1]);
+    o.uz = float(u[2]);
+    o.hn = roundUp(0.5 * (mxx[0] - mn[0]) + pad);
+    o.hu = roundUp(0.5 * (mxx[1] - mn[1]) + pad);
+    o.hv = roundUp(0.5 * (mxx[2] - mn[2]) + pad);
+  }
+}
 
 ebg_status buildMesh(const double*         V,
                      int64_t               nv,
@@ -185,6 +302,8 @@ ebg_status buildMesh(const double*         V,
   for (size_t i = 1; i < N; i++) {
     m->areaCdf[i] += m->areaCdf[i - 1];
   }
+  std::vector<EbgLeafObb> obb;
+  computeLeafObbs(V, F, bvh, obb);
   // upload
   auto up = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (cudaMalloc(dst, std::max<size_t>(bytes, 16)) != cudaSuccess) {
@@ -196,6 +315,7 @@ ebg_status buildMesh(const double*         V,
   if (!up(&m->dNodes, bvh.nodes.data(), nodeBytes) || !up(&m->dHot, hot.data(), N * sizeof(EbgTriHot)) ||
       !up(&m->dSign, sign.data(), N * sizeof(EbgTriSign)) || !up(&m->dTri64, tri64.data(), 30 * N * sizeof(double)) ||
       !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
+      !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgLeafObb)) ||
       cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
       cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
@@ -209,6 +329,7 @@ ebg_status buildMesh(const double*         V,
   v.sign         = static_cast<const EbgTriSign*>(m->dSign);
   v.tri64        = static_cast<const double*>(m->dTri64);
   v.tri_id       = static_cast<const int32_t*>(m->dTriId);
+  v.obb          = static_cast<const EbgLeafObb*>(m->dObb);
   for (int a = 0; a < 3; a++) {
     v.root_lo[a] = roundDown(bvh.lo[a]);
     v.root_hi[a] = roundUp(bvh.hi[a]);
@@ -480,6 +601,7 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dSign);
   cudaFree(m->dTri64);
   cudaFree(m->dTriId);
+  cudaFree(m->dObb);
   cudaFree(m->dStatus);
   delete m;
   return EBG_OK;

@@ -290,7 +290,9 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const float dk = boxD2exact(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
-          const bool  nk = __any_sync(FULL, dk <= bound);
+          // an empty slot (child 0 = the root, count 0) has an infinite box distance, which an
+          // unfilled k-best list (bound +inf) would admit: it is never pushed
+          const bool  nk = __any_sync(FULL, dk <= bound) && (cref[k] | ccnt[k]) != 0u;
           key[k]         = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
           o[k]           = k;
         }

@@ -28,6 +28,11 @@
 
 #define EBG_LEAF_BIT 0x80000000u
 #define EBG_MAX_LEAF 32
+// count[k] of a leaf slot packs the primitive count (low 6 bits) and the leaf's index (upper 26
+// bits, mesh leaves only: it selects the leaf's oriented box).
+#define EBG_COUNT_BITS 6u
+#define EBG_COUNT_MASK 63u
+#define EBG_MAX_LEAVES (1u << 26)
 
 // Traversal stack depth (entries per warp).  The builder rejects trees whose depth would need
 // more (a 4-wide node pushes at most 3 siblings per level besides the one it descends into).
@@ -56,7 +61,19 @@ struct alignas(16) EbgTriSign
   float pad1, pad2;
 };
 
+// Oriented box of one mesh leaf, in the frame of the leaf's mean normal n and an in-plane axis u
+// (v = n x u): centre c and half-extents (hn, hu, hv), padded outward to cover FP32 evaluation.  A
+// leaf on a smooth surface is a thin slab, so its distance bounds the leaf's triangles far more
+// tightly than the axis-aligned box does.
+struct alignas(16) EbgLeafObb
+{
+  float cx, cy, cz, hn;
+  float nx, ny, nz, hu;
+  float ux, uy, uz, hv;
+};
+
 static_assert(sizeof(EbgNode4) == 128, "node must be one 128-byte line");
+static_assert(sizeof(EbgLeafObb) == 48, "leaf box must be 48 bytes");
 static_assert(sizeof(EbgTriHot) == 48, "hot triangle record must be 48 bytes");
 static_assert(sizeof(EbgTriSign) == 96, "sign record must be 96 bytes");
 
@@ -68,6 +85,7 @@ struct EbgMeshView
   const EbgTriSign* sign;
   const double*     tri64;
   const int32_t*    tri_id;
+  const EbgLeafObb* obb;                    // per leaf id
   float             root_lo[3], root_hi[3]; // root box (FP32, outward)
   uint32_t          root_ref;               // node index 0, or a leaf reference for tiny meshes
   uint32_t          root_count;             // leaf count when root_ref is a leaf

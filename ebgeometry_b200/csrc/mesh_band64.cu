@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
       if (!__any_sync(FULL, d2 <= bound)) {
         continue;
       }
-      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
+      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w) & EBG_COUNT_MASK;
       if (ref & EBG_LEAF_BIT) {
         const uint32_t t0 = ref & ~EBG_LEAF_BIT;
         for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
@@ -141,7 +141,8 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
         float           key[4];
         for (int k = 0; k < 4; k++) {
           const float dk = boxDist2(nd.lox[k], nd.loy[k], nd.loz[k], nd.hix[k], nd.hiy[k], nd.hiz[k], px, py, pz);
-          if (__any_sync(FULL, dk <= bound)) {
+          // empty slot: child 0 and count 0 (node 0 is the root and never a child)
+          if (__any_sync(FULL, dk <= bound) && (nd.child[k] | nd.count[k]) != 0u) {
             o[np]   = k;
             key[np] = dk;
             np++;

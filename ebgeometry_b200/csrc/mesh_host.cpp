@@ -219,6 +219,8 @@ struct Builder
   std::vector<uint32_t>&     idx;
   std::vector<EbgNode4>&     nodes;
   std::atomic<uint32_t>      nodeCount{0};
+  std::vector<uint32_t>*     leafFirst = nullptr;
+  std::vector<uint32_t>*     leafCount = nullptr;
   std::atomic<int>           maxDepth{0};
   std::atomic<int64_t>       leaves{0};
 
@@ -389,9 +391,11 @@ struct Builder
       nd.hiz[k]    = roundUp(bx.hi[2]);
       const uint32_t cnt = ch[k].e - ch[k].b;
       if (cnt <= uint32_t(leafSize)) {
-        nd.child[k] = EBG_LEAF_BIT | ch[k].b;
-        nd.count[k] = cnt;
-        leaves.fetch_add(1);
+        const uint32_t id = uint32_t(leaves.fetch_add(1));
+        nd.child[k]       = EBG_LEAF_BIT | ch[k].b;
+        nd.count[k]       = cnt | (id << EBG_COUNT_BITS);
+        (*leafFirst)[id]  = ch[k].b;
+        (*leafCount)[id]  = cnt;
         int d = depth + 1;
         int cur = maxDepth.load();
         while (d > cur && !maxDepth.compare_exchange_weak(cur, d)) {
@@ -497,11 +501,18 @@ bool buildBvh4(const std::vector<double>& boxLo,
     }
   }
 
+  // leaf ids: at most one leaf per primitive
+  out.leafFirst.assign(n, 0);
+  out.leafCount.assign(n, 0);
+  B.leafFirst = &out.leafFirst;
+  B.leafCount = &out.leafCount;
   if (n <= size_t(leafSize)) {
     out.rootRef   = EBG_LEAF_BIT | 0u;
-    out.rootCount = uint32_t(n);
+    out.rootCount = uint32_t(n);  // leaf id 0
     out.depth     = 1;
     out.numLeaves = 1;
+    out.leafFirst.assign(1, 0);
+    out.leafCount.assign(1, uint32_t(n));
     out.nodes.clear();
     return true;
   }
@@ -516,6 +527,12 @@ bool buildBvh4(const std::vector<double>& boxLo,
   out.rootCount = 0;
   out.depth     = B.maxDepth.load();
   out.numLeaves = B.leaves.load();
+  out.leafFirst.resize(size_t(out.numLeaves));
+  out.leafCount.resize(size_t(out.numLeaves));
+  if (out.numLeaves > int64_t(EBG_MAX_LEAVES)) {
+    msg = "too many leaves (at most 2^26)";
+    return false;
+  }
   if (3 * out.depth + 4 > EBG_STACK_DEPTH) {
     msg = "BVH too deep for the traversal stack (depth " + std::to_string(out.depth) + ")";
     return false;

@@ -107,6 +107,21 @@ __device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, cons
 
 __device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
 
+// Squared distance from p to a leaf's oriented box, scaled down by 4e-6 relative so FP32 rounding
+// (about 3e-7 relative on the projections) can only make it smaller than the exact value.
+__device__ __forceinline__ float obbDist2(const float4 o0, const float4 o1, const float4 o2, float px, float py,
+                                          float pz)
+{
+  const float qx = px - o0.x, qy = py - o0.y, qz = pz - o0.z;
+  const float a  = fmaf(o1.x, qx, fmaf(o1.y, qy, o1.z * qz));
+  const float b  = fmaf(o2.x, qx, fmaf(o2.y, qy, o2.z * qz));
+  const float vx = fmaf(o1.y, o2.z, -o1.z * o2.y), vy = fmaf(o1.z, o2.x, -o1.x * o2.z),
+              vz = fmaf(o1.x, o2.y, -o1.y * o2.x);
+  const float e  = fmaf(vx, qx, fmaf(vy, qy, vz * qz));
+  const float dn = fmaxf(fabsf(a) - o0.w, 0.f), du = fmaxf(fabsf(b) - o1.w, 0.f), dv = fmaxf(fabsf(e) - o2.w, 0.f);
+  return fmaf(dn, dn, fmaf(du, du, dv * dv)) * (1.f - 4e-6f);
+}
+
 // a[k] for a warp-uniform k without dynamic register-array indexing (which would go to local memory)
 __device__ __forceinline__ float sel4(const float (&a)[4], int k)
 {
@@ -213,10 +228,17 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
         if (!__any_sync(FULL, need)) {
           continue;
         }
-        const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
+        const uint32_t ref = __float_as_uint(A.w), cntw = __float_as_uint(B.w);
         if (ref & EBG_LEAF_BIT) {
-          const uint32_t t0 = ref & ~EBG_LEAF_BIT;
-          if (STATS && need) {
+          const uint32_t t0 = ref & ~EBG_LEAF_BIT, cnt = cntw & EBG_COUNT_MASK;
+          // the leaf's oriented box (a thin slab on smooth surfaces) before its triangles
+          const float4* ob = reinterpret_cast<const float4*>(m.obb + (cntw >> EBG_COUNT_BITS));
+          const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
+          const bool    needObb = obbDist2(o0, o1, o2, px, py, pz) <= best;
+          if (!__any_sync(FULL, needObb)) {
+            continue;
+          }
+          if (STATS && needObb) {
             cLeaf++;
             cTri += cnt;
           }
@@ -252,7 +274,8 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
-            const bool  nk = __any_sync(FULL, dk <= best);
+            // an empty slot (child 0, count 0: node 0 is the root, never a child) is never pushed
+            const bool  nk = __any_sync(FULL, dk <= best) && (cref[k] | ccnt[k]) != 0u;
             // uniform ordering key; children nobody needs get -1 and are not pushed
             key[k] = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
             o[k]   = k;

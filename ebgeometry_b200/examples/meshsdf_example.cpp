@@ -1,0 +1,54 @@
+// A C++ caller of the drop-in classes: builds a mesh from a soup, evaluates signed distances one
+// point at a time through the virtual value() the reference's callers use, and in one batched call,
+// then a point cloud's nearest neighbours.  Prints "ok" and exits 0 when the single-point and the
+// batched values agree.
+//
+//   g++ -std=c++17 -I<repo> meshsdf_example.cpp -L<repo>/ebgeometry_b200 -lebgb200 -o meshsdf_example
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "ebgeometry_b200/include/EBGeometry_B200.hpp"
+
+using namespace EBGeometry::B200;
+
+int main()
+{
+  // an octahedron of radius 1
+  const std::vector<std::array<double, 3>> v = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  const std::vector<std::array<int32_t, 3>> f = {{0, 2, 4}, {2, 1, 4}, {1, 3, 4}, {3, 0, 4},
+                                                 {2, 0, 5}, {1, 2, 5}, {3, 1, 5}, {0, 3, 5}};
+  TriMeshSDF    sdf(v, f);
+  const ImplicitBase& asImplicit = sdf; // the reference's interface: virtual value(point)
+
+  std::vector<float> pts;
+  for (int i = 0; i < 1000; i++) {
+    pts.push_back(float(std::sin(0.7 * i) * 1.5));
+    pts.push_back(float(std::cos(1.3 * i) * 1.5));
+    pts.push_back(float(std::sin(2.1 * i + 0.3) * 1.5));
+  }
+  std::vector<float> d(pts.size() / 3);
+  sdf.signedDistances(pts.data(), d.size(), d.data());
+  double maxDiff = 0;
+  for (size_t i = 0; i < d.size(); i += 37) {
+    const double one = asImplicit.value(Vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
+    maxDiff          = std::fmax(maxDiff, std::fabs(one - double(d[i])));
+  }
+  // the octahedron's exact signed distance is (|x|+|y|+|z|-1)/sqrt(3) where the closest feature
+  // is a face; check the centre
+  const double centre = asImplicit.value(Vec3(0, 0, 0));
+
+  std::vector<std::array<float, 3>> cloud;
+  for (int i = 0; i < 5000; i++) {
+    cloud.push_back({float(std::fmod(i * 0.618034, 1.0)), float(std::fmod(i * 0.414214, 1.0)),
+                     float(std::fmod(i * 0.732051, 1.0))});
+  }
+  PointCloudBVH     pc(cloud);
+  const auto        hit = pc.closestPoint(cloud[123]);
+  std::printf("batch/single max diff %.3g, centre %.6f (expect %.6f), nearest of point 123: %zu (d2 %g)\n", maxDiff,
+              centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared));
+  const bool ok = maxDiff <= 1e-6 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-6 && hit.index == 123 &&
+                  hit.distanceSquared == 0.f;
+  std::printf("%s\n", ok ? "ok" : "FAILED");
+  return ok ? 0 : 1;
+}

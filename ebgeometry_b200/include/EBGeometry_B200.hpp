@@ -1,0 +1,243 @@
+// C++17 drop-in host classes over the C ABI (include/ebgeometry_b200.h).
+//
+// They mirror the reference's (rmrsk/EBGeometry) query objects and keep its single-point
+// interface -- ImplicitFunction<T>::value(point) / SignedDistanceFunction<T>::signedDistance(point)
+// (Source/EBGeometry_ImplicitFunction.hpp:51-60, Source/EBGeometry_SignedDistanceFunction.hpp:53-62)
+// -- while adding the batched calls that reach the GPU's throughput:
+//
+//   EBGeometry::B200::TriMeshSDF     ~ TriMeshSDF<T,Meta,K,W>   (MeshDistanceFunctions.hpp:309-489)
+//   EBGeometry::B200::PointCloudBVH  ~ PointCloudBVH<T,Meta,K,W> (PointCloudBVH.hpp:56-350)
+//   EBGeometry::B200::SeedModel      the learned pruning radius (no reference counterpart)
+//
+// Define EBGEOMETRY_B200_WITH_REFERENCE before including this header (with the reference's
+// EBGeometry.hpp on the include path) and TriMeshSDF derives from the reference's own
+// EBGeometry::SignedDistanceFunction<double>, so it plugs into the reference's CSG unions,
+// transforms and integrations unchanged.  Without it, a minimal ImplicitFunction base with the same
+// virtual value() is provided.
+//
+// Errors: constructors and batched calls throw EBGeometry::B200::Error carrying the C status and
+// message; value() is noexcept like the reference's and returns NaN if the device call fails.
+#ifndef EBGEOMETRY_B200_HPP
+#define EBGEOMETRY_B200_HPP
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/ebgeometry_b200.h"
+
+#ifdef EBGEOMETRY_B200_WITH_REFERENCE
+#include <EBGeometry.hpp>
+#endif
+
+namespace EBGeometry {
+namespace B200 {
+
+class Error : public std::runtime_error
+{
+public:
+  Error(ebg_status s, const std::string& what) : std::runtime_error(what), status(s) {}
+  ebg_status status;
+};
+
+inline void
+check(ebg_status s)
+{
+  if (s != EBG_OK) {
+    throw Error(s, ebg_last_error());
+  }
+}
+
+#ifdef EBGEOMETRY_B200_WITH_REFERENCE
+using Vec3          = EBGeometry::Vec3T<double>;
+using ImplicitBase  = EBGeometry::SignedDistanceFunction<double>;
+inline double x(const Vec3& p) { return p[0]; }
+inline double y(const Vec3& p) { return p[1]; }
+inline double z(const Vec3& p) { return p[2]; }
+#else
+struct Vec3
+{
+  double v[3];
+  Vec3(double a = 0, double b = 0, double c = 0) : v{a, b, c} {}
+  double operator[](int i) const { return v[i]; }
+};
+inline double x(const Vec3& p) { return p[0]; }
+inline double y(const Vec3& p) { return p[1]; }
+inline double z(const Vec3& p) { return p[2]; }
+
+// Same virtual single-point surface as the reference's ImplicitFunction / SignedDistanceFunction.
+class ImplicitBase
+{
+public:
+  virtual ~ImplicitBase() = default;
+  virtual double value(const Vec3& a_point) const noexcept { return this->signedDistance(a_point); }
+  double operator()(const Vec3& a_point) const noexcept { return this->value(a_point); }
+  virtual double signedDistance(const Vec3& a_point) const noexcept = 0;
+};
+#endif
+
+enum class Build : int32_t
+{
+  SAH    = EBG_BUILD_SAH,
+  Morton = EBG_BUILD_MORTON
+};
+
+class SeedModel;
+
+// Signed distance to a watertight triangle mesh; pseudonormals as the reference's DCEL computes them.
+class TriMeshSDF : public ImplicitBase
+{
+public:
+  TriMeshSDF(const std::vector<std::array<double, 3>>& a_vertices,
+             const std::vector<std::array<int32_t, 3>>& a_triangles,
+             Build                                      a_build    = Build::SAH,
+             int                                        a_leafSize = 8,
+             int                                        a_device   = -1)
+  {
+    ebg_build_opts o{static_cast<int32_t>(a_build), a_leafSize, a_device, 0};
+    check(ebg_mesh_create(&a_vertices[0][0], int64_t(a_vertices.size()), &a_triangles[0][0],
+                          int64_t(a_triangles.size()), &o, &m_mesh));
+  }
+  TriMeshSDF(const TriMeshSDF&) = delete;
+  TriMeshSDF& operator=(const TriMeshSDF&) = delete;
+  ~TriMeshSDF() override { ebg_mesh_destroy(m_mesh); }
+
+  // ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance for one point
+  // (one small synchronous launch per call -- batch where you can).
+  double signedDistance(const Vec3& a_point) const noexcept override
+  {
+    double d = std::numeric_limits<double>::quiet_NaN();
+    if (ebg_mesh_value(m_mesh, x(a_point), y(a_point), z(a_point), &d) != EBG_OK) {
+      return std::numeric_limits<double>::quiet_NaN();
+    }
+    return d;
+  }
+
+  // Batched signed distances of n host points (xyz float32 interleaved), synchronous.
+  void signedDistances(const float* a_pointsHost, size_t a_n, float* a_distHost, const SeedModel* a_seed = nullptr,
+                       int32_t* a_closestTriangleHost = nullptr) const;
+
+  // Batched, device buffers, asynchronous on a_stream (a cudaStream_t).
+  void signedDistancesDevice(const float* a_pointsDev, size_t a_n, float* a_distDev, void* a_stream = nullptr,
+                             const SeedModel* a_seed = nullptr) const;
+
+  ebg_mesh_info info() const
+  {
+    ebg_mesh_info i{};
+    check(ebg_mesh_get_info(m_mesh, &i));
+    return i;
+  }
+  const ebg_mesh* handle() const noexcept { return m_mesh; }
+
+private:
+  ebg_mesh* m_mesh = nullptr;
+};
+
+// The learned pruning radius (trained on the device from the mesh's own exact distances).
+class SeedModel
+{
+public:
+  explicit SeedModel(const TriMeshSDF& a_mesh, const ebg_seed_opts* a_opts = nullptr)
+  {
+    check(ebg_seed_train(a_mesh.handle(), a_opts, &m_seed, nullptr, nullptr));
+  }
+  explicit SeedModel(const std::string& a_checkpoint, int a_device = -1)
+  {
+    check(ebg_seed_load(a_checkpoint.c_str(), a_device, &m_seed));
+  }
+  SeedModel(const SeedModel&) = delete;
+  SeedModel& operator=(const SeedModel&) = delete;
+  ~SeedModel() { ebg_seed_destroy(m_seed); }
+  void save(const std::string& a_path) const { check(ebg_seed_save(m_seed, a_path.c_str())); }
+  ebg_seed_report report() const
+  {
+    ebg_seed_report r{};
+    check(ebg_seed_get_report(m_seed, &r));
+    return r;
+  }
+  const ebg_seed* handle() const noexcept { return m_seed; }
+
+private:
+  ebg_seed* m_seed = nullptr;
+};
+
+inline void
+TriMeshSDF::signedDistances(const float* a_pointsHost, size_t a_n, float* a_distHost, const SeedModel* a_seed,
+                            int32_t* a_closestTriangleHost) const
+{
+  ebg_query_opts o{};
+  o.seed = a_seed ? a_seed->handle() : nullptr;
+  check(ebg_mesh_signed_distance_host(m_mesh, a_pointsHost, int64_t(a_n), a_distHost, a_closestTriangleHost, &o,
+                                      nullptr));
+}
+
+inline void
+TriMeshSDF::signedDistancesDevice(const float* a_pointsDev, size_t a_n, float* a_distDev, void* a_stream,
+                                  const SeedModel* a_seed) const
+{
+  ebg_query_opts o{};
+  o.seed = a_seed ? a_seed->handle() : nullptr;
+  check(ebg_mesh_signed_distance(m_mesh, a_pointsDev, int64_t(a_n), a_distDev, nullptr, &o, a_stream));
+}
+
+// k nearest neighbours; Hit mirrors PointCloudBVH::Hit (PointCloudBVH.hpp:93-97).
+class PointCloudBVH
+{
+public:
+  struct Hit
+  {
+    size_t index;
+    float  distanceSquared;
+  };
+
+  explicit PointCloudBVH(const std::vector<std::array<float, 3>>& a_points, int a_leafSize = 16, int a_device = -1)
+  {
+    ebg_build_opts o{0, a_leafSize, a_device, 0};
+    check(ebg_cloud_create(&a_points[0][0], int64_t(a_points.size()), &o, &m_cloud));
+  }
+  PointCloudBVH(const PointCloudBVH&) = delete;
+  PointCloudBVH& operator=(const PointCloudBVH&) = delete;
+  ~PointCloudBVH() { ebg_cloud_destroy(m_cloud); }
+
+  size_t numPoints() const noexcept { return size_t(ebg_cloud_size(m_cloud)); }
+
+  // PointCloudBVH::closestPoint / closestPoints for one query (PointCloudBVHImplem.hpp:429-453);
+  // returns how many neighbours were found (< k only if the cloud has fewer points).
+  Hit closestPoint(const std::array<float, 3>& a_q) const
+  {
+    Hit h{};
+    closestPoints(a_q, 1, &h);
+    return h;
+  }
+  size_t closestPoints(const std::array<float, 3>& a_q, size_t a_k, Hit* a_out) const
+  {
+    std::vector<int32_t> idx(a_k);
+    std::vector<float>   d2(a_k);
+    check(ebg_cloud_knn_host(m_cloud, a_q.data(), 1, int32_t(a_k), idx.data(), d2.data(), nullptr, nullptr));
+    size_t found = 0;
+    for (size_t j = 0; j < a_k; j++) {
+      if (idx[j] >= 0) {
+        a_out[found++] = Hit{size_t(idx[j]), d2[j]};
+      }
+    }
+    return found;
+  }
+  // Batched: idx/d2 are (n x k), host buffers, synchronous.
+  void knn(const float* a_queriesHost, size_t a_n, int a_k, int32_t* a_idx, float* a_d2) const
+  {
+    check(ebg_cloud_knn_host(m_cloud, a_queriesHost, int64_t(a_n), a_k, a_idx, a_d2, nullptr, nullptr));
+  }
+
+private:
+  ebg_cloud* m_cloud = nullptr;
+};
+
+} // namespace B200
+} // namespace EBGeometry
+
+#endif
