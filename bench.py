@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-seed", action="store_true", help="time the plain traversal only")
+    ap.add_argument("--perfect-seed", action="store_true",
+                    help="also time the traversal seeded with the exact distances (the bound any seed can reach)")
     ap.add_argument("--seed-samples", type=int, default=1 << 25)
     ap.add_argument("--seed-steps", type=int, default=2000)
     ap.add_argument("--seed-batch", type=int, default=1 << 18)
@@ -231,7 +233,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, dist, local_rank):
+def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, dist, local_rank, hint=None):
     """K steps bracketed by barrier + synchronize, CUDA events on the launching stream, clocks
     sampled meanwhile; per-phase events recorded inside each call.  Returns (ms/step max over
     ranks, phase array, clocks)."""
@@ -245,7 +247,7 @@ def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, di
     e0.record(stream)
     for _ in range(steps):
         tm = _capi.PhaseTimings()
-        mesh.signed_distance(pd, out=out, timings=tm, seed=seed)
+        mesh.signed_distance(pd, out=out, timings=tm, seed=seed, radius_hint=hint)
         tms.append((tm.order_ms, tm.traverse_ms, tm.band_ms, tm.total_ms))
     e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -292,6 +294,21 @@ def run_ours(args, rank, world, local_rank):
     ms_plain, tms_plain, ck_plain = timed_steps(*tsteps, None, *tctx)
     plain_ref = out.clone() if not args.no_seed else None
     log(f"[rank {rank}] plain {ms_plain:.1f} ms/step")
+
+    # what ANY pruning-radius seed could save at best: the exact |d| (from the plain run) as radius
+    perfect = None
+    if args.perfect_seed:
+        hint = out.abs() * (1 + 1e-5) + 1e-6
+        _, st_hint = mesh.stats(pd, radius_hint=hint)
+        hout = torch.empty_like(out)
+        for _ in range(2):
+            mesh.signed_distance(pd, out=hout, radius_hint=hint)
+        ms_hint, _, _ = timed_steps(mesh, pd, hout, max(2, args.steps // 2), None, *tctx, hint=hint)
+        perfect = {"ms_per_step": ms_hint, "value": n * world / (ms_hint * 1e-3),
+                   "speedup_vs_plain": ms_plain / ms_hint, "stats": st_hint,
+                   "equal_to_plain_fraction": float((hout == out).float().mean().item())}
+        log(f"[rank {rank}] perfect radius {ms_hint:.1f} ms/step {st_hint}")
+        del hout, hint
 
     seed, rep, st_seed = None, None, None
     if not args.no_seed:
@@ -414,6 +431,7 @@ def run_ours(args, rank, world, local_rank):
                    f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
                    "plain": {"value": plain_value, "ms_per_step": ms_plain, "phase_ms_mean": phases(tms_plain),
                              "per_query": per_query(st), "clocks": ck_plain},
+                   "perfect_radius_bound": perfect,
                    "seeded": None if seed is None else {
                        "value": value, "ms_per_step": ms_seed, "speedup_vs_plain": value / plain_value,
                        "phase_ms_mean": phases(tms_seed), "per_query": per_query(st_seed),

@@ -8,6 +8,8 @@ Python mirror of the reference's (rmrsk/EBGeometry) C++ query objects on top of 
   51-60) and a batched ``signed_distance(points)`` over CUDA tensors or numpy arrays.
 * :class:`PointCloudBVH` -- ``PointCloudBVH(positions, meta)`` (PointCloudBVH.hpp:56-350) with
   ``closestPoint`` / ``closestPoints`` for one point and a batched ``knn(queries, k)``.
+* :class:`BVHUnion` -- ``BVHUnion(prims, bvs)`` (CSG.hpp:99-101) over spheres and
+  ``Translate(Rotate(TriMeshSDF))`` instances, with ``value(point)`` and batched ``values(points)``.
 
 There is no CPU fallback: every query runs in the CUDA kernels of ``libebgb200.so``, and importing
 this package fails if that library is missing.
@@ -21,7 +23,7 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["TriMeshSDF", "PointCloudBVH", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
+__all__ = ["TriMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
 BUILD_MORTON = 1
@@ -103,11 +105,12 @@ class TriMeshSDF:
         return fn, vn, en
 
     @staticmethod
-    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None):
+    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None):
         return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
                                seed.handle if seed is not None else None,
                                int(warps_per_block or 0), 0,
-                               C.pointer(timings) if timings is not None else None)
+                               C.pointer(timings) if timings is not None else None,
+                               radius_hint.data_ptr() if radius_hint is not None else None)
 
     # --- ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance -----------------
     def value(self, point) -> float:
@@ -121,13 +124,15 @@ class TriMeshSDF:
 
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
-                        fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None):
+                        fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None,
+                        radius_hint=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
         times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
-        radius seeds the traversal's pruning bound (results stay exact)."""
-        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed)
+        radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
+        float32 tensor of per-point upper bounds on |d| that seed the bound the same way."""
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint)
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
             n = p.shape[0]
@@ -149,13 +154,13 @@ class TriMeshSDF:
                                            C.byref(opts), _stream_ptr(stream)))
         return (d, closest_tri) if closest_tri is not None else d
 
-    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None, seed=None):
+    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None, seed=None, radius_hint=None):
         """Traversal counters summed over the points (synchronous; CUDA tensor input)."""
         import torch
         n = points.numel() // 3
         d = torch.empty(n, dtype=torch.float32, device=points.device)
         st = _capi.QueryStats()
-        opts = self._opts(band, sort, fp64_band, None, None, seed)
+        opts = self._opts(band, sort, fp64_band, None, None, seed, radius_hint)
         check(lib.ebg_mesh_signed_distance_stats(self._h, C.c_void_p(points.data_ptr()), n,
                                                  C.c_void_p(d.data_ptr()), C.byref(opts),
                                                  C.byref(st), _stream_ptr(stream)))
@@ -329,3 +334,50 @@ class SeedModel:
         check(lib.ebg_seed_gradients(self._h, C.c_void_p(pt.data_ptr()), C.c_void_p(tt.data_ptr()),
                                      pt.shape[0], float(eps), C.byref(loss), _ptr(gt), _ptr(gp)))
         return loss.value, gt, gp
+
+
+class BVHUnion:
+    """Union of spheres and posed mesh instances (the reference's BVHUnionIF over SphereSDF and
+    Translate(Rotate(TriMeshSDF)) objects).  ``spheres``: (S,4) centre xyz + radius; ``meshes``:
+    list of :class:`TriMeshSDF`; ``poses``: (M,5) angle in degrees, axis (0/1/2), translation."""
+
+    def __init__(self, spheres=None, meshes=(), poses=None, leaf_size=3, device=-1):
+        sp = np.ascontiguousarray(spheres if spheres is not None else np.zeros((0, 4)), np.float64).reshape(-1, 4)
+        ps = np.ascontiguousarray(poses if poses is not None else np.zeros((0, 5)), np.float64).reshape(-1, 5)
+        self._meshes = list(meshes)  # kept alive: the scene references their device data
+        arr = (C.c_void_p * max(1, len(self._meshes)))(*[m.handle.value for m in self._meshes])
+        opts = _capi.BuildOpts(0, int(leaf_size), int(device), 0)
+        h = C.c_void_p()
+        check(lib.ebg_scene_create(sp.shape[0], _ptr(sp), len(self._meshes), arr, _ptr(ps), C.byref(opts),
+                                   C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_scene_destroy(h)
+            self._h = None
+
+    def num_objects(self) -> int:
+        return int(lib.ebg_scene_num_objects(self._h))
+
+    def values(self, points, out=None, sort=True, stream=None):
+        """Union value at (n,3) float32 points (CUDA tensor: asynchronous; numpy: synchronous)."""
+        opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0, None, 0, 0, None)
+        if isinstance(points, np.ndarray):
+            p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+            d = out if out is not None else np.empty(p.shape[0], np.float32)
+            check(lib.ebg_scene_value_host(self._h, _ptr(p), p.shape[0], _ptr(d), C.byref(opts), None))
+            return d
+        import torch
+        n = points.numel() // 3
+        d = out if out is not None else torch.empty(n, dtype=torch.float32, device=points.device)
+        check(lib.ebg_scene_value(self._h, C.c_void_p(points.data_ptr()), n, C.c_void_p(d.data_ptr()),
+                                  C.byref(opts), _stream_ptr(stream)))
+        return d
+
+    def value(self, point) -> float:
+        return float(self.values(np.asarray(point, np.float32).reshape(1, 3))[0])
+
+    def check_status(self, stream=None):
+        check(lib.ebg_scene_check_status(self._h, _stream_ptr(stream)))

@@ -25,7 +25,7 @@ class PhaseTimings(C.Structure):
 class QueryOpts(C.Structure):
     _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
                 ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("reserved", C.c_int32),
-                ("timings", C.POINTER(PhaseTimings))]
+                ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p)]
 
 
 class SeedOpts(C.Structure):
@@ -90,6 +90,12 @@ SIGNATURES = {
     "ebg_cloud_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_check_status": (C.c_int, [_P, _P]),
+    "ebg_scene_create": (C.c_int, [_I64, _P, _I64, _P, _P, C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "ebg_scene_destroy": (C.c_int, [_P]),
+    "ebg_scene_num_objects": (_I64, [_P]),
+    "ebg_scene_value": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_scene_value_host": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_scene_check_status": (C.c_int, [_P, _P]),
     "ebg_seed_create": (C.c_int, [C.POINTER(SeedOpts), C.POINTER(_P)]),
     "ebg_seed_train": (C.c_int, [_P, C.POINTER(SeedOpts), C.POINTER(_P), C.POINTER(SeedReport), _P]),
     "ebg_seed_destroy": (C.c_int, [_P]),

@@ -13,6 +13,7 @@
 
 #include "capi_common.h"
 #include "capi_internal.h"
+#include "ebg_device.cuh"
 #include "ebgeometry_b200.h"
 #include "mesh_host.h"
 #include "mesh_kernels.h"
@@ -481,6 +482,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.points     = pts;
   a.order      = order;
   a.seed_r     = seedR;
+  a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
   a.n          = n;
   a.out_d      = outD;
   a.out_tri    = outTri;
@@ -520,19 +522,6 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   return EBG_OK;
 }
 
-namespace {
-
-bool checkPoints(const float* p, int64_t n)
-{
-  for (int64_t i = 0; i < 3 * n; i++) {
-    if (!std::isfinite(p[i])) {
-      return false;
-    }
-  }
-  return true;
-}
-
-} // namespace
 
 extern "C" {
 
@@ -666,9 +655,6 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
   if (n == 0) {
     return EBG_OK;
   }
-  if (!checkPoints(points_host, n)) {
-    return setError(EBG_ERR_INVALID, "non-finite query coordinate");
-  }
   DeviceGuard  guard;
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -772,6 +758,9 @@ ebg_status ebg_check_status(const ebg_mesh* m, void* stream)
   }
   if (st != 0) {
     cudaMemsetAsync(m->dStatus, 0, sizeof(int), s);
+    if (st & ST_INPUT) {
+      return setError(EBG_ERR_INVALID, "non-finite query coordinate");
+    }
     return setError(EBG_ERR_TRAVERSAL, "traversal stopped early (status " + std::to_string(st) + ")");
   }
   return EBG_OK;

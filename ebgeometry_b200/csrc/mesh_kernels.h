@@ -15,6 +15,7 @@ struct MeshQueryArgs
   const float*       points;     // caller's xyz (n x 3)
   const uint32_t*    order;      // sorted position -> caller index (nullptr = identity)
   const float*       seed_r;     // per packet of 32 sorted queries: predicted radius (nullptr = none)
+  const float*       hint;       // per query (caller order): radius upper bound (nullptr = none)
   int64_t            n;
   float*             out_d;      // caller order
   int32_t*           out_tri;    // caller order (nullable)

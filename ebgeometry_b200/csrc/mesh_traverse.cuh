@@ -1,0 +1,267 @@
+// Device-side packet traversal of one mesh BVH, shared by the mesh SDF kernel and the CSG scene
+// kernel (which runs it once per mesh object a packet reaches, on the object-local query points).
+#ifndef EBG_MESH_TRAVERSE_CUH
+#define EBG_MESH_TRAVERSE_CUH
+
+#include <cfloat>
+
+#include "ebg_device.cuh"
+
+namespace ebg {
+
+// Closest point of triangle (v0, v0+ab, v0+ac) to p by Voronoi region (the standard barycentric
+// region tests).  Returns the squared distance; s, t are the barycentric weights of ab and ac of
+// the closest point and region is 0 face, 1..3 vertex 0..2, 4 edge 0-1, 5 edge 1-2, 6 edge 2-0.
+// Equivalent to the reference's triangle test (TriangleSoAImplem.hpp:1199-1293): its "inside"
+// test (all three (e_i x n).p_i of one sign) is the face region, and outside it the minimum over
+// vertices and interior edge points is the closest boundary point.
+template <bool WANT_REGION>
+__device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, const float4 h2, float px, float py,
+                                          float pz, float& s, float& t, int& region)
+{
+  const float apx = px - h0.x, apy = py - h0.y, apz = pz - h0.z;
+  const float ab2 = h0.w, abac = h1.w, ac2 = h2.w;
+  const float d1 = fmaf(h1.x, apx, fmaf(h1.y, apy, h1.z * apz));
+  const float d2 = fmaf(h2.x, apx, fmaf(h2.y, apy, h2.z * apz));
+  const float d3 = d1 - ab2, d4 = d2 - abac;
+  const float d5 = d1 - abac, d6 = d2 - ac2;
+  const float vc = fmaf(d1, d4, -d3 * d2);
+  const float vb = fmaf(d5, d2, -d1 * d6);
+  const float va = fmaf(d3, d6, -d5 * d4);
+
+  // face region by default; each test below overrides, the highest-priority region last
+  float sn = vb, tn = vc, den = va + vb + vc;
+  int   r  = 0;
+  const float bc1 = d4 - d3, bc2 = d5 - d6;
+  if (va <= 0.f && bc1 >= 0.f && bc2 >= 0.f) { // edge 1-2
+    sn = bc2;
+    tn = bc1;
+    den = bc1 + bc2;
+    r   = 5;
+  }
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) { // edge 2-0 (along ac)
+    sn  = 0.f;
+    tn  = d2;
+    den = d2 - d6;
+    r   = 6;
+  }
+  if (d6 >= 0.f && d5 <= d6) { // vertex 2
+    sn  = 0.f;
+    tn  = 1.f;
+    den = 1.f;
+    r   = 3;
+  }
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) { // edge 0-1 (along ab)
+    sn  = d1;
+    tn  = 0.f;
+    den = d1 - d3;
+    r   = 4;
+  }
+  if (d3 >= 0.f && d4 <= d3) { // vertex 1
+    sn  = 1.f;
+    tn  = 0.f;
+    den = 1.f;
+    r   = 2;
+  }
+  if (d1 <= 0.f && d2 <= 0.f) { // vertex 0
+    sn  = 0.f;
+    tn  = 0.f;
+    den = 1.f;
+    r   = 1;
+  }
+  const float inv = __fdividef(1.f, den);
+  s               = sn * inv;
+  t               = tn * inv;
+  const float dx  = fmaf(-t, h2.x, fmaf(-s, h1.x, apx));
+  const float dy  = fmaf(-t, h2.y, fmaf(-s, h1.y, apy));
+  const float dz  = fmaf(-t, h2.z, fmaf(-s, h1.z, apz));
+  if (WANT_REGION) {
+    region = r;
+  }
+  return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+__device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
+
+// Squared distance from p to a leaf's oriented box, scaled down by 4e-6 relative so FP32 rounding
+// (about 3e-7 relative on the projections) can only make it smaller than the exact value.
+__device__ __forceinline__ float obbDist2(const float4 o0, const float4 o1, const float4 o2, float px, float py,
+                                          float pz)
+{
+  const float qx = px - o0.x, qy = py - o0.y, qz = pz - o0.z;
+  const float a  = fmaf(o1.x, qx, fmaf(o1.y, qy, o1.z * qz));
+  const float b  = fmaf(o2.x, qx, fmaf(o2.y, qy, o2.z * qz));
+  const float vx = fmaf(o1.y, o2.z, -o1.z * o2.y), vy = fmaf(o1.z, o2.x, -o1.x * o2.z),
+              vz = fmaf(o1.x, o2.y, -o1.y * o2.x);
+  const float e  = fmaf(vx, qx, fmaf(vy, qy, vz * qz));
+  const float dn = fmaxf(fabsf(a) - o0.w, 0.f), du = fmaxf(fabsf(b) - o1.w, 0.f), dv = fmaxf(fabsf(e) - o2.w, 0.f);
+  return fmaf(dn, dn, fmaf(du, du, dv * dv)) * (1.f - 4e-6f);
+}
+
+// a[k] for a warp-uniform k without dynamic register-array indexing (which would go to local memory)
+__device__ __forceinline__ float sel4(const float (&a)[4], int k)
+{
+  return k == 0 ? a[0] : (k == 1 ? a[1] : (k == 2 ? a[2] : a[3]));
+}
+__device__ __forceinline__ uint32_t sel4u(const uint32_t (&a)[4], int k)
+{
+  return k == 0 ? a[0] : (k == 1 ? a[1] : (k == 2 ? a[2] : a[3]));
+}
+
+// Signed distance of p to triangle `tri` (leaf order), sign from the pseudonormal of the closest
+// feature (the reference's sign-bit convention, TriangleSoAImplem.hpp:1076-1082: +0 -> +1).
+__device__ __forceinline__ float signedFromWinner(const EbgMeshView& m, uint32_t tri, float px, float py, float pz)
+{
+  const float4* h = reinterpret_cast<const float4*>(m.hot + tri);
+  const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+  float         s, t;
+  int           region;
+  const float   d2 = triDist2<true>(h0, h1, h2, px, py, pz, s, t, region);
+  const float*  sg = reinterpret_cast<const float*>(m.sign + tri);
+  const float   apx = px - h0.x, apy = py - h0.y, apz = pz - h0.z;
+  if (region == 0) {
+    // face: the reference returns n . (p - v0) itself
+    return fmaf(__ldg(sg + 0), apx, fmaf(__ldg(sg + 1), apy, __ldg(sg + 2) * apz));
+  }
+  const float dx = fmaf(-t, h2.x, fmaf(-s, h1.x, apx));
+  const float dy = fmaf(-t, h2.y, fmaf(-s, h1.y, apy));
+  const float dz = fmaf(-t, h2.z, fmaf(-s, h1.z, apz));
+  // vertex i -> vn[3i..], edge j -> en[3j..]: sign record = n(3) pad vn(9) en(9)
+  const int   o  = (region <= 3) ? (4 + 3 * (region - 1)) : (13 + 3 * (region - 4));
+  const float sd = fmaf(__ldg(sg + o), dx, fmaf(__ldg(sg + o + 1), dy, __ldg(sg + o + 2) * dz));
+  return signOf(sd) * sqrtf(d2);
+}
+
+
+struct TraversalCounters
+{
+  uint32_t node = 0, leaf = 0, tri = 0, fall = 0;
+};
+
+// One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
+// already seeded or FLT_MAX) and winning triangle `besttri` (leaf order) are updated; (cx, cy, cz)
+// is the packet centroid used to order children.  `stk` is this warp's stack region (2 float4 per
+// entry, EBG_STACK_DEPTH entries); `iters` counts loop trips against MAX_ITERS; `err` receives
+// ST_* bits.  All 32 lanes must call it together.
+template <bool STATS>
+__device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float cx, float cy,
+                                             float cz, float& best, int& besttri, float4* stk, uint32_t& iters,
+                                             int& err, TraversalCounters& cnt_)
+{
+  const int lane = threadIdx.x & 31;
+      int sp = 1;
+      if (lane == 0) {
+        stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
+        stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+      }
+      __syncwarp();
+#pragma unroll 1
+      while (sp > 0) {
+        if (++iters > MAX_ITERS) {
+          err |= ST_ITERS;
+          break;
+        }
+        --sp;
+        const float4 A    = stk[2 * sp];
+        const float4 B    = stk[2 * sp + 1];
+        const float  d2   = boxDist2(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
+        const bool   need = d2 <= best;
+        if (!__any_sync(FULL, need)) {
+          continue;
+        }
+        const uint32_t ref = __float_as_uint(A.w), cntw = __float_as_uint(B.w);
+        if (ref & EBG_LEAF_BIT) {
+          const uint32_t t0 = ref & ~EBG_LEAF_BIT, cnt = cntw & EBG_COUNT_MASK;
+          // the leaf's oriented box (a thin slab on smooth surfaces) before its triangles
+          const float4* ob = reinterpret_cast<const float4*>(m.obb + (cntw >> EBG_COUNT_BITS));
+          const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
+          const bool    needObb = obbDist2(o0, o1, o2, px, py, pz) <= best;
+          if (!__any_sync(FULL, needObb)) {
+            continue;
+          }
+          if (STATS && needObb) {
+            cnt_.leaf++;
+            cnt_.tri += cnt;
+          }
+#pragma unroll 1
+          for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
+            const float4* h = reinterpret_cast<const float4*>(m.hot + tt);
+            const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+            float         s, t;
+            int           r;
+            const float   dd = triDist2<false>(h0, h1, h2, px, py, pz, s, t, r);
+            if (dd < best) {
+              best    = dd;
+              besttri = int(tt);
+            }
+          }
+        }
+        else {
+          if (STATS && need) {
+            cnt_.node++;
+          }
+          const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
+          const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+          const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+          const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
+          const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+          const float   clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
+                      clz[4] = {lz.x, lz.y, lz.z, lz.w};
+          const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
+                      chz[4] = {hz.x, hz.y, hz.z, hz.w};
+          const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
+          float key[4];
+          int   o[4];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
+            // an empty slot (child 0, count 0: node 0 is the root, never a child) is never pushed
+            const bool  nk = __any_sync(FULL, dk <= best) && (cref[k] | ccnt[k]) != 0u;
+            // uniform ordering key; children nobody needs get -1 and are not pushed
+            key[k] = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
+            o[k]   = k;
+          }
+          // sort (key, slot) pairs by key, descending (far first): a 5-comparator network on
+          // registers (constant indices only, so nothing spills to local memory)
+#define EBG_CSWAP(i, j)                                                                                               \
+  if (key[i] < key[j]) {                                                                                              \
+    const float tk = key[i];                                                                                          \
+    key[i]         = key[j];                                                                                          \
+    key[j]         = tk;                                                                                              \
+    const int to   = o[i];                                                                                            \
+    o[i]           = o[j];                                                                                            \
+    o[j]           = to;                                                                                              \
+  }
+          EBG_CSWAP(0, 1);
+          EBG_CSWAP(2, 3);
+          EBG_CSWAP(0, 2);
+          EBG_CSWAP(1, 3);
+          EBG_CSWAP(1, 2);
+#undef EBG_CSWAP
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            if (key[j] >= 0.f) {
+              if (sp >= EBG_STACK_DEPTH) {
+                err |= ST_STACK;
+                break;
+              }
+              const int k = o[j];
+              if (lane == 0) {
+                stk[2 * sp] = make_float4(sel4(clx, k), sel4(cly, k), sel4(clz, k), __uint_as_float(sel4u(cref, k)));
+                stk[2 * sp + 1] =
+                  make_float4(sel4(chx, k), sel4(chy, k), sel4(chz, k), __uint_as_float(sel4u(ccnt, k)));
+              }
+              sp++;
+            }
+          }
+          __syncwarp();
+          if (err) {
+            break;
+          }
+        }
+      }
+}
+
+} // namespace ebg
+
+#endif

@@ -34,7 +34,8 @@ typedef enum ebg_status
   EBG_ERR_INVALID    = 1, /* bad argument (null pointer, negative size, k out of range, ...) */
   EBG_ERR_CUDA       = 2, /* a CUDA runtime call failed */
   EBG_ERR_NO_MEMORY  = 3, /* device or host allocation failed */
-  EBG_ERR_TRAVERSAL  = 4, /* a kernel hit its stack-depth or iteration bound and stopped early */
+  EBG_ERR_TRAVERSAL  = 4, /* a kernel hit its stack-depth or iteration bound and stopped early,
+                             or (device entry points) a query coordinate was not finite */
   EBG_ERR_NOT_FOUND  = 5, /* the library or a device could not be found */
   EBG_ERR_TOO_LARGE  = 6  /* input exceeds a documented limit */
 } ebg_status;
@@ -79,6 +80,12 @@ typedef struct ebg_query_opts
   int32_t            reserved;
   ebg_phase_timings* timings;         /* non-NULL: record events per phase; the call then
                                          synchronises the stream and fills this struct */
+  const float*       radius_hint;     /* device, one per point (caller order): an upper bound on
+                                         |d| (e.g. a coarser level's distance plus the cell
+                                         diagonal) that seeds the pruning radius; <= 0 or non-finite
+                                         = no hint for that point.  A hint below the true |d| only
+                                         costs a second traversal of that point.  Ignored when
+                                         seed is set. */
 } ebg_query_opts;
 
 /* Mesh summary. */
@@ -236,6 +243,41 @@ ebg_status ebg_cloud_knn_host(const ebg_cloud*      cloud,
                               void*                 stream);
 /* Synchronises stream and reports a device-side traversal error of earlier k-NN calls. */
 ebg_status ebg_cloud_check_status(const ebg_cloud* cloud, void* stream);
+
+/* ---- CSG union: BVHUnionIF (CSG.hpp:401-468) ------------------------------------------------
+ *
+ * ebg_scene_create replaces BVHUnion<T, ImplicitFunction<T>, AABB, K>(prims, bvs) (CSG.hpp:99-101,
+ * CSGImplem.hpp:51-95) over SphereSDF objects (AnalyticDistanceFunctions.hpp:137-246; spheres[4i..]
+ * = centre xyz, radius) and instances Translate(Rotate(mesh, angle, axis), t) of existing mesh
+ * handles (TransformImplem.hpp:38-47,152-225; poses[5i..] = angle in degrees, axis 0/1/2, tx, ty,
+ * tz).  The object hierarchy is a 4-wide SAH BVH with opts->leaf_size objects per leaf (default 3,
+ * the reference's "fewer than K").  Mesh handles must outlive the scene and share its device. */
+ebg_status ebg_scene_create(int64_t                num_spheres,
+                            const double*          spheres,
+                            int64_t                num_meshes,
+                            const ebg_mesh* const* meshes,
+                            const double*          poses,
+                            const ebg_build_opts*  opts,
+                            ebg_scene**            out);
+ebg_status ebg_scene_destroy(ebg_scene* scene);
+int64_t    ebg_scene_num_objects(const ebg_scene* scene);
+/* BVHUnionIF::value (CSGImplem.hpp:465-501) at n device points: min over the objects, the object
+ * BVH pruned with max(0, best)^2.  One persistent launch for the whole array, so many query batches
+ * of uneven length go in one call when concatenated.  Asynchronous on stream; only opts->no_sort is
+ * used. */
+ebg_status ebg_scene_value(const ebg_scene*      scene,
+                           const float*          points_dev,
+                           int64_t               n,
+                           float*                out_dev,
+                           const ebg_query_opts* opts,
+                           void*                 stream);
+ebg_status ebg_scene_value_host(const ebg_scene*      scene,
+                                const float*          points_host,
+                                int64_t               n,
+                                float*                out_host,
+                                const ebg_query_opts* opts,
+                                void*                 stream);
+ebg_status ebg_scene_check_status(const ebg_scene* scene, void* stream);
 
 /* ---- learned pruning radius (no counterpart in the reference) --------------------------------
  *
