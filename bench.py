@@ -44,6 +44,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["mesh", "knn", "csg"], default="mesh",
+                    help="mesh: the headline mesh-SDF configuration; knn: 16M-point cloud, 4M queries, k=1 and 8; "
+                         "csg: 4,096 spheres + 256 posed meshes, 2,048 query batches in one launch")
+    ap.add_argument("--knn-points", type=int, default=16 * 1024 * 1024)
+    ap.add_argument("--knn-queries", type=int, default=4 * 1024 * 1024)
+    ap.add_argument("--csg-batches", type=int, default=2048)
+    ap.add_argument("--csg-meshes", type=int, default=256)
+    ap.add_argument("--csg-spheres", type=int, default=4096)
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--band-points", type=int, default=16 * 1024 * 1024)
@@ -454,6 +462,105 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+def device_timed(fn, steps, warmup, torch, dev, stream):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / steps
+
+
+def run_knn(args, rank, world, local_rank):
+    """Point-cloud k-NN (16M points: half uniform, half in 64 anisotropic clusters; 4M uniform
+    queries; k = 1 and 8)."""
+    import torch
+
+    from ebgeometry_b200 import PointCloudBVH
+    from ebgeometry_b200 import workloads as W
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    pts = W.point_cloud(args.knn_points, 1)
+    q = W.uniform_points(args.knn_queries, 2, 0.0, 1.0)
+    pd = torch.from_numpy(pts).to(dev)
+    qd = torch.from_numpy(q).to(dev)
+    t0 = time.time()
+    cloud = PointCloudBVH(pd)
+    torch.cuda.synchronize(dev)
+    build_ms = (time.time() - t0) * 1e3
+    build_dev = device_timed(lambda: PointCloudBVH(pd), 2, 1, torch, dev, stream)
+    res = {}
+    for k in (1, 8):
+        ms = device_timed(lambda: cloud.knn(qd, k), args.steps, args.warmup, torch, dev, stream)
+        res[f"k{k}"] = {"ms_per_step": ms, "value": q.shape[0] * world / (ms * 1e-3)}
+    if rank != 0:
+        return 0
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            R = oracle.ref()
+            t0 = time.time()
+            rc = R.cloud(pts)
+            tb = time.time() - t0
+            ns = 200000
+            sq = q[:ns]
+            cpu = {}
+            for k in (1, 8):
+                t0 = time.perf_counter()
+                ri, rd = rc.knn(sq, k, lex=False)
+                dt = time.perf_counter() - t0
+                gi, gd = cloud.knn(torch.from_numpy(sq).to(dev), k)
+                cpu[f"k{k}"] = {"value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
+                                "sample": f"first {ns} queries, reference PointCloudBVH<float> closestPoints "
+                                          f"(build {tb:.1f}s)",
+                                "d2_equal_fraction": float(np.mean(gd.cpu().numpy() == rd))}
+    print(json.dumps({"metric": "k-NN queries/s on 1 B200", "workload": "knn", "n_gpus": world,
+                      "config": {"points": int(pts.shape[0]), "queries": int(q.shape[0]), "leaf": 16},
+                      "build_ms_device": build_dev, "results": res, "cpu_baseline": cpu}), flush=True)
+    return 0
+
+
+def run_csg(args, rank, world, local_rank):
+    """Batched CSG union: spheres + posed displaced icospheres (levels 3-7), batches of log-uniform
+    length 1k-1M concatenated into one call (one persistent launch)."""
+    import torch
+
+    from ebgeometry_b200 import BVHUnion, TriMeshSDF
+    from ebgeometry_b200 import workloads as W
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.time()
+    sc = W.csg_scene(11, n_spheres=args.csg_spheres, n_meshes=args.csg_meshes)
+    tms = [TriMeshSDF(v, f, device=local_rank) for v, f in sc["meshes"]]
+    scene = BVHUnion(sc["spheres"], tms, sc["poses"], device=local_rank)
+    t_build = time.time() - t0
+    rng = np.random.default_rng(12)
+    lens = np.exp(rng.uniform(np.log(1e3), np.log(1e6), args.csg_batches)).astype(np.int64)
+    n = int(lens.sum())
+    lo = np.minimum(sc["spheres"][:, :3].min(0), sc["poses"][:, 2:5].min(0)) - 0.2
+    hi = np.maximum(sc["spheres"][:, :3].max(0), sc["poses"][:, 2:5].max(0)) + 0.2
+    pts = (rng.random((n, 3), dtype=np.float32) * (hi - lo).astype(np.float32) + lo.astype(np.float32))
+    pd = torch.from_numpy(pts).to(dev)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    ms = device_timed(lambda: scene.values(pd, out=out), args.steps, args.warmup, torch, dev, stream)
+    scene.check_status()
+    if rank != 0:
+        return 0
+    ntris = int(sum(f.shape[0] for _, f in sc["meshes"]))
+    print(json.dumps({"metric": "CSG union queries/s on 1 B200", "workload": "csg", "n_gpus": world,
+                      "value": n * world / (ms * 1e-3), "ms_per_step": ms,
+                      "config": {"spheres": args.csg_spheres, "meshes": args.csg_meshes, "mesh_triangles": ntris,
+                                 "batches": args.csg_batches, "points": n, "build_s": t_build}}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -469,6 +576,10 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, rank, world)
+        if args.workload == "knn":
+            return run_knn(args, rank, world, local_rank)
+        if args.workload == "csg":
+            return run_csg(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)
     finally:
         if world > 1 and args.impl == "ours":
