@@ -1,0 +1,180 @@
+// Allocation-free variant of the batched mesh signed-distance query.
+//
+// Who needs it: callers that cannot let a library allocate device memory.  The reference's main
+// callers are adaptive-mesh codes (AMReX, Chombo) that evaluate value(point) while they build their
+// embedded boundaries; AMReX reserves most of the GPU's memory for its own arena when it starts, so
+// a cudaMalloc (or a stream-ordered allocation) issued by a library it calls can fail for lack of
+// memory, and codes with their own memory managers or hard latency budgets forbid allocations in
+// the query loop altogether.  ebg_mesh_signed_distance takes its per-call workspace (sort keys,
+// the point order, the near-surface list, counters) from the device's memory pool; this entry point
+// takes it from one array of fixed size compiled into the library instead.
+//
+// The scratch array below is a file-scope __device__ variable: every GPU that loads the library
+// holds its EBG_NOALLOC_SCRATCH_BYTES until the process exits.  In host code the name
+// g_noallocScratch is only a stand-in for the device variable, not a device address; the address a
+// kernel may use is obtained once per device with cudaGetSymbolAddress (with that device current)
+// and cached.  The first call on a device performs that set-up, so make it before capturing a CUDA
+// graph on that device.  All calls on a device share the one array and it keeps the contents of the
+// last call: the counters are cleared at the start of every call, and two calls whose work overlaps
+// on the GPU (different streams, or different threads without ordering) race on it and must be
+// serialised by the caller.  The call itself allocates nothing: no cudaMalloc, cudaMallocAsync,
+// cudaFree or allocating library routine (the radix sort is given its temporary storage from the
+// same array).
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include "capi_common.h"
+#include "capi_internal.h"
+#include "ebg_device.cuh"
+#include "mesh_kernels.h"
+#include "seed_kernels.h"
+
+// Largest point count one allocation-free call accepts, and the scratch that covers it: four
+// uint32 arrays for the Morton ordering, the near-surface list (index + FP32 distance), one radius
+// per 32-point packet, two counters, and the radix sort's temporary storage (under 5 MiB at this
+// size on sm_100a; checked at every call).
+#define EBG_NOALLOC_MAX_POINTS (int64_t(1) << 19)
+#define EBG_NOALLOC_SCRATCH_BYTES (size_t(24) << 20)
+
+static __device__ __align__(256) unsigned char g_noallocScratch[EBG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex    g_mutex;
+void*         g_scratch[kMaxDevices] = {nullptr};
+
+// Device address of the scratch array on `device` (the current device), looked up once.
+ebg_status scratchAddress(int device, unsigned char** out)
+{
+  if (device < 0 || device >= kMaxDevices) {
+    return ebg::setError(EBG_ERR_NOT_FOUND, "device ordinal out of range for the allocation-free entry point");
+  }
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (g_scratch[device] == nullptr) {
+    void*             p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noallocScratch);
+    if (e != cudaSuccess || p == nullptr) {
+      return ebg::setError(EBG_ERR_CUDA, std::string("cannot resolve the scratch array's device address: ") +
+                                            cudaGetErrorString(e));
+    }
+    g_scratch[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_scratch[device]);
+  return EBG_OK;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+} // namespace
+
+extern "C" {
+
+ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
+                                            const float*          points_dev,
+                                            int64_t               n,
+                                            float*                dist_dev,
+                                            int32_t*              closest_tri_dev,
+                                            const ebg_query_opts* opts,
+                                            void*                 stream)
+{
+  using namespace ebg;
+  if (m == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n > EBG_NOALLOC_MAX_POINTS) {
+    return setError(EBG_ERR_TOO_LARGE, "ebg_mesh_signed_distance_noalloc accepts at most " +
+                                         std::to_string(EBG_NOALLOC_MAX_POINTS) + " points per call (got " +
+                                         std::to_string(n) + "); split the batch or use ebg_mesh_signed_distance");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  const ebg_seed* seed = opts ? opts->seed : nullptr;
+  if (seed && seed->device != m->device) {
+    return setError(EBG_ERR_INVALID, "seed model lives on another device than the mesh");
+  }
+  DeviceGuard guard;
+  if (cudaSetDevice(m->device) != cudaSuccess) {
+    return setError(EBG_ERR_NOT_FOUND, "cannot select the mesh's device");
+  }
+  unsigned char* base = nullptr;
+  ebg_status     rc   = scratchAddress(m->device, &base);
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  cudaStream_t s    = static_cast<cudaStream_t>(stream);
+  const bool   sort = !(opts && opts->no_sort);
+  const bool   b64  = !(opts && opts->no_fp64_band);
+  const int    wpb  = (opts && opts->warps_per_block > 0) ? opts->warps_per_block : 4;
+  const double band = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
+
+  // carve the scratch
+  const size_t u32n = align256(size_t(n) * sizeof(uint32_t));
+  size_t       off  = 0;
+  auto         take = [&](size_t bytes) {
+    unsigned char* p = base + off;
+    off += align256(bytes);
+    return p;
+  };
+  auto* counters = reinterpret_cast<unsigned long long*>(take(2 * sizeof(unsigned long long)));
+  auto* keysIn   = reinterpret_cast<uint32_t*>(take(u32n));
+  auto* keysOut  = reinterpret_cast<uint32_t*>(take(u32n));
+  auto* idsIn    = reinterpret_cast<uint32_t*>(take(u32n));
+  auto* order    = reinterpret_cast<uint32_t*>(take(u32n));
+  auto* bandList = reinterpret_cast<uint32_t*>(take(u32n));
+  auto* bandD    = reinterpret_cast<float*>(take(u32n));
+  auto* seedR    = reinterpret_cast<float*>(take(size_t((n + 31) / 32) * sizeof(float)));
+  size_t sortBytes = 0;
+  if (sort) {
+    cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, keysIn, keysOut, idsIn, order, int(n), 0, 30, s);
+  }
+  void* sortTemp = take(sortBytes);
+  if (off > EBG_NOALLOC_SCRATCH_BYTES) {
+    return setError(EBG_ERR_TOO_LARGE, "allocation-free scratch too small for this call (" + std::to_string(off) +
+                                         " of " + std::to_string(size_t(EBG_NOALLOC_SCRATCH_BYTES)) + " bytes)");
+  }
+
+  // the array keeps the previous call's contents: clear what must start at zero
+  cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s);
+  if (sort) {
+    launchQueryKeys(points_dev, n, m->view.morton_lo, m->view.morton_scale, keysIn, idsIn, s);
+    if (cub::DeviceRadixSort::SortPairs(sortTemp, sortBytes, keysIn, keysOut, idsIn, order, int(n), 0, 30, s) !=
+        cudaSuccess) {
+      return setError(EBG_ERR_CUDA, "query sort failed");
+    }
+  }
+  if (seed && launchSeedPackets(seed->view, points_dev, sort ? order : nullptr, n, seedR, m->numSms, s) !=
+                cudaSuccess) {
+    return setError(EBG_ERR_CUDA, "seed inference launch failed");
+  }
+  MeshQueryArgs a{};
+  a.mesh       = m->view;
+  a.points     = points_dev;
+  a.order      = sort ? order : nullptr;
+  a.seed_r     = seed ? seedR : nullptr;
+  a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
+  a.n          = n;
+  a.out_d      = dist_dev;
+  a.out_tri    = closest_tri_dev;
+  a.band       = float(band);
+  a.band_list  = b64 ? bandList : nullptr;
+  a.band_count = reinterpret_cast<uint32_t*>(counters + 1);
+  a.band_d32   = bandD;
+  a.work       = counters;
+  a.status     = m->dStatus;
+  a.stats      = nullptr;
+  if (launchMeshSdf32(a, wpb, m->numSms, s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  if (b64 && launchMeshBand64(a, float(2e-6 * m->info.diagonal) + 1e-30f, m->numSms, s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, "band launch failed");
+  }
+  return EBG_OK;
+}
+
+} // extern "C"

@@ -189,6 +189,24 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       mesh,
                                          const ebg_query_opts* opts,
                                          void*                 stream);
 
+/* The same batched query WITHOUT ANY DEVICE ALLOCATION (no counterpart in the reference).  For
+ * callers that cannot let a library allocate: AMR codes such as AMReX reserve most of the GPU's memory
+ * for their own arena at start-up, so a library's cudaMalloc or stream-ordered allocation can fail
+ * inside their embedded-boundary loop, and other codes forbid allocations there for latency.  The
+ * per-call workspace comes from a fixed 24 MiB array compiled into the library (held on every device
+ * that loads it until exit) instead of the memory pool.  Limits: n <= 524,288 points per call (larger
+ * n returns EBG_ERR_TOO_LARGE); opts->timings is ignored.  The first call on a device resolves the
+ * array's address there; make it before capturing a CUDA graph.  All calls on a device share the
+ * array, so calls whose work overlaps on the GPU (different streams) race and must be serialised.
+ * Results are those of ebg_mesh_signed_distance. */
+ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       mesh,
+                                            const float*          points_dev,
+                                            int64_t               n,
+                                            float*                dist_dev,
+                                            int32_t*              closest_tri_dev,
+                                            const ebg_query_opts* opts,
+                                            void*                 stream);
+
 /* Synchronous variant that also returns traversal counters (slower: counts with atomics). */
 ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       mesh,
                                           const float*          points_dev,
