@@ -105,10 +105,10 @@ class TriMeshSDF:
         return fn, vn, en
 
     @staticmethod
-    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None):
+    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None, occupancy=None):
         return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
                                seed.handle if seed is not None else None,
-                               int(warps_per_block or 0), 0,
+                               int(warps_per_block or 0), int(occupancy or 0),
                                C.pointer(timings) if timings is not None else None,
                                radius_hint.data_ptr() if radius_hint is not None else None)
 
@@ -125,14 +125,14 @@ class TriMeshSDF:
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
                         fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None,
-                        radius_hint=None):
+                        radius_hint=None, occupancy=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
         times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
         radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
         float32 tensor of per-point upper bounds on |d| that seed the bound the same way."""
-        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint)
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy)
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
             n = p.shape[0]

@@ -24,7 +24,7 @@ class PhaseTimings(C.Structure):
 
 class QueryOpts(C.Structure):
     _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
-                ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("reserved", C.c_int32),
+                ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("occupancy", C.c_int32),
                 ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p)]
 
 
@@ -52,7 +52,8 @@ class MeshInfo(C.Structure):
 class QueryStats(C.Structure):
     _fields_ = [("nodes_visited", C.c_int64), ("leaves_visited", C.c_int64),
                 ("triangles_tested", C.c_int64), ("band_queries", C.c_int64),
-                ("seed_fallbacks", C.c_int64)]
+                ("seed_fallbacks", C.c_int64), ("packets", C.c_int64), ("packet_pops", C.c_int64),
+                ("packet_nodes", C.c_int64), ("packet_leaves", C.c_int64), ("packet_triangles", C.c_int64)]
 
 
 EBG_OK = 0

@@ -493,7 +493,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.work       = counters;
   a.status     = m->dStatus;
   a.stats      = statsDev;
-  if (launchMeshSdf32(a, wpb, m->numSms, s) != cudaSuccess) {
+  if (launchMeshSdf32(a, wpb, m->numSms, s, opts ? opts->occupancy : 0) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
   }
   if (tm) {
@@ -702,14 +702,14 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   ebg_status   rc;
-  unsigned long long host[5] = {0, 0, 0, 0, 0};
+  unsigned long long host[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   {
     Workspace           ws(s);
-    unsigned long long* dev = ws.get<unsigned long long>(5);
+    unsigned long long* dev = ws.get<unsigned long long>(10);
     if (!ws.ok) {
       return setError(EBG_ERR_NO_MEMORY, "stats buffer");
     }
-    cudaMemsetAsync(dev, 0, 5 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(dev, 0, 10 * sizeof(unsigned long long), s);
     rc = meshQuery(m, points_dev, n, dist_dev, nullptr, opts, dev, s);
     if (rc == EBG_OK) {
       cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, s);
@@ -726,6 +726,11 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   stats->triangles_tested = int64_t(host[2]);
   stats->band_queries     = int64_t(host[3] & 0xffffffffull);
   stats->seed_fallbacks   = int64_t(host[4]);
+  stats->packets          = int64_t(host[5]);
+  stats->packet_pops      = int64_t(host[6]);
+  stats->packet_nodes     = int64_t(host[7]);
+  stats->packet_leaves    = int64_t(host[8]);
+  stats->packet_triangles = int64_t(host[9]);
   return ebg_check_status(m, stream);
 }
 

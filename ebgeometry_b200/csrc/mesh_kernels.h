@@ -25,15 +25,15 @@ struct MeshQueryArgs
   float*             band_d32;   // FP32 distance of each band entry
   unsigned long long* work;      // packet counter (zeroed before the launch)
   int*               status;     // device status word (ST_* bits)
-  unsigned long long* stats;     // 5 counters (nullable)
+  unsigned long long* stats;     // 10 counters (nullable): 5 per query, 5 per packet
 };
 
 // Morton keys of the query points (30 bits) and the identity permutation.
 void launchQueryKeys(const float* points, int64_t n, const float* lo, const float* scale, uint32_t* keys,
                      uint32_t* ids, cudaStream_t s);
 
-// FP32 packet traversal.  warpsPerBlock in {1,2,4,8}.
-cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int warpsPerBlock, int numSms, cudaStream_t s);
+// FP32 packet traversal.  warpsPerBlock in {1,2,4,8}; occupancy 0..3 (see ebg_query_opts).
+cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int warpsPerBlock, int numSms, cudaStream_t s, int occupancy = 0);
 
 // FP64 re-evaluation of the band list (reads band_count on the device).
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s);

@@ -35,8 +35,17 @@ namespace ebg {
 namespace {
 
 // SEED: 0 plain, 1 learned radius per packet (+ distance to the centroid), 2 per-query radius hint
-template <bool STATS, int SEED>
-__global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
+// OCC selects the register budget: 0 = 256-thread blocks, compiler's choice; 1..3 = 128-thread
+// blocks with 8, 10, 12 resident blocks per SM (at most 64, 51, 42 registers).
+template <int OCC>
+struct Bounds
+{
+  static constexpr int threads = OCC == 0 ? 256 : 128;
+  static constexpr int blocks  = OCC == 0 ? 1 : (OCC == 1 ? 8 : (OCC == 2 ? 10 : 12));
+};
+
+template <bool STATS, int SEED, int OCC>
+__global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMeshSdf32(const MeshQueryArgs a)
 {
   extern __shared__ float4 smem[];
   const int     lane = threadIdx.x & 31;
@@ -82,6 +91,7 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
     uint32_t iters = 0;
     int      err   = 0;
     uint32_t cNode = 0, cLeaf = 0, cTri = 0, cFall = 0;
+    uint32_t pPops = 0, pNode = 0, pLeaf = 0, pTri = 0;
 
 #pragma unroll 1
     for (int pass = 0; pass < (SEEDED ? 2 : 1); pass++) {
@@ -100,6 +110,10 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
       cNode += tc.node;
       cLeaf += tc.leaf;
       cTri += tc.tri;
+      pPops += tc.pops;
+      pNode += tc.pnode;
+      pLeaf += tc.pleaf;
+      pTri += tc.ptri;
       if (err) {
         break;
       }
@@ -142,6 +156,13 @@ __global__ void __launch_bounds__(256) kMeshSdf32(const MeshQueryArgs a)
       atomicAdd(a.stats + 1, (unsigned long long)cLeaf);
       atomicAdd(a.stats + 2, (unsigned long long)cTri);
       atomicAdd(a.stats + 4, (unsigned long long)cFall);
+      if (lane == 0) {
+        atomicAdd(a.stats + 5, 1ull);
+        atomicAdd(a.stats + 6, (unsigned long long)pPops);
+        atomicAdd(a.stats + 7, (unsigned long long)pNode);
+        atomicAdd(a.stats + 8, (unsigned long long)pLeaf);
+        atomicAdd(a.stats + 9, (unsigned long long)pTri);
+      }
     }
   }
 }
@@ -162,13 +183,16 @@ __global__ void kQueryKeys(const float* __restrict__ pts, int64_t n, float lx, f
   ids[i]  = uint32_t(i);
 }
 
-template <bool STATS, int SEED>
+template <bool STATS, int SEED, int OCC>
 cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
+  if (OCC != 0 && wpb > 4) {
+    wpb = 4;
+  }
   const int    threads = 32 * wpb;
   const size_t smem    = size_t(wpb) * 2 * EBG_STACK_DEPTH * sizeof(float4);
   int          perSm   = 0;
-  cudaError_t  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED>, threads, smem);
+  cudaError_t  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC>, threads, smem);
   if (e != cudaSuccess) {
     return e;
   }
@@ -177,7 +201,7 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
   int64_t       grid  = int64_t(numSms) * perSm;
   grid                = grid < need ? grid : need;
   grid                = grid < 1 ? 1 : grid;
-  kMeshSdf32<STATS, SEED><<<unsigned(grid), threads, smem, s>>>(a);
+  kMeshSdf32<STATS, SEED, OCC><<<unsigned(grid), threads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -192,19 +216,35 @@ void launchQueryKeys(const float* points, int64_t n, const float* lo, const floa
                                                   ids);
 }
 
-cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
+template <int SEED, int OCC>
+cudaError_t launchStats(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
+{
+  return a.stats != nullptr ? launchOne<true, SEED, OCC>(a, wpb, numSms, s) : launchOne<false, SEED, OCC>(a, wpb, numSms, s);
+}
+
+template <int OCC>
+cudaError_t launchSeed(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
+{
+  const int mode = a.seed_r != nullptr ? 1 : (a.hint != nullptr ? 2 : 0);
+  return mode == 1 ? launchStats<1, OCC>(a, wpb, numSms, s)
+                   : (mode == 2 ? launchStats<2, OCC>(a, wpb, numSms, s) : launchStats<0, OCC>(a, wpb, numSms, s));
+}
+
+cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s, int occupancy)
 {
   if (wpb != 1 && wpb != 2 && wpb != 4 && wpb != 8) {
     wpb = 4;
   }
-  const bool stats = a.stats != nullptr;
-  const int  mode  = a.seed_r != nullptr ? 1 : (a.hint != nullptr ? 2 : 0);
-  if (stats) {
-    return mode == 1 ? launchOne<true, 1>(a, wpb, numSms, s)
-                     : (mode == 2 ? launchOne<true, 2>(a, wpb, numSms, s) : launchOne<true, 0>(a, wpb, numSms, s));
+  switch (occupancy) {
+  case 1:
+    return launchSeed<1>(a, wpb, numSms, s);
+  case 2:
+    return launchSeed<2>(a, wpb, numSms, s);
+  case 3:
+    return launchSeed<3>(a, wpb, numSms, s);
+  default:
+    return launchSeed<0>(a, wpb, numSms, s);
   }
-  return mode == 1 ? launchOne<false, 1>(a, wpb, numSms, s)
-                   : (mode == 2 ? launchOne<false, 2>(a, wpb, numSms, s) : launchOne<false, 0>(a, wpb, numSms, s));
 }
 
 } // namespace ebg

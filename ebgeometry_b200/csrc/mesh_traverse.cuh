@@ -135,7 +135,8 @@ __device__ __forceinline__ float signedFromWinner(const EbgMeshView& m, uint32_t
 
 struct TraversalCounters
 {
-  uint32_t node = 0, leaf = 0, tri = 0, fall = 0;
+  uint32_t node = 0, leaf = 0, tri = 0, fall = 0;      // per lane: what this query needed
+  uint32_t pops = 0, pnode = 0, pleaf = 0, ptri = 0;   // per packet: what the warp executed
 };
 
 // One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
@@ -162,6 +163,9 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           break;
         }
         --sp;
+        if (STATS) {
+          cnt_.pops++;
+        }
         const float4 A    = stk[2 * sp];
         const float4 B    = stk[2 * sp + 1];
         const float  d2   = boxDist2(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
@@ -183,6 +187,10 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             cnt_.leaf++;
             cnt_.tri += cnt;
           }
+          if (STATS) {
+            cnt_.pleaf++;
+            cnt_.ptri += cnt;
+          }
 #pragma unroll 1
           for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
             const float4* h = reinterpret_cast<const float4*>(m.hot + tt);
@@ -199,6 +207,9 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
         else {
           if (STATS && need) {
             cnt_.node++;
+          }
+          if (STATS) {
+            cnt_.pnode++;
           }
           const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
           const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
@@ -217,8 +228,10 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
             // an empty slot (child 0, count 0: node 0 is the root, never a child) is never pushed
             const bool  nk = __any_sync(FULL, dk <= best) && (cref[k] | ccnt[k]) != 0u;
-            // uniform ordering key; children nobody needs get -1 and are not pushed
-            key[k] = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
+            // uniform ordering key: the child's smallest distance over the packet's lanes (one
+            // warp min-reduction; non-negative floats order like their bit patterns); children
+            // nobody needs get -1 and are not pushed
+            key[k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
             o[k]   = k;
           }
           // sort (key, slot) pairs by key, descending (far first): a 5-comparator network on

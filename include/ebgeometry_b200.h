@@ -77,7 +77,9 @@ typedef struct ebg_query_opts
   int32_t            no_fp64_band;    /* 1: skip the FP64 near-surface re-evaluation */
   const ebg_seed*    seed;            /* learned pruning-radius model (NULL = plain traversal) */
   int32_t            warps_per_block; /* 0 = tuned default */
-  int32_t            reserved;
+  int32_t            occupancy;       /* traversal register budget: 0 = default; 1, 2, 3 = at most
+                                         64, 51, 42 registers per thread (8, 10, 12 blocks of 128
+                                         threads per SM; warps_per_block <= 4) */
   ebg_phase_timings* timings;         /* non-NULL: record events per phase; the call then
                                          synchronises the stream and fills this struct */
   const float*       radius_hint;     /* device, one per point (caller order): an upper bound on
@@ -111,6 +113,12 @@ typedef struct ebg_query_stats
   int64_t triangles_tested;  /* point-triangle tests, per query */
   int64_t band_queries;      /* queries re-evaluated in FP64 */
   int64_t seed_fallbacks;    /* seeded queries whose predicted radius held no triangle */
+  /* per 32-query packet (what the warp actually executes: the union over its lanes) */
+  int64_t packets;
+  int64_t packet_pops;       /* stack entries popped */
+  int64_t packet_nodes;      /* interior nodes whose children were tested */
+  int64_t packet_leaves;     /* leaves whose triangles were tested */
+  int64_t packet_triangles;  /* point-triangle tests executed by the warp */
 } ebg_query_stats;
 
 const char* ebg_last_error(void);
