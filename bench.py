@@ -34,6 +34,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from ebgeometry_b200.ranks import max_over_ranks  # noqa: E402  (pure Python, no library load)
+
 METRIC = "SDF queries/s on 1 B200: learned-seeded vs plain GPU BVH at equal accuracy"
 UNIT = "queries/s"
 
@@ -260,11 +262,7 @@ def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, di
     e1.record(stream)
     torch.cuda.synchronize(dev)
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dev)
     mesh.check_status()
     return ms / steps, np.array(tms), ck
 
@@ -369,11 +367,7 @@ def run_ours(args, rank, world, local_rank):
         host_call()
     h1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = h0.elapsed_time(h1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(h0.elapsed_time(h1) / e2e_steps, dev)
     same = bool(torch.equal(oh, out.cpu()))
 
     if rank != 0:

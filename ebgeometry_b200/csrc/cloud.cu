@@ -221,8 +221,6 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
     const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
     const float    px = __ldg(a.queries + 3 * size_t(id)), py = __ldg(a.queries + 3 * size_t(id) + 1),
                 pz = __ldg(a.queries + 3 * size_t(id) + 2);
-    const float cx = warpSum(px) * (1.f / 32.f), cy = warpSum(py) * (1.f / 32.f), cz = warpSum(pz) * (1.f / 32.f);
-
     float    kd[K];
     uint32_t ki[K];
 #pragma unroll
@@ -285,55 +283,45 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
         const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
                     chz[4] = {hz.x, hz.y, hz.z, hz.w};
         const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
-        float          key[4];
-        int            o[4];
+        float key[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const float dk = boxD2exact(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
           // an empty slot (child 0 = the root, count 0) has an infinite box distance, which an
           // unfilled k-best list (bound +inf) would admit: it is never pushed
-          const bool  nk = __any_sync(FULL, dk <= bound) && (cref[k] | ccnt[k]) != 0u;
-          key[k]         = nk ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], cx, cy, cz) : -1.f;
-          o[k]           = k;
+          const bool nk = __any_sync(FULL, dk <= bound) && (cref[k] | ccnt[k]) != 0u;
+          // ordering key: the child's smallest distance over the lanes (finite: nk excludes empty)
+          key[k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
         }
-#define EBG_CSWAP(i, j)                                                                                               \
-  if (key[i] < key[j]) {                                                                                              \
-    const float tk = key[i];                                                                                          \
-    key[i]         = key[j];                                                                                          \
-    key[j]         = tk;                                                                                              \
-    const int to   = o[i];                                                                                            \
-    o[i]           = o[j];                                                                                            \
-    o[j]           = to;                                                                                              \
-  }
-        EBG_CSWAP(0, 1);
-        EBG_CSWAP(2, 3);
-        EBG_CSWAP(0, 2);
-        EBG_CSWAP(1, 3);
-        EBG_CSWAP(1, 2);
-#undef EBG_CSWAP
+        const int np = int(key[0] >= 0.f) + int(key[1] >= 0.f) + int(key[2] >= 0.f) + int(key[3] >= 0.f);
+        if (sp + np > EBG_STACK_DEPTH) {
+          err |= ST_STACK;
+          break;
+        }
+        // lane k (< 4) writes child k into its slot, farther children deeper (ties by slot index)
+        if (lane < 4) {
+          const float kk = lane == 0 ? key[0] : (lane == 1 ? key[1] : (lane == 2 ? key[2] : key[3]));
+          if (kk >= 0.f) {
+            int rank = 0;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          if (key[j] >= 0.f) {
-            if (sp >= EBG_STACK_DEPTH) {
-              err |= ST_STACK;
-              break;
+            for (int j = 0; j < 4; j++) {
+              rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
             }
-            const int k = o[j];
-            if (lane == 0) {
-              const float lxk = k == 0 ? clx[0] : (k == 1 ? clx[1] : (k == 2 ? clx[2] : clx[3]));
-              const float lyk = k == 0 ? cly[0] : (k == 1 ? cly[1] : (k == 2 ? cly[2] : cly[3]));
-              const float lzk = k == 0 ? clz[0] : (k == 1 ? clz[1] : (k == 2 ? clz[2] : clz[3]));
-              const float hxk = k == 0 ? chx[0] : (k == 1 ? chx[1] : (k == 2 ? chx[2] : chx[3]));
-              const float hyk = k == 0 ? chy[0] : (k == 1 ? chy[1] : (k == 2 ? chy[2] : chy[3]));
-              const float hzk = k == 0 ? chz[0] : (k == 1 ? chz[1] : (k == 2 ? chz[2] : chz[3]));
-              const uint32_t rk = k == 0 ? cref[0] : (k == 1 ? cref[1] : (k == 2 ? cref[2] : cref[3]));
-              const uint32_t nk = k == 0 ? ccnt[0] : (k == 1 ? ccnt[1] : (k == 2 ? ccnt[2] : ccnt[3]));
-              stk[2 * sp]     = make_float4(lxk, lyk, lzk, __uint_as_float(rk));
-              stk[2 * sp + 1] = make_float4(hxk, hyk, hzk, __uint_as_float(nk));
-            }
-            sp++;
+            const int k   = lane;
+            float4*   e   = stk + 2 * (sp + rank);
+            const float lxk = k == 0 ? clx[0] : (k == 1 ? clx[1] : (k == 2 ? clx[2] : clx[3]));
+            const float lyk = k == 0 ? cly[0] : (k == 1 ? cly[1] : (k == 2 ? cly[2] : cly[3]));
+            const float lzk = k == 0 ? clz[0] : (k == 1 ? clz[1] : (k == 2 ? clz[2] : clz[3]));
+            const float hxk = k == 0 ? chx[0] : (k == 1 ? chx[1] : (k == 2 ? chx[2] : chx[3]));
+            const float hyk = k == 0 ? chy[0] : (k == 1 ? chy[1] : (k == 2 ? chy[2] : chy[3]));
+            const float hzk = k == 0 ? chz[0] : (k == 1 ? chz[1] : (k == 2 ? chz[2] : chz[3]));
+            const uint32_t rk = k == 0 ? cref[0] : (k == 1 ? cref[1] : (k == 2 ? cref[2] : cref[3]));
+            const uint32_t nn = k == 0 ? ccnt[0] : (k == 1 ? ccnt[1] : (k == 2 ? ccnt[2] : ccnt[3]));
+            e[0] = make_float4(lxk, lyk, lzk, __uint_as_float(rk));
+            e[1] = make_float4(hxk, hyk, hzk, __uint_as_float(nn));
           }
         }
+        sp += np;
         __syncwarp();
         if (err) {
           break;

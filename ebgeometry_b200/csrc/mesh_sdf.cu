@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         }
       }
       TraversalCounters tc;
-      traverseMesh<STATS>(m, px, py, pz, cx, cy, cz, best, besttri, stk, iters, err, tc);
+      traverseMesh<STATS>(m, px, py, pz, best, besttri, stk, iters, err, tc);
       cNode += tc.node;
       cLeaf += tc.leaf;
       cTri += tc.tri;
@@ -191,10 +191,17 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
   }
   const int    threads = 32 * wpb;
   const size_t smem    = size_t(wpb) * 2 * EBG_STACK_DEPTH * sizeof(float4);
-  int          perSm   = 0;
-  cudaError_t  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC>, threads, smem);
-  if (e != cudaSuccess) {
-    return e;
+  // resident blocks per SM for each block size, looked up once (the query path then issues no
+  // runtime calls besides its launches, so it can be captured in a CUDA graph)
+  static int cache[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int        perSm    = cache[wpb];
+  if (perSm == 0) {
+    const cudaError_t e =
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC>, threads, smem);
+    if (e != cudaSuccess) {
+      return e;
+    }
+    cache[wpb] = perSm;
   }
   perSm               = perSm < 1 ? 1 : perSm;
   const int64_t need  = ((int64_t(a.n) + 31) / 32 + wpb - 1) / wpb;
@@ -235,7 +242,10 @@ cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStr
   if (wpb != 1 && wpb != 2 && wpb != 4 && wpb != 8) {
     wpb = 4;
   }
+  // occupancy 0 (default) takes the 64-register budget: fastest on B200 in the sweep over
+  // budgets and block sizes (full level-8 workload)
   switch (occupancy) {
+  case 0:
   case 1:
     return launchSeed<1>(a, wpb, numSms, s);
   case 2:
@@ -243,7 +253,7 @@ cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStr
   case 3:
     return launchSeed<3>(a, wpb, numSms, s);
   default:
-    return launchSeed<0>(a, wpb, numSms, s);
+    return launchSeed<0>(a, wpb, numSms, s);  // 4: the compiler's own budget (256-thread blocks)
   }
 }
 

@@ -140,14 +140,14 @@ struct TraversalCounters
 };
 
 // One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
-// already seeded or FLT_MAX) and winning triangle `besttri` (leaf order) are updated; (cx, cy, cz)
-// is the packet centroid used to order children.  `stk` is this warp's stack region (2 float4 per
-// entry, EBG_STACK_DEPTH entries); `iters` counts loop trips against MAX_ITERS; `err` receives
-// ST_* bits.  All 32 lanes must call it together.
+// already seeded or FLT_MAX) and winning triangle `besttri` (leaf order) are updated.  Children are
+// ordered by their smallest distance over the packet's lanes.  `stk` is this warp's stack region
+// (2 float4 per entry, EBG_STACK_DEPTH entries); `iters` counts loop trips against MAX_ITERS; `err`
+// receives ST_* bits.  All 32 lanes must call it together.
 template <bool STATS>
-__device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float cx, float cy,
-                                             float cz, float& best, int& besttri, float4* stk, uint32_t& iters,
-                                             int& err, TraversalCounters& cnt_)
+__device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
+                                             int& besttri, float4* stk, uint32_t& iters, int& err,
+                                             TraversalCounters& cnt_)
 {
   const int lane = threadIdx.x & 31;
       int sp = 1;
@@ -222,7 +222,6 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
                       chz[4] = {hz.x, hz.y, hz.z, hz.w};
           const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
           float key[4];
-          int   o[4];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
             const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
@@ -232,41 +231,28 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             // warp min-reduction; non-negative floats order like their bit patterns); children
             // nobody needs get -1 and are not pushed
             key[k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
-            o[k]   = k;
           }
-          // sort (key, slot) pairs by key, descending (far first): a 5-comparator network on
-          // registers (constant indices only, so nothing spills to local memory)
-#define EBG_CSWAP(i, j)                                                                                               \
-  if (key[i] < key[j]) {                                                                                              \
-    const float tk = key[i];                                                                                          \
-    key[i]         = key[j];                                                                                          \
-    key[j]         = tk;                                                                                              \
-    const int to   = o[i];                                                                                            \
-    o[i]           = o[j];                                                                                            \
-    o[j]           = to;                                                                                              \
-  }
-          EBG_CSWAP(0, 1);
-          EBG_CSWAP(2, 3);
-          EBG_CSWAP(0, 2);
-          EBG_CSWAP(1, 3);
-          EBG_CSWAP(1, 2);
-#undef EBG_CSWAP
+          const int np = int(key[0] >= 0.f) + int(key[1] >= 0.f) + int(key[2] >= 0.f) + int(key[3] >= 0.f);
+          if (sp + np > EBG_STACK_DEPTH) {
+            err |= ST_STACK;
+            break;
+          }
+          // lane k (< 4) writes child k straight into its slot: farther children sit deeper, so the
+          // nearest is popped first; ties go by slot index (a total order, so slots are distinct)
+          if (lane < 4) {
+            const float kk = sel4(key, lane);
+            if (kk >= 0.f) {
+              int rank = 0;
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            if (key[j] >= 0.f) {
-              if (sp >= EBG_STACK_DEPTH) {
-                err |= ST_STACK;
-                break;
+              for (int j = 0; j < 4; j++) {
+                rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
               }
-              const int k = o[j];
-              if (lane == 0) {
-                stk[2 * sp] = make_float4(sel4(clx, k), sel4(cly, k), sel4(clz, k), __uint_as_float(sel4u(cref, k)));
-                stk[2 * sp + 1] =
-                  make_float4(sel4(chx, k), sel4(chy, k), sel4(chz, k), __uint_as_float(sel4u(ccnt, k)));
-              }
-              sp++;
+              float4* e = stk + 2 * (sp + rank);
+              e[0]      = make_float4(sel4(clx, lane), sel4(cly, lane), sel4(clz, lane), __uint_as_float(sel4u(cref, lane)));
+              e[1]      = make_float4(sel4(chx, lane), sel4(chy, lane), sel4(chz, lane), __uint_as_float(sel4u(ccnt, lane)));
             }
           }
+          sp += np;
           __syncwarp();
           if (err) {
             break;

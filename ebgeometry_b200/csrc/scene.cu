@@ -51,8 +51,6 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
     const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
     const float px = __ldg(a.points + 3 * size_t(id)), py = __ldg(a.points + 3 * size_t(id) + 1),
                 pz = __ldg(a.points + 3 * size_t(id) + 2);
-    const float cx = warpSum(px) * (1.f / 32.f), cy = warpSum(py) * (1.f / 32.f), cz = warpSum(pz) * (1.f / 32.f);
-
     float    best  = __int_as_float(0x7f800000); // +inf, as the reference starts
     uint32_t iters = 0;
     int      err   = 0;
@@ -85,15 +83,11 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
             best = fminf(best, sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz))) - ob.radius);
             continue;
           }
-          // mesh object: local = R (p - t); the packet centroid moves with it (ordering only)
+          // mesh object: local = R (p - t)
           const float qx = px - ob.t[0], qy = py - ob.t[1], qz = pz - ob.t[2];
           const float lx = fmaf(ob.R[0], qx, fmaf(ob.R[1], qy, ob.R[2] * qz));
           const float ly = fmaf(ob.R[3], qx, fmaf(ob.R[4], qy, ob.R[5] * qz));
           const float lz = fmaf(ob.R[6], qx, fmaf(ob.R[7], qy, ob.R[8] * qz));
-          const float rx = cx - ob.t[0], ry = cy - ob.t[1], rz = cz - ob.t[2];
-          const float kx = fmaf(ob.R[0], rx, fmaf(ob.R[1], ry, ob.R[2] * rz));
-          const float ky = fmaf(ob.R[3], rx, fmaf(ob.R[4], ry, ob.R[5] * rz));
-          const float kz = fmaf(ob.R[6], rx, fmaf(ob.R[7], ry, ob.R[8] * rz));
           const EbgMeshView& mv = sc.meshes[ob.mesh];
           const bool outsideBox = lx < mv.root_lo[0] || lx > mv.root_hi[0] || ly < mv.root_lo[1] ||
                                   ly > mv.root_hi[1] || lz < mv.root_lo[2] || lz > mv.root_hi[2];
@@ -101,7 +95,7 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
           float      mb     = seeded ? best * best * 1.000004f : FLT_MAX;
           int        bt     = -1;
           TraversalCounters tc;
-          traverseMesh<false>(mv, lx, ly, lz, kx, ky, kz, mb, bt, istk, iters, err, tc);
+          traverseMesh<false>(mv, lx, ly, lz, mb, bt, istk, iters, err, tc);
           if (err) {
             break;
           }
@@ -116,43 +110,32 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
       else {
         const EbgNode4& nd = sc.nodes[ref];
         float           key[4];
-        int             o[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
           const float dk = boxDist2(nd.lox[k], nd.loy[k], nd.loz[k], nd.hix[k], nd.hiy[k], nd.hiz[k], px, py, pz);
           const bool  nk = __any_sync(FULL, dk <= bound) && (nd.child[k] | nd.count[k]) != 0u;
-          key[k] = nk ? boxDist2(nd.lox[k], nd.loy[k], nd.loz[k], nd.hix[k], nd.hiy[k], nd.hiz[k], cx, cy, cz) : -1.f;
-          o[k]   = k;
+          key[k]         = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
         }
-#define EBG_CSWAP(i, j)                                                                                               \
-  if (key[i] < key[j]) {                                                                                              \
-    const float tk = key[i];                                                                                          \
-    key[i]         = key[j];                                                                                          \
-    key[j]         = tk;                                                                                              \
-    const int to   = o[i];                                                                                            \
-    o[i]           = o[j];                                                                                            \
-    o[j]           = to;                                                                                              \
-  }
-        EBG_CSWAP(0, 1);
-        EBG_CSWAP(2, 3);
-        EBG_CSWAP(0, 2);
-        EBG_CSWAP(1, 3);
-        EBG_CSWAP(1, 2);
-#undef EBG_CSWAP
-        for (int j = 0; j < 4; j++) {
-          if (key[j] >= 0.f) {
-            if (sp >= OUTER_DEPTH) {
-              err |= ST_STACK;
-              break;
+        const int np = int(key[0] >= 0.f) + int(key[1] >= 0.f) + int(key[2] >= 0.f) + int(key[3] >= 0.f);
+        if (sp + np > OUTER_DEPTH) {
+          err |= ST_STACK;
+          break;
+        }
+        // lane k (< 4) writes child k into its slot, farther children deeper (ties by slot index)
+        if (lane < 4) {
+          const float kk = lane == 0 ? key[0] : (lane == 1 ? key[1] : (lane == 2 ? key[2] : key[3]));
+          if (kk >= 0.f) {
+            int rank = 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
             }
-            const int k = o[j];
-            if (lane == 0) {
-              ostk[2 * sp]     = make_float4(nd.lox[k], nd.loy[k], nd.loz[k], __uint_as_float(nd.child[k]));
-              ostk[2 * sp + 1] = make_float4(nd.hix[k], nd.hiy[k], nd.hiz[k], __uint_as_float(nd.count[k]));
-            }
-            sp++;
+            float4* e = ostk + 2 * (sp + rank);
+            e[0]      = make_float4(nd.lox[lane], nd.loy[lane], nd.loz[lane], __uint_as_float(nd.child[lane]));
+            e[1]      = make_float4(nd.hix[lane], nd.hiy[lane], nd.hiz[lane], __uint_as_float(nd.count[lane]));
           }
         }
+        sp += np;
         __syncwarp();
         if (err) {
           break;

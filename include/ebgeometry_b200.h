@@ -77,9 +77,10 @@ typedef struct ebg_query_opts
   int32_t            no_fp64_band;    /* 1: skip the FP64 near-surface re-evaluation */
   const ebg_seed*    seed;            /* learned pruning-radius model (NULL = plain traversal) */
   int32_t            warps_per_block; /* 0 = tuned default */
-  int32_t            occupancy;       /* traversal register budget: 0 = default; 1, 2, 3 = at most
-                                         64, 51, 42 registers per thread (8, 10, 12 blocks of 128
-                                         threads per SM; warps_per_block <= 4) */
+  int32_t            occupancy;       /* traversal register budget: 0 = default (= 1); 1, 2, 3 = at
+                                         most 64, 51, 42 registers per thread (8, 10, 12 blocks of
+                                         128 threads per SM; warps_per_block <= 4); 4 = the
+                                         compiler's own choice with 256-thread blocks */
   ebg_phase_timings* timings;         /* non-NULL: record events per phase; the call then
                                          synchronises the stream and fills this struct */
   const float*       radius_hint;     /* device, one per point (caller order): an upper bound on

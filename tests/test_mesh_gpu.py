@@ -177,3 +177,28 @@ def test_level8_properties_full_size():
     rs = 1.0 + (np.sin(u @ w.T + phi) * a).sum(axis=1)
     far = np.abs(r - rs) > 1e-3
     assert np.all(np.sign(d.ravel()[far]) == np.sign(r - rs)[far])
+
+
+def test_cuda_graph_capture(ref):
+    """The query path issues only stream-ordered work (launches, stream-ordered allocations, the
+    radix sort), so a caller can capture it once and replay it."""
+    v, f = W.displaced_icosphere(4, 31)
+    m = TriMeshSDF(v, f)
+    p = W.uniform_points(50000, 32)
+    d_ref = ref.mesh(v, f).sdf(p.astype(np.float64))
+    pd = torch.from_numpy(p).cuda()
+    out = torch.empty(p.shape[0], device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            m.signed_distance(pd, out=out, stream=s)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        m.signed_distance(pd, out=out, stream=s)
+    out.zero_()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    check_parity(out.cpu().numpy(), d_ref, m.diagonal, "graph replay")
