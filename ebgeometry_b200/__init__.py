@@ -169,6 +169,14 @@ class TriMeshSDF:
     def check_status(self, stream=None):
         check(lib.ebg_check_status(self._h, _stream_ptr(stream)))
 
+    def autotune(self, sample_points, stream=None):
+        """Times the traversal launch shapes on a CUDA tensor of sample points and keeps the fastest
+        as this mesh's default; returns {"occupancy", "warps_per_block", "ms"}."""
+        o, w, ms = C.c_int32(), C.c_int32(), C.c_float()
+        check(lib.ebg_mesh_autotune(self._h, C.c_void_p(sample_points.data_ptr()), sample_points.numel() // 3,
+                                    C.byref(o), C.byref(w), C.byref(ms), _stream_ptr(stream)))
+        return {"occupancy": o.value, "warps_per_block": w.value, "ms": ms.value}
+
 
 class PointCloudBVH:
     """k-nearest-neighbour search over a point cloud (the reference's PointCloudBVH).

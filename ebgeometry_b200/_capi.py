@@ -84,6 +84,7 @@ SIGNATURES = {
     "ebg_mesh_signed_distance_stats": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts),
                                                  C.POINTER(QueryStats), _P]),
     "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),
+    "ebg_mesh_autotune": (C.c_int, [_P, _P, _I64, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_float), _P]),
     "ebg_check_status": (C.c_int, [_P, _P]),
     "ebg_cloud_create": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_cloud_create_device": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P), _P]),

@@ -28,6 +28,9 @@ struct ebg_mesh
   // host copies of the pseudonormals (soup order) and the cumulative triangle area (leaf order)
   std::vector<double> triN, cornerVN, edgeN;
   std::vector<double> areaCdf;
+  // launch shape chosen by ebg_mesh_autotune (0 = library defaults)
+  int tunedOccupancy = 0;
+  int tunedWpb       = 0;
 };
 
 struct ebg_seed

@@ -403,7 +403,9 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   }
   const bool sort   = !(opts && opts->no_sort);
   const bool band64 = !(opts && opts->no_fp64_band);
-  const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block : 4;
+  const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block
+                                                          : (m->tunedWpb > 0 ? m->tunedWpb : 4);
+  const int  occ    = (opts && opts->occupancy > 0) ? opts->occupancy : m->tunedOccupancy;
   double     band   = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
   const ebg_seed* seed = opts ? opts->seed : nullptr;
   if (seed && seed->device != m->device) {
@@ -493,7 +495,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.work       = counters;
   a.status     = m->dStatus;
   a.stats      = statsDev;
-  if (launchMeshSdf32(a, wpb, m->numSms, s, opts ? opts->occupancy : 0) != cudaSuccess) {
+  if (launchMeshSdf32(a, wpb, m->numSms, s, occ) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
   }
   if (tm) {
@@ -732,6 +734,74 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   stats->packet_leaves    = int64_t(host[8]);
   stats->packet_triangles = int64_t(host[9]);
   return ebg_check_status(m, stream);
+}
+
+ebg_status ebg_mesh_autotune(ebg_mesh*    m,
+                             const float* sample_points_dev,
+                             int64_t      n,
+                             int32_t*     best_occupancy,
+                             int32_t*     best_warps_per_block,
+                             float*       best_ms,
+                             void*        stream)
+{
+  if (m == nullptr || sample_points_dev == nullptr || n < 32) {
+    return setError(EBG_ERR_INVALID, "autotune needs a mesh and at least 32 sample points");
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  float*       out = nullptr;
+  cudaStream_t s   = static_cast<cudaStream_t>(stream);
+  if (cudaMallocAsync(reinterpret_cast<void**>(&out), size_t(n) * sizeof(float), s) != cudaSuccess) {
+    cudaGetLastError();
+    return setError(EBG_ERR_NO_MEMORY, "autotune output buffer");
+  }
+  float     bestMs = INFINITY;
+  int       bestO = 1, bestW = 4;
+  const int occs[] = {1, 4, 2};
+  const int wpbs[] = {2, 4, 8};
+  for (int o : occs) {
+    for (int w : wpbs) {
+      if (o != 4 && w > 4) {
+        continue;
+      }
+      ebg_query_opts    q{};
+      ebg_phase_timings t{};
+      q.occupancy       = o;
+      q.warps_per_block = w;
+      q.no_fp64_band    = 1;
+      float ms          = INFINITY;
+      for (int rep = 0; rep < 3; rep++) {  // the first run warms caches and the pool
+        q.timings           = &t;
+        const ebg_status rc = meshQuery(m, sample_points_dev, n, out, nullptr, &q, nullptr, s);
+        if (rc != EBG_OK) {
+          cudaFreeAsync(out, s);
+          return rc;
+        }
+        if (rep > 0) {
+          ms = std::min(ms, t.traverse_ms);
+        }
+      }
+      if (ms < bestMs) {
+        bestMs = ms;
+        bestO  = o;
+        bestW  = w;
+      }
+    }
+  }
+  cudaFreeAsync(out, s);
+  cudaStreamSynchronize(s);
+  m->tunedOccupancy = bestO;
+  m->tunedWpb       = bestW;
+  if (best_occupancy) {
+    *best_occupancy = bestO;
+  }
+  if (best_warps_per_block) {
+    *best_warps_per_block = bestW;
+  }
+  if (best_ms) {
+    *best_ms = bestMs;
+  }
+  return EBG_OK;
 }
 
 ebg_status ebg_mesh_value(const ebg_mesh* m, double x, double y, double z, double* value)

@@ -105,45 +105,63 @@ bool computePseudonormals(const double*        V,
     return false;
   }
 
-  // Pair half-edges: sort (undirected edge key, half-edge id).
-  const int64_t                              ne = 3 * nt;
-  std::vector<std::pair<uint64_t, int64_t>> he(ne);
-#pragma omp parallel for schedule(static)
+  // Faces around each vertex, in facet order (a stable counting sort): the order the reference's
+  // DCEL vertex keeps its faces in (soupToDCEL adds them facet by facet, SoupImplem.hpp:204-207).
+  std::vector<int64_t> start(nv + 1, 0);
+  for (int64_t i = 0; i < 3 * nt; i++) {
+    start[int64_t(F[i]) + 1]++;
+  }
+  for (int64_t v = 0; v < nv; v++) {
+    start[v + 1] += start[v];
+  }
+  std::vector<int64_t> fill(start.begin(), start.end() - 1);
+  std::vector<int64_t> around(3 * nt); // entries f * 3 + corner
   for (int64_t f = 0; f < nt; f++) {
-    for (int i = 0; i < 3; i++) {
-      const uint64_t a = uint32_t(F[3 * f + i]), b = uint32_t(F[3 * f + (i + 1) % 3]);
-      he[3 * f + i]    = {(std::min(a, b) << 32) | std::max(a, b), 3 * f + i};
+    for (int k = 0; k < 3; k++) {
+      around[fill[F[3 * f + k]]++] = 3 * f + k;
     }
   }
-  std::sort(he.begin(), he.end());
+
+  // Edge pseudonormals: the pair of half-edge (a -> b) of face f is the half-edge (b -> a) of the
+  // other face around a that also holds b.
   bool nonManifold = false;
-  for (int64_t s = 0; s < ne;) {
-    int64_t e = s + 1;
-    while (e < ne && he[e].first == he[s].first) {
-      e++;
-    }
-    if (e - s > 2) {
-      nonManifold = true;
-    }
-    for (int64_t q = s; q < e; q++) {
-      const int64_t h = he[q].second, f = h / 3, i = h % 3;
-      V3            n = ld3(&faceN[3 * f]);
-      if (e - s == 2) {
-        const int64_t g = he[q == s ? s + 1 : s].second / 3;
-        n               = {n.x + faceN[3 * g], n.y + faceN[3 * g + 1], n.z + faceN[3 * g + 2]};
+#pragma omp parallel for schedule(static) reduction(|| : nonManifold)
+  for (int64_t f = 0; f < nt; f++) {
+    for (int i = 0; i < 3; i++) {
+      const int32_t a = F[3 * f + i], b = F[3 * f + (i + 1) % 3];
+      int64_t       pair = -1, found = 0;
+      for (int64_t e = start[a]; e < start[a + 1]; e++) {
+        const int64_t g = around[e] / 3;
+        if (g == f) {
+          continue;
+        }
+        for (int k = 0; k < 3; k++) {
+          if (F[3 * g + k] == b) {
+            found++;
+            pair = g;
+          }
+        }
+      }
+      if (found > 1) {
+        nonManifold = true;
+      }
+      V3 n = ld3(&faceN[3 * f]);
+      if (pair >= 0) {
+        n = {n.x + faceN[3 * pair], n.y + faceN[3 * pair + 1], n.z + faceN[3 * pair + 2]};
       }
       const double l = len(n);
       st3(&edgeN[9 * f + 3 * i], (l > std::numeric_limits<double>::epsilon()) ? divs(n, l) : V3{0, 0, 0});
     }
-    s = e;
   }
   if (nonManifold) {
     msg = "non-manifold edge (shared by more than two triangles)";
     return false;
   }
 
-  // Angle-weighted vertex normals, accumulated per vertex in facet order.
-  std::vector<double> vn(3 * nv, 0.0);
+  // Angle-weighted vertex normals: each corner's alpha * n_face in parallel, then each vertex sums
+  // its corners in facet order with the reference's operation order (m_normal += alpha * n).
+  std::vector<double> contrib(9 * nt);
+#pragma omp parallel for schedule(static)
   for (int64_t f = 0; f < nt; f++) {
     const int32_t a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
     // neighbours of each corner in half-edge loop order: a:(b,c) b:(a,c) c:(b,a)
@@ -156,19 +174,24 @@ bool computePseudonormals(const double*        V,
       e1          = divs(e1, len(e1));
       e2          = divs(e2, len(e2));
       const double alpha = std::acos(std::clamp(dot(e1, e2), -1.0, 1.0));
-      double*      dst   = &vn[3 * int64_t(corner[k])];
-      dst[0] += alpha * fn.x;
-      dst[1] += alpha * fn.y;
-      dst[2] += alpha * fn.z;
+      contrib[9 * f + 3 * k + 0] = alpha * fn.x;
+      contrib[9 * f + 3 * k + 1] = alpha * fn.y;
+      contrib[9 * f + 3 * k + 2] = alpha * fn.z;
     }
   }
+  std::vector<double> vn(3 * nv, 0.0);
 #pragma omp parallel for schedule(static)
   for (int64_t v = 0; v < nv; v++) {
-    const V3     n = ld3(&vn[3 * v]);
-    const double l = len(n);
-    if (l > std::numeric_limits<double>::epsilon()) {
-      st3(&vn[3 * v], divs(n, l));
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int64_t e = start[v]; e < start[v + 1]; e++) {
+      const double* c = &contrib[3 * around[e]];
+      x += c[0];
+      y += c[1];
+      z += c[2];
     }
+    const V3     n = {x, y, z};
+    const double l = len(n);
+    st3(&vn[3 * v], (l > std::numeric_limits<double>::epsilon()) ? divs(n, l) : n);
   }
 #pragma omp parallel for schedule(static)
   for (int64_t f = 0; f < nt; f++) {

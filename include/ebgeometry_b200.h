@@ -225,6 +225,19 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       mesh,
                                           ebg_query_stats*      stats,
                                           void*                 stream);
 
+/* Autotuner (no reference counterpart): times the traversal's launch shapes -- register budget
+ * (ebg_query_opts.occupancy 1..4) x warps per block (2, 4, 8) -- on the caller's sample points
+ * (device), keeps the fastest as this mesh's default for queries that leave those options at 0, and
+ * returns it (best_occupancy / best_warps_per_block, best_ms = the sample's traversal time).
+ * Synchronous. */
+ebg_status ebg_mesh_autotune(ebg_mesh*    mesh,
+                             const float* sample_points_dev,
+                             int64_t      n,
+                             int32_t*     best_occupancy,
+                             int32_t*     best_warps_per_block,
+                             float*       best_ms,
+                             void*        stream);
+
 /* ImplicitFunction<T>::value(point) for one point (ImplicitFunction.hpp:51-52): the drop-in
  * single-point call.  Synchronous; each call is one tiny launch, so batch where you can. */
 ebg_status ebg_mesh_value(const ebg_mesh* mesh, double x, double y, double z, double* value);
