@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-seed", action="store_true", help="time the plain traversal only")
     ap.add_argument("--perfect-seed", action="store_true",
                     help="also time the traversal seeded with the exact distances (the bound any seed can reach)")
+    ap.add_argument("--hint-slack", default="0.02:4e-4,0.005:1e-4",
+                    help="with --perfect-seed: also time radius hints |d|(1+a)+b for these a:b pairs")
     ap.add_argument("--seed-samples", type=int, default=1 << 25)
     ap.add_argument("--seed-steps", type=int, default=2000)
     ap.add_argument("--seed-batch", type=int, default=1 << 18)
@@ -314,6 +316,19 @@ def run_ours(args, rank, world, local_rank):
                    "speedup_vs_plain": ms_plain / ms_hint, "stats": st_hint,
                    "equal_to_plain_fraction": float((hout == out).float().mean().item())}
         log(f"[rank {rank}] perfect radius {ms_hint:.1f} ms/step {st_hint}")
+        # radius slack a seed would carry: |d| (1 + a) + b
+        slack = []
+        for pair in filter(None, args.hint_slack.split(",")):
+            sa, sb = (float(x) for x in pair.split(":"))
+            hint = out.abs() * (1 + sa) + sb
+            _, st_s = mesh.stats(pd, radius_hint=hint)
+            mesh.signed_distance(pd, out=hout, radius_hint=hint)
+            ms_s, _, _ = timed_steps(mesh, pd, hout, max(2, args.steps // 2), None, *tctx, hint=hint)
+            slack.append({"a": sa, "b": sb, "ms_per_step": ms_s, "speedup_vs_plain": ms_plain / ms_s,
+                          "nodes_per_query": st_s["nodes_visited"] / n, "leaves_per_query": st_s["leaves_visited"] / n,
+                          "triangles_per_query": st_s["triangles_tested"] / n})
+            log(f"[rank {rank}] radius |d|(1+{sa})+{sb}: {ms_s:.1f} ms/step")
+        perfect["slack"] = slack
         del hout, hint
 
     seed, rep, st_seed = None, None, None

@@ -24,6 +24,7 @@ struct ebg_mesh
   void* dTri64  = nullptr;
   void* dTriId  = nullptr;
   void* dObb    = nullptr;
+  void* dNodeObb = nullptr;
   int*  dStatus = nullptr;
   // host copies of the pseudonormals (soup order) and the cumulative triangle area (leaf order)
   std::vector<double> triN, cornerVN, edgeN;

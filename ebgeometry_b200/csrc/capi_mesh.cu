@@ -23,119 +23,154 @@ using namespace ebg;
 
 namespace {
 
-// Oriented box of each leaf (see EbgLeafObb): n = area-weighted mean face normal (the smallest
-// extent axis of the leaf's AABB if the normals cancel), u = principal in-plane direction of the
-// leaf's vertices, extents from the vertex projections, padded by `pad` so FP32 evaluation of the
-// box distance never exceeds the FP64 distance to a triangle inside.
-void computeLeafObbs(const double* V, const int32_t* F, const Bvh4& bvh, std::vector<EbgLeafObb>& out)
+// Oriented box of the triangles at leaf positions [first, end) (see EbgObb): n = area-weighted
+// mean face normal (the smallest extent axis of their AABB if the normals nearly cancel), u =
+// principal in-plane direction of their vertices, extents from the vertex projections, padded by
+// `pad` so FP32 evaluation of the box distance never exceeds the FP64 distance to a triangle
+// inside.  Returns the box's volume over the AABB's (how much tighter it is).
+double obbOfRange(const double* V, const int32_t* F, const std::vector<uint32_t>& order, uint32_t first, uint32_t end,
+                  double pad, EbgObb& o)
 {
-  const size_t nl = bvh.leafFirst.size();
-  out.resize(nl);
-  double scale = 0;
-  for (int a = 0; a < 3; a++) {
-    scale = std::max(scale, std::max(std::fabs(bvh.lo[a]), std::fabs(bvh.hi[a])));
-  }
-  const double pad = 2e-6 * std::max(scale, 1e-30);
-#pragma omp parallel for schedule(static)
-  for (int64_t l = 0; l < int64_t(nl); l++) {
-    const uint32_t b = bvh.leafFirst[l], c = bvh.leafCount[l];
-    double         n[3] = {0, 0, 0}, area = 0, lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    std::vector<std::array<double, 3>> pts;
-    pts.reserve(3 * c);
-    for (uint32_t i = b; i < b + c; i++) {
-      const int64_t f = bvh.order[i];
-      const double* p0 = V + 3 * int64_t(F[3 * f]);
-      const double* p1 = V + 3 * int64_t(F[3 * f + 1]);
-      const double* p2 = V + 3 * int64_t(F[3 * f + 2]);
-      const double  e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-      const double  e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-      const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+  auto vert = [&](uint32_t i, int c) { return V + 3 * int64_t(F[3 * int64_t(order[i]) + c]); };
+  double n[3] = {0, 0, 0}, area = 0, lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (uint32_t i = first; i < end; i++) {
+    const double* p0 = vert(i, 0);
+    const double* p1 = vert(i, 1);
+    const double* p2 = vert(i, 2);
+    const double  e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+    const double  e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+    const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    for (int a = 0; a < 3; a++) {
+      n[a] += cr[a];
+    }
+    area += std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    for (const double* p : {p0, p1, p2}) {
       for (int a = 0; a < 3; a++) {
-        n[a] += cr[a];
-      }
-      area += std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-      for (const double* p : {p0, p1, p2}) {
-        pts.push_back({p[0], p[1], p[2]});
-        for (int a = 0; a < 3; a++) {
-          lo[a] = std::min(lo[a], p[a]);
-          hi[a] = std::max(hi[a], p[a]);
-        }
+        lo[a] = std::min(lo[a], p[a]);
+        hi[a] = std::max(hi[a], p[a]);
       }
     }
-    double ln = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-    if (!(ln > 0.5 * area) || !(ln > 0)) {
-      int ax = 0;
-      for (int a = 1; a < 3; a++) {
-        if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
-          ax = a;
-        }
+  }
+  double ln = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  if (!(ln > 0.5 * area) || !(ln > 0)) {
+    int ax = 0;
+    for (int a = 1; a < 3; a++) {
+      if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
+        ax = a;
       }
-      n[0] = n[1] = n[2] = 0;
-      n[ax] = 1;
-      ln    = 1;
     }
-    for (int a = 0; a < 3; a++) {
-      n[a] /= ln;
-    }
-    // a first in-plane axis t1 (any perpendicular), then the principal direction in that plane
-    double t1[3];
-    if (std::fabs(n[0]) < 0.9) {
-      t1[0] = 0;
-      t1[1] = n[2];
-      t1[2] = -n[1];
-    }
-    else {
-      t1[0] = -n[2];
-      t1[1] = 0;
-      t1[2] = n[0];
-    }
-    double l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
-    for (int a = 0; a < 3; a++) {
-      t1[a] /= l1;
-    }
-    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
-    double       mx = 0, my = 0;
-    for (const auto& p : pts) {
+    n[0] = n[1] = n[2] = 0;
+    n[ax] = 1;
+    ln    = 1;
+  }
+  for (int a = 0; a < 3; a++) {
+    n[a] /= ln;
+  }
+  // a first in-plane axis t1 (any perpendicular), then the principal direction in that plane
+  double t1[3];
+  if (std::fabs(n[0]) < 0.9) {
+    t1[0] = 0;
+    t1[1] = n[2];
+    t1[2] = -n[1];
+  }
+  else {
+    t1[0] = -n[2];
+    t1[1] = 0;
+    t1[2] = n[0];
+  }
+  const double l1 = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+  for (int a = 0; a < 3; a++) {
+    t1[a] /= l1;
+  }
+  const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
+  const double cnt   = 3.0 * double(end - first);
+  double       mx = 0, my = 0;
+  for (uint32_t i = first; i < end; i++) {
+    for (int c = 0; c < 3; c++) {
+      const double* p = vert(i, c);
       mx += p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2];
       my += p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2];
     }
-    mx /= double(pts.size());
-    my /= double(pts.size());
-    double sxx = 0, syy = 0, sxy = 0;
-    for (const auto& p : pts) {
-      const double x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - mx;
-      const double y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - my;
+  }
+  mx /= cnt;
+  my /= cnt;
+  double sxx = 0, syy = 0, sxy = 0;
+  for (uint32_t i = first; i < end; i++) {
+    for (int c = 0; c < 3; c++) {
+      const double* p = vert(i, c);
+      const double  x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - mx;
+      const double  y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - my;
       sxx += x * x;
       syy += y * y;
       sxy += x * y;
     }
-    const double th = 0.5 * std::atan2(2 * sxy, sxx - syy);
-    const double u[3] = {std::cos(th) * t1[0] + std::sin(th) * t2[0], std::cos(th) * t1[1] + std::sin(th) * t2[1],
-                         std::cos(th) * t1[2] + std::sin(th) * t2[2]};
-    const double w[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2], n[0] * u[1] - n[1] * u[0]};
-    double       mn[3] = {1e300, 1e300, 1e300}, mxx[3] = {-1e300, -1e300, -1e300};
-    for (const auto& p : pts) {
-      const double pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
-                            p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
+  }
+  const double th   = 0.5 * std::atan2(2 * sxy, sxx - syy);
+  const double u[3] = {std::cos(th) * t1[0] + std::sin(th) * t2[0], std::cos(th) * t1[1] + std::sin(th) * t2[1],
+                       std::cos(th) * t1[2] + std::sin(th) * t2[2]};
+  const double w[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2], n[0] * u[1] - n[1] * u[0]};
+  double       mn[3] = {1e300, 1e300, 1e300}, mxx[3] = {-1e300, -1e300, -1e300};
+  for (uint32_t i = first; i < end; i++) {
+    for (int c = 0; c < 3; c++) {
+      const double* p     = vert(i, c);
+      const double  pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
+                             p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
       for (int a = 0; a < 3; a++) {
         mn[a]  = std::min(mn[a], pr[a]);
         mxx[a] = std::max(mxx[a], pr[a]);
       }
     }
-    const double cn = 0.5 * (mn[0] + mxx[0]), cu = 0.5 * (mn[1] + mxx[1]), cw = 0.5 * (mn[2] + mxx[2]);
-    EbgLeafObb&  o  = out[l];
-    o.cx = float(cn * n[0] + cu * u[0] + cw * w[0]);
-    o.cy = float(cn * n[1] + cu * u[1] + cw * w[1]);
-    o.cz = float(cn * n[2] + cu * u[2] + cw * w[2]);
-    o.nx = float(n[0]);
-    o.ny = float(n[1]);
-    o.nz = float(n[2]);
-    o.ux = float(u[0]);
-    o.uy = float(u[1]);
-    o.uz = float(u[2]);
-    o.hn = roundUp(0.5 * (mxx[0] - mn[0]) + pad);
-    o.hu = roundUp(0.5 * (mxx[1] - mn[1]) + pad);
-    o.hv = roundUp(0.5 * (mxx[2] - mn[2]) + pad);
+  }
+  const double cn = 0.5 * (mn[0] + mxx[0]), cu = 0.5 * (mn[1] + mxx[1]), cw = 0.5 * (mn[2] + mxx[2]);
+  o.cx = float(cn * n[0] + cu * u[0] + cw * w[0]);
+  o.cy = float(cn * n[1] + cu * u[1] + cw * w[1]);
+  o.cz = float(cn * n[2] + cu * u[2] + cw * w[2]);
+  o.nx = float(n[0]);
+  o.ny = float(n[1]);
+  o.nz = float(n[2]);
+  o.ux = float(u[0]);
+  o.uy = float(u[1]);
+  o.uz = float(u[2]);
+  o.hn = roundUp(0.5 * (mxx[0] - mn[0]) + pad);
+  o.hu = roundUp(0.5 * (mxx[1] - mn[1]) + pad);
+  o.hv = roundUp(0.5 * (mxx[2] - mn[2]) + pad);
+  const double obbVol  = 8.0 * double(o.hn) * double(o.hu) * double(o.hv);
+  const double aabbVol = (hi[0] - lo[0] + 2 * pad) * (hi[1] - lo[1] + 2 * pad) * (hi[2] - lo[2] + 2 * pad);
+  return aabbVol > 0 ? obbVol / aabbVol : 1.0;
+}
+
+// Oriented boxes of every leaf and every interior node.  An interior node's box is flagged in its
+// parent's slot (EBG_NODE_HAS_OBB) only when its volume is at most half the axis-aligned box's, so
+// the traversal spends the extra test where it can prune.
+void computeObbs(const double* V, const int32_t* F, Bvh4& bvh, std::vector<EbgObb>& leafObb, std::vector<EbgObb>& nodeObb)
+{
+  double scale = 0;
+  for (int a = 0; a < 3; a++) {
+    scale = std::max(scale, std::max(std::fabs(bvh.lo[a]), std::fabs(bvh.hi[a])));
+  }
+  const double pad = 2e-6 * std::max(scale, 1e-30);
+  const size_t nl  = bvh.leafFirst.size();
+  leafObb.resize(nl);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t l = 0; l < int64_t(nl); l++) {
+    obbOfRange(V, F, bvh.order, bvh.leafFirst[l], bvh.leafFirst[l] + bvh.leafCount[l], pad, leafObb[l]);
+  }
+  const size_t       nn = bvh.nodes.size();
+  std::vector<char>  useful(nn, 0);
+  nodeObb.resize(std::max<size_t>(nn, 1));
+  std::memset(nodeObb.data(), 0, nodeObb.size() * sizeof(EbgObb));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t j = 0; j < int64_t(nn); j++) {
+    useful[j] = obbOfRange(V, F, bvh.order, bvh.nodeFirst[j], bvh.nodeEnd[j], pad, nodeObb[j]) <= 0.5;
+  }
+  for (size_t j = 0; j < nn; j++) {
+    EbgNode4& nd = bvh.nodes[j];
+    for (int k = 0; k < 4; k++) {
+      const uint32_t c = nd.child[k];
+      if (!(c & EBG_LEAF_BIT) && c != 0 && useful[c]) {
+        nd.count[k] = EBG_NODE_HAS_OBB;
+      }
+    }
   }
 }
 
@@ -303,8 +338,8 @@ ebg_status buildMesh(const double*         V,
   for (size_t i = 1; i < N; i++) {
     m->areaCdf[i] += m->areaCdf[i - 1];
   }
-  std::vector<EbgLeafObb> obb;
-  computeLeafObbs(V, F, bvh, obb);
+  std::vector<EbgObb> obb, nodeObb;
+  computeObbs(V, F, bvh, obb, nodeObb);
   // upload
   auto up = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (cudaMalloc(dst, std::max<size_t>(bytes, 16)) != cudaSuccess) {
@@ -316,7 +351,8 @@ ebg_status buildMesh(const double*         V,
   if (!up(&m->dNodes, bvh.nodes.data(), nodeBytes) || !up(&m->dHot, hot.data(), N * sizeof(EbgTriHot)) ||
       !up(&m->dSign, sign.data(), N * sizeof(EbgTriSign)) || !up(&m->dTri64, tri64.data(), 30 * N * sizeof(double)) ||
       !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
-      !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgLeafObb)) ||
+      !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgObb)) ||
+      !up(&m->dNodeObb, nodeObb.data(), nodeObb.size() * sizeof(EbgObb)) ||
       cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
       cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
@@ -330,7 +366,8 @@ ebg_status buildMesh(const double*         V,
   v.sign         = static_cast<const EbgTriSign*>(m->dSign);
   v.tri64        = static_cast<const double*>(m->dTri64);
   v.tri_id       = static_cast<const int32_t*>(m->dTriId);
-  v.obb          = static_cast<const EbgLeafObb*>(m->dObb);
+  v.obb          = static_cast<const EbgObb*>(m->dObb);
+  v.node_obb     = static_cast<const EbgObb*>(m->dNodeObb);
   for (int a = 0; a < 3; a++) {
     v.root_lo[a] = roundDown(bvh.lo[a]);
     v.root_hi[a] = roundUp(bvh.hi[a]);
@@ -593,6 +630,7 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dTri64);
   cudaFree(m->dTriId);
   cudaFree(m->dObb);
+  cudaFree(m->dNodeObb);
   cudaFree(m->dStatus);
   delete m;
   return EBG_OK;

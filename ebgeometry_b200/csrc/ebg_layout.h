@@ -18,9 +18,14 @@
 //                                 reference's TriangleSoA lane data, TriangleSoAImplem.hpp:28-70).
 //   int32   tri_id[num_tris]      leaf position -> triangle index in the caller's soup.
 //
-// child[k] of an interior slot is a node index; of a leaf slot, the first triangle (leaf order)
-// with EBG_LEAF_BIT set, count[k] its triangle count.  An empty slot has count 0 and an empty box
-// (lo = +inf, hi = -inf), whose point distance is +inf, so no bound ever admits it.
+//   Obb     leaf_obb[num_leaves]  48 B: oriented box of each leaf's triangles.
+//   Obb     node_obb[num_nodes]   48 B: oriented box of all triangles below each interior node.
+//
+// child[k] of an interior slot is a node index and count[k] is 0, or EBG_NODE_HAS_OBB when the
+// child's oriented box is tighter than its axis-aligned one (the traversal then tests it before
+// reading the child); of a leaf slot, child[k] is the first triangle (leaf order) with
+// EBG_LEAF_BIT set and count[k] its triangle count.  An empty slot has child 0, count 0 and an
+// empty box (lo = +inf, hi = -inf), whose point distance is +inf.
 #ifndef EBG_LAYOUT_H
 #define EBG_LAYOUT_H
 
@@ -33,6 +38,8 @@
 #define EBG_COUNT_BITS 6u
 #define EBG_COUNT_MASK 63u
 #define EBG_MAX_LEAVES (1u << 26)
+// count[k] of an interior slot: the child node has an oriented box worth testing.
+#define EBG_NODE_HAS_OBB 0x80000000u
 
 // Traversal stack depth (entries per warp).  The builder rejects trees whose depth would need
 // more (a 4-wide node pushes at most 3 siblings per level besides the one it descends into).
@@ -61,11 +68,12 @@ struct alignas(16) EbgTriSign
   float pad1, pad2;
 };
 
-// Oriented box of one mesh leaf, in the frame of the leaf's mean normal n and an in-plane axis u
-// (v = n x u): centre c and half-extents (hn, hu, hv), padded outward to cover FP32 evaluation.  A
-// leaf on a smooth surface is a thin slab, so its distance bounds the leaf's triangles far more
-// tightly than the axis-aligned box does.
-struct alignas(16) EbgLeafObb
+// Oriented box of the triangles of one mesh leaf or of one subtree, in the frame of their
+// area-weighted mean normal n and an in-plane principal axis u (v = n x u): centre c and
+// half-extents (hn, hu, hv), padded outward to cover FP32 evaluation.  A patch of a smooth surface
+// is a thin slab, so its distance bounds the patch's triangles far more tightly than the
+// axis-aligned box does.
+struct alignas(16) EbgObb
 {
   float cx, cy, cz, hn;
   float nx, ny, nz, hu;
@@ -73,7 +81,7 @@ struct alignas(16) EbgLeafObb
 };
 
 static_assert(sizeof(EbgNode4) == 128, "node must be one 128-byte line");
-static_assert(sizeof(EbgLeafObb) == 48, "leaf box must be 48 bytes");
+static_assert(sizeof(EbgObb) == 48, "oriented box must be 48 bytes");
 static_assert(sizeof(EbgTriHot) == 48, "hot triangle record must be 48 bytes");
 static_assert(sizeof(EbgTriSign) == 96, "sign record must be 96 bytes");
 
@@ -85,7 +93,8 @@ struct EbgMeshView
   const EbgTriSign* sign;
   const double*     tri64;
   const int32_t*    tri_id;
-  const EbgLeafObb* obb;                    // per leaf id
+  const EbgObb*     obb;                    // per leaf id
+  const EbgObb*     node_obb;               // per interior node index
   float             root_lo[3], root_hi[3]; // root box (FP32, outward)
   uint32_t          root_ref;               // node index 0, or a leaf reference for tiny meshes
   uint32_t          root_count;             // leaf count when root_ref is a leaf

@@ -7,12 +7,14 @@
 // TriangleSoAT::signedDistance (TriangleSoAImplem.hpp:1029-1180) -- over every triangle whose FP32
 // (outward-rounded) box lies within |d32| + delta of the point, keeping the value of smallest
 // magnitude with strict < (MeshDistanceFunctionsImplem.hpp:492-502).  delta covers the FP32
-// distance error, so the FP64 winner is never pruned.  Packets of 32 band queries share one
+// distance error, so the FP64 winner is never pruned; leaves and nodes are also pruned by their
+// oriented boxes, which bound the exact distance to every triangle inside from below.  Packets of 32 band queries share one
 // traversal stack exactly as in the FP32 kernel.
 #include <cfloat>
 
 #include "ebg_device.cuh"
 #include "mesh_kernels.h"
+#include "mesh_traverse.cuh"
 
 namespace ebg {
 
@@ -121,7 +123,18 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
       if (!__any_sync(FULL, d2 <= bound)) {
         continue;
       }
-      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w) & EBG_COUNT_MASK;
+      const uint32_t cntw = __float_as_uint(B.w);
+      const uint32_t ref = __float_as_uint(A.w), cnt = cntw & EBG_COUNT_MASK;
+      // the leaf's or node's oriented box (padded to bound the exact distance of every triangle
+      // inside from below) before its triangles or children
+      const EbgObb* obx = (ref & EBG_LEAF_BIT) ? m.obb + (cntw >> EBG_COUNT_BITS)
+                                               : ((cntw & EBG_NODE_HAS_OBB) ? m.node_obb + ref : nullptr);
+      if (obx != nullptr) {
+        const float4* ob = reinterpret_cast<const float4*>(obx);
+        if (!__any_sync(FULL, obbDist2(__ldg(ob), __ldg(ob + 1), __ldg(ob + 2), px, py, pz) <= bound)) {
+          continue;
+        }
+      }
       if (ref & EBG_LEAF_BIT) {
         const uint32_t t0 = ref & ~EBG_LEAF_BIT;
         for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {

@@ -244,6 +244,8 @@ struct Builder
   std::atomic<uint32_t>      nodeCount{0};
   std::vector<uint32_t>*     leafFirst = nullptr;
   std::vector<uint32_t>*     leafCount = nullptr;
+  std::vector<uint32_t>*     nodeFirst = nullptr;
+  std::vector<uint32_t>*     nodeEnd   = nullptr;
   std::atomic<int>           maxDepth{0};
   std::atomic<int64_t>       leaves{0};
 
@@ -396,7 +398,9 @@ struct Builder
       ch[pick]  = l;
       ch[nc++]  = r;
     }
-    EbgNode4& nd = nodes[self];
+    EbgNode4& nd       = nodes[self];
+    (*nodeFirst)[self] = b;
+    (*nodeEnd)[self]   = e;
     for (int k = 0; k < 4; k++) {
       nd.lox[k] = nd.loy[k] = nd.loz[k] = std::numeric_limits<float>::infinity();
       nd.hix[k] = nd.hiy[k] = nd.hiz[k] = -std::numeric_limits<float>::infinity();
@@ -529,6 +533,10 @@ bool buildBvh4(const std::vector<double>& boxLo,
   out.leafCount.assign(n, 0);
   B.leafFirst = &out.leafFirst;
   B.leafCount = &out.leafCount;
+  out.nodeFirst.assign(n, 0);
+  out.nodeEnd.assign(n, 0);
+  B.nodeFirst = &out.nodeFirst;
+  B.nodeEnd   = &out.nodeEnd;
   if (n <= size_t(leafSize)) {
     out.rootRef   = EBG_LEAF_BIT | 0u;
     out.rootCount = uint32_t(n);  // leaf id 0
@@ -537,6 +545,8 @@ bool buildBvh4(const std::vector<double>& boxLo,
     out.leafFirst.assign(1, 0);
     out.leafCount.assign(1, uint32_t(n));
     out.nodes.clear();
+    out.nodeFirst.clear();
+    out.nodeEnd.clear();
     return true;
   }
   B.nodeCount = 1;
@@ -545,6 +555,8 @@ bool buildBvh4(const std::vector<double>& boxLo,
   B.node(0, 0, uint32_t(n), 1);
 
   nodes.resize(B.nodeCount.load());
+  out.nodeFirst.resize(nodes.size());
+  out.nodeEnd.resize(nodes.size());
   out.nodes     = std::move(nodes);
   out.rootRef   = 0;
   out.rootCount = 0;

@@ -28,6 +28,7 @@ struct Bvh4
   std::vector<EbgNode4> nodes;
   std::vector<uint32_t> order; // leaf position -> primitive index
   std::vector<uint32_t> leafFirst, leafCount; // per leaf id: first position and primitive count
+  std::vector<uint32_t> nodeFirst, nodeEnd;   // per interior node: its subtree's positions [first, end)
   uint32_t              rootRef   = 0;
   uint32_t              rootCount = 0;
   int                   depth     = 0;

@@ -178,7 +178,7 @@ __global__ void kQueryKeys(const float* __restrict__ pts, int64_t n, float lx, f
   const float fx = fminf(fmaxf((x - lx) * sx, 0.f), 1023.f);
   const float fy = fminf(fmaxf((y - ly) * sy, 0.f), 1023.f);
   const float fz = fminf(fmaxf((z - lz) * sz, 0.f), 1023.f);
-  // NaN coordinates quantise to 0 (fmaxf drops NaN); they are rejected on the host before launch
+  // NaN coordinates quantise to 0 (fmaxf drops NaN); the traversal kernel reports them (ST_INPUT)
   keys[i] = (spread10(uint32_t(fx)) << 2) | (spread10(uint32_t(fy)) << 1) | spread10(uint32_t(fz));
   ids[i]  = uint32_t(i);
 }

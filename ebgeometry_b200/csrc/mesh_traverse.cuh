@@ -205,17 +205,28 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           }
         }
         else {
-          if (STATS && need) {
-            cnt_.node++;
-          }
-          if (STATS) {
-            cnt_.pnode++;
-          }
+          // the node's loads go out first; the oriented-box test below overlaps their latency
           const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
           const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
           const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
           const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
           const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+          // lanes for which the node's own oriented box (all triangles below it) is within bound
+          bool needN = need;
+          if (cntw & EBG_NODE_HAS_OBB) {
+            const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
+            const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
+            needN            = need && obbDist2(o0, o1, o2, px, py, pz) <= best;
+            if (!__any_sync(FULL, needN)) {
+              continue;
+            }
+          }
+          if (STATS && needN) {
+            cnt_.node++;
+          }
+          if (STATS) {
+            cnt_.pnode++;
+          }
           const float   clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
                       clz[4] = {lz.x, lz.y, lz.z, lz.w};
           const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
@@ -224,7 +235,9 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           float key[4];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
-            const float dk = boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
+            // lanes that ruled the node out cannot gain from its children
+            const float dk = needN ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz)
+                                   : __int_as_float(0x7f800000);
             // an empty slot (child 0, count 0: node 0 is the root, never a child) is never pushed
             const bool  nk = __any_sync(FULL, dk <= best) && (cref[k] | ccnt[k]) != 0u;
             // uniform ordering key: the child's smallest distance over the packet's lanes (one
