@@ -392,17 +392,23 @@ def run_ours(args, rank, world, local_rank):
     # equal work unit for both runs) over the traversal phase's event-timed duration
     hbm_peak, peak_kind = measured_peaks()
     l2_gbs = l2_read_bandwidth()
-    node_b, tri_b = 128, 48
+    node_b, box_b, tri_b = 128, 48, 48
     nq = float(n)
-    bq = 12 + 4 + st["nodes_visited"] / nq * node_b + st["triangles_tested"] / nq * tri_b
+    bq = (12 + 4 + st["nodes_visited"] / nq * node_b + st["boxes_tested"] / nq * box_b +
+          st["triangles_tested"] / nq * tri_b)
     trav_ms = float(tms[:, 1].mean())
     achieved = nq * bq / (trav_ms * 1e-3) / 1e9
+    # DRAM bytes of one traversal launch on this workload, from a single-pass ncu capture recorded
+    # in the profile summaries as "traffic <workload key> <bytes>" lines
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as fh:
-            tj = json.load(fh)
-        traffic = tj.get(f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}")
+    key = f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}"
+    for fn in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
+        if fn.endswith(".md"):
+            with open(os.path.join(ROOT, "profiles", fn)) as fh:
+                for ln in fh:
+                    parts = ln.split()
+                    if len(parts) >= 3 and parts[0] == "traffic" and parts[1] == key:
+                        traffic = int(parts[2])
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -429,6 +435,7 @@ def run_ours(args, rank, world, local_rank):
     def per_query(s):
         return None if s is None else {"nodes": s["nodes_visited"] / nq, "leaves": s["leaves_visited"] / nq,
                                        "triangles": s["triangles_tested"] / nq,
+                                       "oriented_boxes": s["boxes_tested"] / nq,
                                        "band_fraction": s["band_queries"] / nq,
                                        "seed_fallback_fraction": s["seed_fallbacks"] / nq}
 
@@ -457,7 +464,8 @@ def run_ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "kMeshSdf32 (FP32 packet traversal" + (", seeded)" if seed is not None else ")"),
-                     "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit)",
+                     "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit): 16 B query in/out + 128 B per node + "
+                                    "48 B per oriented box + 48 B per triangle",
                      "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
         "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                 "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},

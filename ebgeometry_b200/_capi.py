@@ -53,7 +53,8 @@ class QueryStats(C.Structure):
     _fields_ = [("nodes_visited", C.c_int64), ("leaves_visited", C.c_int64),
                 ("triangles_tested", C.c_int64), ("band_queries", C.c_int64),
                 ("seed_fallbacks", C.c_int64), ("packets", C.c_int64), ("packet_pops", C.c_int64),
-                ("packet_nodes", C.c_int64), ("packet_leaves", C.c_int64), ("packet_triangles", C.c_int64)]
+                ("packet_nodes", C.c_int64), ("packet_leaves", C.c_int64), ("packet_triangles", C.c_int64),
+                ("boxes_tested", C.c_int64), ("packet_boxes", C.c_int64)]
 
 
 EBG_OK = 0

@@ -742,14 +742,15 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   ebg_status   rc;
-  unsigned long long host[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  constexpr int      NSTAT    = 12;
+  unsigned long long host[NSTAT] = {};
   {
     Workspace           ws(s);
-    unsigned long long* dev = ws.get<unsigned long long>(10);
+    unsigned long long* dev = ws.get<unsigned long long>(NSTAT);
     if (!ws.ok) {
       return setError(EBG_ERR_NO_MEMORY, "stats buffer");
     }
-    cudaMemsetAsync(dev, 0, 10 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(dev, 0, NSTAT * sizeof(unsigned long long), s);
     rc = meshQuery(m, points_dev, n, dist_dev, nullptr, opts, dev, s);
     if (rc == EBG_OK) {
       cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, s);
@@ -771,6 +772,8 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   stats->packet_nodes     = int64_t(host[7]);
   stats->packet_leaves    = int64_t(host[8]);
   stats->packet_triangles = int64_t(host[9]);
+  stats->boxes_tested     = int64_t(host[10]);
+  stats->packet_boxes     = int64_t(host[11]);
   return ebg_check_status(m, stream);
 }
 

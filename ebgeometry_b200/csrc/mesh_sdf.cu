@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
     }
     uint32_t iters = 0;
     int      err   = 0;
-    uint32_t cNode = 0, cLeaf = 0, cTri = 0, cFall = 0;
-    uint32_t pPops = 0, pNode = 0, pLeaf = 0, pTri = 0;
+    uint32_t cNode = 0, cLeaf = 0, cTri = 0, cFall = 0, cBox = 0;
+    uint32_t pPops = 0, pNode = 0, pLeaf = 0, pTri = 0, pBox = 0;
 
 #pragma unroll 1
     for (int pass = 0; pass < (SEEDED ? 2 : 1); pass++) {
@@ -110,6 +110,8 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       cNode += tc.node;
       cLeaf += tc.leaf;
       cTri += tc.tri;
+      cBox += tc.box;
+      pBox += tc.pbox;
       pPops += tc.pops;
       pNode += tc.pnode;
       pLeaf += tc.pleaf;
@@ -150,8 +152,9 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
     }
     if (STATS) {
       if (!valid) {
-        cNode = cLeaf = cTri = cFall = 0;
+        cNode = cLeaf = cTri = cFall = cBox = 0;
       }
+      atomicAdd(a.stats + 10, (unsigned long long)cBox);
       atomicAdd(a.stats + 0, (unsigned long long)cNode);
       atomicAdd(a.stats + 1, (unsigned long long)cLeaf);
       atomicAdd(a.stats + 2, (unsigned long long)cTri);
@@ -162,6 +165,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         atomicAdd(a.stats + 7, (unsigned long long)pNode);
         atomicAdd(a.stats + 8, (unsigned long long)pLeaf);
         atomicAdd(a.stats + 9, (unsigned long long)pTri);
+        atomicAdd(a.stats + 11, (unsigned long long)pBox);
       }
     }
   }

@@ -135,8 +135,8 @@ __device__ __forceinline__ float signedFromWinner(const EbgMeshView& m, uint32_t
 
 struct TraversalCounters
 {
-  uint32_t node = 0, leaf = 0, tri = 0, fall = 0;      // per lane: what this query needed
-  uint32_t pops = 0, pnode = 0, pleaf = 0, ptri = 0;   // per packet: what the warp executed
+  uint32_t node = 0, leaf = 0, tri = 0, fall = 0, box = 0; // per lane: what this query needed
+  uint32_t pops = 0, pnode = 0, pleaf = 0, ptri = 0, pbox = 0; // per packet: what the warp executed
 };
 
 // One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
@@ -180,6 +180,10 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           const float4* ob = reinterpret_cast<const float4*>(m.obb + (cntw >> EBG_COUNT_BITS));
           const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
           const bool    needObb = obbDist2(o0, o1, o2, px, py, pz) <= best;
+          if (STATS) {
+            cnt_.box += need;
+            cnt_.pbox++;
+          }
           if (!__any_sync(FULL, needObb)) {
             continue;
           }
@@ -217,6 +221,10 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
             const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
             needN            = need && obbDist2(o0, o1, o2, px, py, pz) <= best;
+            if (STATS) {
+              cnt_.box += need;
+              cnt_.pbox++;
+            }
             if (!__any_sync(FULL, needN)) {
               continue;
             }

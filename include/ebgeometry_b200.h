@@ -120,6 +120,8 @@ typedef struct ebg_query_stats
   int64_t packet_nodes;      /* interior nodes whose children were tested */
   int64_t packet_leaves;     /* leaves whose triangles were tested */
   int64_t packet_triangles;  /* point-triangle tests executed by the warp */
+  int64_t boxes_tested;      /* oriented leaf/node boxes evaluated, per query */
+  int64_t packet_boxes;      /* oriented boxes the warp evaluated */
 } ebg_query_stats;
 
 const char* ebg_last_error(void);
