@@ -128,11 +128,21 @@ class TriMeshSDF:
                         radius_hint=None, occupancy=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
-        point (synchronous).  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
+        point (synchronous).  Float64 points (numpy or CUDA) take the FP64 entry points: every
+        query is re-evaluated in FP64 and the distances come back as float64.  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
         times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
         radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
         float32 tensor of per-point upper bounds on |d| that seed the bound the same way."""
         opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy)
+        if isinstance(points, np.ndarray) and points.dtype == np.float64:
+            p = np.ascontiguousarray(points).reshape(-1, 3)
+            n = p.shape[0]
+            d = out if out is not None else np.empty(n, np.float64)
+            t = closest_tri
+            check(lib.ebg_mesh_signed_distance_f64_host(self._h, _ptr(p), n, _ptr(d),
+                                                        _ptr(t) if t is not None else None,
+                                                        C.byref(opts), None))
+            return (d, t) if t is not None else d
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
             n = p.shape[0]
@@ -144,8 +154,15 @@ class TriMeshSDF:
             return (d, t) if t is not None else d
         import torch
         p = points
+        if p.is_cuda and p.dtype == torch.float64 and p.is_contiguous():
+            n = p.numel() // 3
+            d = out if out is not None else torch.empty(n, dtype=torch.float64, device=p.device)
+            check(lib.ebg_mesh_signed_distance_f64(self._h, C.c_void_p(p.data_ptr()), n, C.c_void_p(d.data_ptr()),
+                                                   C.c_void_p(closest_tri.data_ptr()) if closest_tri is not None
+                                                   else None, C.byref(opts), _stream_ptr(stream)))
+            return (d, closest_tri) if closest_tri is not None else d
         if not (p.is_cuda and p.dtype == torch.float32 and p.is_contiguous()):
-            raise ValueError("points must be a contiguous float32 CUDA tensor of shape (n,3)")
+            raise ValueError("points must be a contiguous float32 or float64 CUDA tensor of shape (n,3)")
         n = p.numel() // 3
         d = out if out is not None else torch.empty(n, dtype=torch.float32, device=p.device)
         check(lib.ebg_mesh_signed_distance(self._h, C.c_void_p(p.data_ptr()), n,

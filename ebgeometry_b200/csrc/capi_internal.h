@@ -55,7 +55,8 @@ struct ebg_seed
 namespace ebg {
 
 // The mesh query pipeline (ordering, optional seed inference, FP32 traversal, FP64 band pass) on
-// device buffers, asynchronous on s.
+// device buffers, asynchronous on s.  With pts64/out64 (the caller's FP64 points, of which pts is
+// the FP32 rounding, and an FP64 result array) every query is re-evaluated in FP64.
 ebg_status meshQuery(const ebg_mesh*       m,
                      const float*          pts,
                      int64_t               n,
@@ -63,7 +64,9 @@ ebg_status meshQuery(const ebg_mesh*       m,
                      int32_t*              outTri,
                      const ebg_query_opts* opts,
                      unsigned long long*   statsDev,
-                     cudaStream_t          s);
+                     cudaStream_t          s,
+                     const double*         pts64 = nullptr,
+                     double*               out64 = nullptr);
 
 } // namespace ebg
 

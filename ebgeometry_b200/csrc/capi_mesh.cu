@@ -433,17 +433,21 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
                           int32_t*              outTri,
                           const ebg_query_opts* opts,
                           unsigned long long*   statsDev,
-                          cudaStream_t          s)
+                          cudaStream_t          s,
+                          const double*         pts64,
+                          double*               out64)
 {
   if (n > int64_t(INT32_MAX)) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
   }
   const bool sort   = !(opts && opts->no_sort);
-  const bool band64 = !(opts && opts->no_fp64_band);
+  // an FP64 result re-evaluates every query in FP64 (the band covers all distances)
+  const bool fp64all = out64 != nullptr;
+  const bool band64  = fp64all || !(opts && opts->no_fp64_band);
   const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block
                                                           : (m->tunedWpb > 0 ? m->tunedWpb : 4);
   const int  occ    = (opts && opts->occupancy > 0) ? opts->occupancy : m->tunedOccupancy;
-  double     band   = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
+  double     band   = fp64all ? double(INFINITY) : ((opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal);
   const ebg_seed* seed = opts ? opts->seed : nullptr;
   if (seed && seed->device != m->device) {
     return setError(EBG_ERR_INVALID, "seed model lives on another device than the mesh");
@@ -493,11 +497,12 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
       return setError(EBG_ERR_CUDA, "query sort failed");
     }
   }
-  // learned pruning radius per packet of 32 sorted queries (the traversal widens it per lane by the
-  // distance to the packet centroid, which keeps it an upper bound wherever it holds at the centroid)
-  float* seedR = nullptr;
+  // learned pruning radius per packet of 32 sorted queries, predicted at the packet's centre (the
+  // traversal widens it per lane by the distance to that centre, which keeps it an upper bound
+  // wherever it holds at the centre)
+  float4* seedPk = nullptr;
   if (seed) {
-    seedR = ws.get<float>((n + 31) / 32);
+    seedPk = ws.get<float4>((n + 31) / 32);
     if (!ws.ok) {
       return setError(EBG_ERR_NO_MEMORY, "seed workspace allocation failed");
     }
@@ -512,15 +517,17 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   if (tm) {
     cudaEventRecord(ev[1], s);
   }
-  if (seed && launchSeedPackets(seed->view, pts, order, n, seedR, m->numSms, s) != cudaSuccess) {
+  if (seed && launchSeedPackets(seed->view, pts, order, n, seedPk, m->numSms, s) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, "seed inference launch failed");
   }
 
   MeshQueryArgs a{};
   a.mesh       = m->view;
   a.points     = pts;
+  a.points64   = pts64;
+  a.out_d64    = out64;
   a.order      = order;
-  a.seed_r     = seedR;
+  a.seed_pk    = seedPk;
   a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
   a.n          = n;
   a.out_d      = outD;
@@ -723,6 +730,75 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
   return ebg_check_status(m, stream);
 }
 
+ebg_status ebg_mesh_signed_distance_f64(const ebg_mesh*       m,
+                                        const double*         points_dev,
+                                        int64_t               n,
+                                        double*               dist_dev,
+                                        int32_t*              closest_tri_dev,
+                                        const ebg_query_opts* opts,
+                                        void*                 stream)
+{
+  if (m == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard  guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Workspace    ws(s);
+  float*       p32 = ws.get<float>(3 * n);
+  float*       d32 = ws.get<float>(n);
+  if (!ws.ok) {
+    return setError(EBG_ERR_NO_MEMORY, "FP32 copy of the FP64 points");
+  }
+  launchDoubleToFloat(points_dev, p32, 3 * n, s);
+  return meshQuery(m, p32, n, d32, closest_tri_dev, opts, nullptr, s, points_dev, dist_dev);
+}
+
+ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       m,
+                                             const double*         points_host,
+                                             int64_t               n,
+                                             double*               dist_host,
+                                             int32_t*              closest_tri_host,
+                                             const ebg_query_opts* opts,
+                                             void*                 stream)
+{
+  if (m == nullptr || n < 0 || (n > 0 && (points_host == nullptr || dist_host == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard  guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaMemsetAsync(m->dStatus, 0, sizeof(int), s);
+  ebg_status rc;
+  {
+    Workspace ws(s);
+    double*   dp = ws.get<double>(3 * n);
+    double*   dd = ws.get<double>(n);
+    int32_t*  dt = closest_tri_host ? ws.get<int32_t>(n) : nullptr;
+    if (!ws.ok) {
+      return setError(EBG_ERR_NO_MEMORY, "device buffers for the host call");
+    }
+    cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s);
+    rc = ebg_mesh_signed_distance_f64(m, dp, n, dd, dt, opts, stream);
+    if (rc == EBG_OK) {
+      cudaMemcpyAsync(dist_host, dd, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+      if (dt) {
+        cudaMemcpyAsync(closest_tri_host, dt, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      }
+    }
+  }
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  return ebg_check_status(m, stream);
+}
+
 ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
                                           const float*          points_dev,
                                           int64_t               n,
@@ -850,13 +926,11 @@ ebg_status ebg_mesh_value(const ebg_mesh* m, double x, double y, double z, doubl
   if (m == nullptr || value == nullptr) {
     return setError(EBG_ERR_INVALID, "null argument");
   }
-  const float p[3] = {float(x), float(y), float(z)};
-  float       d    = 0.f;
+  // one point, evaluated in FP64 like the reference's value()
+  const double   p[3] = {x, y, z};
   ebg_query_opts o{};
   o.no_sort = 1;
-  const ebg_status rc = ebg_mesh_signed_distance_host(m, p, 1, &d, nullptr, &o, nullptr);
-  *value              = double(d);
-  return rc;
+  return ebg_mesh_signed_distance_f64_host(m, p, 1, value, nullptr, &o, nullptr);
 }
 
 ebg_status ebg_check_status(const ebg_mesh* m, void* stream)

@@ -128,7 +128,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
   auto* order    = reinterpret_cast<uint32_t*>(take(u32n));
   auto* bandList = reinterpret_cast<uint32_t*>(take(u32n));
   auto* bandD    = reinterpret_cast<float*>(take(u32n));
-  auto* seedR    = reinterpret_cast<float*>(take(size_t((n + 31) / 32) * sizeof(float)));
+  auto* seedPk   = reinterpret_cast<float4*>(take(size_t((n + 31) / 32) * sizeof(float4)));
   size_t sortBytes = 0;
   if (sort) {
     cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, keysIn, keysOut, idsIn, order, int(n), 0, 30, s);
@@ -148,7 +148,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
       return setError(EBG_ERR_CUDA, "query sort failed");
     }
   }
-  if (seed && launchSeedPackets(seed->view, points_dev, sort ? order : nullptr, n, seedR, m->numSms, s) !=
+  if (seed && launchSeedPackets(seed->view, points_dev, sort ? order : nullptr, n, seedPk, m->numSms, s) !=
                 cudaSuccess) {
     return setError(EBG_ERR_CUDA, "seed inference launch failed");
   }
@@ -156,7 +156,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
   a.mesh       = m->view;
   a.points     = points_dev;
   a.order      = sort ? order : nullptr;
-  a.seed_r     = seed ? seedR : nullptr;
+  a.seed_pk    = seed ? seedPk : nullptr;
   a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
   a.n          = n;
   a.out_d      = dist_dev;

@@ -95,11 +95,20 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
     const uint32_t jj    = valid ? j : count - 1;
     const uint32_t pos   = a.band_list[jj];
     const uint32_t id    = a.order ? a.order[pos] : pos;
-    const D3       P     = {double(a.points[3 * size_t(id)]), double(a.points[3 * size_t(id) + 1]),
-                    double(a.points[3 * size_t(id) + 2])};
-    const float    px = float(P.x), py = float(P.y), pz = float(P.z);
+    // the FP64 point: the caller's own when it passed FP64, else its FP32 point
+    const D3       P     = a.points64 ? D3{a.points64[3 * size_t(id)], a.points64[3 * size_t(id) + 1],
+                                          a.points64[3 * size_t(id) + 2]}
+                                      : D3{double(a.points[3 * size_t(id)]), double(a.points[3 * size_t(id) + 1]),
+                                           double(a.points[3 * size_t(id) + 2])};
+    const float    px = a.points[3 * size_t(id)], py = a.points[3 * size_t(id) + 1], pz = a.points[3 * size_t(id) + 2];
     const float    d32 = a.band_d32[jj];
-    float          r   = (fabsf(d32) + delta) * 1.000001f;
+    // Boxes are tested at the FP32 point, `shift` from the FP64 point.  The mesh is within
+    // |d32| + delta of the FP32 point (delta covers the FP32 distance error near the surface, the
+    // relative term far from it), so the FP64 winner is within |d32| + delta + shift of the FP64
+    // point and within |d32| + delta + 2 shift of the FP32 point.
+    const double   ex = P.x - double(px), ey = P.y - double(py), ez = P.z - double(pz);
+    const float    shift = float(sqrt(ex * ex + ey * ey + ez * ez)) * 1.0001f;
+    float          r   = (fabsf(d32) * 1.00001f + delta + 2.f * shift) * 1.000001f;
     float          bound = r * r;
     double         best  = DBL_MAX;
     int            bt    = -1;
@@ -142,8 +151,9 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
           if (fabs(d) < fabs(best)) {
             best = d;
             bt   = int(tt);
-            // shrink the bound to the FP64 winner (with the same relative margin)
-            const float rb = float(fabs(d)) * 1.000001f + 1e-30f;
+            // shrink the bound to the FP64 winner (with the same relative margin), measured at the
+            // FP32 point where the boxes are tested
+            const float rb = (float(fabs(d)) + shift) * 1.000001f + 1e-30f;
             bound          = fminf(bound, rb * rb);
           }
         }
@@ -196,6 +206,9 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
     if (err && lane == 0) {
       atomicOr(a.status, err);
     }
+    if (valid && a.out_d64 != nullptr) {
+      a.out_d64[id] = bt >= 0 ? best : double(d32);
+    }
     if (valid && bt >= 0) {
       a.out_d[id] = float(best);
       if (a.out_tri) {
@@ -206,6 +219,22 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
 }
 
 } // namespace
+
+namespace {
+__global__ void kDoubleToFloat(const double* __restrict__ in, float* __restrict__ out, int64_t count)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += int64_t(gridDim.x) * blockDim.x) {
+    out[i] = float(in[i]);
+  }
+}
+} // namespace
+
+void launchDoubleToFloat(const double* in, float* out, int64_t count, cudaStream_t s)
+{
+  int64_t blocks = (count + 255) / 256;
+  blocks         = blocks < 4096 ? blocks : 4096;
+  kDoubleToFloat<<<unsigned(blocks < 1 ? 1 : blocks), 256, 0, s>>>(in, out, count);
+}
 
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s)
 {

@@ -13,11 +13,14 @@ struct MeshQueryArgs
 {
   EbgMeshView        mesh;
   const float*       points;     // caller's xyz (n x 3)
+  const double*      points64;   // the caller's FP64 xyz when it passed FP64 (nullable)
   const uint32_t*    order;      // sorted position -> caller index (nullptr = identity)
-  const float*       seed_r;     // per packet of 32 sorted queries: predicted radius (nullptr = none)
+  const float4*      seed_pk;    // per packet of 32 sorted queries: centre xyz and the radius
+                                 // predicted there (nullptr = none)
   const float*       hint;       // per query (caller order): radius upper bound (nullptr = none)
   int64_t            n;
   float*             out_d;      // caller order
+  double*            out_d64;    // caller order, FP64 results of the band pass (nullable)
   int32_t*           out_tri;    // caller order (nullable)
   float              band;       // |d| <= band -> FP64 re-evaluation list
   uint32_t*          band_list;  // sorted positions needing FP64 (nullable = no band pass)
@@ -25,7 +28,7 @@ struct MeshQueryArgs
   float*             band_d32;   // FP32 distance of each band entry
   unsigned long long* work;      // packet counter (zeroed before the launch)
   int*               status;     // device status word (ST_* bits)
-  unsigned long long* stats;     // 10 counters (nullable): 5 per query, 5 per packet
+  unsigned long long* stats;     // 12 counters (nullable): 6 per query, 6 per packet
 };
 
 // Morton keys of the query points (30 bits) and the identity permutation.
@@ -37,6 +40,9 @@ cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int warpsPerBlock, int numSm
 
 // FP64 re-evaluation of the band list (reads band_count on the device).
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s);
+
+// out[i] = float(in[i]) for i < count (round to nearest).
+void launchDoubleToFloat(const double* in, float* out, int64_t count, cudaStream_t s);
 
 } // namespace ebg
 

@@ -68,7 +68,6 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
     const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
     const float    px = __ldg(a.points + 3 * size_t(id)), py = __ldg(a.points + 3 * size_t(id) + 1),
                 pz = __ldg(a.points + 3 * size_t(id) + 2);
-    const float cx = warpSum(px) * (1.f / 32.f), cy = warpSum(py) * (1.f / 32.f), cz = warpSum(pz) * (1.f / 32.f);
 
     if (valid && !(isfinite(px) && isfinite(py) && isfinite(pz))) {
       atomicOr(a.status, ST_INPUT);
@@ -81,11 +80,11 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       best          = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
     }
     if (SEED == 1) {
-      // packet radius at the centroid, widened by this lane's distance to the centroid (the SDF is
-      // 1-Lipschitz), squared and rounded up so FP32 rounding never makes the bound too tight
-      const float rp = __ldg(a.seed_r + pk);
-      const float ex = px - cx, ey = py - cy, ez = pz - cz;
-      const float r  = rp + sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+      // packet radius at the packet's centre, widened by this lane's distance to that centre (the
+      // SDF is 1-Lipschitz), squared and rounded up so FP32 rounding never makes the bound too tight
+      const float4 sp = __ldg(a.seed_pk + pk);
+      const float  ex = px - sp.x, ey = py - sp.y, ez = pz - sp.z;
+      const float  r  = sp.w + sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez))) * 1.000001f;
       best           = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
     }
     uint32_t iters = 0;
@@ -236,7 +235,7 @@ cudaError_t launchStats(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_
 template <int OCC>
 cudaError_t launchSeed(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
-  const int mode = a.seed_r != nullptr ? 1 : (a.hint != nullptr ? 2 : 0);
+  const int mode = a.seed_pk != nullptr ? 1 : (a.hint != nullptr ? 2 : 0);
   return mode == 1 ? launchStats<1, OCC>(a, wpb, numSms, s)
                    : (mode == 2 ? launchStats<2, OCC>(a, wpb, numSms, s) : launchStats<0, OCC>(a, wpb, numSms, s));
 }

@@ -29,10 +29,14 @@ int main()
   }
   std::vector<float> d(pts.size() / 3);
   sdf.signedDistances(pts.data(), d.size(), d.data());
-  double maxDiff = 0;
+  // the same points in FP64 end to end: value() is FP64 too, so these agree exactly
+  std::vector<double> pts64(pts.begin(), pts.end()), d64(d.size());
+  sdf.signedDistances(pts64.data(), d64.size(), d64.data());
+  double maxDiff = 0, maxDiff64 = 0;
   for (size_t i = 0; i < d.size(); i += 37) {
     const double one = asImplicit.value(Vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
     maxDiff          = std::fmax(maxDiff, std::fabs(one - double(d[i])));
+    maxDiff64        = std::fmax(maxDiff64, std::fabs(one - d64[i]));
   }
   // the octahedron's exact signed distance is (|x|+|y|+|z|-1)/sqrt(3) where the closest feature
   // is a face; check the centre
@@ -45,10 +49,11 @@ int main()
   }
   PointCloudBVH     pc(cloud);
   const auto        hit = pc.closestPoint(cloud[123]);
-  std::printf("batch/single max diff %.3g, centre %.6f (expect %.6f), nearest of point 123: %zu (d2 %g)\n", maxDiff,
-              centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared));
-  const bool ok = maxDiff <= 1e-6 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-6 && hit.index == 123 &&
-                  hit.distanceSquared == 0.f;
+  std::printf("batch/single max diff %.3g (FP64 batch: %.3g), centre %.6f (expect %.6f), nearest of point 123: "
+              "%zu (d2 %g)\n",
+              maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared));
+  const bool ok = maxDiff <= 1e-6 && maxDiff64 == 0.0 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-12 &&
+                  hit.index == 123 && hit.distanceSquared == 0.f;
   std::printf("%s\n", ok ? "ok" : "FAILED");
   return ok ? 0 : 1;
 }

@@ -126,6 +126,22 @@ public:
   void signedDistancesDevice(const float* a_pointsDev, size_t a_n, float* a_distDev, void* a_stream = nullptr,
                              const SeedModel* a_seed = nullptr) const;
 
+  // FP64 end to end (the reference's own precision): host points, synchronous.
+  void signedDistances(const double* a_pointsHost, size_t a_n, double* a_distHost,
+                       int32_t* a_closestTriangleHost = nullptr) const
+  {
+    ebg_query_opts o{};
+    check(ebg_mesh_signed_distance_f64_host(m_mesh, a_pointsHost, int64_t(a_n), a_distHost, a_closestTriangleHost,
+                                            &o, nullptr));
+  }
+
+  // FP64 end to end, device buffers, asynchronous on a_stream.
+  void signedDistancesDevice(const double* a_pointsDev, size_t a_n, double* a_distDev, void* a_stream = nullptr) const
+  {
+    ebg_query_opts o{};
+    check(ebg_mesh_signed_distance_f64(m_mesh, a_pointsDev, int64_t(a_n), a_distDev, nullptr, &o, a_stream));
+  }
+
   ebg_mesh_info info() const
   {
     ebg_mesh_info i{};

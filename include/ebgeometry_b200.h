@@ -17,7 +17,8 @@
  *  - stream is a cudaStream_t passed as void* (NULL = the legacy default stream).  Device entry
  *    points are asynchronous on that stream unless stated otherwise; status codes that depend on
  *    device-side checks are reported by the next synchronising call (ebg_check_status).
- *  - Points are float32 xyz triples (interleaved, 12 bytes per point).
+ *  - Points are float32 xyz triples (interleaved, 12 bytes per point), except in the *_f64 entry
+ *    points, which take and return FP64.
  */
 #ifndef EBGEOMETRY_B200_H
 #define EBGEOMETRY_B200_H
@@ -200,6 +201,29 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       mesh,
                                          const ebg_query_opts* opts,
                                          void*                 stream);
 
+/* Batched TriMeshSDF<double>::signedDistance in FP64 end to end (the reference's own precision,
+ * MeshDistanceFunctionsImplem.hpp:480-509 with TriangleSoAImplem.hpp:1029-1180): FP64 points in,
+ * FP64 distances out.  The FP32 traversal finds each query's candidate bound; every query is then
+ * re-evaluated with the reference's FP64 triangle test over all triangles within that bound of the
+ * caller's FP64 point, so the result is the reference's value (opts->band and no_fp64_band are
+ * ignored).  Asynchronous on stream. */
+ebg_status ebg_mesh_signed_distance_f64(const ebg_mesh*       mesh,
+                                        const double*         points_dev,
+                                        int64_t               n,
+                                        double*               dist_dev,
+                                        int32_t*              closest_tri_dev,
+                                        const ebg_query_opts* opts,
+                                        void*                 stream);
+
+/* The same with host buffers (copies in, evaluates, copies out, synchronises). */
+ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       mesh,
+                                             const double*         points_host,
+                                             int64_t               n,
+                                             double*               dist_host,
+                                             int32_t*              closest_tri_host,
+                                             const ebg_query_opts* opts,
+                                             void*                 stream);
+
 /* The same batched query WITHOUT ANY DEVICE ALLOCATION (no counterpart in the reference).  For
  * callers that cannot let a library allocate: AMR codes such as AMReX reserve most of the GPU's memory
  * for their own arena at start-up, so a library's cudaMalloc or stream-ordered allocation can fail
@@ -241,7 +265,8 @@ ebg_status ebg_mesh_autotune(ebg_mesh*    mesh,
                              void*        stream);
 
 /* ImplicitFunction<T>::value(point) for one point (ImplicitFunction.hpp:51-52): the drop-in
- * single-point call.  Synchronous; each call is one tiny launch, so batch where you can. */
+ * single-point call, in FP64 (ebg_mesh_signed_distance_f64_host).  Synchronous; each call is a few
+ * tiny launches, so batch where you can. */
 ebg_status ebg_mesh_value(const ebg_mesh* mesh, double x, double y, double z, double* value);
 
 /* Blocks until the stream's work for this mesh is done and reports any device-side error

@@ -93,7 +93,8 @@ class _Ref:
     # meshes ------------------------------------------------------------------------------------
     class Mesh:
         """Reference TriMeshSDF built through Soup::soupToDCEL.  kind 0: <double,short,4,4>;
-        kind 1: ISA-default K/W.  build 0 SAH, 1 Morton."""
+        kind 1: ISA-default K/W; kind 3: MeshSDF<double,short,4> over the DCEL faces.  build 0 SAH,
+        1 Morton."""
 
         def __init__(self, ref, v, f, kind=0, build=0, max_leaf_groups=4):
             self.ref = ref
@@ -107,10 +108,12 @@ class _Ref:
                 self.ref.lib.ref_mesh_destroy(self.h)
                 self.h = None
 
-        def sdf(self, p, flat=False, threads=0):
+        def sdf(self, p, flat=False, threads=0, dcel=False):
+            """flat: FlatMeshSDF (DCEL faces, brute force); dcel: the MeshSDF (needs kind 3)."""
             p = np.ascontiguousarray(p, np.float64).reshape(-1, 3)
             out = np.empty(p.shape[0])
-            rc = self.ref.lib.ref_mesh_sdf(self.h, _ptr(p), p.shape[0], _ptr(out), 1 if flat else 0, threads)
+            which = 1 if flat else (2 if dcel else 0)
+            rc = self.ref.lib.ref_mesh_sdf(self.h, _ptr(p), p.shape[0], _ptr(out), which, threads)
             assert rc == 0
             return out
 
@@ -218,6 +221,8 @@ class _Port:
             "port_triangle_sd_scalar": (_D, [_P, _P, _P, _P, _P]),
             "port_mesh_normals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _P]),
             "port_mesh_sdf_brute": (None, [_P, _P, _I64, _P, _P, _P, _P, _I64, _P, _P]),
+            "port_mesh_sdf_flat": (None, [_P, _P, _I64, _P, _P, _P, _P, _I64, _P, _P]),
+            "port_dcel_face_sd": (_D, [_P, _P, _P, _P, _P]),
             "port_knn_brute": (None, [_P, _I64, _P, _I64, C.c_int, _P, _P]),
             "port_sphere_sd": (_D, [_P, _D, _P]),
             "port_rotate_point": (None, [_D, C.c_int, _P, _P]),
@@ -259,6 +264,26 @@ class _Port:
         self.lib.port_mesh_sdf_brute(_ptr(v), _ptr(f64), f64.shape[0], _ptr(tn), _ptr(vn_v), _ptr(en), _ptr(p),
                                      p.shape[0], _ptr(out), _ptr(tri))
         return out, tri
+
+    def mesh_sdf_flat(self, v, f, p):
+        """FlatMeshSDF (DCEL faces, Direct2 search): values and winning faces."""
+        v = np.ascontiguousarray(v, np.float64)
+        f64 = np.ascontiguousarray(f, np.int64)
+        tn, vn, en = self.mesh_normals(v, f64)
+        vn_v = np.empty((v.shape[0], 3))
+        vn_v[f64.ravel()] = vn.reshape(-1, 3)
+        tn, vn_v, en = (np.ascontiguousarray(x, np.float64) for x in (tn, vn_v, en))
+        p = np.ascontiguousarray(p, np.float64).reshape(-1, 3)
+        out = np.empty(p.shape[0])
+        tri = np.empty(p.shape[0], np.int64)
+        self.lib.port_mesh_sdf_flat(_ptr(v), _ptr(f64), f64.shape[0], _ptr(tn), _ptr(vn_v), _ptr(en), _ptr(p),
+                                    p.shape[0], _ptr(out), _ptr(tri))
+        return out, tri
+
+    def dcel_face_sd(self, v, fn, vn, en, p):
+        """One triangle as a DCEL face: v (3,3) loop order, fn the DCEL face normal, vn (3,3), en (3,3)."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (v, fn, vn, en, p)]
+        return float(self.lib.port_dcel_face_sd(*[_ptr(x) for x in a]))
 
     def knn_brute(self, pts, q, k):
         pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)

@@ -317,6 +317,160 @@ void port_mesh_sdf_brute(const double* V, const int64_t* F, int64_t nf, const do
 }
 
 /*
+ * Signed distance to one triangle as a DCEL face, the algorithm of MeshSDF and FlatMeshSDF
+ * (FaceT::signedDistance, DCEL_FaceImplem.hpp:388-423), which differs in the last bits from the
+ * Triangle/TriangleSoA test above:
+ *   - centroid c = ((x0 + x1) + x2) * (1/3) (computeCentroid, :120-133, Vec3T::operator/);
+ *   - inside test: the point projected into the face plane, p - n (n.(p - c)) (:370-378), then
+ *     the crossing number of its 2D projection that drops the axis of largest |n| (first on
+ *     ties) and keeps the other two in increasing order (Polygon2DImplem.hpp:80-118,164-193);
+ *   - inside: n.(p - c) with the DCEL face normal n (normalised twice);
+ *   - outside: the edge of smallest |d| (strict <, edges in loop order), where an edge gives the
+ *     distance to its start vertex for t <= 0, to its end vertex for t >= 1 and to its interior
+ *     otherwise, signed by (pseudonormal . delta > 0 ? +1 : -1) (DCEL_EdgeImplem.hpp:283-331,
+ *     DCEL_VertexImplem.hpp:368-380).
+ * v: 3 vertices in loop order; fn: DCEL face normal; vn: the 3 vertex normals; en: the 3 edge
+ * normals (edge i from vertex i to vertex i+1).
+ */
+static double dcel_vertex_sd(v3 x, v3 vn, v3 p)
+{
+  const v3     delta = sub(p, x);
+  const double dist  = length(delta);
+  return dist * ((dot(vn, delta) > 0.0) ? 1.0 : -1.0);
+}
+
+static double dcel_edge_sd(v3 x1, v3 x2, v3 en, v3 vn1, v3 vn2, v3 p)
+{
+  const v3     x2x1 = sub(x2, x1);
+  const double t    = dot(sub(p, x1), x2x1) / dot(x2x1, x2x1);
+  if (t <= 0.0) {
+    return dcel_vertex_sd(x1, vn1, p);
+  }
+  if (t >= 1.0) {
+    return dcel_vertex_sd(x2, vn2, p);
+  }
+  const v3 delta = sub(p, add(x1, scale(t, x2x1)));
+  return ((dot(en, delta) > 0.0) ? 1.0 : -1.0) * length(delta);
+}
+
+static double dcel_edge_ud2(v3 x1, v3 x2, v3 p)
+{
+  const v3 x2x1 = sub(x2, x1);
+  double   t    = dot(sub(p, x1), x2x1) / dot(x2x1, x2x1);
+  t             = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+  const v3 delta = sub(p, add(x1, scale(t, x2x1)));
+  return dot(delta, delta);
+}
+
+static v3 dcel_centroid(const v3* x)
+{
+  const double is = 1.0 / 3.0;
+  return scale(is, add(add(x[0], x[1]), x[2]));
+}
+
+static int dcel_inside(const v3* x, v3 n, v3 c, v3 p)
+{
+  const double a[3] = {fabs(n.x), fabs(n.y), fabs(n.z)};
+  int          ig   = 0;
+  for (int d = 1; d < 3; d++) {
+    if (a[d] > a[ig]) {
+      ig = d;
+    }
+  }
+  const int xd = ig == 0 ? 1 : 0, yd = ig == 2 ? 1 : 2;
+  const v3  q  = sub(p, scale(dot(n, sub(p, c)), n));
+  const double qa[3] = {q.x, q.y, q.z};
+  int          cn    = 0;
+  for (int i = 0; i < 3; i++) {
+    const double p1[3] = {x[i].x, x[i].y, x[i].z}, p2[3] = {x[(i + 1) % 3].x, x[(i + 1) % 3].y, x[(i + 1) % 3].z};
+    const int up = (p1[yd] <= qa[yd]) && (p2[yd] > qa[yd]), down = (p1[yd] > qa[yd]) && (p2[yd] <= qa[yd]);
+    if (up || down) {
+      const double t = (qa[yd] - p1[yd]) / (p2[yd] - p1[yd]);
+      if (qa[xd] < p1[xd] + t * (p2[xd] - p1[xd])) {
+        cn++;
+      }
+    }
+  }
+  return cn & 1;
+}
+
+double port_dcel_face_sd(const double* v, const double* fn, const double* vn, const double* en, const double* pp)
+{
+  const v3 x[3] = {ld(v), ld(v + 3), ld(v + 6)}, n = ld(fn), p = ld(pp);
+  const v3 c    = dcel_centroid(x);
+  if (dcel_inside(x, n, c, p)) {
+    return dot(n, sub(p, c));
+  }
+  double best = INFINITY;
+  for (int i = 0; i < 3; i++) {
+    const int    j = (i + 1) % 3;
+    const double d = dcel_edge_sd(x[i], x[j], ld(en + 3 * i), ld(vn + 3 * i), ld(vn + 3 * j), p);
+    best           = fabs(d) < fabs(best) ? d : best;
+  }
+  return best;
+}
+
+/* FaceT::unsignedDistance2 (DCEL_FaceImplem.hpp:425-458). */
+double port_dcel_face_ud2(const double* v, const double* fn, const double* pp)
+{
+  const v3 x[3] = {ld(v), ld(v + 3), ld(v + 6)}, n = ld(fn), p = ld(pp);
+  const v3 c    = dcel_centroid(x);
+  if (dcel_inside(x, n, c, p)) {
+    const double nd = dot(n, sub(p, c));
+    return nd * nd;
+  }
+  double best = INFINITY;
+  for (int i = 0; i < 3; i++) {
+    const double d2 = dcel_edge_ud2(x[i], x[(i + 1) % 3], p);
+    best            = d2 < best ? d2 : best;
+  }
+  return best;
+}
+
+/*
+ * FlatMeshSDF::signedDistance with the DCEL mesh's default search (MeshT::DirectSignedDistance2,
+ * DCEL_MeshImplem.hpp:574-595): the first face in soup order with the smallest unsigned
+ * distance^2, then its signed distance.  triN: the Triangle normals (normalised once); the DCEL
+ * face normal is that normalised again.  tri_out (nullable) receives the winning face.
+ */
+void port_mesh_sdf_flat(const double* V, const int64_t* F, int64_t nf, const double* triN, const double* vertN,
+                        const double* edgeN, const double* P, int64_t n, double* out, int64_t* tri_out)
+{
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t q = 0; q < n; q++) {
+    double  best = INFINITY;
+    int64_t bt   = -1;
+    double  fnb[3], vb[9], vnb[9];
+    for (int64_t f = 0; f < nf; f++) {
+      double v[9];
+      for (int k = 0; k < 3; k++) {
+        for (int c = 0; c < 3; c++) {
+          v[3 * k + c] = V[3 * F[3 * f + k] + c];
+        }
+      }
+      const v3 fd = divs(ld(triN + 3 * f), length(ld(triN + 3 * f)));
+      const double fn[3] = {fd.x, fd.y, fd.z};
+      const double d2    = port_dcel_face_ud2(v, fn, P + 3 * q);
+      if (bt < 0 || d2 < best) {
+        best = d2;
+        bt   = f;
+        memcpy(fnb, fn, sizeof(fnb));
+        memcpy(vb, v, sizeof(vb));
+        for (int k = 0; k < 3; k++) {
+          for (int c = 0; c < 3; c++) {
+            vnb[3 * k + c] = vertN[3 * F[3 * f + k] + c];
+          }
+        }
+      }
+    }
+    out[q] = bt >= 0 ? port_dcel_face_sd(vb, fnb, vnb, edgeN + 9 * bt, P + 3 * q) : INFINITY;
+    if (tri_out) {
+      tri_out[q] = bt;
+    }
+  }
+}
+
+/*
  * Brute-force k nearest neighbours ordered lexicographically by (d2, index) -- the order
  * closestPointBruteForce / bruteForceK (PointCloudBVHImplem.hpp:509-576) give for k = 1 (lowest
  * index on ties) extended to k > 1.  d2 is PointSoAT::getDistances2's float arithmetic

@@ -46,6 +46,7 @@ struct RefMesh
   std::shared_ptr<TriSDF44>               sdf44;
   std::shared_ptr<TriSDFDef>              sdfdef;
   std::shared_ptr<FlatMeshSDF<double, short>> flat;
+  std::shared_ptr<MeshSDF<double, short, 4>>  dcel;
 };
 
 std::shared_ptr<MeshD>
@@ -90,7 +91,8 @@ ref_omp_max_threads()
 // --- meshes -----------------------------------------------------------------------------------
 
 // Builds the reference TriMeshSDF from a vertex/triangle soup.  a_kind: 0 = <double,short,4,4>,
-// 1 = ISA-default K/W, 2 = FlatMeshSDF only (brute force, no BVH).  a_build: 0 SAH, 1 Morton,
+// 1 = ISA-default K/W, 2 = FlatMeshSDF only (brute force, no BVH), 3 = MeshSDF<double,short,4>
+// (BVH over the DCEL faces, MeshDistanceFunctionsImplem.hpp:249-295).  a_build: 0 SAH, 1 Morton,
 // 2 TopDown.  a_maxLeafGroups follows TriMeshSDF(mesh, build, maxLeafGroups).
 void*
 ref_mesh_create(const double* V, int64_t nv, const int64_t* F, int64_t nf, int a_kind, int a_build, int a_maxLeafGroups)
@@ -103,6 +105,9 @@ ref_mesh_create(const double* V, int64_t nv, const int64_t* F, int64_t nf, int a
   else if (a_kind == 1) {
     h->sdfdef = std::make_shared<TriSDFDef>(h->mesh, buildOf(a_build), size_t(a_maxLeafGroups));
   }
+  else if (a_kind == 3) {
+    h->dcel = std::make_shared<MeshSDF<double, short, 4>>(h->mesh, buildOf(a_build));
+  }
   h->flat = std::make_shared<FlatMeshSDF<double, short>>(h->mesh);
   return h;
 }
@@ -114,7 +119,7 @@ ref_mesh_destroy(void* a_h)
 }
 
 // Signed distance of n points (xyz interleaved, double) through the virtual value() entry point.
-// a_which: 0 = the TriMeshSDF built above, 1 = FlatMeshSDF (DCEL brute force).
+// a_which: 0 = the TriMeshSDF built above, 1 = FlatMeshSDF (DCEL brute force), 2 = the MeshSDF.
 int
 ref_mesh_sdf(void* a_h, const double* P, int64_t n, double* out, int a_which, int a_threads)
 {
@@ -122,6 +127,9 @@ ref_mesh_sdf(void* a_h, const double* P, int64_t n, double* out, int a_which, in
   const ImplicitFunction<double>* f = nullptr;
   if (a_which == 1) {
     f = h->flat.get();
+  }
+  else if (a_which == 2) {
+    f = h->dcel.get();
   }
   else if (h->sdf44) {
     f = h->sdf44.get();

@@ -79,8 +79,9 @@ def main(reference: str) -> None:
     dq = np.concatenate([q10, qr])
     m = R.mesh(dv, df, kind=0, build=0, max_leaf_groups=4)
     fn, vn, en = m.normals()
+    md = R.mesh(dv, df, kind=3, build=0)  # MeshSDF<double,short,4> over the DCEL faces
     np.savez(os.path.join(HERE, "dodecahedron.npz"), v=dv, f=df.astype(np.int32), p=dq, ref=m.sdf(dq),
-             flat=m.sdf(dq, flat=True), face_n=fn, vert_n=vn, edge_n=en)
+             flat=m.sdf(dq, flat=True), dcel=md.sdf(dq, dcel=True), face_n=fn, vert_n=vn, edge_n=en)
 
     # --- displaced icosphere, level 2 ------------------------------------------------------------------
     iv, iff = W.displaced_icosphere(2, 1234)
@@ -89,8 +90,9 @@ def main(reference: str) -> None:
     qa = W.uniform_points(1500, 5, -1.5, 1.5).astype(np.float64)
     qb = W.band_points(iv, iff, 500, 6, 1e-3).astype(np.float64)
     iq = np.concatenate([qa, qb])
-    np.savez(os.path.join(HERE, "icosphere_l2.npz"), v=iv, f=iff, p=iq, ref=m.sdf(iq), face_n=fn, vert_n=vn,
-             edge_n=en)
+    md = R.mesh(iv, iff, kind=3, build=0)
+    np.savez(os.path.join(HERE, "icosphere_l2.npz"), v=iv, f=iff, p=iq, ref=m.sdf(iq), flat=m.sdf(iq, flat=True),
+             dcel=md.sdf(iq, dcel=True), face_n=fn, vert_n=vn, edge_n=en)
 
     # --- point cloud (TestPointCloudBVH.cpp:58-120) ----------------------------------------------------
     pts = R.make_cloud_mt19937(2000, 20260708)

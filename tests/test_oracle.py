@@ -47,6 +47,17 @@ def test_mesh_normals_and_sdf_bitexact(port, golden, name):
     assert np.max(np.abs(d - g["ref"])) <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["dodecahedron.npz", "icosphere_l2.npz"])
+def test_dcel_face_port_bitexact(port, golden, name):
+    """The DCEL face algorithm (MeshSDF / FlatMeshSDF) restated in C reproduces the reference's
+    FlatMeshSDF and MeshSDF<double,short,4> values bit for bit (they differ from TriMeshSDF's
+    TriangleSoA test in the last bits)."""
+    g = golden(name)
+    d, _ = port.mesh_sdf_flat(g["v"], g["f"], g["p"])
+    assert np.array_equal(d, g["flat"])
+    assert np.array_equal(d, g["dcel"])
+
+
 def test_dodecahedron_flat_agrees(golden):
     g = golden("dodecahedron.npz")
     # the reference's own relational check (Tests/TestBVH.cpp:112-194, margin 1e-6 for double)
