@@ -392,7 +392,7 @@ def run_ours(args, rank, world, local_rank):
     # equal work unit for both runs) over the traversal phase's event-timed duration
     hbm_peak, peak_kind = measured_peaks()
     l2_gbs = l2_read_bandwidth()
-    node_b, box_b, tri_b = 128, 48, 48
+    node_b, box_b, tri_b = 128, 64, 48
     nq = float(n)
     bq = (12 + 4 + st["nodes_visited"] / nq * node_b + st["boxes_tested"] / nq * box_b +
           st["triangles_tested"] / nq * tri_b)
@@ -465,7 +465,7 @@ def run_ours(args, rank, world, local_rank):
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "kMeshSdf32 (FP32 packet traversal" + (", seeded)" if seed is not None else ")"),
                      "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit): 16 B query in/out + 128 B per node + "
-                                    "48 B per oriented box + 48 B per triangle",
+                                    "64 B per oriented box + 48 B per triangle",
                      "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
         "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                 "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},

@@ -23,7 +23,8 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["TriMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
+__all__ = ["TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH",
+           "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
 BUILD_MORTON = 1
@@ -193,6 +194,58 @@ class TriMeshSDF:
         check(lib.ebg_mesh_autotune(self._h, C.c_void_p(sample_points.data_ptr()), sample_points.numel() // 3,
                                     C.byref(o), C.byref(w), C.byref(ms), _stream_ptr(stream)))
         return {"occupancy": o.value, "warps_per_block": w.value, "ms": ms.value}
+
+
+def _fp64_call(mesh, dev_fn, host_fn, points, closest_tri, stream, with_opts):
+    """FP64 points (numpy: host entry, synchronous; CUDA tensor: device entry, asynchronous)."""
+    opts = (C.byref(_capi.QueryOpts()),) if with_opts else ()
+    t = closest_tri
+    if isinstance(points, np.ndarray):
+        p = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        d = np.empty(p.shape[0], np.float64)
+        check(host_fn(mesh._h, _ptr(p), p.shape[0], _ptr(d), _ptr(t) if t is not None else None, *opts, None))
+        return (d, t) if t is not None else d
+    import torch
+    if not (points.is_cuda and points.dtype == torch.float64 and points.is_contiguous()):
+        raise ValueError("points must be a contiguous float64 CUDA tensor of shape (n,3) or a numpy array")
+    n = points.numel() // 3
+    d = torch.empty(n, dtype=torch.float64, device=points.device)
+    check(dev_fn(mesh._h, C.c_void_p(points.data_ptr()), n, C.c_void_p(d.data_ptr()),
+                 C.c_void_p(t.data_ptr()) if t is not None else None, *opts, _stream_ptr(stream)))
+    return (d, t) if t is not None else d
+
+
+class MeshSDF(TriMeshSDF):
+    """The reference's MeshSDF: the same mesh and tree, each triangle evaluated as a DCEL face
+    (crossing-number inside test, n . (p - centroid) inside, else the nearest edge or vertex signed
+    by its pseudonormal).  FP64 end to end; its values differ from TriMeshSDF's in the last bits,
+    exactly as the reference's two classes do."""
+
+    def signed_distance(self, points, closest_tri=None, stream=None):
+        return _fp64_call(self, lib.ebg_mesh_signed_distance_dcel_f64, lib.ebg_mesh_signed_distance_dcel_f64_host,
+                          points, closest_tri, stream, True)
+
+    def value(self, point) -> float:
+        return float(self.signed_distance(np.asarray(point, np.float64).reshape(1, 3))[0])
+
+    signedDistance = value
+    __call__ = value
+
+
+class FlatMeshSDF(TriMeshSDF):
+    """The reference's FlatMeshSDF: no tree search; every triangle for every point (DCEL face
+    algorithm, the first triangle in soup order with the smallest unsigned distance wins).
+    O(points x triangles), FP64: a ground truth for small meshes."""
+
+    def signed_distance(self, points, closest_tri=None, stream=None):
+        return _fp64_call(self, lib.ebg_mesh_signed_distance_flat_f64, lib.ebg_mesh_signed_distance_flat_f64_host,
+                          points, closest_tri, stream, False)
+
+    def value(self, point) -> float:
+        return float(self.signed_distance(np.asarray(point, np.float64).reshape(1, 3))[0])
+
+    signedDistance = value
+    __call__ = value
 
 
 class PointCloudBVH:

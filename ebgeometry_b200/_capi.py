@@ -84,6 +84,10 @@ SIGNATURES = {
     "ebg_mesh_signed_distance_noalloc": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_mesh_signed_distance_f64": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_mesh_signed_distance_f64_host": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_mesh_signed_distance_dcel_f64": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_mesh_signed_distance_dcel_f64_host": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_mesh_signed_distance_flat_f64": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "ebg_mesh_signed_distance_flat_f64_host": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
     "ebg_mesh_signed_distance_stats": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts),
                                                  C.POINTER(QueryStats), _P]),
     "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),

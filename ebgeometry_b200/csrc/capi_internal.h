@@ -25,6 +25,7 @@ struct ebg_mesh
   void* dTriId  = nullptr;
   void* dObb    = nullptr;
   void* dNodeObb = nullptr;
+  void* dDcelN   = nullptr;
   int*  dStatus = nullptr;
   // host copies of the pseudonormals (soup order) and the cumulative triangle area (leaf order)
   std::vector<double> triN, cornerVN, edgeN;
@@ -56,7 +57,8 @@ namespace ebg {
 
 // The mesh query pipeline (ordering, optional seed inference, FP32 traversal, FP64 band pass) on
 // device buffers, asynchronous on s.  With pts64/out64 (the caller's FP64 points, of which pts is
-// the FP32 rounding, and an FP64 result array) every query is re-evaluated in FP64.
+// the FP32 rounding, and an FP64 result array) every query is re-evaluated in FP64, with the
+// Triangle test (evalKind 0, TriMeshSDF) or the DCEL face algorithm (1, MeshSDF).
 ebg_status meshQuery(const ebg_mesh*       m,
                      const float*          pts,
                      int64_t               n,
@@ -65,8 +67,9 @@ ebg_status meshQuery(const ebg_mesh*       m,
                      const ebg_query_opts* opts,
                      unsigned long long*   statsDev,
                      cudaStream_t          s,
-                     const double*         pts64 = nullptr,
-                     double*               out64 = nullptr);
+                     const double*         pts64    = nullptr,
+                     double*               out64    = nullptr,
+                     int                   evalKind = 0);
 
 } // namespace ebg
 

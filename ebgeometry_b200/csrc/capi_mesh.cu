@@ -121,19 +121,23 @@ double obbOfRange(const double* V, const int32_t* F, const std::vector<uint32_t>
       }
     }
   }
-  const double cn = 0.5 * (mn[0] + mxx[0]), cu = 0.5 * (mn[1] + mxx[1]), cw = 0.5 * (mn[2] + mxx[2]);
-  o.cx = float(cn * n[0] + cu * u[0] + cw * w[0]);
-  o.cy = float(cn * n[1] + cu * u[1] + cw * w[1]);
-  o.cz = float(cn * n[2] + cu * u[2] + cw * w[2]);
-  o.nx = float(n[0]);
-  o.ny = float(n[1]);
-  o.nz = float(n[2]);
-  o.ux = float(u[0]);
-  o.uy = float(u[1]);
-  o.uz = float(u[2]);
-  o.hn = roundUp(0.5 * (mxx[0] - mn[0]) + pad);
-  o.hu = roundUp(0.5 * (mxx[1] - mn[1]) + pad);
-  o.hv = roundUp(0.5 * (mxx[2] - mn[2]) + pad);
+  // the box centre's offset along each axis, and the half-extents
+  o.nx  = float(n[0]);
+  o.ny  = float(n[1]);
+  o.nz  = float(n[2]);
+  o.dn  = float(0.5 * (mn[0] + mxx[0]));
+  o.ux  = float(u[0]);
+  o.uy  = float(u[1]);
+  o.uz  = float(u[2]);
+  o.du  = float(0.5 * (mn[1] + mxx[1]));
+  o.vx  = float(w[0]);
+  o.vy  = float(w[1]);
+  o.vz  = float(w[2]);
+  o.dv  = float(0.5 * (mn[2] + mxx[2]));
+  o.hn  = roundUp(0.5 * (mxx[0] - mn[0]) + pad);
+  o.hu  = roundUp(0.5 * (mxx[1] - mn[1]) + pad);
+  o.hv  = roundUp(0.5 * (mxx[2] - mn[2]) + pad);
+  o.pad = 0.f;
   const double obbVol  = 8.0 * double(o.hn) * double(o.hu) * double(o.hv);
   const double aabbVol = (hi[0] - lo[0] + 2 * pad) * (hi[1] - lo[1] + 2 * pad) * (hi[2] - lo[2] + 2 * pad);
   return aabbVol > 0 ? obbVol / aabbVol : 1.0;
@@ -284,6 +288,7 @@ ebg_status buildMesh(const double*         V,
   std::vector<EbgTriHot>  hot(N);
   std::vector<EbgTriSign> sign(N);
   std::vector<double>     tri64(30 * N);
+  std::vector<double>     dcelN(3 * N);
   std::vector<int32_t>    triId(N);
   m->areaCdf.resize(N);
 #pragma omp parallel for schedule(static)
@@ -333,6 +338,14 @@ ebg_status buildMesh(const double*         V,
       t[12 + k] = m->cornerVN[9 * f + k];
       t[21 + k] = m->edgeN[9 * f + k];
     }
+    {
+      // the DCEL face normal: the Triangle normal normalised again (a multiply by the reciprocal)
+      const double* tn = &m->triN[3 * f];
+      const double  is = 1.0 / std::sqrt(tn[0] * tn[0] + tn[1] * tn[1] + tn[2] * tn[2]);
+      for (int k = 0; k < 3; k++) {
+        dcelN[3 * size_t(i) + k] = is * tn[k];
+      }
+    }
   }
 
   for (size_t i = 1; i < N; i++) {
@@ -353,6 +366,7 @@ ebg_status buildMesh(const double*         V,
       !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
       !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgObb)) ||
       !up(&m->dNodeObb, nodeObb.data(), nodeObb.size() * sizeof(EbgObb)) ||
+      !up(&m->dDcelN, dcelN.data(), dcelN.size() * sizeof(double)) ||
       cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
       cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
@@ -368,6 +382,7 @@ ebg_status buildMesh(const double*         V,
   v.tri_id       = static_cast<const int32_t*>(m->dTriId);
   v.obb          = static_cast<const EbgObb*>(m->dObb);
   v.node_obb     = static_cast<const EbgObb*>(m->dNodeObb);
+  v.dcel_n       = static_cast<const double*>(m->dDcelN);
   for (int a = 0; a < 3; a++) {
     v.root_lo[a] = roundDown(bvh.lo[a]);
     v.root_hi[a] = roundUp(bvh.hi[a]);
@@ -394,7 +409,8 @@ ebg_status buildMesh(const double*         V,
     d2 += (bvh.hi[a] - bvh.lo[a]) * (bvh.hi[a] - bvh.lo[a]);
   }
   inf.diagonal     = std::sqrt(d2);
-  inf.device_bytes = int64_t(nodeBytes + N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 30 * sizeof(double) + 4));
+  inf.device_bytes = int64_t(nodeBytes + N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 33 * sizeof(double) + 4) +
+                             (obb.size() + nodeObb.size()) * sizeof(EbgObb));
   *out             = m;
   return EBG_OK;
 }
@@ -435,7 +451,8 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
                           unsigned long long*   statsDev,
                           cudaStream_t          s,
                           const double*         pts64,
-                          double*               out64)
+                          double*               out64,
+                          int                   evalKind)
 {
   if (n > int64_t(INT32_MAX)) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
@@ -526,6 +543,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.points     = pts;
   a.points64   = pts64;
   a.out_d64    = out64;
+  a.eval       = evalKind;
   a.order      = order;
   a.seed_pk    = seedPk;
   a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
@@ -638,6 +656,7 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dTriId);
   cudaFree(m->dObb);
   cudaFree(m->dNodeObb);
+  cudaFree(m->dDcelN);
   cudaFree(m->dStatus);
   delete m;
   return EBG_OK;
@@ -706,7 +725,11 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaMemsetAsync(m->dStatus, 0, sizeof(int), s);
-  ebg_status rc;
+  // Large calls go in chunks on two streams, so that a chunk's copies in and out overlap its
+  // neighbours' traversals (results are per point, so chunking changes none of them).  Calls that
+  // ask for phase timings run as one piece.
+  const int64_t pieces = (opts && opts->timings) ? 1 : std::min<int64_t>(8, n / (int64_t(1) << 21));
+  ebg_status    rc     = EBG_OK;
   {
     Workspace ws(s);
     float*    dp = ws.get<float>(3 * n);
@@ -715,28 +738,90 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
     if (!ws.ok) {
       return setError(EBG_ERR_NO_MEMORY, "device buffers for the host call");
     }
-    cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s);
-    rc = meshQuery(m, dp, n, dd, dt, opts, nullptr, s);
-    if (rc == EBG_OK) {
-      cudaMemcpyAsync(dist_host, dd, n * sizeof(float), cudaMemcpyDeviceToHost, s);
-      if (dt) {
-        cudaMemcpyAsync(closest_tri_host, dt, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (pieces <= 1) {
+      cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(float), cudaMemcpyHostToDevice, s);
+      rc = meshQuery(m, dp, n, dd, dt, opts, nullptr, s);
+      if (rc == EBG_OK) {
+        cudaMemcpyAsync(dist_host, dd, n * sizeof(float), cudaMemcpyDeviceToHost, s);
+        if (dt) {
+          cudaMemcpyAsync(closest_tri_host, dt, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+        }
+      }
+    }
+    else {
+      cudaStream_t aux[2] = {nullptr, nullptr};
+      cudaEvent_t  ev[3]  = {nullptr, nullptr, nullptr};
+      bool         ok     = true;
+      for (int i = 0; i < 2; i++) {
+        ok = ok && cudaStreamCreateWithFlags(&aux[i], cudaStreamNonBlocking) == cudaSuccess;
+      }
+      for (int i = 0; i < 3; i++) {
+        ok = ok && cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) == cudaSuccess;
+      }
+      if (ok) {
+        // the chunks start after what the caller queued on s (including the buffers' allocation)
+        cudaEventRecord(ev[0], s);
+        cudaStreamWaitEvent(aux[0], ev[0], 0);
+        cudaStreamWaitEvent(aux[1], ev[0], 0);
+        const int64_t chunk = ((n + pieces - 1) / pieces + 31) / 32 * 32;
+        for (int64_t off = 0, c = 0; off < n && rc == EBG_OK; off += chunk, c++) {
+          const int64_t  cnt = std::min(chunk, n - off);
+          cudaStream_t   st  = aux[c & 1];
+          ebg_query_opts o   = opts ? *opts : ebg_query_opts{};
+          if (o.radius_hint) {
+            o.radius_hint += off;
+          }
+          cudaMemcpyAsync(dp + 3 * off, points_host + 3 * off, 3 * cnt * sizeof(float), cudaMemcpyHostToDevice, st);
+          rc = meshQuery(m, dp + 3 * off, cnt, dd + off, dt ? dt + off : nullptr, &o, nullptr, st);
+          if (rc == EBG_OK) {
+            cudaMemcpyAsync(dist_host + off, dd + off, cnt * sizeof(float), cudaMemcpyDeviceToHost, st);
+            if (dt) {
+              cudaMemcpyAsync(closest_tri_host + off, dt + off, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+            }
+          }
+        }
+        // s resumes (and frees the buffers) once both streams are done
+        cudaEventRecord(ev[1], aux[0]);
+        cudaEventRecord(ev[2], aux[1]);
+        cudaStreamWaitEvent(s, ev[1], 0);
+        cudaStreamWaitEvent(s, ev[2], 0);
+      }
+      else {
+        rc = setError(EBG_ERR_CUDA, "streams for the chunked host call");
+      }
+      for (int i = 0; i < 3; i++) {
+        if (ev[i]) {
+          cudaEventDestroy(ev[i]);
+        }
+      }
+      for (int i = 0; i < 2; i++) {
+        if (aux[i]) {
+          cudaStreamDestroy(aux[i]);
+        }
       }
     }
   }
   if (rc != EBG_OK) {
+    cudaStreamSynchronize(s);
     return rc;
   }
   return ebg_check_status(m, stream);
 }
 
-ebg_status ebg_mesh_signed_distance_f64(const ebg_mesh*       m,
-                                        const double*         points_dev,
-                                        int64_t               n,
-                                        double*               dist_dev,
-                                        int32_t*              closest_tri_dev,
-                                        const ebg_query_opts* opts,
-                                        void*                 stream)
+} // extern "C"
+
+namespace {
+
+// FP64 points in, FP64 distances out: the FP32 copy of the points drives the traversal, the FP64
+// pass evaluates every query with evaluator evalKind (0 Triangle test, 1 DCEL face).
+ebg_status meshQuery64(const ebg_mesh*       m,
+                       const double*         points_dev,
+                       int64_t               n,
+                       double*               dist_dev,
+                       int32_t*              closest_tri_dev,
+                       const ebg_query_opts* opts,
+                       void*                 stream,
+                       int                   evalKind)
 {
   if (m == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
     return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
@@ -754,16 +839,49 @@ ebg_status ebg_mesh_signed_distance_f64(const ebg_mesh*       m,
     return setError(EBG_ERR_NO_MEMORY, "FP32 copy of the FP64 points");
   }
   launchDoubleToFloat(points_dev, p32, 3 * n, s);
-  return meshQuery(m, p32, n, d32, closest_tri_dev, opts, nullptr, s, points_dev, dist_dev);
+  return meshQuery(m, p32, n, d32, closest_tri_dev, opts, nullptr, s, points_dev, dist_dev, evalKind);
 }
 
-ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       m,
-                                             const double*         points_host,
-                                             int64_t               n,
-                                             double*               dist_host,
-                                             int32_t*              closest_tri_host,
-                                             const ebg_query_opts* opts,
-                                             void*                 stream)
+// FlatMeshSDF: every triangle for every point (FP64, DCEL face algorithm).
+ebg_status meshFlat64(const ebg_mesh*       m,
+                      const double*         points_dev,
+                      int64_t               n,
+                      double*               dist_dev,
+                      int32_t*              closest_tri_dev,
+                      const ebg_query_opts* opts,
+                      void*                 stream,
+                      int                   evalKind)
+{
+  (void)opts;
+  (void)evalKind;
+  if (m == nullptr || n < 0 || (n > 0 && (points_dev == nullptr || dist_dev == nullptr))) {
+    return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  if (launchMeshFlat64(m->view, m->info.num_triangles, points_dev, n, dist_dev, closest_tri_dev, m->dStatus,
+                       m->numSms, static_cast<cudaStream_t>(stream)) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("brute-force launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  return EBG_OK;
+}
+
+using Entry64 = ebg_status (*)(const ebg_mesh*, const double*, int64_t, double*, int32_t*, const ebg_query_opts*,
+                               void*, int);
+
+// Host-buffer form of an FP64 entry: copies in, evaluates, copies out, synchronises.
+ebg_status hostCall64(Entry64               fn,
+                      int                   evalKind,
+                      const ebg_mesh*       m,
+                      const double*         points_host,
+                      int64_t               n,
+                      double*               dist_host,
+                      int32_t*              closest_tri_host,
+                      const ebg_query_opts* opts,
+                      void*                 stream)
 {
   if (m == nullptr || n < 0 || (n > 0 && (points_host == nullptr || dist_host == nullptr))) {
     return setError(EBG_ERR_INVALID, "null mesh/buffer or negative count");
@@ -785,7 +903,7 @@ ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       m,
       return setError(EBG_ERR_NO_MEMORY, "device buffers for the host call");
     }
     cudaMemcpyAsync(dp, points_host, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s);
-    rc = ebg_mesh_signed_distance_f64(m, dp, n, dd, dt, opts, stream);
+    rc = fn(m, dp, n, dd, dt, opts, stream, evalKind);
     if (rc == EBG_OK) {
       cudaMemcpyAsync(dist_host, dd, n * sizeof(double), cudaMemcpyDeviceToHost, s);
       if (dt) {
@@ -797,6 +915,74 @@ ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       m,
     return rc;
   }
   return ebg_check_status(m, stream);
+}
+
+} // namespace
+
+extern "C" {
+
+ebg_status ebg_mesh_signed_distance_f64(const ebg_mesh*       m,
+                                        const double*         points_dev,
+                                        int64_t               n,
+                                        double*               dist_dev,
+                                        int32_t*              closest_tri_dev,
+                                        const ebg_query_opts* opts,
+                                        void*                 stream)
+{
+  return meshQuery64(m, points_dev, n, dist_dev, closest_tri_dev, opts, stream, 0);
+}
+
+ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       m,
+                                             const double*         points_host,
+                                             int64_t               n,
+                                             double*               dist_host,
+                                             int32_t*              closest_tri_host,
+                                             const ebg_query_opts* opts,
+                                             void*                 stream)
+{
+  return hostCall64(meshQuery64, 0, m, points_host, n, dist_host, closest_tri_host, opts, stream);
+}
+
+ebg_status ebg_mesh_signed_distance_dcel_f64(const ebg_mesh*       m,
+                                             const double*         points_dev,
+                                             int64_t               n,
+                                             double*               dist_dev,
+                                             int32_t*              closest_tri_dev,
+                                             const ebg_query_opts* opts,
+                                             void*                 stream)
+{
+  return meshQuery64(m, points_dev, n, dist_dev, closest_tri_dev, opts, stream, 1);
+}
+
+ebg_status ebg_mesh_signed_distance_dcel_f64_host(const ebg_mesh*       m,
+                                                  const double*         points_host,
+                                                  int64_t               n,
+                                                  double*               dist_host,
+                                                  int32_t*              closest_tri_host,
+                                                  const ebg_query_opts* opts,
+                                                  void*                 stream)
+{
+  return hostCall64(meshQuery64, 1, m, points_host, n, dist_host, closest_tri_host, opts, stream);
+}
+
+ebg_status ebg_mesh_signed_distance_flat_f64(const ebg_mesh* m,
+                                             const double*   points_dev,
+                                             int64_t         n,
+                                             double*         dist_dev,
+                                             int32_t*        closest_tri_dev,
+                                             void*           stream)
+{
+  return meshFlat64(m, points_dev, n, dist_dev, closest_tri_dev, nullptr, stream, 0);
+}
+
+ebg_status ebg_mesh_signed_distance_flat_f64_host(const ebg_mesh* m,
+                                                  const double*   points_host,
+                                                  int64_t         n,
+                                                  double*         dist_host,
+                                                  int32_t*        closest_tri_host,
+                                                  void*           stream)
+{
+  return hostCall64(meshFlat64, 0, m, points_host, n, dist_host, closest_tri_host, nullptr, stream);
 }
 
 ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,

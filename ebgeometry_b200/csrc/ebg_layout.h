@@ -18,8 +18,10 @@
 //                                 reference's TriangleSoA lane data, TriangleSoAImplem.hpp:28-70).
 //   int32   tri_id[num_tris]      leaf position -> triangle index in the caller's soup.
 //
-//   Obb     leaf_obb[num_leaves]  48 B: oriented box of each leaf's triangles.
-//   Obb     node_obb[num_nodes]   48 B: oriented box of all triangles below each interior node.
+//   Obb     leaf_obb[num_leaves]  64 B: oriented box of each leaf's triangles.
+//   Obb     node_obb[num_nodes]   64 B: oriented box of all triangles below each interior node.
+//   double  dcel_n[num_tris][3]   24 B: the DCEL face normal (the Triangle normal normalised once
+//                                 more), for the DCEL face distance of MeshSDF / FlatMeshSDF.
 //
 // child[k] of an interior slot is a node index and count[k] is 0, or EBG_NODE_HAS_OBB when the
 // child's oriented box is tighter than its axis-aligned one (the traversal then tests it before
@@ -68,20 +70,22 @@ struct alignas(16) EbgTriSign
   float pad1, pad2;
 };
 
-// Oriented box of the triangles of one mesh leaf or of one subtree, in the frame of their
-// area-weighted mean normal n and an in-plane principal axis u (v = n x u): centre c and
-// half-extents (hn, hu, hv), padded outward to cover FP32 evaluation.  A patch of a smooth surface
-// is a thin slab, so its distance bounds the patch's triangles far more tightly than the
-// axis-aligned box does.
+// Oriented box of the triangles of one mesh leaf or of one subtree, as three slabs: unit axes n
+// (their area-weighted mean normal), u (in-plane principal axis) and v = n x u, each with the
+// offset of the box centre along it (dn = n . c, ...), and the half-extents (hn, hu, hv), padded
+// outward to cover FP32 evaluation.  A point's distance to the box follows from three plane
+// distances (n . p - dn, ...).  A patch of a smooth surface is a thin slab, so its distance bounds
+// the patch's triangles far more tightly than the axis-aligned box does.
 struct alignas(16) EbgObb
 {
-  float cx, cy, cz, hn;
-  float nx, ny, nz, hu;
-  float ux, uy, uz, hv;
+  float nx, ny, nz, dn;
+  float ux, uy, uz, du;
+  float vx, vy, vz, dv;
+  float hn, hu, hv, pad;
 };
 
 static_assert(sizeof(EbgNode4) == 128, "node must be one 128-byte line");
-static_assert(sizeof(EbgObb) == 48, "oriented box must be 48 bytes");
+static_assert(sizeof(EbgObb) == 64, "oriented box must be 64 bytes");
 static_assert(sizeof(EbgTriHot) == 48, "hot triangle record must be 48 bytes");
 static_assert(sizeof(EbgTriSign) == 96, "sign record must be 96 bytes");
 
@@ -95,6 +99,7 @@ struct EbgMeshView
   const int32_t*    tri_id;
   const EbgObb*     obb;                    // per leaf id
   const EbgObb*     node_obb;               // per interior node index
+  const double*     dcel_n;                 // per triangle (leaf order): the DCEL face normal (3)
   float             root_lo[3], root_hi[3]; // root box (FP32, outward)
   uint32_t          root_ref;               // node index 0, or a leaf reference for tiny meshes
   uint32_t          root_count;             // leaf count when root_ref is a leaf

@@ -12,6 +12,8 @@
 // traversal stack exactly as in the FP32 kernel.
 #include <cfloat>
 
+#include <math_constants.h>
+
 #include "ebg_device.cuh"
 #include "mesh_kernels.h"
 #include "mesh_traverse.cuh"
@@ -78,6 +80,114 @@ __device__ double triSd64(const double* __restrict__ tri, D3 P)
   return bs * sqrt(bd2);
 }
 
+// ---- one triangle as a DCEL face: the algorithm of MeshSDF and FlatMeshSDF ----------------------
+// (FaceT::signedDistance / unsignedDistance2, DCEL_FaceImplem.hpp:388-458; EdgeT, DCEL_EdgeImplem.hpp:
+// 283-358; VertexT, DCEL_VertexImplem.hpp:368-380; Polygon2D crossing number,
+// Polygon2DImplem.hpp:80-118,164-193).  It differs from the Triangle test above in the last bits:
+// the face value is n . (p - centroid) with the DCEL normal, and vertex/edge signs are
+// (pseudonormal . delta > 0 ? +1 : -1).
+
+__device__ __forceinline__ D3 add3(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ double len3(D3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+
+__device__ __forceinline__ double dcelVertexSd(D3 x, D3 vn, D3 P)
+{
+  const D3 d = sub(P, x);
+  return len3(d) * ((dot(vn, d) > 0.0) ? 1.0 : -1.0);
+}
+
+__device__ __forceinline__ D3 dcelCentroid(D3 x0, D3 x1, D3 x2)
+{
+  const double is = 1.0 / 3.0;
+  return scl(is, add3(add3(x0, x1), x2));
+}
+
+// crossing number of P projected into the face plane, in the 2D projection that drops the axis of
+// largest |n| (the first on ties)
+__device__ __forceinline__ bool dcelInside(const D3 (&x)[3], D3 n, D3 c, D3 P)
+{
+  const double ax = fabs(n.x), ay = fabs(n.y), az = fabs(n.z);
+  int          ig = 0;
+  if (ay > ax) {
+    ig = 1;
+  }
+  if (az > (ig == 0 ? ax : ay)) {
+    ig = 2;
+  }
+  const D3     q  = sub(P, scl(dot(n, sub(P, c)), n));
+  const double qx = ig == 0 ? q.y : q.x, qy = ig == 2 ? q.y : q.z;
+  int          cn = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const D3     a = x[i], b = x[(i + 1) % 3];
+    const double ax2 = ig == 0 ? a.y : a.x, ay2 = ig == 2 ? a.y : a.z;
+    const double bx2 = ig == 0 ? b.y : b.x, by2 = ig == 2 ? b.y : b.z;
+    const bool   up = (ay2 <= qy) && (by2 > qy), down = (ay2 > qy) && (by2 <= qy);
+    if (up || down) {
+      const double t = (qy - ay2) / (by2 - ay2);
+      if (qx < ax2 + t * (bx2 - ax2)) {
+        cn++;
+      }
+    }
+  }
+  return (cn & 1) != 0;
+}
+
+// tri: the 30-double record (v0 v1 v2 n vn0 vn1 vn2 en0 en1 en2); fn: the DCEL face normal
+__device__ double dcelFaceSd(const double* __restrict__ tri, const double* __restrict__ fn, D3 P)
+{
+  const D3 x[3] = {ld3(tri), ld3(tri + 3), ld3(tri + 6)};
+  const D3 n    = ld3(fn);
+  const D3 c    = dcelCentroid(x[0], x[1], x[2]);
+  if (dcelInside(x, n, c, P)) {
+    return dot(n, sub(P, c));
+  }
+  double best = CUDART_INF;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const int    j    = (i + 1) % 3;
+    const D3     x2x1 = sub(x[j], x[i]);
+    const double t    = dot(sub(P, x[i]), x2x1) / dot(x2x1, x2x1);
+    double       d;
+    if (t <= 0.0) {
+      d = dcelVertexSd(x[i], ld3(tri + 12 + 3 * i), P);
+    }
+    else if (t >= 1.0) {
+      d = dcelVertexSd(x[j], ld3(tri + 12 + 3 * j), P);
+    }
+    else {
+      const D3 delta = sub(P, add3(x[i], scl(t, x2x1)));
+      d              = ((dot(ld3(tri + 21 + 3 * i), delta) > 0.0) ? 1.0 : -1.0) * len3(delta);
+    }
+    best = fabs(d) < fabs(best) ? d : best;
+  }
+  return best;
+}
+
+__device__ double dcelFaceUd2(const double* __restrict__ tri, const double* __restrict__ fn, D3 P)
+{
+  const D3 x[3] = {ld3(tri), ld3(tri + 3), ld3(tri + 6)};
+  const D3 n    = ld3(fn);
+  const D3 c    = dcelCentroid(x[0], x[1], x[2]);
+  if (dcelInside(x, n, c, P)) {
+    const double nd = dot(n, sub(P, c));
+    return nd * nd;
+  }
+  double best = CUDART_INF;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const D3 x2x1 = sub(x[(i + 1) % 3], x[i]);
+    double   t    = dot(sub(P, x[i]), x2x1) / dot(x2x1, x2x1);
+    t             = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    const D3     delta = sub(P, add3(x[i], scl(t, x2x1)));
+    const double d2    = dot(delta, delta);
+    best               = d2 < best ? d2 : best;
+  }
+  return best;
+}
+
+// EVAL 0: the reference's Triangle/TriangleSoA test (TriMeshSDF); 1: the DCEL face (MeshSDF).
+template <int EVAL>
 __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float delta)
 {
   __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
@@ -140,14 +250,15 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
                                                : ((cntw & EBG_NODE_HAS_OBB) ? m.node_obb + ref : nullptr);
       if (obx != nullptr) {
         const float4* ob = reinterpret_cast<const float4*>(obx);
-        if (!__any_sync(FULL, obbDist2(__ldg(ob), __ldg(ob + 1), __ldg(ob + 2), px, py, pz) <= bound)) {
+        if (!__any_sync(FULL, obbDist2(__ldg(ob), __ldg(ob + 1), __ldg(ob + 2), __ldg(ob + 3), px, py, pz) <= bound)) {
           continue;
         }
       }
       if (ref & EBG_LEAF_BIT) {
         const uint32_t t0 = ref & ~EBG_LEAF_BIT;
         for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
-          const double d = triSd64(m.tri64 + 30 * size_t(tt), P);
+          const double d = EVAL == 0 ? triSd64(m.tri64 + 30 * size_t(tt), P)
+                                     : dcelFaceSd(m.tri64 + 30 * size_t(tt), m.dcel_n + 3 * size_t(tt), P);
           if (fabs(d) < fabs(best)) {
             best = d;
             bt   = int(tt);
@@ -218,7 +329,70 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
   }
 }
 
+// FlatMeshSDF (MeshT::DirectSignedDistance2, DCEL_MeshImplem.hpp:574-595): every face, the first
+// in soup order with the smallest unsigned distance^2 wins, and its signed distance is the value.
+// One query per thread; the block walks the triangles (leaf order) through shared-memory tiles of
+// their vertices and DCEL normals and keeps the lexicographic minimum of (d^2, soup index).
+constexpr int FLAT_TILE = 64;
+
+__global__ void __launch_bounds__(128) kMeshFlat64(const EbgMeshView m, int64_t numTris, const double* __restrict__ pts,
+                                                   int64_t n, double* __restrict__ out, int32_t* __restrict__ outTri,
+                                                   int* __restrict__ status)
+{
+  __shared__ double  sv[FLAT_TILE][12];
+  __shared__ int32_t sid[FLAT_TILE];
+  for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < n; base += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t q     = base + threadIdx.x;
+    const bool    valid = q < n;
+    const D3      P     = valid ? D3{pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]} : D3{0.0, 0.0, 0.0};
+    const bool    finite = isfinite(P.x) && isfinite(P.y) && isfinite(P.z);
+    if (valid && !finite) {
+      atomicOr(status, ST_INPUT);
+    }
+    double        best  = CUDART_INF;
+    int32_t       bsoup = INT32_MAX;
+    int64_t       bpos  = -1;
+    for (int64_t t0 = 0; t0 < numTris; t0 += FLAT_TILE) {
+      __syncthreads();
+      for (int k = threadIdx.x; k < FLAT_TILE * 12; k += blockDim.x) {
+        const int64_t tt = t0 + k / 12;
+        const int     c  = k % 12;
+        sv[k / 12][c]    = tt < numTris ? (c < 9 ? m.tri64[30 * tt + c] : m.dcel_n[3 * tt + (c - 9)]) : 0.0;
+      }
+      for (int k = threadIdx.x; k < FLAT_TILE; k += blockDim.x) {
+        sid[k] = t0 + k < numTris ? m.tri_id[t0 + k] : INT32_MAX;
+      }
+      __syncthreads();
+      const int cnt = int(numTris - t0 < FLAT_TILE ? numTris - t0 : FLAT_TILE);
+      for (int k = 0; k < cnt; k++) {
+        const double d2 = dcelFaceUd2(sv[k], sv[k] + 9, P);
+        if (d2 < best || (d2 == best && sid[k] < bsoup)) {
+          best  = d2;
+          bsoup = sid[k];
+          bpos  = t0 + k;
+        }
+      }
+    }
+    if (valid) {
+      // a non-finite point (reported through the status word) gets NaN
+      out[q] = (finite && bpos >= 0) ? dcelFaceSd(m.tri64 + 30 * bpos, m.dcel_n + 3 * bpos, P) : CUDART_NAN;
+      if (outTri) {
+        outTri[q] = (finite && bpos >= 0) ? bsoup : -1;
+      }
+    }
+  }
+}
+
 } // namespace
+
+cudaError_t launchMeshFlat64(const EbgMeshView& m, int64_t numTris, const double* pts, int64_t n, double* out,
+                             int32_t* outTri, int* status, int numSms, cudaStream_t s)
+{
+  int64_t blocks = (n + 127) / 128;
+  blocks         = blocks < int64_t(numSms) * 16 ? blocks : int64_t(numSms) * 16;
+  kMeshFlat64<<<unsigned(blocks < 1 ? 1 : blocks), 128, 0, s>>>(m, numTris, pts, n, out, outTri, status);
+  return cudaGetLastError();
+}
 
 namespace {
 __global__ void kDoubleToFloat(const double* __restrict__ in, float* __restrict__ out, int64_t count)
@@ -238,7 +412,12 @@ void launchDoubleToFloat(const double* in, float* out, int64_t count, cudaStream
 
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s)
 {
-  kMeshBand64<<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+  if (a.eval == 1) {
+    kMeshBand64<1><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+  }
+  else {
+    kMeshBand64<0><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+  }
   return cudaGetLastError();
 }
 

@@ -21,6 +21,7 @@ struct MeshQueryArgs
   int64_t            n;
   float*             out_d;      // caller order
   double*            out_d64;    // caller order, FP64 results of the band pass (nullable)
+  int                eval;       // FP64 evaluator: 0 the Triangle test (TriMeshSDF), 1 the DCEL face (MeshSDF)
   int32_t*           out_tri;    // caller order (nullable)
   float              band;       // |d| <= band -> FP64 re-evaluation list
   uint32_t*          band_list;  // sorted positions needing FP64 (nullable = no band pass)
@@ -40,6 +41,11 @@ cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int warpsPerBlock, int numSm
 
 // FP64 re-evaluation of the band list (reads band_count on the device).
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s);
+
+// FlatMeshSDF over every triangle (FP64 points and results, DCEL face algorithm); outTri nullable;
+// non-finite points set ST_INPUT in *status and get NaN.
+cudaError_t launchMeshFlat64(const EbgMeshView& m, int64_t numTris, const double* pts, int64_t n, double* out,
+                             int32_t* outTri, int* status, int numSms, cudaStream_t s);
 
 // out[i] = float(in[i]) for i < count (round to nearest).
 void launchDoubleToFloat(const double* in, float* out, int64_t count, cudaStream_t s);

@@ -49,7 +49,8 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
 {
   extern __shared__ float4 smem[];
   const int     lane = threadIdx.x & 31;
-  float4*       stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
+  float4*       stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH + 32);
+  float4*       lpts = stk + 2 * EBG_STACK_DEPTH; // the warp's 32 spread-leaf points
   const EbgMeshView& m = a.mesh;
   const uint64_t numPackets = (uint64_t(a.n) + 31) / 32;
 
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         }
       }
       TraversalCounters tc;
-      traverseMesh<STATS>(m, px, py, pz, best, besttri, stk, iters, err, tc);
+      traverseMesh<STATS>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc);
       cNode += tc.node;
       cLeaf += tc.leaf;
       cTri += tc.tri;
@@ -193,7 +194,7 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
     wpb = 4;
   }
   const int    threads = 32 * wpb;
-  const size_t smem    = size_t(wpb) * 2 * EBG_STACK_DEPTH * sizeof(float4);
+  const size_t smem    = size_t(wpb) * (2 * EBG_STACK_DEPTH + 32) * sizeof(float4);
   // resident blocks per SM for each block size, looked up once (the query path then issues no
   // runtime calls besides its launches, so it can be captured in a CUDA graph)
   static int cache[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};

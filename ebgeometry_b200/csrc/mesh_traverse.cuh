@@ -83,18 +83,17 @@ __device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, cons
 
 __device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
 
-// Squared distance from p to a leaf's oriented box, scaled down by 4e-6 relative so FP32 rounding
-// (about 3e-7 relative on the projections) can only make it smaller than the exact value.
-__device__ __forceinline__ float obbDist2(const float4 o0, const float4 o1, const float4 o2, float px, float py,
-                                          float pz)
+// Squared distance from p to an oriented box (EbgObb as four float4: n|dn, u|du, v|dv, h), scaled
+// down by 4e-6 relative.  The FP32 error of each plane distance n . p - dn is about 1e-7 of |p|,
+// which the padding of the half-extents (2e-6 of the mesh's extent) covers near the mesh and the
+// relative scaling covers far from it (there the box distance itself is about |p|).
+__device__ __forceinline__ float obbDist2(const float4 o0, const float4 o1, const float4 o2, const float4 o3, float px,
+                                          float py, float pz)
 {
-  const float qx = px - o0.x, qy = py - o0.y, qz = pz - o0.z;
-  const float a  = fmaf(o1.x, qx, fmaf(o1.y, qy, o1.z * qz));
-  const float b  = fmaf(o2.x, qx, fmaf(o2.y, qy, o2.z * qz));
-  const float vx = fmaf(o1.y, o2.z, -o1.z * o2.y), vy = fmaf(o1.z, o2.x, -o1.x * o2.z),
-              vz = fmaf(o1.x, o2.y, -o1.y * o2.x);
-  const float e  = fmaf(vx, qx, fmaf(vy, qy, vz * qz));
-  const float dn = fmaxf(fabsf(a) - o0.w, 0.f), du = fmaxf(fabsf(b) - o1.w, 0.f), dv = fmaxf(fabsf(e) - o2.w, 0.f);
+  const float a  = fmaf(o0.x, px, fmaf(o0.y, py, fmaf(o0.z, pz, -o0.w)));
+  const float b  = fmaf(o1.x, px, fmaf(o1.y, py, fmaf(o1.z, pz, -o1.w)));
+  const float e  = fmaf(o2.x, px, fmaf(o2.y, py, fmaf(o2.z, pz, -o2.w)));
+  const float dn = fmaxf(fabsf(a) - o3.x, 0.f), du = fmaxf(fabsf(b) - o3.y, 0.f), dv = fmaxf(fabsf(e) - o3.z, 0.f);
   return fmaf(dn, dn, fmaf(du, du, dv * dv)) * (1.f - 4e-6f);
 }
 
@@ -142,11 +141,12 @@ struct TraversalCounters
 // One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
 // already seeded or FLT_MAX) and winning triangle `besttri` (leaf order) are updated.  Children are
 // ordered by their smallest distance over the packet's lanes.  `stk` is this warp's stack region
-// (2 float4 per entry, EBG_STACK_DEPTH entries); `iters` counts loop trips against MAX_ITERS; `err`
+// (2 float4 per entry, EBG_STACK_DEPTH entries); `pts` is this warp's 32-entry scratch for the
+// points of the lanes a leaf is spread over; `iters` counts loop trips against MAX_ITERS; `err`
 // receives ST_* bits.  All 32 lanes must call it together.
 template <bool STATS>
 __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
-                                             int& besttri, float4* stk, uint32_t& iters, int& err,
+                                             int& besttri, float4* stk, float4* pts, uint32_t& iters, int& err,
                                              TraversalCounters& cnt_)
 {
   const int lane = threadIdx.x & 31;
@@ -178,22 +178,73 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           const uint32_t t0 = ref & ~EBG_LEAF_BIT, cnt = cntw & EBG_COUNT_MASK;
           // the leaf's oriented box (a thin slab on smooth surfaces) before its triangles
           const float4* ob = reinterpret_cast<const float4*>(m.obb + (cntw >> EBG_COUNT_BITS));
-          const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
-          const bool    needObb = obbDist2(o0, o1, o2, px, py, pz) <= best;
+          const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2), o3 = __ldg(ob + 3);
+          const bool    needObb = need && obbDist2(o0, o1, o2, o3, px, py, pz) <= best;
           if (STATS) {
             cnt_.box += need;
             cnt_.pbox++;
           }
-          if (!__any_sync(FULL, needObb)) {
+          const unsigned needMask = __ballot_sync(FULL, needObb);
+          if (needMask == 0u) {
             continue;
           }
+          // Few lanes need the leaf: spread their (lane, triangle) pairs over the warp, 32 / cnt
+          // lanes per pass, instead of every lane testing every triangle.  A pass costs about two
+          // triangle tests, so this runs when it needs fewer passes than cnt - 1.
+          const int nNeed  = __popc(needMask);
+          const int lpp    = 32 / int(cnt);
+          const int passes = (nNeed + lpp - 1) / lpp;
           if (STATS && needObb) {
             cnt_.leaf++;
             cnt_.tri += cnt;
           }
           if (STATS) {
             cnt_.pleaf++;
-            cnt_.ptri += cnt;
+            cnt_.ptri += passes < int(cnt) - 1 ? uint32_t(passes) : cnt;
+          }
+          if (passes < int(cnt) - 1) {
+            const int rank = __popc(needMask & ((1u << lane) - 1u));
+            if (needObb) {
+              pts[rank] = make_float4(px, py, pz, 0.f);
+            }
+            __syncwarp();
+            const int     li = lane / int(cnt), ti = lane - li * int(cnt);
+            const float4* h  = reinterpret_cast<const float4*>(m.hot + t0 + uint32_t(ti));
+#pragma unroll 1
+            for (int ps = 0; ps < passes; ps++) {
+              const int slot = ps * lpp + li;
+              float     dd   = __int_as_float(0x7f800000);
+              int       bi   = ti;
+              if (li < lpp && slot < nNeed) {
+                const float4 q  = pts[slot];
+                const float4 h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+                float        s, t;
+                int          r;
+                dd = triDist2<false>(h0, h1, h2, q.x, q.y, q.z, s, t, r);
+              }
+              // minimum of (d2, triangle) over the cnt threads serving one lane; the first thread
+              // of the segment ends with it
+#pragma unroll
+              for (int off = 16; off > 0; off >>= 1) {
+                const float od = __shfl_down_sync(FULL, dd, off);
+                const int   oi = __shfl_down_sync(FULL, bi, off);
+                if (ti + off < int(cnt) && (od < dd || (od == dd && oi < bi))) {
+                  dd = od;
+                  bi = oi;
+                }
+              }
+              const int  seg  = rank - ps * lpp;
+              const bool mine = needObb && seg >= 0 && seg < lpp;
+              const int  from = mine ? seg * int(cnt) : 0;
+              const float rd = __shfl_sync(FULL, dd, from);
+              const int   ri = __shfl_sync(FULL, bi, from);
+              if (mine && rd < best) {
+                best    = rd;
+                besttri = int(t0) + ri;
+              }
+            }
+            __syncwarp();
+            continue;
           }
 #pragma unroll 1
           for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
@@ -219,8 +270,8 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           bool needN = need;
           if (cntw & EBG_NODE_HAS_OBB) {
             const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
-            const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2);
-            needN            = need && obbDist2(o0, o1, o2, px, py, pz) <= best;
+            const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2), o3 = __ldg(ob + 3);
+            needN            = need && obbDist2(o0, o1, o2, o3, px, py, pz) <= best;
             if (STATS) {
               cnt_.box += need;
               cnt_.pbox++;

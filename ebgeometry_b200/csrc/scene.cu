@@ -29,10 +29,11 @@ constexpr int OUTER_DEPTH = 48; // object-BVH stack entries per warp (builder ch
 
 __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
 {
-  __shared__ float4 smem[4 * 2 * (OUTER_DEPTH + EBG_STACK_DEPTH)];
+  __shared__ float4 smem[4 * (2 * (OUTER_DEPTH + EBG_STACK_DEPTH) + 32)];
   const int         lane  = threadIdx.x & 31;
-  float4*           ostk  = smem + (threadIdx.x >> 5) * (2 * (OUTER_DEPTH + EBG_STACK_DEPTH));
+  float4*           ostk  = smem + (threadIdx.x >> 5) * (2 * (OUTER_DEPTH + EBG_STACK_DEPTH) + 32);
   float4*           istk  = ostk + 2 * OUTER_DEPTH;
+  float4*           lpts  = istk + 2 * EBG_STACK_DEPTH; // the warp's 32 spread-leaf points
   const SceneView&  sc    = a.scene;
   const uint64_t    numPk = (uint64_t(a.n) + 31) / 32;
 
@@ -95,7 +96,7 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
           float      mb     = seeded ? best * best * 1.000004f : FLT_MAX;
           int        bt     = -1;
           TraversalCounters tc;
-          traverseMesh<false>(mv, lx, ly, lz, mb, bt, istk, iters, err, tc);
+          traverseMesh<false>(mv, lx, ly, lz, mb, bt, istk, lpts, iters, err, tc);
           if (err) {
             break;
           }

@@ -41,6 +41,14 @@ int main()
   // the octahedron's exact signed distance is (|x|+|y|+|z|-1)/sqrt(3) where the closest feature
   // is a face; check the centre
   const double centre = asImplicit.value(Vec3(0, 0, 0));
+  // the DCEL-face classes (MeshSDF with a tree, FlatMeshSDF without) agree with each other
+  MeshSDF     msdf(v, f);
+  FlatMeshSDF flat(v, f);
+  double      maxDcel = 0;
+  for (size_t i = 0; i < d.size(); i += 37) {
+    const Vec3 q(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+    maxDcel = std::fmax(maxDcel, std::fabs(msdf.value(q) - flat.value(q)));
+  }
 
   std::vector<std::array<float, 3>> cloud;
   for (int i = 0; i < 5000; i++) {
@@ -52,7 +60,7 @@ int main()
   std::printf("batch/single max diff %.3g (FP64 batch: %.3g), centre %.6f (expect %.6f), nearest of point 123: "
               "%zu (d2 %g)\n",
               maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared));
-  const bool ok = maxDiff <= 1e-6 && maxDiff64 == 0.0 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-12 &&
+  const bool ok = maxDiff <= 1e-6 && maxDiff64 == 0.0 && maxDcel == 0.0 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-12 &&
                   hit.index == 123 && hit.distanceSquared == 0.f;
   std::printf("%s\n", ok ? "ok" : "FAILED");
   return ok ? 0 : 1;

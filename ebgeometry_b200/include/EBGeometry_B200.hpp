@@ -154,6 +154,51 @@ private:
   ebg_mesh* m_mesh = nullptr;
 };
 
+// MeshSDF<double,short,K>: the same mesh, each triangle evaluated as a DCEL face (the reference's
+// MeshSDF values, which differ from TriMeshSDF's in the last bits).  FP64 end to end.
+class MeshSDF : public TriMeshSDF
+{
+public:
+  using TriMeshSDF::TriMeshSDF;
+  double signedDistance(const Vec3& a_point) const noexcept override
+  {
+    const double   p[3] = {x(a_point), y(a_point), z(a_point)};
+    double         d    = std::numeric_limits<double>::quiet_NaN();
+    ebg_query_opts o{};
+    o.no_sort = 1;
+    return ebg_mesh_signed_distance_dcel_f64_host(handle(), p, 1, &d, nullptr, &o, nullptr) == EBG_OK
+             ? d
+             : std::numeric_limits<double>::quiet_NaN();
+  }
+  // Batched, host buffers (xyz interleaved), synchronous.
+  void signedDistances(const double* a_pointsHost, size_t a_n, double* a_distHost) const
+  {
+    ebg_query_opts o{};
+    check(ebg_mesh_signed_distance_dcel_f64_host(handle(), a_pointsHost, int64_t(a_n), a_distHost, nullptr, &o,
+                                                 nullptr));
+  }
+};
+
+// FlatMeshSDF<double,short>: every triangle for every point (the DCEL mesh's default search);
+// a ground truth for small meshes.
+class FlatMeshSDF : public TriMeshSDF
+{
+public:
+  using TriMeshSDF::TriMeshSDF;
+  double signedDistance(const Vec3& a_point) const noexcept override
+  {
+    const double p[3] = {x(a_point), y(a_point), z(a_point)};
+    double       d    = std::numeric_limits<double>::quiet_NaN();
+    return ebg_mesh_signed_distance_flat_f64_host(handle(), p, 1, &d, nullptr, nullptr) == EBG_OK
+             ? d
+             : std::numeric_limits<double>::quiet_NaN();
+  }
+  void signedDistances(const double* a_pointsHost, size_t a_n, double* a_distHost) const
+  {
+    check(ebg_mesh_signed_distance_flat_f64_host(handle(), a_pointsHost, int64_t(a_n), a_distHost, nullptr, nullptr));
+  }
+};
+
 // The learned pruning radius (trained on the device from the mesh's own exact distances).
 class SeedModel
 {

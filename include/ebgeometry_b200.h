@@ -224,6 +224,45 @@ ebg_status ebg_mesh_signed_distance_f64_host(const ebg_mesh*       mesh,
                                              const ebg_query_opts* opts,
                                              void*                 stream);
 
+/* MeshSDF<double,short,K>::signedDistance (MeshDistanceFunctionsImplem.hpp:269-295): the same FP64
+ * query with each triangle evaluated as a DCEL face (FaceT::signedDistance,
+ * DCEL_FaceImplem.hpp:388-423: crossing-number inside test in the face's 2D projection, then
+ * n . (p - centroid) inside, else the nearest edge or vertex signed by its pseudonormal), which
+ * differs from the Triangle test of TriMeshSDF in the last bits.  Keeps the value of smallest |d|
+ * (strict <), as MeshSDF's leaf loop does.  Asynchronous on stream. */
+ebg_status ebg_mesh_signed_distance_dcel_f64(const ebg_mesh*       mesh,
+                                             const double*         points_dev,
+                                             int64_t               n,
+                                             double*               dist_dev,
+                                             int32_t*              closest_tri_dev,
+                                             const ebg_query_opts* opts,
+                                             void*                 stream);
+ebg_status ebg_mesh_signed_distance_dcel_f64_host(const ebg_mesh*       mesh,
+                                                  const double*         points_host,
+                                                  int64_t               n,
+                                                  double*               dist_host,
+                                                  int32_t*              closest_tri_host,
+                                                  const ebg_query_opts* opts,
+                                                  void*                 stream);
+
+/* FlatMeshSDF<double,short>::signedDistance (MeshDistanceFunctionsImplem.hpp:218-228 through
+ * MeshT::DirectSignedDistance2, DCEL_MeshImplem.hpp:574-595): no tree; every triangle is tested
+ * for every point, the first triangle in soup order with the smallest unsigned distance wins and
+ * its DCEL-face signed distance is the value.  O(points x triangles): a ground truth for small
+ * meshes.  closest_tri (nullable) receives the winner's soup index.  Asynchronous on stream. */
+ebg_status ebg_mesh_signed_distance_flat_f64(const ebg_mesh* mesh,
+                                             const double*   points_dev,
+                                             int64_t         n,
+                                             double*         dist_dev,
+                                             int32_t*        closest_tri_dev,
+                                             void*           stream);
+ebg_status ebg_mesh_signed_distance_flat_f64_host(const ebg_mesh* mesh,
+                                                  const double*   points_host,
+                                                  int64_t         n,
+                                                  double*         dist_host,
+                                                  int32_t*        closest_tri_host,
+                                                  void*           stream);
+
 /* The same batched query WITHOUT ANY DEVICE ALLOCATION (no counterpart in the reference).  For
  * callers that cannot let a library allocate: AMR codes such as AMReX reserve most of the GPU's memory
  * for their own arena at start-up, so a library's cudaMalloc or stream-ordered allocation can fail

@@ -202,3 +202,21 @@ def test_cuda_graph_capture(ref):
         g.replay()
     torch.cuda.synchronize()
     check_parity(out.cpu().numpy(), d_ref, m.diagonal, "graph replay")
+
+
+def test_chunked_host_call_matches_device_path():
+    """Host calls of more than 4M points run in overlapping chunks on two streams; the results are
+    those of the one-piece device call, including the closest triangles and a per-point hint."""
+    v, f = W.displaced_icosphere(4, 41)
+    m = TriMeshSDF(v, f)
+    p = W.uniform_points(5_000_000, 42)
+    pd = torch.from_numpy(p).cuda()
+    tri_d = torch.empty(p.shape[0], dtype=torch.int32, device="cuda")
+    d_dev, _ = m.signed_distance(pd, closest_tri=tri_d)
+    torch.cuda.synchronize()
+    d_host, tri_h = m.signed_distance(p, closest_tri=np.empty(p.shape[0], np.int32))
+    assert np.array_equal(d_host, d_dev.cpu().numpy())
+    assert np.array_equal(tri_h, tri_d.cpu().numpy())
+    hint = (d_dev.abs() * 1.01 + 1e-3).contiguous()
+    d_hint = m.signed_distance(p, radius_hint=hint)
+    assert np.array_equal(d_hint, d_host)
