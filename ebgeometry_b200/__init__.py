@@ -313,6 +313,48 @@ class PointCloudBVH:
         idx, d2 = self.knn(np.asarray(q, np.float32).reshape(1, 3), k)
         return [(int(i), float(d)) for i, d in zip(idx[0], d2[0]) if i >= 0]
 
+    # --- self queries (PointCloudBVHImplem.hpp:455-507): the point itself is excluded -------------
+    def all_nearest_neighbors(self, k=1, device=False, stream=None):
+        """allNearestNeighbors: (idx (n,k) int32, d2 (n,k) float32), row i = the k nearest other
+        points of cloud point i, in (d2, index) order.  device=True returns CUDA tensors
+        (asynchronous on ``stream``)."""
+        if not device:
+            idx = np.empty((self.n, k), np.int32)
+            d2 = np.empty((self.n, k), np.float32)
+            check(lib.ebg_cloud_self_knn_host(self._h, int(k), _ptr(idx), _ptr(d2), None))
+            return idx, d2
+        import torch
+        idx = torch.empty((self.n, k), dtype=torch.int32, device="cuda")
+        d2 = torch.empty((self.n, k), dtype=torch.float32, device="cuda")
+        check(lib.ebg_cloud_self_knn(self._h, int(k), C.c_void_p(idx.data_ptr()), C.c_void_p(d2.data_ptr()),
+                                     _stream_ptr(stream)))
+        return idx, d2
+
+    allNearestNeighbors = all_nearest_neighbors
+
+    def nearest_neighbors(self, point_ids, k=1, stream=None):
+        """nearestNeighbors(point, k) for a list of cloud indices (CUDA int64 tensor, or anything
+        numpy can turn into int64: then the call synchronises and returns numpy arrays)."""
+        import torch
+        host = not (isinstance(point_ids, torch.Tensor) and point_ids.is_cuda)
+        ids = torch.as_tensor(np.asarray(point_ids, np.int64) if host else point_ids, dtype=torch.int64).cuda()
+        ids = ids.contiguous().reshape(-1)
+        m = ids.numel()
+        idx = torch.empty((m, k), dtype=torch.int32, device=ids.device)
+        d2 = torch.empty((m, k), dtype=torch.float32, device=ids.device)
+        check(lib.ebg_cloud_self_knn_points(self._h, C.c_void_p(ids.data_ptr()), m, int(k),
+                                            C.c_void_p(idx.data_ptr()), C.c_void_p(d2.data_ptr()),
+                                            _stream_ptr(stream)))
+        if host:
+            self.check_status(stream)
+            return idx.cpu().numpy(), d2.cpu().numpy()
+        return idx, d2
+
+    def nearestNeighbor(self, point_id):
+        """(index, squared distance) of the nearest other point of cloud point ``point_id``."""
+        idx, d2 = self.nearest_neighbors([int(point_id)], 1)
+        return int(idx[0, 0]), float(d2[0, 0])
+
     def check_status(self, stream=None):
         check(lib.ebg_cloud_check_status(self._h, _stream_ptr(stream)))
 

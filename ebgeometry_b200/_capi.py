@@ -99,6 +99,9 @@ SIGNATURES = {
     "ebg_cloud_size": (_I64, [_P]),
     "ebg_cloud_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_cloud_self_knn": (C.c_int, [_P, _I32, _P, _P, _P]),
+    "ebg_cloud_self_knn_points": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
+    "ebg_cloud_self_knn_host": (C.c_int, [_P, _I32, _P, _P, _P]),
     "ebg_cloud_check_status": (C.c_int, [_P, _P]),
     "ebg_scene_create": (C.c_int, [_I64, _P, _I64, _P, _P, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_scene_destroy": (C.c_int, [_P]),

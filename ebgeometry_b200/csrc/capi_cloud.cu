@@ -10,6 +10,7 @@
 
 #include "capi_common.h"
 #include "cloud_kernels.h"
+#include "ebg_device.cuh"
 #include "ebgeometry_b200.h"
 #include "mesh_kernels.h"
 
@@ -25,6 +26,7 @@ struct ebg_cloud
   EbgCloudView view{};
   void*        dNodes  = nullptr;
   void*        dPoints = nullptr;
+  uint32_t*    dInv    = nullptr; // cloud index -> leaf position (self queries of given points)
   int*         dStatus = nullptr;
 };
 
@@ -72,6 +74,7 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
   }
   if (cudaMalloc(&c->dNodes, std::max<int64_t>(totalNodes, 1) * sizeof(EbgNode4)) != cudaSuccess ||
       cudaMalloc(&c->dPoints, size_t(n) * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&c->dInv), size_t(n) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&c->dStatus), sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     ebg_cloud_destroy(c);
@@ -99,6 +102,10 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
   cudaError_t e = buildCloud(pointsDev, n, L, b, static_cast<EbgNode4*>(c->dNodes), static_cast<float4*>(c->dPoints),
                              levelNodes, c->levels, rootBox, s);
   freeAll(ws, s);
+  if (e == cudaSuccess) {
+    launchInvertOrder(static_cast<const float4*>(c->dPoints), n, c->dInv, s);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
     ebg_cloud_destroy(c);
     return setError(EBG_ERR_CUDA, std::string("point cloud build failed: ") + cudaGetErrorString(cudaGetLastError()));
@@ -126,10 +133,12 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
   return EBG_OK;
 }
 
+// self = 1: the queries are the cloud's own points -- all of them in leaf order when selfIds is
+// null (nq = n, rows = cloud indices), else the nq cloud indices in selfIds (rows = list order).
 ebg_status runKnn(const ebg_cloud* c, const float* q, int64_t nq, int k, int32_t* idx, float* d2,
-                  const ebg_query_opts* opts, cudaStream_t s)
+                  const ebg_query_opts* opts, cudaStream_t s, int self = 0, const int64_t* selfIds = nullptr)
 {
-  const bool sort = !(opts && opts->no_sort);
+  const bool sort = !self && !(opts && opts->no_sort);
   int        kt   = 1;
   while (kt < k) {
     kt *= 2;
@@ -151,6 +160,23 @@ ebg_status runKnn(const ebg_cloud* c, const float* q, int64_t nq, int k, int32_t
     launchQueryKeys(q, nq, c->view.morton_lo, c->view.morton_scale, kin, iin, s);
     cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(nq), 0, 30, s);
   }
+  uint32_t* selfPos = nullptr;
+  if (self && selfIds) {
+    // leaf positions of the given points, sorted: leaf order is Morton order
+    uint32_t* kin  = devAlloc<uint32_t>(nq, s, ws);
+    uint32_t* rin  = devAlloc<uint32_t>(nq, s, ws);
+    selfPos        = devAlloc<uint32_t>(nq, s, ws);
+    order          = devAlloc<uint32_t>(nq, s, ws);
+    size_t tb      = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, selfPos, rin, order, int(nq), 0, 32, s);
+    void* tmp = devAlloc<char>(tb, s, ws);
+    if (!kin || !rin || !selfPos || !order || !tmp) {
+      freeAll(ws, s);
+      return setError(EBG_ERR_NO_MEMORY, "k-NN query workspace");
+    }
+    launchSelfKeys(selfIds, nq, c->dInv, c->n, kin, rin, c->dStatus, s);
+    cub::DeviceRadixSort::SortPairs(tmp, tb, kin, selfPos, rin, order, int(nq), 0, 32, s);
+  }
   auto* work = devAlloc<unsigned long long>(1, s, ws);
   if (!work) {
     freeAll(ws, s);
@@ -160,14 +186,15 @@ ebg_status runKnn(const ebg_cloud* c, const float* q, int64_t nq, int k, int32_t
   CloudQueryArgs a{};
   a.cloud   = c->view;
   a.queries = q;
-  a.order   = order;
-  a.n       = nq;
+  a.order    = order;
+  a.self_pos = selfPos;
+  a.n        = nq;
   a.k       = k;
   a.out_idx = idx;
   a.out_d2  = d2;
   a.work    = work;
   a.status  = c->dStatus;
-  const cudaError_t e = launchCloudKnn(a, kt, c->numSms, s);
+  const cudaError_t e = launchCloudKnn(a, kt, c->numSms, s, self != 0);
   freeAll(ws, s);
   if (e != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("k-NN launch failed: ") + cudaGetErrorString(e));
@@ -241,6 +268,7 @@ ebg_status ebg_cloud_destroy(ebg_cloud* c)
   cudaSetDevice(c->device);
   cudaFree(c->dNodes);
   cudaFree(c->dPoints);
+  cudaFree(c->dInv);
   cudaFree(c->dStatus);
   delete c;
   return EBG_OK;
@@ -321,6 +349,69 @@ ebg_status ebg_cloud_knn_host(const ebg_cloud*      c,
   return rc;
 }
 
+ebg_status ebg_cloud_self_knn(const ebg_cloud* c, int32_t k, int32_t* idx_dev, float* d2_dev, void* stream)
+{
+  if (c == nullptr || k < 1 || k > 32 || idx_dev == nullptr || d2_dev == nullptr) {
+    return setError(EBG_ERR_INVALID, "bad self k-NN arguments (k must be in [1, 32])");
+  }
+  if (c->n > int64_t(INT32_MAX)) {
+    return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points");
+  }
+  DeviceGuard guard;
+  cudaSetDevice(c->device);
+  return runKnn(c, nullptr, c->n, k, idx_dev, d2_dev, nullptr, static_cast<cudaStream_t>(stream), 1);
+}
+
+ebg_status ebg_cloud_self_knn_points(const ebg_cloud* c,
+                                     const int64_t*   point_ids_dev,
+                                     int64_t          m,
+                                     int32_t          k,
+                                     int32_t*         idx_dev,
+                                     float*           d2_dev,
+                                     void*            stream)
+{
+  if (c == nullptr || m < 0 || k < 1 || k > 32 || (m > 0 && (!point_ids_dev || !idx_dev || !d2_dev))) {
+    return setError(EBG_ERR_INVALID, "bad self k-NN arguments (k must be in [1, 32])");
+  }
+  if (m > int64_t(INT32_MAX)) {
+    return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
+  }
+  if (m == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard guard;
+  cudaSetDevice(c->device);
+  return runKnn(c, nullptr, m, k, idx_dev, d2_dev, nullptr, static_cast<cudaStream_t>(stream), 1, point_ids_dev);
+}
+
+ebg_status ebg_cloud_self_knn_host(const ebg_cloud* c, int32_t k, int32_t* idx_host, float* d2_host, void* stream)
+{
+  if (c == nullptr || k < 1 || k > 32 || idx_host == nullptr || d2_host == nullptr) {
+    return setError(EBG_ERR_INVALID, "bad self k-NN arguments (k must be in [1, 32])");
+  }
+  DeviceGuard        guard;
+  cudaSetDevice(c->device);
+  cudaStream_t       s = static_cast<cudaStream_t>(stream);
+  std::vector<void*> ws;
+  int32_t*           di = devAlloc<int32_t>(c->n * k, s, ws);
+  float*             dd = devAlloc<float>(c->n * k, s, ws);
+  if (!di || !dd) {
+    freeAll(ws, s);
+    return setError(EBG_ERR_NO_MEMORY, "device buffers for the host self k-NN call");
+  }
+  cudaMemsetAsync(c->dStatus, 0, sizeof(int), s);
+  ebg_status rc = ebg_cloud_self_knn(c, k, di, dd, stream);
+  if (rc == EBG_OK) {
+    cudaMemcpyAsync(idx_host, di, size_t(c->n) * k * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(d2_host, dd, size_t(c->n) * k * sizeof(float), cudaMemcpyDeviceToHost, s);
+  }
+  freeAll(ws, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  }
+  return rc == EBG_OK ? ebg_cloud_check_status(c, stream) : rc;
+}
+
 ebg_status ebg_cloud_check_status(const ebg_cloud* c, void* stream)
 {
   if (c == nullptr) {
@@ -336,6 +427,9 @@ ebg_status ebg_cloud_check_status(const ebg_cloud* c, void* stream)
   }
   if (st != 0) {
     cudaMemsetAsync(c->dStatus, 0, sizeof(int), s);
+    if (st & ST_INPUT) {
+      return setError(EBG_ERR_INVALID, "point index out of range in a self k-NN query");
+    }
     return setError(EBG_ERR_TRAVERSAL, "k-NN traversal stopped early (status " + std::to_string(st) + ")");
   }
   return EBG_OK;

@@ -197,7 +197,9 @@ __device__ __forceinline__ bool lexLess(float da, uint32_t ia, float db, uint32_
   return da < db || (da == db && ia < ib);
 }
 
-template <int K>
+// SELF: the queries are cloud points (self_pos), each excluded from its own neighbours
+// (nearestNeighbors / allNearestNeighbors, PointCloudBVHImplem.hpp:455-507).
+template <int K, bool SELF>
 __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
 {
   __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
@@ -218,9 +220,24 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
     const int64_t  pos   = int64_t(pk) * 32 + lane;
     const bool     valid = pos < a.n;
     const int64_t  src   = valid ? pos : a.n - 1;
-    const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
-    const float    px = __ldg(a.queries + 3 * size_t(id)), py = __ldg(a.queries + 3 * size_t(id) + 1),
-                pz = __ldg(a.queries + 3 * size_t(id) + 2);
+    uint32_t       id, self = 0xffffffffu;
+    float          px, py, pz;
+    if (SELF) {
+      // the query point comes from the cloud's own leaf array, which carries its index
+      const uint32_t lp = a.self_pos ? __ldg(a.self_pos + src) : uint32_t(src);
+      const float4   qp = __ldg(c.points + lp);
+      px                = qp.x;
+      py                = qp.y;
+      pz                = qp.z;
+      self              = __float_as_uint(qp.w);
+      id                = a.order ? __ldg(a.order + src) : self;
+    }
+    else {
+      id = a.order ? __ldg(a.order + src) : uint32_t(src);
+      px = __ldg(a.queries + 3 * size_t(id));
+      py = __ldg(a.queries + 3 * size_t(id) + 1);
+      pz = __ldg(a.queries + 3 * size_t(id) + 2);
+    }
     float    kd[K];
     uint32_t ki[K];
 #pragma unroll
@@ -255,7 +272,7 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
           const float4   q  = __ldg(c.points + t);
           const float    dd = d2exact(px - q.x, py - q.y, pz - q.z);
           const uint32_t ii = __float_as_uint(q.w);
-          if (lexLess(dd, ii, kd[K - 1], ki[K - 1])) {
+          if ((!SELF || ii != self) && lexLess(dd, ii, kd[K - 1], ki[K - 1])) {
             kd[K - 1] = dd;
             ki[K - 1] = ii;
 #pragma unroll
@@ -344,18 +361,48 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
   }
 }
 
-template <int K>
-cudaError_t launchKnnK(const CloudQueryArgs& a, int numSms, cudaStream_t s)
+template <int K, bool SELF>
+cudaError_t launchKnnKS(const CloudQueryArgs& a, int numSms, cudaStream_t s)
 {
   int perSm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kCloudKnn<K>, 128, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kCloudKnn<K, SELF>, 128, 0);
   perSm              = perSm < 1 ? 1 : perSm;
   const int64_t need = ((int64_t(a.n) + 31) / 32 + 3) / 4;
   int64_t       grid = int64_t(numSms) * perSm;
   grid               = grid < need ? grid : need;
   grid               = grid < 1 ? 1 : grid;
-  kCloudKnn<K><<<unsigned(grid), 128, 0, s>>>(a);
+  kCloudKnn<K, SELF><<<unsigned(grid), 128, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launchKnnK(const CloudQueryArgs& a, bool self, int numSms, cudaStream_t s)
+{
+  return self ? launchKnnKS<K, true>(a, numSms, s) : launchKnnKS<K, false>(a, numSms, s);
+}
+
+// inv[cloud index] = leaf position
+__global__ void kInvertOrder(const float4* __restrict__ pts, int64_t n, uint32_t* __restrict__ inv)
+{
+  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+    inv[__float_as_uint(pts[j].w)] = uint32_t(j);
+  }
+}
+
+// self queries of a caller's list of cloud indices: sort keys = their leaf positions, values = the
+// caller's row; an index out of range is reported (ST_INPUT) and replaced by 0
+__global__ void kSelfKeys(const int64_t* __restrict__ ids, int64_t m, const uint32_t* __restrict__ inv, int64_t n,
+                          uint32_t* __restrict__ keys, uint32_t* __restrict__ rows, int* __restrict__ status)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t id = ids[i];
+    const bool    ok = id >= 0 && id < n;
+    if (!ok) {
+      atomicOr(status, ST_INPUT);
+    }
+    keys[i] = inv[ok ? id : 0];
+    rows[i] = uint32_t(i);
+  }
 }
 
 inline unsigned blocksFor(int64_t n, int t) { return unsigned((n + t - 1) / t); }
@@ -421,22 +468,35 @@ size_t cloudSortTempBytes(int64_t n)
   return tb;
 }
 
-cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s)
+cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s, bool self)
 {
   switch (kTemplate) {
   case 1:
-    return launchKnnK<1>(a, numSms, s);
+    return launchKnnK<1>(a, self, numSms, s);
   case 2:
-    return launchKnnK<2>(a, numSms, s);
+    return launchKnnK<2>(a, self, numSms, s);
   case 4:
-    return launchKnnK<4>(a, numSms, s);
+    return launchKnnK<4>(a, self, numSms, s);
   case 8:
-    return launchKnnK<8>(a, numSms, s);
+    return launchKnnK<8>(a, self, numSms, s);
   case 16:
-    return launchKnnK<16>(a, numSms, s);
+    return launchKnnK<16>(a, self, numSms, s);
   default:
-    return launchKnnK<32>(a, numSms, s);
+    return launchKnnK<32>(a, self, numSms, s);
   }
+}
+
+void launchInvertOrder(const float4* pts, int64_t n, uint32_t* inv, cudaStream_t s)
+{
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, 8192);
+  kInvertOrder<<<unsigned(blocks < 1 ? 1 : blocks), 256, 0, s>>>(pts, n, inv);
+}
+
+void launchSelfKeys(const int64_t* ids, int64_t m, const uint32_t* inv, int64_t n, uint32_t* keys, uint32_t* rows,
+                    int* status, cudaStream_t s)
+{
+  const int64_t blocks = std::min<int64_t>((m + 255) / 256, 8192);
+  kSelfKeys<<<unsigned(blocks < 1 ? 1 : blocks), 256, 0, s>>>(ids, m, inv, n, keys, rows, status);
 }
 
 } // namespace ebg

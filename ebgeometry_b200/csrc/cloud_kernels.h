@@ -24,7 +24,10 @@ struct CloudQueryArgs
 {
   EbgCloudView        cloud;
   const float*        queries; // caller's xyz
-  const uint32_t*     order;   // sorted position -> caller index (nullptr = identity)
+  const uint32_t*     order;   // sorted position -> caller index (nullptr = identity; in self
+                               // queries: the query point's own cloud index)
+  const uint32_t*     self_pos; // self queries: sorted position -> the query's leaf position in
+                                // cloud.points (nullptr = identity: every cloud point in leaf order)
   int64_t             n;
   int                 k;       // neighbours written per query (<= template K)
   int32_t*            out_idx; // n x k, caller order
@@ -51,7 +54,15 @@ int         cloudLevels(int64_t nLeaves, int64_t* levelNodes, int maxLevels);
 size_t      cloudSortTempBytes(int64_t n);
 cudaError_t buildCloud(const float* points, int64_t n, int L, const CloudBuildBuffers& b, EbgNode4* nodes,
                        float4* leafPts, const int64_t* levelNodes, int nLevels, float* rootBoxHost, cudaStream_t s);
-cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s);
+cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s, bool self = false);
+
+// inv[cloud index] = leaf position, from the leaf points' index words.
+void launchInvertOrder(const float4* pts, int64_t n, uint32_t* inv, cudaStream_t s);
+
+// Self queries of caller-given cloud indices: keys = their leaf positions (the sort key that makes
+// packets coherent), rows = 0..m-1; out-of-range indices set ST_INPUT.
+void launchSelfKeys(const int64_t* ids, int64_t m, const uint32_t* inv, int64_t n, uint32_t* keys, uint32_t* rows,
+                    int* status, cudaStream_t s);
 
 } // namespace ebg
 

@@ -259,7 +259,9 @@ __global__ void __launch_bounds__(128) kMeshBand64(const MeshQueryArgs a, float 
         for (uint32_t tt = t0; tt < t0 + cnt; ++tt) {
           const double d = EVAL == 0 ? triSd64(m.tri64 + 30 * size_t(tt), P)
                                      : dcelFaceSd(m.tri64 + 30 * size_t(tt), m.dcel_n + 3 * size_t(tt), P);
-          if (fabs(d) < fabs(best)) {
+          // strict < as the reference's leaf loop, ties to the lower leaf position (the winner is
+          // then independent of the traversal order)
+          if (fabs(d) < fabs(best) || (fabs(d) == fabs(best) && int(tt) < bt)) {
             best = d;
             bt   = int(tt);
             // shrink the bound to the FP64 winner (with the same relative margin), measured at the

@@ -238,7 +238,9 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
               const int  from = mine ? seg * int(cnt) : 0;
               const float rd = __shfl_sync(FULL, dd, from);
               const int   ri = __shfl_sync(FULL, bi, from);
-              if (mine && rd < best) {
+              // ties go to the lower leaf position, so the winner does not depend on the order
+              // in which packets meet the triangles
+              if (mine && (rd < best || (rd == best && int(t0) + ri < besttri))) {
                 best    = rd;
                 besttri = int(t0) + ri;
               }
@@ -253,7 +255,7 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             float         s, t;
             int           r;
             const float   dd = triDist2<false>(h0, h1, h2, px, py, pz, s, t, r);
-            if (dd < best) {
+            if (dd < best || (dd == best && int(tt) < besttri)) {
               best    = dd;
               besttri = int(tt);
             }

@@ -347,7 +347,26 @@ ebg_status ebg_cloud_knn_host(const ebg_cloud*      cloud,
                               float*                d2_host,
                               const ebg_query_opts* opts,
                               void*                 stream);
-/* Synchronises stream and reports a device-side traversal error of earlier k-NN calls. */
+/* Self queries, PointCloudBVH::allNearestNeighbors(k) (PointCloudBVHImplem.hpp:488-507): the k
+ * nearest OTHER points of every cloud point (the point itself excluded; another point at the same
+ * position is a neighbour at d2 = 0), ordered by (d2, index) -- ties to the lowest index -- into
+ * idx_dev / d2_dev (n x k, row = the point's cloud index; missing neighbours: -1 / +inf).  The
+ * queries run in the cloud's own leaf order, so a packet starts next to its own leaves.
+ * Asynchronous on stream. */
+ebg_status ebg_cloud_self_knn(const ebg_cloud* cloud, int32_t k, int32_t* idx_dev, float* d2_dev, void* stream);
+/* The same for a list of m cloud indices (nearestNeighbors(point, k), PointCloudBVHImplem.hpp:
+ * 470-486); row i answers point_ids_dev[i].  Indices out of range are reported by the next
+ * ebg_cloud_check_status as EBG_ERR_INVALID. */
+ebg_status ebg_cloud_self_knn_points(const ebg_cloud* cloud,
+                                     const int64_t*   point_ids_dev,
+                                     int64_t          m,
+                                     int32_t          k,
+                                     int32_t*         idx_dev,
+                                     float*           d2_dev,
+                                     void*            stream);
+/* ebg_cloud_self_knn with host output arrays (n x k), synchronous. */
+ebg_status ebg_cloud_self_knn_host(const ebg_cloud* cloud, int32_t k, int32_t* idx_host, float* d2_host, void* stream);
+/* Synchronises stream and reports a device-side error of earlier k-NN calls. */
 ebg_status ebg_cloud_check_status(const ebg_cloud* cloud, void* stream);
 
 /* ---- CSG union: BVHUnionIF (CSG.hpp:401-468) ------------------------------------------------

@@ -76,6 +76,8 @@ class _Ref:
             "ref_cloud_destroy": (None, [_P]),
             "ref_cloud_knn": (C.c_int, [_P, _P, _I64, C.c_int, _P, _P, C.c_int]),
             "ref_cloud_knn_lex": (C.c_int, [_P, _P, _I64, C.c_int, _P, _P, C.c_int]),
+            "ref_cloud_knn_lex_excl": (C.c_int, [_P, _P, _I64, C.c_int, _P, _P, C.c_int, C.c_int]),
+            "ref_cloud_all_nn": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
             "ref_scene_create": (_P, [_I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P]),
             "ref_scene_destroy": (None, [_P]),
             "ref_scene_value": (C.c_int, [_P, _P, _I64, _P, C.c_int, C.c_int]),
@@ -176,6 +178,19 @@ class _Ref:
             assert fn(self.h, _ptr(q), q.shape[0], k, _ptr(idx), _ptr(d2), threads) == 0
             return idx, d2
 
+        def self_knn(self, k, lex=True, threads=0):
+            """Every cloud point's k neighbours, itself excluded.  lex: the reference's traversal
+            with a (d2, index) state (lowest index on ties); else its own allNearestNeighbors."""
+            n = self.p.shape[0]
+            idx = np.empty((n, k), np.int64)
+            d2 = np.empty((n, k), np.float32)
+            if lex:
+                rc = self.ref.lib.ref_cloud_knn_lex_excl(self.h, _ptr(self.p), n, k, _ptr(idx), _ptr(d2), threads, 1)
+            else:
+                rc = self.ref.lib.ref_cloud_all_nn(self.h, k, n, _ptr(idx), _ptr(d2))
+            assert rc == 0
+            return idx, d2
+
     def cloud(self, p):
         return _Ref.Cloud(self, p)
 
@@ -224,6 +239,7 @@ class _Port:
             "port_mesh_sdf_flat": (None, [_P, _P, _I64, _P, _P, _P, _P, _I64, _P, _P]),
             "port_dcel_face_sd": (_D, [_P, _P, _P, _P, _P]),
             "port_knn_brute": (None, [_P, _I64, _P, _I64, C.c_int, _P, _P]),
+            "port_knn_brute_self": (None, [_P, _I64, C.c_int, _P, _P]),
             "port_sphere_sd": (_D, [_P, _D, _P]),
             "port_rotate_point": (None, [_D, C.c_int, _P, _P]),
             "port_scene_brute": (None, [_I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I64, _P]),
@@ -291,6 +307,14 @@ class _Port:
         idx = np.empty((q.shape[0], k), np.int32)
         d2 = np.empty((q.shape[0], k), np.float32)
         self.lib.port_knn_brute(_ptr(pts), pts.shape[0], _ptr(q), q.shape[0], k, _ptr(idx), _ptr(d2))
+        return idx, d2
+
+    def knn_brute_self(self, pts, k):
+        """Every point's k nearest other points, lexicographic (d2, index)."""
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        idx = np.empty((pts.shape[0], k), np.int32)
+        d2 = np.empty((pts.shape[0], k), np.float32)
+        self.lib.port_knn_brute_self(_ptr(pts), pts.shape[0], k, _ptr(idx), _ptr(d2))
         return idx, d2
 
     def scene_brute(self, spheres, meshes, poses, p):

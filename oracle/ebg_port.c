@@ -477,7 +477,8 @@ void port_mesh_sdf_flat(const double* V, const int64_t* F, int64_t nf, const dou
  * (PointSoAImplem.hpp:214-230): dx = q - p, d2 = (dx*dx + dy*dy) + dz*dz, no fused multiply-add.
  * Missing neighbours (k > n) are index -1, d2 = +inf.
  */
-void port_knn_brute(const float* P, int64_t n, const float* Q, int64_t nq, int k, int32_t* idx, float* d2)
+void port_knn_brute_excl(const float* P, int64_t n, const float* Q, int64_t nq, int k, int32_t* idx, float* d2,
+                         int exclude_self)
 {
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t q = 0; q < nq; q++) {
@@ -485,6 +486,9 @@ void port_knn_brute(const float* P, int64_t n, const float* Q, int64_t nq, int k
     int32_t bi[64];
     int     found = 0;
     for (int64_t i = 0; i < n; i++) {
+      if (exclude_self && i == q) {
+        continue;
+      }
       const float dx = Q[3 * q + 0] - P[3 * i + 0];
       const float dy = Q[3 * q + 1] - P[3 * i + 1];
       const float dz = Q[3 * q + 2] - P[3 * i + 2];
@@ -510,6 +514,20 @@ void port_knn_brute(const float* P, int64_t n, const float* Q, int64_t nq, int k
       d2[q * k + j]  = j < found ? bd[j] : INFINITY;
     }
   }
+}
+
+void port_knn_brute(const float* P, int64_t n, const float* Q, int64_t nq, int k, int32_t* idx, float* d2)
+{
+  port_knn_brute_excl(P, n, Q, nq, k, idx, d2, 0);
+}
+
+/*
+ * Self queries (nearestNeighbors / allNearestNeighbors, PointCloudBVHImplem.hpp:455-507): query i is
+ * cloud point i and is excluded from its own neighbours; same order and tie rule as above.
+ */
+void port_knn_brute_self(const float* P, int64_t n, int k, int32_t* idx, float* d2)
+{
+  port_knn_brute_excl(P, n, P, n, k, idx, d2, 1);
 }
 
 /* SphereSDF::signedDistance (AnalyticDistanceFunctions.hpp:238-246): |p - c| - r. */

@@ -336,7 +336,20 @@ ref_cloud_knn(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, float*
 // with a k-best state ordered lexicographically by (d2, index): ties resolve to the lowest index.
 // The leaf scan reads the reference's PointSoA squared distances (PointSoAImplem.hpp:60-230).
 int
+ref_cloud_knn_lex_excl(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, float* d2, int a_threads,
+                       int a_excludeSelf);
+
+int
 ref_cloud_knn_lex(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, float* d2, int a_threads)
+{
+  return ref_cloud_knn_lex_excl(a_h, Q, nq, k, idx, d2, a_threads, 0);
+}
+
+// The same with, when a_excludeSelf is set, query i being cloud point i and excluded from its own
+// result (the self queries nearestNeighbors / allNearestNeighbors, PointCloudBVHImplem.hpp:455-507).
+int
+ref_cloud_knn_lex_excl(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, float* d2, int a_threads,
+                       int a_excludeSelf)
 {
   auto*     c  = static_cast<Cloud*>(a_h);
   const int nt = a_threads > 0 ? a_threads : omp_get_max_threads();
@@ -355,12 +368,16 @@ ref_cloud_knn_lex(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, fl
     s.d.assign(k, std::numeric_limits<float>::max());
     s.id.assign(k, std::numeric_limits<size_t>::max());
     const auto& groups   = c->getPrimitives();
-    auto        evalLeaf = [&groups, &q](State& st, size_t off, size_t cnt) noexcept {
+    const size_t self     = a_excludeSelf ? size_t(i) : std::numeric_limits<size_t>::max();
+    auto        evalLeaf = [&groups, &q, self](State& st, size_t off, size_t cnt) noexcept {
       for (size_t g = off; g < off + cnt; g++) {
         const auto dist = groups[g].getDistances2(q);
         for (size_t lane = 0; lane < dist.size(); lane++) {
           const float  dd = dist[lane];
           const size_t ii = groups[g].getMetaData(lane);
+          if (ii == self) {
+            continue;
+          }
           // Padded lanes repeat the last real point; skip duplicates already held.
           bool dup = false;
           for (int j = 0; j < st.found; j++) {
@@ -392,6 +409,24 @@ ref_cloud_knn_lex(void* a_h, const float* Q, int64_t nq, int k, int64_t* idx, fl
       idx[i * k + j] = (j < s.found) ? int64_t(s.id[j]) : -1;
       d2[i * k + j]  = (j < s.found) ? s.d[j] : std::numeric_limits<float>::infinity();
     }
+  }
+  return 0;
+}
+
+// The reference's own allNearestNeighbors(k) (PointCloudBVHImplem.hpp:488-507): k neighbours of every
+// cloud point, itself excluded, in the reference's order (ties in traversal order).
+int
+ref_cloud_all_nn(void* a_h, int k, int64_t n, int64_t* idx, float* d2)
+{
+  auto*      c    = static_cast<Cloud*>(a_h);
+  const auto hits = c->allNearestNeighbors(size_t(k));
+  if (int64_t(hits.size()) != n * k) {
+    return -1;
+  }
+  for (int64_t i = 0; i < n * k; i++) {
+    const bool none = hits[i].index == std::numeric_limits<size_t>::max();
+    idx[i]          = none ? -1 : int64_t(hits[i].index);
+    d2[i]           = none ? std::numeric_limits<float>::infinity() : hits[i].distanceSquared;
   }
   return 0;
 }

@@ -16,7 +16,8 @@ It builds nothing but the oracle (``make -C oracle``) and writes small .npz file
   TriMeshSDF<double,short,4,4> (SAH) and FlatMeshSDF values and DCEL pseudonormals.
 * ``icosphere_l2.npz``   -- a displaced level-2 icosphere with the reference's pseudonormals and
   TriMeshSDF values at 2000 seeded points (including 500 within 1e-3 of the surface).
-* ``cloud2000.npz``      -- Tests/TestPointCloudBVH.cpp's 2000-point cloud (mt19937 seed 20260708)
+* ``cloud2000.npz``      -- Tests/TestPointCloudBVH.cpp's 2000-point cloud (mt19937 seed 20260708),
+  external queries and the self queries of allNearestNeighbors (k = 1, 5 and lexicographic k = 8)
   and 200 external queries (seed 99), with the reference's PointCloudBVH closestPoints (k = 1, 5)
   and the same traversal with (d2, index) ordering.
 * ``csg_small.npz``      -- a union of 40 spheres and 3 posed displaced icospheres evaluated by the
@@ -102,8 +103,12 @@ def main(reference: str) -> None:
     i5, d5 = c.knn(qs, 5, lex=False)
     l1, e1 = c.knn(qs, 1, lex=True)
     l8, e8 = c.knn(qs, 8, lex=True)
+    # self queries: the reference's allNearestNeighbors (itself excluded) and the lexicographic state
+    s1, t1 = c.self_knn(1, lex=False)
+    s5, t5 = c.self_knn(5, lex=False)
+    sl8, tl8 = c.self_knn(8, lex=True)
     np.savez(os.path.join(HERE, "cloud2000.npz"), points=pts, queries=qs, idx1=i1, d1=d1, idx5=i5, d5=d5, lex1=l1,
-             lexd1=e1, lex8=l8, lexd8=e8)
+             lexd1=e1, lex8=l8, lexd8=e8, self1=s1, selfd1=t1, self5=s5, selfd5=t5, selflex8=sl8, selflexd8=tl8)
 
     # --- small CSG union --------------------------------------------------------------------------------
     sc = W.csg_scene(77, n_spheres=40, n_meshes=3, levels=(1, 3), mesh_radius=(0.15, 0.3))

@@ -105,3 +105,48 @@ def test_full_size_cloud_against_reference_sample():
         ri, rd = rc.knn(q, k, lex=True)
         assert np.array_equal(d2, rd)
         assert np.mean(idx == ri) > 0.9999  # the reference traversal's own ties at equal box distance
+
+
+# --- self queries: allNearestNeighbors / nearestNeighbors ------------------------------------------
+def test_self_knn_reference_fixture(golden):
+    """The reference's own allNearestNeighbors on its test cloud (k = 1, 5) and the (d2, index)
+    ordered traversal (k = 8): bit-identical."""
+    g = golden("cloud2000.npz")
+    c = PointCloudBVH(g["points"])
+    for k, idx_key, d2_key in ((1, "self1", "selfd1"), (5, "self5", "selfd5"), (8, "selflex8", "selflexd8")):
+        idx, d2 = c.all_nearest_neighbors(k)
+        assert np.array_equal(d2, g[d2_key]), k
+        assert np.array_equal(idx, g[idx_key].astype(np.int32)), k
+
+
+@pytest.mark.parametrize("k", [1, 4, 16])
+def test_self_knn_against_brute_force_with_duplicates(k):
+    rng = np.random.default_rng(5)
+    p = rng.uniform(0, 1, size=(12000, 3)).astype(np.float32)
+    p[6000:6500] = p[:500]                         # exact duplicates: neighbours at d2 = 0
+    p[7000:7200] = np.round(p[7000:7200] * 8) / 8  # lattice points: many equal distances
+    c = PointCloudBVH(p, leaf_size=8)
+    idx, d2 = c.all_nearest_neighbors(k)
+    bi, bd = oracle.port().knn_brute_self(p, k)
+    assert np.array_equal(d2, bd)
+    assert np.array_equal(idx, bi)
+    assert not np.any(idx == np.arange(p.shape[0])[:, None])  # never itself
+
+
+def test_self_knn_points_subset_and_errors():
+    rng = np.random.default_rng(6)
+    p = rng.uniform(-1, 1, size=(30000, 3)).astype(np.float32)
+    c = PointCloudBVH(p)
+    all_idx, all_d2 = c.all_nearest_neighbors(3)
+    ids = rng.integers(0, p.shape[0], size=5000)
+    ids[:10] = ids[10]                               # repeated ids are fine
+    idx, d2 = c.nearest_neighbors(ids, 3)
+    assert np.array_equal(idx, all_idx[ids]) and np.array_equal(d2, all_d2[ids])
+    i1, dd1 = c.nearestNeighbor(123)
+    assert i1 == all_idx[123, 0] and dd1 == all_d2[123, 0]
+    with pytest.raises(EbgError):
+        c.nearest_neighbors([0, p.shape[0]], 1)
+    # a one-point cloud has no other point
+    one = PointCloudBVH(p[:1])
+    idx1, d21 = one.all_nearest_neighbors(2)
+    assert np.all(idx1 == -1) and np.all(np.isinf(d21))

@@ -94,3 +94,13 @@ def test_reference_reproduces_fixtures(golden):
     c = golden("cloud2000.npz")
     idx, d2 = R.cloud(c["points"]).knn(c["queries"], 8, lex=True)
     assert np.array_equal(idx, c["lex8"])
+
+
+def test_self_knn_brute_matches_reference(port, golden):
+    """The C restatement of the self queries (the point itself excluded, (d2, index) order) against
+    the reference's allNearestNeighbors on its own test cloud."""
+    g = golden("cloud2000.npz")
+    for k, idx_key, d2_key in ((1, "self1", "selfd1"), (5, "self5", "selfd5"), (8, "selflex8", "selflexd8")):
+        idx, d2 = port.knn_brute_self(g["points"], k)
+        assert np.array_equal(d2, g[d2_key])
+        assert np.array_equal(idx, g[idx_key].astype(np.int32))
