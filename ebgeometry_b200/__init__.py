@@ -57,15 +57,16 @@ class TriMeshSDF:
     ``vertices``: (V,3) float64; ``triangles``: (T,3) int32 corner indices, counter-clockwise seen
     from outside.  Pseudonormals are computed the way the reference's DCEL computes them unless
     ``vertex_normals`` (per corner, (T,3,3)) and ``edge_normals`` ((T,3,3), edge i from corner i to
-    i+1) are given.  ``build``: "SAH" or "Morton"; ``leaf_size``: max triangles per leaf.
+    i+1) are given.  ``build``: "SAH" or "Morton"; ``leaf_size``: max triangles per leaf;
+    ``on_device``: build the (Morton) tree, records and boxes on the GPU.
     """
 
     def __init__(self, vertices, triangles, build="SAH", leaf_size=8, device=-1,
-                 vertex_normals=None, edge_normals=None):
+                 vertex_normals=None, edge_normals=None, on_device=False):
         v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
         f = np.ascontiguousarray(triangles, dtype=np.int32).reshape(-1, 3)
         b = {"SAH": BUILD_SAH, "MORTON": BUILD_MORTON}[str(build).upper()] if isinstance(build, str) else int(build)
-        opts = _capi.BuildOpts(b, int(leaf_size), int(device), 0)
+        opts = _capi.BuildOpts(b, int(leaf_size), int(device), 1 if on_device else 0)
         h = C.c_void_p()
         if vertex_normals is not None or edge_normals is not None:
             vn = np.ascontiguousarray(vertex_normals, dtype=np.float64).reshape(-1, 9)

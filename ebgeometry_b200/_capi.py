@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libebgb200.so")
 
 class BuildOpts(C.Structure):
     _fields_ = [("build", C.c_int32), ("leaf_size", C.c_int32), ("device", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("flags", C.c_int32)]
 
 
 class PhaseTimings(C.Structure):

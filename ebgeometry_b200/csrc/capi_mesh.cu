@@ -15,6 +15,7 @@
 #include "capi_internal.h"
 #include "ebg_device.cuh"
 #include "ebgeometry_b200.h"
+#include "mesh_build_gpu.h"
 #include "mesh_host.h"
 #include "mesh_kernels.h"
 #include "seed_kernels.h"
@@ -178,6 +179,53 @@ void computeObbs(const double* V, const int32_t* F, Bvh4& bvh, std::vector<EbgOb
   }
 }
 
+// The device view and the summary of a mesh whose device arrays are in place (either build).
+ebg_status finishMesh(ebg_mesh* m, int64_t nv, int64_t nt, int leafSize, const double* lo, const double* hi,
+                      ebg_mesh** out)
+{
+  if (cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
+      cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    ebg_mesh_destroy(m);
+    return setError(EBG_ERR_NO_MEMORY, "device allocation for the mesh status");
+  }
+  EbgMeshView& v = m->view;
+  v.nodes        = static_cast<const EbgNode4*>(m->dNodes);
+  v.hot          = static_cast<const EbgTriHot*>(m->dHot);
+  v.sign         = static_cast<const EbgTriSign*>(m->dSign);
+  v.tri64        = static_cast<const double*>(m->dTri64);
+  v.tri_id       = static_cast<const int32_t*>(m->dTriId);
+  v.obb          = static_cast<const EbgObb*>(m->dObb);
+  v.node_obb     = static_cast<const EbgObb*>(m->dNodeObb);
+  v.dcel_n       = static_cast<const double*>(m->dDcelN);
+  for (int a = 0; a < 3; a++) {
+    v.root_lo[a] = roundDown(lo[a]);
+    v.root_hi[a] = roundUp(hi[a]);
+    // Morton domain for query ordering: the mesh box grown to twice its extent about its centre
+    const double c    = 0.5 * (lo[a] + hi[a]);
+    const double ext  = std::max(hi[a] - lo[a], 1e-30);
+    v.morton_lo[a]    = float(c - ext);
+    v.morton_scale[a] = float(1024.0 / (2.0 * ext));
+  }
+  ebg_mesh_info& inf = m->info;
+  inf.num_triangles  = nt;
+  inf.num_vertices   = nv;
+  inf.leaf_size      = leafSize;
+  double d2          = 0;
+  for (int a = 0; a < 3; a++) {
+    inf.lo[a] = lo[a];
+    inf.hi[a] = hi[a];
+    d2 += (hi[a] - lo[a]) * (hi[a] - lo[a]);
+  }
+  inf.diagonal     = std::sqrt(d2);
+  const size_t N   = size_t(nt);
+  inf.device_bytes = int64_t(size_t(std::max<int64_t>(inf.num_nodes, 1)) * (sizeof(EbgNode4) + sizeof(EbgObb)) +
+                             size_t(inf.num_leaves) * sizeof(EbgObb) +
+                             N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 33 * sizeof(double) + 4));
+  *out             = m;
+  return EBG_OK;
+}
+
 ebg_status buildMesh(const double*         V,
                      int64_t               nv,
                      const int32_t*        F,
@@ -263,6 +311,27 @@ ebg_status buildMesh(const double*         V,
   else if (!computePseudonormals(V, nv, F, nt, m->triN, m->cornerVN, m->edgeN, msg)) {
     delete m;
     return setError(EBG_ERR_INVALID, msg);
+  }
+
+  if (opts && (opts->flags & EBG_BUILD_ON_DEVICE)) {
+    if (build != EBG_BUILD_MORTON) {
+      delete m;
+      return setError(EBG_ERR_INVALID, "the device build makes Morton trees only");
+    }
+    cudaStream_t bs = nullptr;
+    if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) {
+      delete m;
+      return setError(EBG_ERR_CUDA, "stream for the device build");
+    }
+    double           lo[3], hi[3];
+    const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, leafSize, lo, hi, bs);
+    cudaStreamDestroy(bs);
+    if (rc != EBG_OK) {
+      const std::string keep = ebg_last_error();
+      ebg_mesh_destroy(m);
+      return setError(rc, keep);
+    }
+    return finishMesh(m, nv, nt, leafSize, lo, hi, out);
   }
 
   // primitive boxes / centroids
@@ -366,53 +435,18 @@ ebg_status buildMesh(const double*         V,
       !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
       !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgObb)) ||
       !up(&m->dNodeObb, nodeObb.data(), nodeObb.size() * sizeof(EbgObb)) ||
-      !up(&m->dDcelN, dcelN.data(), dcelN.size() * sizeof(double)) ||
-      cudaMalloc(reinterpret_cast<void**>(&m->dStatus), sizeof(int)) != cudaSuccess ||
-      cudaMemset(m->dStatus, 0, sizeof(int)) != cudaSuccess) {
+      !up(&m->dDcelN, dcelN.data(), dcelN.size() * sizeof(double))) {
     cudaGetLastError();
     ebg_mesh_destroy(m);
     return setError(EBG_ERR_NO_MEMORY, "device allocation or upload failed for the mesh");
   }
 
-  EbgMeshView& v = m->view;
-  v.nodes        = static_cast<const EbgNode4*>(m->dNodes);
-  v.hot          = static_cast<const EbgTriHot*>(m->dHot);
-  v.sign         = static_cast<const EbgTriSign*>(m->dSign);
-  v.tri64        = static_cast<const double*>(m->dTri64);
-  v.tri_id       = static_cast<const int32_t*>(m->dTriId);
-  v.obb          = static_cast<const EbgObb*>(m->dObb);
-  v.node_obb     = static_cast<const EbgObb*>(m->dNodeObb);
-  v.dcel_n       = static_cast<const double*>(m->dDcelN);
-  for (int a = 0; a < 3; a++) {
-    v.root_lo[a] = roundDown(bvh.lo[a]);
-    v.root_hi[a] = roundUp(bvh.hi[a]);
-    // Morton domain for query ordering: the mesh box grown to twice its extent about its centre
-    const double c   = 0.5 * (bvh.lo[a] + bvh.hi[a]);
-    const double ext = std::max(bvh.hi[a] - bvh.lo[a], 1e-30);
-    v.morton_lo[a]   = float(c - ext);
-    v.morton_scale[a] = float(1024.0 / (2.0 * ext));
-  }
-  v.root_ref   = bvh.rootRef;
-  v.root_count = bvh.rootCount;
-
-  ebg_mesh_info& inf = m->info;
-  inf.num_triangles  = nt;
-  inf.num_vertices   = nv;
-  inf.num_nodes      = int64_t(bvh.nodes.size());
-  inf.num_leaves     = bvh.numLeaves;
-  inf.depth          = bvh.depth;
-  inf.leaf_size      = leafSize;
-  double d2          = 0;
-  for (int a = 0; a < 3; a++) {
-    inf.lo[a] = bvh.lo[a];
-    inf.hi[a] = bvh.hi[a];
-    d2 += (bvh.hi[a] - bvh.lo[a]) * (bvh.hi[a] - bvh.lo[a]);
-  }
-  inf.diagonal     = std::sqrt(d2);
-  inf.device_bytes = int64_t(nodeBytes + N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 33 * sizeof(double) + 4) +
-                             (obb.size() + nodeObb.size()) * sizeof(EbgObb));
-  *out             = m;
-  return EBG_OK;
+  m->info.num_nodes  = int64_t(bvh.nodes.size());
+  m->info.num_leaves = bvh.numLeaves;
+  m->info.depth      = bvh.depth;
+  m->view.root_ref   = bvh.rootRef;
+  m->view.root_count = bvh.rootCount;
+  return finishMesh(m, nv, nt, leafSize, bvh.lo, bvh.hi, out);
 }
 
 struct Workspace

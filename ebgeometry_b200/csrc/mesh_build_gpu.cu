@@ -1,0 +1,860 @@
+// Device build of a mesh's Morton 4-wide BVH and its leaf-ordered records (sm_100a).
+//
+// The same tree family as the host Morton build (mesh_host.cpp): triangles sorted by the 63-bit
+// Morton code of their centroid (21 bits per axis over the centroids' box), every range split at
+// the highest bit in which its first and last codes differ, 4-wide nodes made by repeatedly
+// splitting the child of largest box area, leaves of at most leafSize triangles.  On the device:
+//   1. per triangle: FP64 box and centroid, the centroids' box (warp-reduced atomics on
+//      order-preserving integer keys), the Morton code; CUB radix sort of (code, triangle);
+//   2. the binary radix tree of the sorted codes, each internal node found independently from the
+//      common-prefix lengths of its neighbours (equal codes are told apart by position), so its
+//      split is the highest differing bit of its range -- the host's Morton split;
+//   3. FP64 node boxes bottom-up: each triangle walks to the root and the second of two siblings to
+//      arrive computes the parent (an atomic counter per node, no waiting);
+//   4. the 4-wide tree top-down, one launch per level: each node expands its largest-area children
+//      up to four, as the host does; leaves and nodes get their indices from atomic counters;
+//   5. leaf-ordered triangle records (the FP32 hot and sign records, the FP64 lane records, the DCEL
+//      normals, areas), and the oriented box of every leaf and node (one block per range).
+// The pseudonormals come from the host (bit-identical to the reference's DCEL).  Results do not
+// depend on the tree's shape, so a mesh built here answers exactly as a host-built one.
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cuda_runtime.h>
+
+#include "capi_common.h"
+#include "capi_internal.h"
+#include "ebg_device.cuh"
+#include "mesh_build_gpu.h"
+#include "mesh_host.h"
+
+namespace ebg {
+
+namespace {
+
+constexpr uint32_t NONE = 0xffffffffu;
+
+// order-preserving map of a double onto uint64 (for atomic min / max)
+__device__ __forceinline__ unsigned long long dkey(double x)
+{
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(x));
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dval(unsigned long long k)
+{
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double(static_cast<long long>(b));
+}
+__host__ double hostDval(unsigned long long k)
+{
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  double                   d;
+  std::memcpy(&d, &b, sizeof(d));
+  return d;
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t x)
+{
+  x &= 0x1fffff;
+  x = (x | x << 32) & 0x1f00000000ffffULL;
+  x = (x | x << 16) & 0x1f0000ff0000ffULL;
+  x = (x | x << 8) & 0x100f00f00f00f00fULL;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+  x = (x | x << 2) & 0x1249249249249249ULL;
+  return x;
+}
+
+// 1a. triangle boxes and centroids; bounds: [0..2] centroid lo, [3..5] centroid hi, [6..8] box lo,
+// [9..11] box hi, as dkey values
+__global__ void kTriBounds(const double* __restrict__ V, const int32_t* __restrict__ F, int64_t nt,
+                           double* __restrict__ boxLo, double* __restrict__ boxHi, double* __restrict__ cen,
+                           unsigned long long* __restrict__ bounds)
+{
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < nt; base += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t f     = base + threadIdx.x;
+    const bool    valid = f < nt;
+    double        c[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (valid) {
+      for (int a = 0; a < 3; a++) {
+        const double x0 = V[3 * int64_t(F[3 * f]) + a], x1 = V[3 * int64_t(F[3 * f + 1]) + a],
+                     x2 = V[3 * int64_t(F[3 * f + 2]) + a];
+        lo[a]           = fmin(x0, fmin(x1, x2));
+        hi[a]           = fmax(x0, fmax(x1, x2));
+        c[a]            = (x0 + x1 + x2) / 3.0;
+        boxLo[3 * f + a] = lo[a];
+        boxHi[3 * f + a] = hi[a];
+        cen[3 * f + a]   = c[a];
+      }
+    }
+    // warp-reduce the twelve keys, then one atomic each per warp
+    unsigned long long k[12];
+    for (int a = 0; a < 3; a++) {
+      k[a]     = valid ? dkey(c[a]) : ~0ull;
+      k[3 + a] = valid ? dkey(c[a]) : 0ull;
+      k[6 + a] = valid ? dkey(lo[a]) : ~0ull;
+      k[9 + a] = valid ? dkey(hi[a]) : 0ull;
+    }
+    for (int j = 0; j < 12; j++) {
+      const bool isMin = (j < 3) || (j >= 6 && j < 9);
+      for (int off = 16; off > 0; off >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(FULL, k[j], off);
+        k[j]                       = isMin ? (o < k[j] ? o : k[j]) : (o > k[j] ? o : k[j]);
+      }
+      if (lane == 0) {
+        if (isMin) {
+          atomicMin(bounds + j, k[j]);
+        }
+        else {
+          atomicMax(bounds + j, k[j]);
+        }
+      }
+    }
+  }
+}
+
+// 1b. Morton codes of the centroids over their box (the host build's codes exactly)
+__global__ void kTriMorton(const double* __restrict__ cen, int64_t nt, const unsigned long long* __restrict__ bounds,
+                           uint64_t* __restrict__ codes, uint32_t* __restrict__ ids)
+{
+  double cl[3], ext[3];
+  for (int a = 0; a < 3; a++) {
+    cl[a]  = dval(bounds[a]);
+    ext[a] = dval(bounds[3 + a]) - cl[a];
+  }
+  for (int64_t f = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; f < nt; f += int64_t(gridDim.x) * blockDim.x) {
+    uint64_t c = 0;
+    for (int a = 0; a < 3; a++) {
+      const double   u = ext[a] > 0 ? (cen[3 * f + a] - cl[a]) / ext[a] : 0.0;
+      const uint64_t q = uint64_t(fmin(fmax(u * 2097151.0, 0.0), 2097151.0));
+      c |= spread21(q) << (2 - a);
+    }
+    codes[f] = c;
+    ids[f]   = uint32_t(f);
+  }
+}
+
+// 2. binary radix tree over the n sorted codes: internal node i in [0, n-1) gets its children
+// (leaf = position | EBG_LEAF_BIT), its range [first, last] and is the parent of its children
+__device__ __forceinline__ int prefixLen(const uint64_t* __restrict__ k, int64_t n, int64_t i, int64_t j)
+{
+  if (j < 0 || j >= n) {
+    return -1;
+  }
+  const uint64_t a = k[i], b = k[j];
+  return a != b ? __clzll(static_cast<long long>(a ^ b)) : 64 + __clz(static_cast<int>(uint32_t(i) ^ uint32_t(j)));
+}
+
+__global__ void kRadixTree(const uint64_t* __restrict__ k, int64_t n, uint32_t* __restrict__ left,
+                           uint32_t* __restrict__ right, uint32_t* __restrict__ first, uint32_t* __restrict__ last,
+                           uint32_t* __restrict__ parentI, uint32_t* __restrict__ parentL, int* __restrict__ err)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n - 1; i += int64_t(gridDim.x) * blockDim.x) {
+    const int d    = prefixLen(k, n, i, i + 1) - prefixLen(k, n, i, i - 1) > 0 ? 1 : -1;
+    const int dmin = prefixLen(k, n, i, i - d);
+    int64_t   lmax = 2;
+    while (prefixLen(k, n, i, i + lmax * d) > dmin) {
+      lmax *= 2;
+    }
+    int64_t l = 0;
+    for (int64_t t = lmax / 2; t >= 1; t /= 2) {
+      if (prefixLen(k, n, i, i + (l + t) * d) > dmin) {
+        l += t;
+      }
+    }
+    const int64_t j     = i + l * d;
+    const int     dnode = prefixLen(k, n, i, j);
+    int64_t       s     = 0;
+    for (int64_t t = (l + 1) / 2;; t = (t + 1) / 2) {
+      if (prefixLen(k, n, i, i + (s + t) * d) > dnode) {
+        s += t;
+      }
+      if (t == 1) {
+        break;
+      }
+    }
+    const int64_t g  = i + s * d + (d < 0 ? -1 : 0);
+    const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+    if (lo < 0 || hi >= n || g < lo || g + 1 > hi) {
+      atomicOr(err, 4); // not a valid split: leave this node unwritten and report
+      continue;
+    }
+    const uint32_t L = (lo == g) ? (EBG_LEAF_BIT | uint32_t(g)) : uint32_t(g);
+    const uint32_t R = (hi == g + 1) ? (EBG_LEAF_BIT | uint32_t(g + 1)) : uint32_t(g + 1);
+    left[i]  = L;
+    right[i] = R;
+    first[i] = uint32_t(lo);
+    last[i]  = uint32_t(hi);
+    if (L & EBG_LEAF_BIT) {
+      parentL[L & ~EBG_LEAF_BIT] = uint32_t(i);
+    }
+    else {
+      parentI[L] = uint32_t(i);
+    }
+    if (R & EBG_LEAF_BIT) {
+      parentL[R & ~EBG_LEAF_BIT] = uint32_t(i);
+    }
+    else {
+      parentI[R] = uint32_t(i);
+    }
+  }
+}
+
+// 3. FP64 boxes bottom-up.  Leaf boxes are the sorted triangles' boxes; an internal node's box is
+// written by whichever of its two children's walks arrives second (the first leaves).
+__device__ __forceinline__ void childBox(uint32_t ref, const double* leafLo, const double* leafHi,
+                                         const double* nodeLo, const double* nodeHi, double* lo, double* hi)
+{
+  const double* l = (ref & EBG_LEAF_BIT) ? leafLo + 3 * size_t(ref & ~EBG_LEAF_BIT) : nodeLo + 3 * size_t(ref);
+  const double* h = (ref & EBG_LEAF_BIT) ? leafHi + 3 * size_t(ref & ~EBG_LEAF_BIT) : nodeHi + 3 * size_t(ref);
+  for (int a = 0; a < 3; a++) {
+    lo[a] = __ldcg(l + a);
+    hi[a] = __ldcg(h + a);
+  }
+}
+
+__device__ __forceinline__ bool validRef(uint32_t ref, int64_t n)
+{
+  return (ref & EBG_LEAF_BIT) ? int64_t(ref & ~EBG_LEAF_BIT) < n : int64_t(ref) < n - 1;
+}
+
+__global__ void kRefit(int64_t n, const uint32_t* __restrict__ ids, const double* __restrict__ triLo,
+                       const double* __restrict__ triHi, double* __restrict__ leafLo, double* __restrict__ leafHi,
+                       const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                       const uint32_t* __restrict__ parentI, const uint32_t* __restrict__ parentL, double* nodeLo,
+                       double* nodeHi, uint32_t* arrivals, int* __restrict__ err)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t f = ids[i];
+    for (int a = 0; a < 3; a++) {
+      leafLo[3 * i + a] = triLo[3 * size_t(f) + a];
+      leafHi[3 * i + a] = triHi[3 * size_t(f) + a];
+    }
+    if (n == 1) {
+      continue;
+    }
+    __threadfence();
+    uint32_t p = parentL[i];
+    // at most n - 1 ancestors
+    for (int64_t step = 0; step < n; step++) {
+      if (int64_t(p) >= n - 1 || !validRef(left[p], n) || !validRef(right[p], n)) {
+        atomicOr(err, 8); // an unset or invalid link: stop and report
+        break;
+      }
+      if (atomicAdd(arrivals + p, 1u) == 0u) {
+        break; // the sibling's walk will write p
+      }
+      __threadfence();
+      double l0[3], h0[3], l1[3], h1[3];
+      childBox(left[p], leafLo, leafHi, nodeLo, nodeHi, l0, h0);
+      childBox(right[p], leafLo, leafHi, nodeLo, nodeHi, l1, h1);
+      for (int a = 0; a < 3; a++) {
+        nodeLo[3 * size_t(p) + a] = fmin(l0[a], l1[a]);
+        nodeHi[3 * size_t(p) + a] = fmax(h0[a], h1[a]);
+      }
+      __threadfence();
+      if (p == 0) {
+        break;
+      }
+      p = parentI[p];
+    }
+  }
+}
+
+struct TreeView
+{
+  int64_t         n; // triangles (leaves of the binary tree)
+  const uint32_t* left;
+  const uint32_t* right;
+  const uint32_t* first;
+  const uint32_t* last;
+  const double*   nodeLo;
+  const double*   nodeHi;
+  const double*   leafLo;
+  const double*   leafHi;
+};
+
+__device__ __forceinline__ uint32_t refCount(const TreeView& t, uint32_t ref)
+{
+  return (ref & EBG_LEAF_BIT) ? 1u : t.last[ref] - t.first[ref] + 1u;
+}
+__device__ __forceinline__ double refArea(const TreeView& t, uint32_t ref)
+{
+  double lo[3], hi[3];
+  childBox(ref, t.leafLo, t.leafHi, t.nodeLo, t.nodeHi, lo, hi);
+  const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+  return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
+
+__device__ __forceinline__ float rdown(double x) { return __double2float_rd(x); }
+__device__ __forceinline__ float rup(double x) { return __double2float_ru(x); }
+
+// 4. one level of the 4-wide tree: frontier[i] = (binary ref, node index)
+__global__ void kCollapse(const TreeView t, const uint2* __restrict__ frontier, uint32_t count, int leafSize,
+                          EbgNode4* __restrict__ nodes, uint2* __restrict__ next, uint32_t* __restrict__ counters,
+                          uint32_t* __restrict__ leafFirst, uint32_t* __restrict__ leafCount,
+                          uint32_t* __restrict__ nodeFirst, uint32_t* __restrict__ nodeEnd,
+                          uint32_t* __restrict__ nodeParent, uint32_t maxNodes, uint32_t maxLeaves, int* overflow)
+{
+  // counters: [0] nodes emitted so far, [1] leaves, [2] next frontier size
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
+    const uint2 fr   = frontier[w];
+    uint32_t    m[4] = {fr.x, NONE, NONE, NONE};
+    int         nc   = 1;
+    while (nc < 4) {
+      int    pick = -1;
+      double best = -1.0;
+      for (int i = 0; i < nc; i++) {
+        if (!(m[i] & EBG_LEAF_BIT) && refCount(t, m[i]) > uint32_t(leafSize)) {
+          const double ar = refArea(t, m[i]);
+          if (pick < 0 || ar > best) {
+            pick = i;
+            best = ar;
+          }
+        }
+      }
+      if (pick < 0) {
+        break;
+      }
+      const uint32_t b = m[pick];
+      m[pick]          = t.left[b];
+      m[nc++]          = t.right[b];
+    }
+    bool bad = false;
+    for (int i = 0; i < nc; i++) {
+      bad = bad || !validRef(m[i], t.n);
+    }
+    if (bad || fr.y >= maxNodes) {
+      atomicOr(overflow, 16);
+      continue;
+    }
+    EbgNode4& nd = nodes[fr.y];
+    for (int k = 0; k < 4; k++) {
+      if (k >= nc) {
+        nd.lox[k] = nd.loy[k] = nd.loz[k] = __int_as_float(0x7f800000);
+        nd.hix[k] = nd.hiy[k] = nd.hiz[k] = -__int_as_float(0x7f800000);
+        nd.child[k] = 0;
+        nd.count[k] = 0;
+        continue;
+      }
+      double lo[3], hi[3];
+      childBox(m[k], t.leafLo, t.leafHi, t.nodeLo, t.nodeHi, lo, hi);
+      nd.lox[k]            = rdown(lo[0]);
+      nd.loy[k]            = rdown(lo[1]);
+      nd.loz[k]            = rdown(lo[2]);
+      nd.hix[k]            = rup(hi[0]);
+      nd.hiy[k]            = rup(hi[1]);
+      nd.hiz[k]            = rup(hi[2]);
+      const uint32_t cnt   = refCount(t, m[k]);
+      const uint32_t first = (m[k] & EBG_LEAF_BIT) ? (m[k] & ~EBG_LEAF_BIT) : t.first[m[k]];
+      if (cnt <= uint32_t(leafSize)) {
+        const uint32_t id = atomicAdd(counters + 1, 1u);
+        if (id >= maxLeaves) {
+          atomicOr(overflow, 1);
+          nd.child[k] = 0;
+          nd.count[k] = 0;
+          continue;
+        }
+        nd.child[k]   = EBG_LEAF_BIT | first;
+        nd.count[k]   = cnt | (id << EBG_COUNT_BITS);
+        leafFirst[id] = first;
+        leafCount[id] = cnt;
+      }
+      else {
+        const uint32_t id = atomicAdd(counters + 0, 1u);
+        if (id >= maxNodes) {
+          atomicOr(overflow, 2);
+          nd.child[k] = 0;
+          nd.count[k] = 0;
+          continue;
+        }
+        nd.child[k]    = id;
+        nd.count[k]    = 0;
+        nodeFirst[id]  = first;
+        nodeEnd[id]    = first + cnt;
+        nodeParent[id] = fr.y * 4u + uint32_t(k);
+        const uint32_t q = atomicAdd(counters + 2, 1u);
+        next[q]          = make_uint2(m[k], id);
+      }
+    }
+  }
+}
+
+// 5a. leaf-ordered records
+__global__ void kRecords(const double* __restrict__ V, const int32_t* __restrict__ F,
+                         const double* __restrict__ triN, const double* __restrict__ cornerVN,
+                         const double* __restrict__ edgeN, const uint32_t* __restrict__ ids, int64_t nt,
+                         EbgTriHot* __restrict__ hot, EbgTriSign* __restrict__ sign, double* __restrict__ tri64,
+                         int32_t* __restrict__ triId, double* __restrict__ dcelN, double* __restrict__ area)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nt; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t f = ids[i];
+    triId[i]        = int32_t(f);
+    const double* a = V + 3 * int64_t(F[3 * f]);
+    const double* b = V + 3 * int64_t(F[3 * f + 1]);
+    const double* c = V + 3 * int64_t(F[3 * f + 2]);
+    const double  ab[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+    const double  ac[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    EbgTriHot     h;
+    h.v0x  = float(a[0]);
+    h.v0y  = float(a[1]);
+    h.v0z  = float(a[2]);
+    h.abx  = float(ab[0]);
+    h.aby  = float(ab[1]);
+    h.abz  = float(ab[2]);
+    h.acx  = float(ac[0]);
+    h.acy  = float(ac[1]);
+    h.acz  = float(ac[2]);
+    h.ab2  = float(__dadd_rn(__dadd_rn(__dmul_rn(ab[0], ab[0]), __dmul_rn(ab[1], ab[1])), __dmul_rn(ab[2], ab[2])));
+    h.abac = float(__dadd_rn(__dadd_rn(__dmul_rn(ab[0], ac[0]), __dmul_rn(ab[1], ac[1])), __dmul_rn(ab[2], ac[2])));
+    h.ac2  = float(__dadd_rn(__dadd_rn(__dmul_rn(ac[0], ac[0]), __dmul_rn(ac[1], ac[1])), __dmul_rn(ac[2], ac[2])));
+    hot[i] = h;
+    EbgTriSign s;
+    s.nx   = float(triN[3 * f]);
+    s.ny   = float(triN[3 * f + 1]);
+    s.nz   = float(triN[3 * f + 2]);
+    s.pad0 = s.pad1 = s.pad2 = 0.f;
+    for (int k = 0; k < 9; k++) {
+      s.vn[k] = float(cornerVN[9 * f + k]);
+      s.en[k] = float(edgeN[9 * f + k]);
+    }
+    sign[i]   = s;
+    double* t = tri64 + 30 * i;
+    for (int k = 0; k < 3; k++) {
+      t[k]     = a[k];
+      t[3 + k] = b[k];
+      t[6 + k] = c[k];
+      t[9 + k] = triN[3 * f + k];
+    }
+    for (int k = 0; k < 9; k++) {
+      t[12 + k] = cornerVN[9 * f + k];
+      t[21 + k] = edgeN[9 * f + k];
+    }
+    // the DCEL face normal: the Triangle normal normalised again (multiply by the reciprocal)
+    const double* tn = triN + 3 * f;
+    const double  is = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(tn[0], tn[0]), __dmul_rn(tn[1], tn[1])),
+                                                           __dmul_rn(tn[2], tn[2]))));
+    for (int k = 0; k < 3; k++) {
+      dcelN[3 * i + k] = __dmul_rn(is, tn[k]);
+    }
+    const double cx = ab[1] * ac[2] - ab[2] * ac[1], cy = ab[2] * ac[0] - ab[0] * ac[2],
+                 cz = ab[0] * ac[1] - ab[1] * ac[0];
+    area[i] = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+  }
+}
+
+// 5b. oriented box of the triangles at sorted positions [first, end): one block per range.  The
+// same construction as the host build (area-weighted mean normal, in-plane principal axis, padded
+// extents) in FP64 block reductions.
+__device__ double blockSum(double v, double* red)
+{
+  for (int off = 16; off > 0; off >>= 1) {
+    v += __shfl_xor_sync(FULL, v, off);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < int(blockDim.x >> 5); w++) {
+    s += red[w];
+  }
+  return s;
+}
+__device__ double blockMin(double v, double* red)
+{
+  for (int off = 16; off > 0; off >>= 1) {
+    v = fmin(v, __shfl_xor_sync(FULL, v, off));
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  double s = DBL_MAX;
+  for (int w = 0; w < int(blockDim.x >> 5); w++) {
+    s = fmin(s, red[w]);
+  }
+  return s;
+}
+__device__ double blockMax(double v, double* red) { return -blockMin(-v, red); }
+
+__global__ void __launch_bounds__(128) kRangeObbs(const double* __restrict__ tri64, const uint32_t* __restrict__ rFirst,
+                                                  const uint32_t* __restrict__ rEnd, const uint32_t* __restrict__ rCount,
+                                                  int64_t numRanges, double pad, EbgObb* __restrict__ out,
+                                                  uint8_t* __restrict__ useful)
+{
+  __shared__ double red[4];
+  for (int64_t r = blockIdx.x; r < numRanges; r += gridDim.x) {
+    const uint32_t b = rFirst[r];
+    const uint32_t e = rEnd ? rEnd[r] : b + rCount[r];
+    // pass 1: normal sum, area, AABB
+    double n[3] = {0, 0, 0}, area = 0, lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const double* t  = tri64 + 30 * size_t(i);
+      const double  e1[3] = {t[3] - t[0], t[4] - t[1], t[5] - t[2]};
+      const double  e2[3] = {t[6] - t[0], t[7] - t[1], t[8] - t[2]};
+      const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      for (int a = 0; a < 3; a++) {
+        n[a] += cr[a];
+        for (int c = 0; c < 3; c++) {
+          lo[a] = fmin(lo[a], t[3 * c + a]);
+          hi[a] = fmax(hi[a], t[3 * c + a]);
+        }
+      }
+      area += sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    }
+    for (int a = 0; a < 3; a++) {
+      n[a]  = blockSum(n[a], red);
+      lo[a] = blockMin(lo[a], red);
+      hi[a] = blockMax(hi[a], red);
+    }
+    area      = blockSum(area, red);
+    double ln = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    if (!(ln > 0.5 * area) || !(ln > 0)) {
+      int ax = 0;
+      for (int a = 1; a < 3; a++) {
+        if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
+          ax = a;
+        }
+      }
+      n[0] = n[1] = n[2] = 0;
+      n[ax]              = 1;
+      ln                 = 1;
+    }
+    for (int a = 0; a < 3; a++) {
+      n[a] /= ln;
+    }
+    double t1[3];
+    if (fabs(n[0]) < 0.9) {
+      t1[0] = 0;
+      t1[1] = n[2];
+      t1[2] = -n[1];
+    }
+    else {
+      t1[0] = -n[2];
+      t1[1] = 0;
+      t1[2] = n[0];
+    }
+    const double l1 = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    for (int a = 0; a < 3; a++) {
+      t1[a] /= l1;
+    }
+    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
+    // pass 2: in-plane mean and covariance of the vertices (about the first vertex, for accuracy)
+    const double* t0  = tri64 + 30 * size_t(b);
+    const double  ox = t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2], oy = t0[0] * t2[0] + t0[1] * t2[1] + t0[2] * t2[2];
+    double        sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const double* t = tri64 + 30 * size_t(i);
+      for (int c = 0; c < 3; c++) {
+        const double* p = t + 3 * c;
+        const double  x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - ox;
+        const double  y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - oy;
+        sx += x;
+        sy += y;
+        sxx += x * x;
+        syy += y * y;
+        sxy += x * y;
+      }
+    }
+    sx              = blockSum(sx, red);
+    sy              = blockSum(sy, red);
+    sxx             = blockSum(sxx, red);
+    syy             = blockSum(syy, red);
+    sxy             = blockSum(sxy, red);
+    const double cn = 3.0 * double(e - b);
+    const double mx = sx / cn, my = sy / cn;
+    const double cxx = sxx / cn - mx * mx, cyy = syy / cn - my * my, cxy = sxy / cn - mx * my;
+    const double th  = 0.5 * atan2(2 * cxy, cxx - cyy);
+    const double u[3] = {cos(th) * t1[0] + sin(th) * t2[0], cos(th) * t1[1] + sin(th) * t2[1],
+                         cos(th) * t1[2] + sin(th) * t2[2]};
+    const double w[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2], n[0] * u[1] - n[1] * u[0]};
+    // pass 3: extents along n, u, w
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mxx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const double* t = tri64 + 30 * size_t(i);
+      for (int c = 0; c < 3; c++) {
+        const double* p     = t + 3 * c;
+        const double  pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
+                               p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
+        for (int a = 0; a < 3; a++) {
+          mn[a]  = fmin(mn[a], pr[a]);
+          mxx[a] = fmax(mxx[a], pr[a]);
+        }
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      mn[a]  = blockMin(mn[a], red);
+      mxx[a] = blockMax(mxx[a], red);
+    }
+    if (threadIdx.x == 0) {
+      EbgObb& o = out[r];
+      o.nx      = float(n[0]);
+      o.ny      = float(n[1]);
+      o.nz      = float(n[2]);
+      o.dn      = float(0.5 * (mn[0] + mxx[0]));
+      o.ux      = float(u[0]);
+      o.uy      = float(u[1]);
+      o.uz      = float(u[2]);
+      o.du      = float(0.5 * (mn[1] + mxx[1]));
+      o.vx      = float(w[0]);
+      o.vy      = float(w[1]);
+      o.vz      = float(w[2]);
+      o.dv      = float(0.5 * (mn[2] + mxx[2]));
+      o.hn      = rup(0.5 * (mxx[0] - mn[0]) + pad);
+      o.hu      = rup(0.5 * (mxx[1] - mn[1]) + pad);
+      o.hv      = rup(0.5 * (mxx[2] - mn[2]) + pad);
+      o.pad     = 0.f;
+      if (useful) {
+        const double obbVol  = 8.0 * double(o.hn) * double(o.hu) * double(o.hv);
+        const double aabbVol = (hi[0] - lo[0] + 2 * pad) * (hi[1] - lo[1] + 2 * pad) * (hi[2] - lo[2] + 2 * pad);
+        useful[r]            = (aabbVol > 0 ? obbVol / aabbVol : 1.0) <= 0.5 ? 1 : 0;
+      }
+    }
+  }
+}
+
+__global__ void kNodeObbFlags(const uint8_t* __restrict__ useful, const uint32_t* __restrict__ nodeParent,
+                              uint32_t numNodes, EbgNode4* __restrict__ nodes)
+{
+  for (uint32_t j = 1 + blockIdx.x * blockDim.x + threadIdx.x; j < numNodes; j += gridDim.x * blockDim.x) {
+    if (useful[j]) {
+      const uint32_t ps = nodeParent[j];
+      nodes[ps >> 2].count[ps & 3u] = EBG_NODE_HAS_OBB;
+    }
+  }
+}
+
+inline unsigned gridFor(int64_t n, int t, int64_t cap = 1 << 20)
+{
+  int64_t g = (n + t - 1) / t;
+  g         = g < cap ? g : cap;
+  return unsigned(g < 1 ? 1 : g);
+}
+
+} // namespace
+
+ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int leafSize,
+                             double* outLo, double* outHi, cudaStream_t s)
+{
+  const int64_t n = nt;
+  std::vector<void*> tmp;
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMallocAsync(p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+      return false;
+    }
+    tmp.push_back(*p);
+    return true;
+  };
+  auto freeTmp = [&]() {
+    for (void* p : tmp) {
+      cudaFreeAsync(p, s);
+    }
+    tmp.clear();
+  };
+  struct Guard
+  {
+    std::function<void()> f;
+    ~Guard() { f(); }
+  } guard{freeTmp};
+
+  double *dV = nullptr, *dTriN = nullptr, *dVN = nullptr, *dEN = nullptr, *triLo = nullptr, *triHi = nullptr,
+         *cen = nullptr, *leafLo = nullptr, *leafHi = nullptr, *nodeLo = nullptr, *nodeHi = nullptr, *area = nullptr;
+  int32_t*            dF     = nullptr;
+  unsigned long long* bounds = nullptr;
+  uint64_t *          codesIn = nullptr, *codesOut = nullptr;
+  uint32_t *idsIn = nullptr, *ids = nullptr, *left = nullptr, *right = nullptr, *first = nullptr, *last = nullptr,
+           *parentI = nullptr, *parentL = nullptr, *arrivals = nullptr, *counters = nullptr, *leafFirst = nullptr,
+           *leafCount = nullptr, *nodeFirst = nullptr, *nodeEnd = nullptr, *nodeParent = nullptr;
+  uint2*   frontier[2] = {nullptr, nullptr};
+  uint8_t* useful      = nullptr;
+  int*     overflow    = nullptr;
+  const size_t N = size_t(n), NI = size_t(std::max<int64_t>(n - 1, 1));
+  bool ok = alloc((void**)&dV, 24 * size_t(nv)) && alloc((void**)&dF, 12 * N) && alloc((void**)&dTriN, 24 * N) &&
+            alloc((void**)&dVN, 72 * N) && alloc((void**)&dEN, 72 * N) && alloc((void**)&triLo, 24 * N) &&
+            alloc((void**)&triHi, 24 * N) && alloc((void**)&cen, 24 * N) && alloc((void**)&leafLo, 24 * N) &&
+            alloc((void**)&leafHi, 24 * N) && alloc((void**)&nodeLo, 24 * NI) && alloc((void**)&nodeHi, 24 * NI) &&
+            alloc((void**)&area, 8 * N) && alloc((void**)&bounds, 12 * 8) && alloc((void**)&codesIn, 8 * N) &&
+            alloc((void**)&codesOut, 8 * N) && alloc((void**)&idsIn, 4 * N) && alloc((void**)&ids, 4 * N) &&
+            alloc((void**)&left, 4 * NI) && alloc((void**)&right, 4 * NI) && alloc((void**)&first, 4 * NI) &&
+            alloc((void**)&last, 4 * NI) && alloc((void**)&parentI, 4 * NI) && alloc((void**)&parentL, 4 * N) &&
+            alloc((void**)&arrivals, 4 * NI) && alloc((void**)&counters, 16) && alloc((void**)&leafFirst, 4 * N) &&
+            alloc((void**)&leafCount, 4 * N) && alloc((void**)&nodeFirst, 4 * N) && alloc((void**)&nodeEnd, 4 * N) &&
+            alloc((void**)&nodeParent, 4 * N) && alloc((void**)&frontier[0], 8 * N) &&
+            alloc((void**)&frontier[1], 8 * N) && alloc((void**)&useful, N) && alloc((void**)&overflow, 4);
+  if (!ok) {
+    return setError(EBG_ERR_NO_MEMORY, "device build workspace");
+  }
+  cudaMemcpyAsync(dV, V, 24 * size_t(nv), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dF, F, 12 * N, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dTriN, m->triN.data(), 24 * N, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dVN, m->cornerVN.data(), 72 * N, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(dEN, m->edgeN.data(), 72 * N, cudaMemcpyHostToDevice, s);
+  {
+    unsigned long long init[12];
+    for (int j = 0; j < 12; j++) {
+      const bool isMin = (j < 3) || (j >= 6 && j < 9);
+      init[j]          = isMin ? ~0ull : 0ull;
+    }
+    cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  }
+  cudaMemsetAsync(arrivals, 0, 4 * NI, s);
+  cudaMemsetAsync(parentI, 0xff, 4 * NI, s);
+  cudaMemsetAsync(left, 0xff, 4 * NI, s);
+  cudaMemsetAsync(right, 0xff, 4 * NI, s);
+  cudaMemsetAsync(parentL, 0xff, 4 * N, s);
+  cudaMemsetAsync(counters, 0, 16, s);
+  cudaMemsetAsync(overflow, 0, 4, s);
+  cudaMemsetAsync(useful, 0, N, s);
+
+  // 1. boxes, bounds, codes, sort
+  kTriBounds<<<gridFor(n, 256, 8192), 256, 0, s>>>(dV, dF, n, triLo, triHi, cen, bounds);
+  kTriMorton<<<gridFor(n, 256), 256, 0, s>>>(cen, n, bounds, codesIn, idsIn);
+  size_t sortBytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, codesIn, codesOut, idsIn, ids, int(n), 0, 63, s);
+  void* sortTemp = nullptr;
+  if (!alloc(&sortTemp, sortBytes)) {
+    return setError(EBG_ERR_NO_MEMORY, "device build sort workspace");
+  }
+  if (cub::DeviceRadixSort::SortPairs(sortTemp, sortBytes, codesIn, codesOut, idsIn, ids, int(n), 0, 63, s) !=
+      cudaSuccess) {
+    return setError(EBG_ERR_CUDA, "device build sort failed");
+  }
+
+  // 2-3. binary radix tree and its boxes
+  if (n > 1) {
+    kRadixTree<<<gridFor(n - 1, 256), 256, 0, s>>>(codesOut, n, left, right, first, last, parentI, parentL, overflow);
+  }
+  kRefit<<<gridFor(n, 256), 256, 0, s>>>(n, ids, triLo, triHi, leafLo, leafHi, left, right, parentI, parentL, nodeLo,
+                                         nodeHi, arrivals, overflow);
+
+  // root box (the whole mesh)
+  unsigned long long hb[12];
+  cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("device build: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  for (int a = 0; a < 3; a++) {
+    outLo[a] = hostDval(hb[6 + a]);
+    outHi[a] = hostDval(hb[9 + a]);
+  }
+  {
+    int ov = 0;
+    cudaMemcpy(&ov, overflow, 4, cudaMemcpyDeviceToHost);
+    if (ov != 0) {
+      return setError(EBG_ERR_INVALID, "device build: inconsistent radix tree (code " + std::to_string(ov) + ")");
+    }
+  }
+
+  // 4. the 4-wide tree, level by level (node 0 = the binary root)
+  uint32_t numNodes = 0, numLeaves = 0;
+  int      depth    = 1;
+  const uint32_t maxNodes = uint32_t(std::max<int64_t>(n, 1)), maxLeaves = uint32_t(std::min<int64_t>(n, EBG_MAX_LEAVES));
+  EbgNode4*      dNodesTmp = nullptr;
+  if (!alloc((void**)&dNodesTmp, sizeof(EbgNode4) * size_t(maxNodes))) {
+    return setError(EBG_ERR_NO_MEMORY, "device build node workspace");
+  }
+  if (n > leafSize) {
+    const uint2 root = make_uint2(0u, 0u);
+    cudaMemcpyAsync(frontier[0], &root, sizeof(root), cudaMemcpyHostToDevice, s);
+    const uint32_t init[3] = {1u, 0u, 0u};
+    cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    const uint32_t nf = 0u, nl = 0u;
+    cudaMemcpyAsync(nodeFirst, &nf, 4, cudaMemcpyHostToDevice, s);
+    const uint32_t ne = uint32_t(n);
+    cudaMemcpyAsync(nodeEnd, &ne, 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(nodeParent, &nl, 4, cudaMemcpyHostToDevice, s);
+    TreeView tv{n, left, right, first, last, nodeLo, nodeHi, leafLo, leafHi};
+    uint32_t count = 1;
+    int      cur   = 0;
+    for (int level = 1; count > 0; level++) {
+      if (level > 64) {
+        return setError(EBG_ERR_INVALID, "device build: tree deeper than 64 levels");
+      }
+      cudaMemsetAsync(counters + 2, 0, 4, s);
+      kCollapse<<<gridFor(count, 128, 1 << 16), 128, 0, s>>>(tv, frontier[cur], count, leafSize, dNodesTmp,
+                                                                frontier[1 - cur], counters, leafFirst, leafCount,
+                                                                nodeFirst, nodeEnd, nodeParent, maxNodes, maxLeaves,
+                                                                overflow);
+      uint32_t hc[3];
+      cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) {
+        return setError(EBG_ERR_CUDA, std::string("device build: ") + cudaGetErrorString(cudaGetLastError()));
+      }
+      count = hc[2];
+      cur   = 1 - cur;
+      depth = level + 1;
+    }
+    uint32_t hc[2];
+    int      ov = 0;
+    cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&ov, overflow, 4, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (ov != 0) {
+      return setError(EBG_ERR_TOO_LARGE, "device build: too many nodes or leaves");
+    }
+    numNodes  = hc[0];
+    numLeaves = hc[1];
+  }
+  else {
+    numLeaves = 1;
+    const uint32_t lf = 0u, lc = uint32_t(n);
+    cudaMemcpyAsync(leafFirst, &lf, 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(leafCount, &lc, 4, cudaMemcpyHostToDevice, s);
+  }
+  if (3 * depth + 4 > EBG_STACK_DEPTH) {
+    return setError(EBG_ERR_INVALID, "BVH too deep for the traversal stack (depth " + std::to_string(depth) + ")");
+  }
+
+  // 5. the mesh's device arrays: nodes, records, oriented boxes
+  auto keep = [&](void** p, size_t bytes) { return cudaMalloc(p, std::max<size_t>(bytes, 16)) == cudaSuccess; };
+  if (!keep(&m->dNodes, sizeof(EbgNode4) * std::max<size_t>(numNodes, 1)) || !keep(&m->dHot, sizeof(EbgTriHot) * N) ||
+      !keep(&m->dSign, sizeof(EbgTriSign) * N) || !keep(&m->dTri64, 240 * N) || !keep(&m->dTriId, 4 * N) ||
+      !keep(&m->dObb, sizeof(EbgObb) * numLeaves) || !keep(&m->dNodeObb, sizeof(EbgObb) * std::max<size_t>(numNodes, 1)) ||
+      !keep(&m->dDcelN, 24 * N)) {
+    cudaGetLastError();
+    return setError(EBG_ERR_NO_MEMORY, "device allocation for the mesh");
+  }
+  kRecords<<<gridFor(n, 256), 256, 0, s>>>(dV, dF, dTriN, dVN, dEN, ids, n, static_cast<EbgTriHot*>(m->dHot),
+                                           static_cast<EbgTriSign*>(m->dSign), static_cast<double*>(m->dTri64),
+                                           static_cast<int32_t*>(m->dTriId), static_cast<double*>(m->dDcelN), area);
+  double scale = 0;
+  for (int a = 0; a < 3; a++) {
+    scale = std::max(scale, std::max(std::fabs(outLo[a]), std::fabs(outHi[a])));
+  }
+  const double pad = 2e-6 * std::max(scale, 1e-30);
+  kRangeObbs<<<gridFor(numLeaves, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), leafFirst, nullptr,
+                                                            leafCount, numLeaves, pad,
+                                                            static_cast<EbgObb*>(m->dObb), nullptr);
+  if (numNodes > 0) {
+    kRangeObbs<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), nodeFirst, nodeEnd,
+                                                             nullptr, numNodes, pad,
+                                                             static_cast<EbgObb*>(m->dNodeObb), useful);
+    kNodeObbFlags<<<gridFor(numNodes, 256), 256, 0, s>>>(useful, nodeParent, numNodes, dNodesTmp);
+    cudaMemcpyAsync(m->dNodes, dNodesTmp, sizeof(EbgNode4) * size_t(numNodes), cudaMemcpyDeviceToDevice, s);
+  }
+  // the cumulative area table stays on the host (the seed trainer's band sampler reads it)
+  m->areaCdf.resize(N);
+  cudaMemcpyAsync(m->areaCdf.data(), area, 8 * N, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("device build: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  for (size_t i = 1; i < N; i++) {
+    m->areaCdf[i] += m->areaCdf[i - 1];
+  }
+  m->info.num_nodes  = numNodes;
+  m->info.num_leaves = numLeaves;
+  m->info.depth      = depth;
+  m->view.root_ref   = n > leafSize ? 0u : (EBG_LEAF_BIT | 0u);
+  m->view.root_count = n > leafSize ? 0u : uint32_t(n);
+  return EBG_OK;
+}
+
+} // namespace ebg

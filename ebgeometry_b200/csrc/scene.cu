@@ -158,9 +158,15 @@ int sceneOuterDepth() { return OUTER_DEPTH; }
 
 cudaError_t launchSceneValue(const SceneQueryArgs& a, int numSms, cudaStream_t s)
 {
-  int perSm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kSceneValue, 128, 0);
-  perSm              = perSm < 1 ? 1 : perSm;
+  // resident blocks per SM, looked up once (the query then issues only stream-ordered work and can
+  // be captured in a CUDA graph)
+  static int cached = 0;
+  int        perSm  = cached;
+  if (perSm == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kSceneValue, 128, 0);
+    perSm  = perSm < 1 ? 1 : perSm;
+    cached = perSm;
+  }
   const int64_t need = ((int64_t(a.n) + 31) / 32 + 3) / 4;
   int64_t       grid = int64_t(numSms) * perSm;
   grid               = grid < need ? grid : need;

@@ -48,12 +48,16 @@ typedef enum ebg_build
   EBG_BUILD_MORTON = 1  /* bottom-up along a Morton curve (bottomUpSortAndPartition, BVHImplem.hpp:207-312) */
 } ebg_build;
 
+/* ebg_build_opts.flags */
+#define EBG_BUILD_ON_DEVICE 1 /* meshes, Morton build: build the tree, records and boxes on the GPU
+                                 (the pseudonormals stay on the host, bit-identical to the DCEL) */
+
 typedef struct ebg_build_opts
 {
   int32_t build;     /* ebg_build */
   int32_t leaf_size; /* max primitives per leaf (the reference's maxLeafGroups * W); 0 = default 8 */
   int32_t device;    /* CUDA device ordinal; -1 = current device */
-  int32_t reserved;
+  int32_t flags;     /* EBG_BUILD_* flags */
 } ebg_build_opts;
 
 typedef struct ebg_mesh  ebg_mesh;

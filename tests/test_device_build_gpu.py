@@ -1,0 +1,81 @@
+"""The device (GPU) build of the Morton tree, records and oriented boxes: a mesh built on the GPU
+answers exactly as the host-built one -- same leaf order (the same Morton sort), so the same
+distances and closest triangles bit for bit -- and matches the reference."""
+import time
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from ebgeometry_b200 import EbgError, MeshSDF, TriMeshSDF
+from ebgeometry_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def query(m, p, **kw):
+    pd = torch.from_numpy(np.ascontiguousarray(p)).cuda()
+    tri = torch.empty(pd.shape[0], dtype=torch.int32, device="cuda")
+    d, tri = m.signed_distance(pd, closest_tri=tri, **kw)
+    torch.cuda.synchronize()
+    m.check_status()
+    return d.cpu().numpy(), tri.cpu().numpy()
+
+
+@pytest.mark.parametrize("level,leaf", [(3, 8), (5, 8), (5, 1), (5, 32)])
+def test_device_build_equals_host_build(level, leaf):
+    v, f = W.displaced_icosphere(level, 3)
+    p = np.concatenate([W.uniform_points(100000, 4), W.band_points(v, f, 30000, 5)])
+    host = TriMeshSDF(v, f, build="Morton", leaf_size=leaf)
+    dev = TriMeshSDF(v, f, build="Morton", leaf_size=leaf, on_device=True)
+    assert dev.info["num_triangles"] == f.shape[0]
+    assert dev.info["leaf_size"] == leaf and dev.info["depth"] >= 2
+    np.testing.assert_array_equal(dev.info["lo"], host.info["lo"])
+    np.testing.assert_array_equal(dev.info["hi"], host.info["hi"])
+    dh, th = query(host, p)
+    dd, td = query(dev, p)
+    assert np.array_equal(dh, dd)
+    assert np.array_equal(th, td)
+    # the FP64 path and the DCEL faces too
+    p64 = p[:20000].astype(np.float64)
+    assert np.array_equal(host.signed_distance(p64), dev.signed_distance(p64))
+
+
+def test_device_build_against_reference():
+    v, f = W.displaced_icosphere(4, 8)
+    p = W.uniform_points(50000, 9).astype(np.float64)
+    m = TriMeshSDF(v, f, build="Morton", on_device=True)
+    d_ref = oracle.ref().mesh(v, f, kind=0, build=1).sdf(p)
+    d = m.signed_distance(p)
+    assert np.max(np.abs(d - d_ref)) <= 1e-12 * m.diagonal
+    ms = MeshSDF(v, f, build="Morton", on_device=True)
+    d_dcel = oracle.ref().mesh(v, f, kind=3, build=1).sdf(p, dcel=True)
+    assert np.max(np.abs(ms.signed_distance(p) - d_dcel)) <= 1e-12 * ms.diagonal
+
+
+def test_device_build_small_and_errors():
+    tv = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1.0]])
+    tf = np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]])
+    p = W.uniform_points(2000, 10, -2, 2)
+    for leaf in (8, 1, 2):
+        host = TriMeshSDF(tv, tf, build="Morton", leaf_size=leaf)
+        dev = TriMeshSDF(tv, tf, build="Morton", leaf_size=leaf, on_device=True)
+        assert np.array_equal(query(host, p)[0], query(dev, p)[0]), leaf
+    with pytest.raises(EbgError):
+        TriMeshSDF(tv, tf, build="SAH", on_device=True)
+
+
+def test_level8_device_build_time():
+    """The level-8 mesh (1,310,720 triangles) built both ways; reported, and equal on a sample."""
+    v, f = W.displaced_icosphere(8, 1)
+    t0 = time.time()
+    host = TriMeshSDF(v, f, build="Morton")
+    t1 = time.time()
+    dev = TriMeshSDF(v, f, build="Morton", on_device=True)
+    t2 = time.time()
+    print(f"level-8 build: host {t1 - t0:.3f} s, device {t2 - t1:.3f} s; "
+          f"nodes {host.info['num_nodes']} / {dev.info['num_nodes']}, leaves {host.info['num_leaves']} / "
+          f"{dev.info['num_leaves']}, depth {host.info['depth']} / {dev.info['depth']}")
+    p = np.concatenate([W.grid_points(64, -1.25, 1.25), W.band_points(v, f, 100000, 11)])
+    assert np.array_equal(query(host, p)[0], query(dev, p)[0])

@@ -80,3 +80,31 @@ def test_scene_errors():
     v, f = W.displaced_icosphere(1, 1)
     with pytest.raises(EbgError):
         BVHUnion(None, [TriMeshSDF(v, f)], np.array([[10.0, 3, 0, 0, 0]]))
+
+
+def test_batched_union_in_a_cuda_graph():
+    """Many query batches of uneven length go in as one concatenated array, one persistent launch;
+    the call issues only stream-ordered work, so it is captured once and replayed."""
+    sc = W.csg_scene(7, n_spheres=200, n_meshes=8, levels=(1, 3), mesh_radius=(0.05, 0.2))
+    tms = [TriMeshSDF(v, f) for v, f in sc["meshes"]]
+    u = BVHUnion(sc["spheres"], tms, sc["poses"])
+    rng = np.random.default_rng(8)
+    lens = np.exp(rng.uniform(np.log(100), np.log(20000), size=40)).astype(int)
+    p = np.concatenate([W.uniform_points(int(k), 100 + i, -1.2, 1.2) for i, k in enumerate(lens)])
+    ref = u.values(torch.from_numpy(p).cuda()).cpu().numpy()
+    pd = torch.from_numpy(p).cuda()
+    out = torch.empty(p.shape[0], device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            u.values(pd, out=out, stream=s)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        u.values(pd, out=out, stream=s)
+    out.zero_()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), ref)
