@@ -23,7 +23,7 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH",
+__all__ = ["read_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH",
            "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
@@ -36,6 +36,22 @@ def version() -> str:
 
 def device_count() -> int:
     return int(lib.ebg_device_count())
+
+
+def read_soup(path):
+    """(vertices (V,3) float64, triangles (T,3) int32) of a mesh file (.stl, .obj, .ply, .vtk) read
+    and merged the way the reference's parser does (host only, no device needed)."""
+    h = C.c_void_p()
+    check(lib.ebg_soup_read(str(path).encode(), C.byref(h)))
+    try:
+        nv, nt = C.c_int64(), C.c_int64()
+        check(lib.ebg_soup_sizes(h, C.byref(nv), C.byref(nt)))
+        v = np.empty((nv.value, 3), np.float64)
+        f = np.empty((nt.value, 3), np.int32)
+        check(lib.ebg_soup_copy(h, _ptr(v), _ptr(f)))
+    finally:
+        lib.ebg_soup_destroy(h)
+    return v, f
 
 
 def _stream_ptr(stream):
@@ -84,6 +100,12 @@ class TriMeshSDF:
         check(lib.ebg_mesh_get_info(self._h, C.byref(inf)))
         self.info = {k: (list(getattr(inf, k)) if k in ("lo", "hi") else getattr(inf, k))
                      for k, _ in _capi.MeshInfo._fields_}
+
+    @classmethod
+    def from_file(cls, path, **kw):
+        """Parser::readIntoTriangleBVH: the mesh of a .stl / .obj / .ply / .vtk file."""
+        v, f = read_soup(path)
+        return cls(v, f, **kw)
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -80,6 +80,11 @@ SIGNATURES = {
     "ebg_mesh_get_info": (C.c_int, [_P, C.POINTER(MeshInfo)]),
     "ebg_mesh_get_normals": (C.c_int, [_P, _P, _P, _P]),
     "ebg_mesh_signed_distance": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
+    "ebg_soup_read": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+    "ebg_soup_sizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64)]),
+    "ebg_soup_copy": (C.c_int, [_P, _P, _P]),
+    "ebg_soup_destroy": (C.c_int, [_P]),
+    "ebg_mesh_create_from_file": (C.c_int, [C.c_char_p, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_mesh_signed_distance_host": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_mesh_signed_distance_noalloc": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_mesh_signed_distance_f64": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),

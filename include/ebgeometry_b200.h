@@ -60,6 +60,7 @@ typedef struct ebg_build_opts
   int32_t flags;     /* EBG_BUILD_* flags */
 } ebg_build_opts;
 
+typedef struct ebg_soup  ebg_soup;
 typedef struct ebg_mesh  ebg_mesh;
 typedef struct ebg_cloud ebg_cloud;
 typedef struct ebg_scene ebg_scene;
@@ -177,6 +178,20 @@ ebg_status ebg_compute_pseudonormals(const double*  vertices,
                                      double*        edge_normals);
 
 ebg_status ebg_mesh_destroy(ebg_mesh* mesh);
+
+/* Mesh files (host only, no device needed): the reading half of Parser::readIntoDCEL
+ * (ParserImplem.hpp:1752-1800) for .stl (ASCII or binary), .obj, .ply (ascii or binary, either byte
+ * order) and legacy ASCII .vtk POLYDATA, with the reference's rules for which triangles a file
+ * yields, then its vertex merging (Soup::compress, SoupImplem.hpp:78-145: equal positions become
+ * one vertex, vertices in lexicographic order, facets in file order).  Only triangle faces are
+ * accepted.  ebg_soup_sizes / ebg_soup_copy hand the soup out (vertices 3 doubles, triangles 3
+ * int32 per entry). */
+ebg_status ebg_soup_read(const char* path, ebg_soup** soup);
+ebg_status ebg_soup_sizes(const ebg_soup* soup, int64_t* num_vertices, int64_t* num_triangles);
+ebg_status ebg_soup_copy(const ebg_soup* soup, double* vertices, int32_t* triangles);
+ebg_status ebg_soup_destroy(ebg_soup* soup);
+/* Parser::readIntoTriangleBVH (ParserImplem.hpp:1893-1903): read + merge + ebg_mesh_create. */
+ebg_status ebg_mesh_create_from_file(const char* path, const ebg_build_opts* opts, ebg_mesh** mesh);
 ebg_status ebg_mesh_get_info(const ebg_mesh* mesh, ebg_mesh_info* info);
 
 /* Pseudonormals the handle computed (per triangle: face normal 3, vertex normals 9, edge normals 9
