@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--band-points", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--build", default="Morton")
     ap.add_argument("--leaf", type=int, default=8)
-    ap.add_argument("--device-build", action="store_true", help="build the Morton tree on the GPU")
+    ap.add_argument("--host-build", action="store_true",
+                    help="build the tree on the host (default: on the GPU for Morton builds)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -284,7 +285,8 @@ def run_ours(args, rank, world, local_rank):
     n = pts.shape[0]
     n_grid, n_band = args.grid ** 3, args.band_points
     t0 = time.time()
-    mesh = TriMeshSDF(v, f, build=args.build, leaf_size=args.leaf, device=local_rank, on_device=args.device_build)
+    on_device = args.build.upper() == "MORTON" and not args.host_build
+    mesh = TriMeshSDF(v, f, build=args.build, leaf_size=args.leaf, device=local_rank, on_device=on_device)
     t_build = time.time() - t0
     log(f"[rank {rank}] mesh {f.shape[0]} tris built in {t_build:.2f}s: {mesh.info}")
 
@@ -452,7 +454,7 @@ def run_ours(args, rank, world, local_rank):
                                f"FP64 band |d| <= 1e-4 diag",
                    "seed": ("learned pruning radius (16-level hash grid + 3x64 BF16 MLP, trained on the GPU)"
                             if seed is not None else "none (plain traversal)"),
-                   "build_on_device": bool(args.device_build),
+                   "build_on_device": bool(on_device),
                    "queries_per_step": n, "l2": "inputs larger than L2 "
                    f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
                    "plain": {"value": plain_value, "ms_per_step": ms_plain, "phase_ms_mean": phases(tms_plain),

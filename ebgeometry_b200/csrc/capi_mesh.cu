@@ -308,12 +308,14 @@ ebg_status buildMesh(const double*         V,
       }
     }
   }
-  else if (!computePseudonormals(V, nv, F, nt, m->triN, m->cornerVN, m->edgeN, msg)) {
+  const bool onDevice    = opts && (opts->flags & EBG_BUILD_ON_DEVICE);
+  const bool givenNormal = givenVN != nullptr && givenEN != nullptr;
+  if (!givenNormal && !onDevice && !computePseudonormals(V, nv, F, nt, m->triN, m->cornerVN, m->edgeN, msg)) {
     delete m;
     return setError(EBG_ERR_INVALID, msg);
   }
 
-  if (opts && (opts->flags & EBG_BUILD_ON_DEVICE)) {
+  if (onDevice) {
     if (build != EBG_BUILD_MORTON) {
       delete m;
       return setError(EBG_ERR_INVALID, "the device build makes Morton trees only");
@@ -324,7 +326,7 @@ ebg_status buildMesh(const double*         V,
       return setError(EBG_ERR_CUDA, "stream for the device build");
     }
     double           lo[3], hi[3];
-    const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, leafSize, lo, hi, bs);
+    const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, leafSize, lo, hi, bs, !givenNormal);
     cudaStreamDestroy(bs);
     if (rc != EBG_OK) {
       const std::string keep = ebg_last_error();

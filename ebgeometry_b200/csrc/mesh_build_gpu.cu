@@ -642,7 +642,7 @@ inline unsigned gridFor(int64_t n, int t, int64_t cap = 1 << 20)
 } // namespace
 
 ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int leafSize,
-                             double* outLo, double* outHi, cudaStream_t s)
+                             double* outLo, double* outHi, cudaStream_t s, bool normalsOnDevice)
 {
   const int64_t n = nt;
   std::vector<void*> tmp;
@@ -694,9 +694,24 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
   }
   cudaMemcpyAsync(dV, V, 24 * size_t(nv), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(dF, F, 12 * N, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dTriN, m->triN.data(), 24 * N, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dVN, m->cornerVN.data(), 72 * N, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(dEN, m->edgeN.data(), 72 * N, cudaMemcpyHostToDevice, s);
+  if (normalsOnDevice) {
+    const ebg_status rc = pseudonormalsOnDevice(dV, nv, dF, nt, dTriN, dVN, dEN, s);
+    if (rc != EBG_OK) {
+      return rc;
+    }
+    // the host keeps a copy (ebg_mesh_get_normals)
+    m->triN.resize(3 * N);
+    m->cornerVN.resize(9 * N);
+    m->edgeN.resize(9 * N);
+    cudaMemcpyAsync(m->triN.data(), dTriN, 24 * N, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(m->cornerVN.data(), dVN, 72 * N, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(m->edgeN.data(), dEN, 72 * N, cudaMemcpyDeviceToHost, s);
+  }
+  else {
+    cudaMemcpyAsync(dTriN, m->triN.data(), 24 * N, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dVN, m->cornerVN.data(), 72 * N, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dEN, m->edgeN.data(), 72 * N, cudaMemcpyHostToDevice, s);
+  }
   {
     unsigned long long init[12];
     for (int j = 0; j < 12; j++) {

@@ -42,6 +42,29 @@ def test_device_build_equals_host_build(level, leaf):
     assert np.array_equal(host.signed_distance(p64), dev.signed_distance(p64))
 
 
+@pytest.mark.parametrize("level", [2, 6])
+def test_device_pseudonormals_bitexact(level, golden):
+    """The device build computes the pseudonormals on the GPU (the angle weights' acos on the host):
+    bit-identical to the host restatement and so to the reference's DCEL."""
+    v, f = W.displaced_icosphere(level, 12)
+    host = TriMeshSDF(v, f, build="Morton")
+    dev = TriMeshSDF(v, f, build="Morton", on_device=True)
+    for a, b in zip(host.normals(), dev.normals()):
+        assert np.array_equal(a, b)
+    g = golden("icosphere_l2.npz")
+    fn, vn, en = TriMeshSDF(g["v"], g["f"], build="Morton", on_device=True).normals()
+    assert np.array_equal(fn, g["face_n"]) and np.array_equal(vn, g["vert_n"]) and np.array_equal(en, g["edge_n"])
+
+
+def test_device_build_rejects_bad_soups():
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [2, 0, 0]], np.float64)
+    with pytest.raises(EbgError):  # zero area
+        TriMeshSDF(v, np.array([[0, 1, 3]]), build="Morton", on_device=True)
+    v5 = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1]], np.float64)
+    with pytest.raises(EbgError):  # one edge (0,1) shared by three triangles
+        TriMeshSDF(v5, np.array([[0, 1, 2], [1, 0, 3], [0, 1, 4]]), build="Morton", on_device=True)
+
+
 def test_device_build_against_reference():
     v, f = W.displaced_icosphere(4, 8)
     p = W.uniform_points(50000, 9).astype(np.float64)
