@@ -46,9 +46,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "knn", "csg"], default="mesh",
+    ap.add_argument("--workload", choices=["mesh", "knn", "grid", "csg"], default="mesh",
                     help="mesh: the headline mesh-SDF configuration; knn: 16M-point cloud, 4M queries, k=1 and 8; "
-                         "csg: 4,096 spheres + 256 posed meshes, 2,048 query batches in one launch")
+                         "grid: the uniform-grid cloud against the BVH cloud on a uniform and a clustered 16M-point "
+                         "cloud; csg: 4,096 spheres + 256 posed meshes, 2,048 query batches in one launch")
     ap.add_argument("--knn-points", type=int, default=16 * 1024 * 1024)
     ap.add_argument("--knn-queries", type=int, default=4 * 1024 * 1024)
     ap.add_argument("--csg-batches", type=int, default=2048)
@@ -547,6 +548,75 @@ def run_knn(args, rank, world, local_rank):
     return 0
 
 
+def run_grid(args, rank, world, local_rank):
+    """PointCloudHashGrid k-NN against PointCloudBVH on the same clouds: --knn-points uniform points
+    (the grid's case) and the knn workload's clustered cloud; --knn-queries uniform queries; k = 1
+    and 8; allNearestNeighbors (k = 1, 8) of each cloud."""
+    import torch
+
+    from ebgeometry_b200 import PointCloudBVH, PointCloudHashGrid
+    from ebgeometry_b200 import workloads as W
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    q = W.uniform_points(args.knn_queries, 2, 0.0, 1.0)
+    qd = torch.from_numpy(q).to(dev)
+    out = {}
+    clouds = {"uniform": np.random.default_rng(5).random((args.knn_points, 3), dtype=np.float32),
+              "clustered": W.point_cloud(args.knn_points, 1)}
+    for name, pts in clouds.items():
+        t0 = time.time()
+        grid = PointCloudHashGrid(pts)
+        torch.cuda.synchronize(dev)
+        build_s = time.time() - t0
+        bvh = PointCloudBVH(torch.from_numpy(pts).to(dev))
+        row = {"grid_build_s": build_s, "cells": list(grid.grid_info()[0])}
+        for k in (1, 8):
+            gms = device_timed(lambda: grid.knn(qd, k), args.steps, args.warmup, torch, dev, stream)
+            bms = device_timed(lambda: bvh.knn(qd, k), args.steps, args.warmup, torch, dev, stream)
+            gi, gd = grid.knn(qd, k)
+            bi, bd = bvh.knn(qd, k)
+            same = bool(torch.equal(gi, bi) and torch.equal(gd, bd))
+            row[f"k{k}"] = {"grid_qps": q.shape[0] / (gms * 1e-3), "bvh_qps": q.shape[0] / (bms * 1e-3),
+                            "identical": same}
+            gms = device_timed(lambda: grid.all_nearest_neighbors(k, device=True), args.steps, args.warmup, torch,
+                               dev, stream)
+            bms = device_timed(lambda: bvh.all_nearest_neighbors(k, device=True), args.steps, args.warmup, torch,
+                               dev, stream)
+            gi, gd = grid.all_nearest_neighbors(k, device=True)
+            bi, bd = bvh.all_nearest_neighbors(k, device=True)
+            same = bool(torch.equal(gi, bi) and torch.equal(gd, bd))
+            row[f"self_k{k}"] = {"grid_qps": pts.shape[0] / (gms * 1e-3), "bvh_qps": pts.shape[0] / (bms * 1e-3),
+                                 "identical": same}
+        grid.check_status()
+        bvh.check_status()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            import oracle
+            if oracle.ref_available():
+                R = oracle.ref()
+                t0 = time.time()
+                rg = R.grid(pts)
+                tb = time.time() - t0
+                ns = 200000
+                sq = q[:ns]
+                for k in (1, 8):
+                    t0 = time.perf_counter()
+                    _, rd = rg.knn(sq, k)
+                    dt = time.perf_counter() - t0
+                    _, gd = grid.knn(sq, k)
+                    row[f"k{k}"]["cpu_baseline"] = {
+                        "value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
+                        "sample": f"first {ns} queries, reference PointCloudHashGrid<float> closestPoints "
+                                  f"(build {tb:.1f}s)", "d2_equal_fraction": float(np.mean(gd == rd))}
+        out[name] = row
+        del grid, bvh
+    if rank == 0:
+        print(json.dumps({"metric": "k-NN queries/s on 1 B200", "workload": "grid", "n_gpus": world,
+                          "config": {"points": args.knn_points, "queries": int(q.shape[0])}, "results": out}),
+              flush=True)
+    return 0
+
+
 def run_csg(args, rank, world, local_rank):
     """Batched CSG union: spheres + posed displaced icospheres (levels 3-7), batches of log-uniform
     length 1k-1M concatenated into one call (one persistent launch)."""
@@ -599,6 +669,8 @@ def main():
             return run_reference(args, rank, world)
         if args.workload == "knn":
             return run_knn(args, rank, world, local_rank)
+        if args.workload == "grid":
+            return run_grid(args, rank, world, local_rank)
         if args.workload == "csg":
             return run_csg(args, rank, world, local_rank)
         return run_ours(args, rank, world, local_rank)

@@ -23,8 +23,8 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["read_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH",
-           "BUILD_MORTON", "version", "device_count"]
+__all__ = ["read_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "PointCloudHashGrid",
+           "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
 BUILD_MORTON = 1
@@ -380,6 +380,105 @@ class PointCloudBVH:
 
     def check_status(self, stream=None):
         check(lib.ebg_cloud_check_status(self._h, _stream_ptr(stream)))
+
+
+class PointCloudHashGrid:
+    """k-nearest-neighbour search over a point cloud on a uniform grid (the reference's
+    PointCloudHashGrid), with PointCloudBVH's interface and results.
+
+    ``points``: (n,3) float32 numpy array (n may be 0).  ``target_per_cell`` sets the cell size as
+    the reference does: cells hold that many points at the cloud's average density.  Neighbours
+    come in increasing (squared distance, index) order -- equal distances resolve to the lowest
+    index -- so the answers equal :class:`PointCloudBVH`'s.
+    """
+
+    def __init__(self, points, target_per_cell=1.0, device=-1):
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        h = C.c_void_p()
+        check(lib.ebg_grid_create(_ptr(p) if p.size else None, p.shape[0], float(target_per_cell), int(device),
+                                  C.byref(h)))
+        self._h = h
+        self.n = p.shape[0]
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_grid_destroy(h)
+            self._h = None
+
+    def numPoints(self) -> int:
+        return int(lib.ebg_grid_size(self._h))
+
+    def grid_info(self):
+        """((cells x, y, z), cell size)."""
+        cells = (C.c_int32 * 3)()
+        h = C.c_double()
+        check(lib.ebg_grid_info(self._h, cells, C.byref(h)))
+        return tuple(cells), h.value
+
+    def knn(self, queries, k, stream=None):
+        """(idx (nq,k) int32, d2 (nq,k) float32) for (nq,3) float32 queries (CUDA tensor: asynchronous
+        on ``stream``; numpy: synchronous host call)."""
+        if isinstance(queries, np.ndarray):
+            q = np.ascontiguousarray(queries, dtype=np.float32).reshape(-1, 3)
+            idx = np.empty((q.shape[0], k), np.int32)
+            d2 = np.empty((q.shape[0], k), np.float32)
+            check(lib.ebg_grid_knn_host(self._h, _ptr(q), q.shape[0], int(k), _ptr(idx), _ptr(d2), None))
+            return idx, d2
+        import torch
+        if not (queries.is_cuda and queries.dtype == torch.float32 and queries.is_contiguous()):
+            raise ValueError("queries must be a contiguous float32 CUDA tensor of shape (n,3)")
+        nq = queries.numel() // 3
+        idx = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        d2 = torch.empty((nq, k), dtype=torch.float32, device=queries.device)
+        check(lib.ebg_grid_knn(self._h, C.c_void_p(queries.data_ptr()), nq, int(k), C.c_void_p(idx.data_ptr()),
+                               C.c_void_p(d2.data_ptr()), _stream_ptr(stream)))
+        return idx, d2
+
+    # --- the reference's single-point API (PointCloudHashGridImplem.hpp:309-333) -----------------
+    def closestPoint(self, q):
+        """(index, squared distance) of the nearest point; (-1, inf) for an empty cloud."""
+        idx, d2 = self.knn(np.asarray(q, np.float32).reshape(1, 3), 1)
+        return int(idx[0, 0]), float(d2[0, 0])
+
+    def closestPoints(self, q, k):
+        """The k nearest as a list of (index, squared distance), nearest first."""
+        idx, d2 = self.knn(np.asarray(q, np.float32).reshape(1, 3), k)
+        return [(int(i), float(d)) for i, d in zip(idx[0], d2[0]) if i >= 0]
+
+    # --- self queries (PointCloudHashGridImplem.hpp:335-385): the point itself is excluded --------
+    def all_nearest_neighbors(self, k=1, device=False, stream=None):
+        """allNearestNeighbors: (idx (n,k) int32, d2 (n,k) float32), row i = the k nearest other
+        points of cloud point i.  device=True returns CUDA tensors (asynchronous on ``stream``)."""
+        if not device:
+            idx = np.empty((self.n, k), np.int32)
+            d2 = np.empty((self.n, k), np.float32)
+            check(lib.ebg_grid_self_knn_host(self._h, int(k), _ptr(idx), _ptr(d2), None))
+            return idx, d2
+        import torch
+        idx = torch.empty((self.n, k), dtype=torch.int32, device="cuda")
+        d2 = torch.empty((self.n, k), dtype=torch.float32, device="cuda")
+        check(lib.ebg_grid_self_knn(self._h, int(k), C.c_void_p(idx.data_ptr()), C.c_void_p(d2.data_ptr()),
+                                    _stream_ptr(stream)))
+        return idx, d2
+
+    allNearestNeighbors = all_nearest_neighbors
+
+    def nearest_neighbors(self, point_ids, k=1):
+        """nearestNeighbors(point, k) for a list of cloud indices; synchronous, numpy results."""
+        ids = np.ascontiguousarray(np.asarray(point_ids, np.int64).reshape(-1))
+        idx = np.empty((ids.size, k), np.int32)
+        d2 = np.empty((ids.size, k), np.float32)
+        check(lib.ebg_grid_self_knn_points_host(self._h, _ptr(ids), ids.size, int(k), _ptr(idx), _ptr(d2), None))
+        return idx, d2
+
+    def nearestNeighbor(self, point_id):
+        """(index, squared distance) of the nearest other point of cloud point ``point_id``."""
+        idx, d2 = self.nearest_neighbors([int(point_id)], 1)
+        return int(idx[0, 0]), float(d2[0, 0])
+
+    def check_status(self, stream=None):
+        check(lib.ebg_grid_check_status(self._h, _stream_ptr(stream)))
 
 
 class SeedModel:

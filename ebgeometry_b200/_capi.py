@@ -107,7 +107,19 @@ SIGNATURES = {
     "ebg_cloud_self_knn": (C.c_int, [_P, _I32, _P, _P, _P]),
     "ebg_cloud_self_knn_points": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
     "ebg_cloud_self_knn_host": (C.c_int, [_P, _I32, _P, _P, _P]),
+    "ebg_cloud_self_knn_points_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
     "ebg_cloud_check_status": (C.c_int, [_P, _P]),
+    "ebg_grid_create": (C.c_int, [_P, _I64, C.c_double, _I32, C.POINTER(_P)]),
+    "ebg_grid_destroy": (C.c_int, [_P]),
+    "ebg_grid_size": (_I64, [_P]),
+    "ebg_grid_info": (C.c_int, [_P, _P, _P]),
+    "ebg_grid_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
+    "ebg_grid_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
+    "ebg_grid_self_knn": (C.c_int, [_P, _I32, _P, _P, _P]),
+    "ebg_grid_self_knn_host": (C.c_int, [_P, _I32, _P, _P, _P]),
+    "ebg_grid_self_knn_points": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
+    "ebg_grid_self_knn_points_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, _P]),
+    "ebg_grid_check_status": (C.c_int, [_P, _P]),
     "ebg_scene_create": (C.c_int, [_I64, _P, _I64, _P, _P, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_scene_destroy": (C.c_int, [_P]),
     "ebg_scene_num_objects": (_I64, [_P]),

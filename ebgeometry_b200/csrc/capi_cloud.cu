@@ -412,6 +412,44 @@ ebg_status ebg_cloud_self_knn_host(const ebg_cloud* c, int32_t k, int32_t* idx_h
   return rc == EBG_OK ? ebg_cloud_check_status(c, stream) : rc;
 }
 
+ebg_status ebg_cloud_self_knn_points_host(const ebg_cloud* c,
+                                          const int64_t*   point_ids_host,
+                                          int64_t          m,
+                                          int32_t          k,
+                                          int32_t*         idx_host,
+                                          float*           d2_host,
+                                          void*            stream)
+{
+  if (c == nullptr || m < 0 || k < 1 || k > 32 || (m > 0 && (!point_ids_host || !idx_host || !d2_host))) {
+    return setError(EBG_ERR_INVALID, "bad self k-NN arguments (k must be in [1, 32])");
+  }
+  if (m == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard        guard;
+  cudaSetDevice(c->device);
+  cudaStream_t       s = static_cast<cudaStream_t>(stream);
+  std::vector<void*> ws;
+  int64_t*           dp = devAlloc<int64_t>(m, s, ws);
+  int32_t*           di = devAlloc<int32_t>(m * k, s, ws);
+  float*             dd = devAlloc<float>(m * k, s, ws);
+  if (!dp || !di || !dd) {
+    freeAll(ws, s);
+    return setError(EBG_ERR_NO_MEMORY, "device buffers for the host self k-NN call");
+  }
+  cudaMemcpyAsync(dp, point_ids_host, size_t(m) * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  ebg_status rc = ebg_cloud_self_knn_points(c, dp, m, k, di, dd, stream);
+  if (rc == EBG_OK) {
+    cudaMemcpyAsync(idx_host, di, size_t(m) * k * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(d2_host, dd, size_t(m) * k * sizeof(float), cudaMemcpyDeviceToHost, s);
+  }
+  freeAll(ws, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+  }
+  return rc == EBG_OK ? ebg_cloud_check_status(c, stream) : rc;
+}
+
 ebg_status ebg_cloud_check_status(const ebg_cloud* c, void* stream)
 {
   if (c == nullptr) {

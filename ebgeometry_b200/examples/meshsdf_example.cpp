@@ -55,13 +55,24 @@ int main()
     cloud.push_back({float(std::fmod(i * 0.618034, 1.0)), float(std::fmod(i * 0.414214, 1.0)),
                      float(std::fmod(i * 0.732051, 1.0))});
   }
-  PointCloudBVH     pc(cloud);
-  const auto        hit = pc.closestPoint(cloud[123]);
+  PointCloudBVH      pc(cloud);
+  PointCloudHashGrid grid(cloud);
+  const auto         hit = pc.closestPoint(cloud[123]);
+  // the grid answers the BVH's queries identically, self queries included
+  bool       same = grid.closestPoint(cloud[123]).index == hit.index;
+  const auto nnB  = pc.allNearestNeighbors(4);
+  const auto nnG  = grid.allNearestNeighbors(4);
+  for (size_t i = 0; i < nnB.size(); i++) {
+    same = same && nnB[i].index == nnG[i].index && nnB[i].distanceSquared == nnG[i].distanceSquared;
+  }
+  PointCloudBVH::Hit one[4];
+  same = same && pc.nearestNeighbors(77, 4, one) == 4 && one[0].index == nnB[77 * 4].index &&
+         grid.nearestNeighbor(77).index == one[0].index;
   std::printf("batch/single max diff %.3g (FP64 batch: %.3g), centre %.6f (expect %.6f), nearest of point 123: "
-              "%zu (d2 %g)\n",
-              maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared));
+              "%zu (d2 %g), grid == BVH: %d\n",
+              maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared), int(same));
   const bool ok = maxDiff <= 1e-6 && maxDiff64 == 0.0 && maxDcel == 0.0 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-12 &&
-                  hit.index == 123 && hit.distanceSquared == 0.f;
+                  hit.index == 123 && hit.distanceSquared == 0.f && same;
   std::printf("%s\n", ok ? "ok" : "FAILED");
   return ok ? 0 : 1;
 }

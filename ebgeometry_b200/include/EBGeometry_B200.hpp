@@ -271,7 +271,7 @@ public:
   // returns how many neighbours were found (< k only if the cloud has fewer points).
   Hit closestPoint(const std::array<float, 3>& a_q) const
   {
-    Hit h{};
+    Hit h{0, std::numeric_limits<float>::max()};
     closestPoints(a_q, 1, &h);
     return h;
   }
@@ -294,8 +294,120 @@ public:
     check(ebg_cloud_knn_host(m_cloud, a_queriesHost, int64_t(a_n), a_k, a_idx, a_d2, nullptr, nullptr));
   }
 
+  // Self queries, the point itself excluded (PointCloudBVHImplem.hpp:455-507).  A neighbour that
+  // does not exist keeps the reference's default Hit (index 0, distanceSquared = float max).
+  Hit nearestNeighbor(size_t a_point) const
+  {
+    Hit h{0, std::numeric_limits<float>::max()};
+    nearestNeighbors(a_point, 1, &h);
+    return h;
+  }
+  size_t nearestNeighbors(size_t a_point, size_t a_k, Hit* a_out) const
+  {
+    std::vector<int32_t> idx(a_k);
+    std::vector<float>   d2(a_k);
+    const int64_t        id = int64_t(a_point);
+    check(ebg_cloud_self_knn_points_host(m_cloud, &id, 1, int32_t(a_k), idx.data(), d2.data(), nullptr));
+    return collect(idx, d2, a_out);
+  }
+  std::vector<Hit> allNearestNeighbors(size_t a_k = 1) const
+  {
+    const size_t         n = numPoints();
+    std::vector<int32_t> idx(n * a_k);
+    std::vector<float>   d2(n * a_k);
+    check(ebg_cloud_self_knn_host(m_cloud, int32_t(a_k), idx.data(), d2.data(), nullptr));
+    return rows(idx, d2);
+  }
+
+  static size_t collect(const std::vector<int32_t>& a_idx, const std::vector<float>& a_d2, Hit* a_out)
+  {
+    size_t found = 0;
+    for (size_t j = 0; j < a_idx.size(); j++) {
+      if (a_idx[j] >= 0) {
+        a_out[found++] = Hit{size_t(a_idx[j]), a_d2[j]};
+      }
+    }
+    return found;
+  }
+  static std::vector<Hit> rows(const std::vector<int32_t>& a_idx, const std::vector<float>& a_d2)
+  {
+    std::vector<Hit> out(a_idx.size(), Hit{0, std::numeric_limits<float>::max()});
+    for (size_t j = 0; j < a_idx.size(); j++) {
+      if (a_idx[j] >= 0) {
+        out[j] = Hit{size_t(a_idx[j]), a_d2[j]};
+      }
+    }
+    return out;
+  }
+
 private:
   ebg_cloud* m_cloud = nullptr;
+};
+
+// Drop-in for PointCloudHashGrid<float, size_t> (PointCloudHashGrid.hpp:54-316): a uniform grid
+// built on the device; the same queries and results as PointCloudBVH above.
+class PointCloudHashGrid
+{
+public:
+  using Hit = PointCloudBVH::Hit;
+
+  explicit PointCloudHashGrid(const std::vector<std::array<float, 3>>& a_points, double a_targetPerCell = 1.0,
+                              int a_device = -1)
+  {
+    check(ebg_grid_create(a_points.empty() ? nullptr : &a_points[0][0], int64_t(a_points.size()), a_targetPerCell,
+                          a_device, &m_grid));
+  }
+  PointCloudHashGrid(const PointCloudHashGrid&) = delete;
+  PointCloudHashGrid& operator=(const PointCloudHashGrid&) = delete;
+  ~PointCloudHashGrid() { ebg_grid_destroy(m_grid); }
+
+  size_t numPoints() const noexcept { return size_t(ebg_grid_size(m_grid)); }
+
+  // closestPoint / closestPoints (PointCloudHashGridImplem.hpp:309-333)
+  Hit closestPoint(const std::array<float, 3>& a_q) const
+  {
+    Hit h{0, std::numeric_limits<float>::max()};
+    closestPoints(a_q, 1, &h);
+    return h;
+  }
+  size_t closestPoints(const std::array<float, 3>& a_q, size_t a_k, Hit* a_out) const
+  {
+    std::vector<int32_t> idx(a_k);
+    std::vector<float>   d2(a_k);
+    check(ebg_grid_knn_host(m_grid, a_q.data(), 1, int32_t(a_k), idx.data(), d2.data(), nullptr));
+    return PointCloudBVH::collect(idx, d2, a_out);
+  }
+  void knn(const float* a_queriesHost, size_t a_n, int a_k, int32_t* a_idx, float* a_d2) const
+  {
+    check(ebg_grid_knn_host(m_grid, a_queriesHost, int64_t(a_n), a_k, a_idx, a_d2, nullptr));
+  }
+
+  // nearestNeighbor(s) / allNearestNeighbors (PointCloudHashGridImplem.hpp:335-385)
+  Hit nearestNeighbor(size_t a_point) const
+  {
+    Hit h{0, std::numeric_limits<float>::max()};
+    nearestNeighbors(a_point, 1, &h);
+    return h;
+  }
+  size_t nearestNeighbors(size_t a_point, size_t a_k, Hit* a_out) const
+  {
+    std::vector<int32_t> idx(a_k);
+    std::vector<float>   d2(a_k);
+    const int64_t        id = int64_t(a_point);
+    check(ebg_grid_self_knn_points_host(m_grid, &id, 1, int32_t(a_k), idx.data(), d2.data(), nullptr));
+    return PointCloudBVH::collect(idx, d2, a_out);
+  }
+  std::vector<Hit> allNearestNeighbors(size_t a_k = 1) const
+  {
+    const size_t         n = numPoints();
+    std::vector<int32_t> idx(n * a_k);
+    std::vector<float>   d2(n * a_k);
+    check(ebg_grid_self_knn_host(m_grid, int32_t(a_k), idx.data(), d2.data(), nullptr));
+    return PointCloudBVH::rows(idx, d2);
+  }
+
+private:
+  ebg_grid* m_grid = nullptr;
 };
 
 } // namespace B200

@@ -63,6 +63,7 @@ typedef struct ebg_build_opts
 typedef struct ebg_soup  ebg_soup;
 typedef struct ebg_mesh  ebg_mesh;
 typedef struct ebg_cloud ebg_cloud;
+typedef struct ebg_grid  ebg_grid;
 typedef struct ebg_scene ebg_scene;
 typedef struct ebg_seed  ebg_seed;
 
@@ -383,10 +384,54 @@ ebg_status ebg_cloud_self_knn_points(const ebg_cloud* cloud,
                                      int32_t*         idx_dev,
                                      float*           d2_dev,
                                      void*            stream);
+/* ebg_cloud_self_knn_points with host arrays, synchronous (reports device-side errors). */
+ebg_status ebg_cloud_self_knn_points_host(const ebg_cloud* cloud,
+                                          const int64_t*   point_ids_host,
+                                          int64_t          m,
+                                          int32_t          k,
+                                          int32_t*         idx_host,
+                                          float*           d2_host,
+                                          void*            stream);
 /* ebg_cloud_self_knn with host output arrays (n x k), synchronous. */
 ebg_status ebg_cloud_self_knn_host(const ebg_cloud* cloud, int32_t k, int32_t* idx_host, float* d2_host, void* stream);
 /* Synchronises stream and reports a device-side error of earlier k-NN calls. */
 ebg_status ebg_cloud_check_status(const ebg_cloud* cloud, void* stream);
+
+/* ---- point clouds: PointCloudHashGrid (PointCloudHashGrid.hpp:54-316) -----------------------
+ *
+ * ebg_grid_create replaces PointCloudHashGrid(positions, meta, targetPerCell)
+ * (PointCloudHashGridImplem.hpp:27-152): a dense uniform grid over the cloud's box, cell size
+ * cbrt(box volume / n * target_per_cell) (target_per_cell <= 0 means 1), coarsened until the grid
+ * has at most 64 + 8 n cells; the points are sorted into their cells on the device.  n = 0 gives an
+ * empty grid whose queries find nothing.  Non-finite coordinates are rejected (EBG_ERR_INVALID).
+ * The queries are those of PointCloudBVH with the same results: the k nearest points by the same
+ * float squared distance, in (d2, index) order -- ties to the lowest index; missing entries -1 and
+ * +inf; 1 <= k <= 32.  The reference's grid query orders equal distances by visiting order instead;
+ * its distances are the same. */
+ebg_status ebg_grid_create(const float* points_host, int64_t n, double target_per_cell, int32_t device, ebg_grid** out);
+ebg_status ebg_grid_destroy(ebg_grid* grid);
+int64_t    ebg_grid_size(const ebg_grid* grid);
+/* Cells per axis and the cell size. */
+ebg_status ebg_grid_info(const ebg_grid* grid, int32_t* cells_xyz, double* cell_size);
+/* closestPoints / closestPoint (PointCloudHashGridImplem.hpp:309-333) for a batch of points;
+ * asynchronous on stream. */
+ebg_status ebg_grid_knn(const ebg_grid* grid, const float* queries_dev, int64_t num_queries, int32_t k, int32_t* idx_dev,
+                        float* d2_dev, void* stream);
+ebg_status ebg_grid_knn_host(const ebg_grid* grid, const float* queries_host, int64_t num_queries, int32_t k,
+                             int32_t* idx_host, float* d2_host, void* stream);
+/* allNearestNeighbors(k) (PointCloudHashGridImplem.hpp:364-385): every point's k nearest OTHER
+ * points, row = cloud index; the queries run in cell order. */
+ebg_status ebg_grid_self_knn(const ebg_grid* grid, int32_t k, int32_t* idx_dev, float* d2_dev, void* stream);
+ebg_status ebg_grid_self_knn_host(const ebg_grid* grid, int32_t k, int32_t* idx_host, float* d2_host, void* stream);
+/* nearestNeighbors(point, k) / nearestNeighbor(point) (PointCloudHashGridImplem.hpp:335-362) for
+ * m cloud indices; row i answers point_ids[i].  Indices out of range give a row of -1 / +inf and
+ * are reported by the next status check as EBG_ERR_INVALID. */
+ebg_status ebg_grid_self_knn_points(const ebg_grid* grid, const int64_t* point_ids_dev, int64_t m, int32_t k,
+                                    int32_t* idx_dev, float* d2_dev, void* stream);
+ebg_status ebg_grid_self_knn_points_host(const ebg_grid* grid, const int64_t* point_ids_host, int64_t m, int32_t k,
+                                         int32_t* idx_host, float* d2_host, void* stream);
+/* Synchronises stream and reports a device-side error of earlier grid queries. */
+ebg_status ebg_grid_check_status(const ebg_grid* grid, void* stream);
 
 /* ---- CSG union: BVHUnionIF (CSG.hpp:401-468) ------------------------------------------------
  *

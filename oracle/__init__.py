@@ -78,6 +78,10 @@ class _Ref:
             "ref_cloud_knn_lex": (C.c_int, [_P, _P, _I64, C.c_int, _P, _P, C.c_int]),
             "ref_cloud_knn_lex_excl": (C.c_int, [_P, _P, _I64, C.c_int, _P, _P, C.c_int, C.c_int]),
             "ref_cloud_all_nn": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
+            "ref_grid_create": (_P, [_P, _I64, C.c_float]),
+            "ref_grid_destroy": (None, [_P]),
+            "ref_grid_knn": (C.c_int, [_P, _P, _P, _I64, C.c_int, _P, _P, C.c_int]),
+            "ref_grid_all_nn": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
             "ref_scene_create": (_P, [_I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P]),
             "ref_scene_destroy": (None, [_P]),
             "ref_scene_value": (C.c_int, [_P, _P, _I64, _P, C.c_int, C.c_int]),
@@ -193,6 +197,43 @@ class _Ref:
 
     def cloud(self, p):
         return _Ref.Cloud(self, p)
+
+    class Grid:
+        """The reference's PointCloudHashGrid<float> (its own tie order: visiting order)."""
+
+        def __init__(self, ref, p, target=1.0):
+            self.ref = ref
+            self.p = np.ascontiguousarray(p, np.float32).reshape(-1, 3)
+            self.h = ref.lib.ref_grid_create(_ptr(self.p) if self.p.size else None, self.p.shape[0], float(target))
+
+        def __del__(self):
+            if getattr(self, "h", None):
+                self.ref.lib.ref_grid_destroy(self.h)
+                self.h = None
+
+        def knn(self, q, k, threads=0):
+            q = np.ascontiguousarray(q, np.float32).reshape(-1, 3)
+            idx = np.empty((q.shape[0], k), np.int64)
+            d2 = np.empty((q.shape[0], k), np.float32)
+            assert self.ref.lib.ref_grid_knn(self.h, _ptr(q), None, q.shape[0], k, _ptr(idx), _ptr(d2), threads) == 0
+            return idx, d2
+
+        def nearest_neighbors(self, ids, k, threads=0):
+            ids = np.ascontiguousarray(ids, np.int64).reshape(-1)
+            idx = np.empty((ids.size, k), np.int64)
+            d2 = np.empty((ids.size, k), np.float32)
+            assert self.ref.lib.ref_grid_knn(self.h, None, _ptr(ids), ids.size, k, _ptr(idx), _ptr(d2), threads) == 0
+            return idx, d2
+
+        def all_nn(self, k):
+            n = self.p.shape[0]
+            idx = np.empty((n, k), np.int64)
+            d2 = np.empty((n, k), np.float32)
+            assert self.ref.lib.ref_grid_all_nn(self.h, k, n, _ptr(idx), _ptr(d2)) == 0
+            return idx, d2
+
+    def grid(self, p, target=1.0):
+        return _Ref.Grid(self, p, target)
 
     # CSG -----------------------------------------------------------------------------------------
     class Scene:

@@ -39,6 +39,7 @@ using TriSDF44 = TriMeshSDF<double, short, 4, 4>;
 using TriSDFDef = TriMeshSDF<double, short, BVH::DefaultBranchingRatio<double>(), TriangleSoA::DefaultWidth<double>()>;
 
 using Cloud = PointCloudBVH<float, std::size_t>;
+using Grid  = PointCloudHashGrid<float, std::size_t>;
 
 struct RefMesh
 {
@@ -425,6 +426,69 @@ ref_cloud_all_nn(void* a_h, int k, int64_t n, int64_t* idx, float* d2)
   }
   for (int64_t i = 0; i < n * k; i++) {
     const bool none = hits[i].index == std::numeric_limits<size_t>::max();
+    idx[i]          = none ? -1 : int64_t(hits[i].index);
+    d2[i]           = none ? std::numeric_limits<float>::infinity() : hits[i].distanceSquared;
+  }
+  return 0;
+}
+
+// --- uniform-grid point clouds ----------------------------------------------------------------
+
+// PointCloudHashGrid(positions, meta, targetPerCell) (PointCloudHashGridImplem.hpp:27-152).
+void*
+ref_grid_create(const float* P, int64_t n, float a_target)
+{
+  std::vector<Vec3f>  pos(n);
+  std::vector<size_t> meta(n);
+  for (int64_t i = 0; i < n; i++) {
+    pos[i]  = Vec3f(P[3 * i + 0], P[3 * i + 1], P[3 * i + 2]);
+    meta[i] = size_t(i);
+  }
+  return new Grid(pos, meta, a_target);
+}
+
+void
+ref_grid_destroy(void* h)
+{
+  delete static_cast<Grid*>(h);
+}
+
+// closestPoints (PointCloudHashGridImplem.hpp:321-333) for a batch of points, or, when a_ids is
+// given, nearestNeighbors(ids[i], k) (:349-362); the reference's own order (ties in visiting order).
+int
+ref_grid_knn(void* a_h, const float* Q, const int64_t* a_ids, int64_t nq, int k, int64_t* idx, float* d2,
+             int a_threads)
+{
+  auto*     g  = static_cast<Grid*>(a_h);
+  const int nt = a_threads > 0 ? a_threads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<Grid::Hit> hits(k);
+#pragma omp for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < nq; i++) {
+      const size_t found = a_ids ? g->nearestNeighbors(size_t(a_ids[i]), size_t(k), hits.data())
+                                 : g->closestPoints(Vec3f(Q[3 * i], Q[3 * i + 1], Q[3 * i + 2]), size_t(k), hits.data());
+      for (int j = 0; j < k; j++) {
+        idx[i * k + j] = (size_t(j) < found) ? int64_t(hits[j].index) : -1;
+        d2[i * k + j]  = (size_t(j) < found) ? hits[j].distanceSquared : std::numeric_limits<float>::infinity();
+      }
+    }
+  }
+  return 0;
+}
+
+// allNearestNeighbors(k) (PointCloudHashGridImplem.hpp:364-385).  Rows with fewer than k other
+// points keep the reference's default Hit (distanceSquared = float max), reported as -1 / +inf.
+int
+ref_grid_all_nn(void* a_h, int k, int64_t n, int64_t* idx, float* d2)
+{
+  auto*      g    = static_cast<Grid*>(a_h);
+  const auto hits = g->allNearestNeighbors(size_t(k));
+  if (int64_t(hits.size()) != n * k) {
+    return -1;
+  }
+  for (int64_t i = 0; i < n * k; i++) {
+    const bool none = hits[i].distanceSquared == std::numeric_limits<float>::max();
     idx[i]          = none ? -1 : int64_t(hits[i].index);
     d2[i]           = none ? std::numeric_limits<float>::infinity() : hits[i].distanceSquared;
   }

@@ -20,6 +20,11 @@ It builds nothing but the oracle (``make -C oracle``) and writes small .npz file
   external queries and the self queries of allNearestNeighbors (k = 1, 5 and lexicographic k = 8)
   and 200 external queries (seed 99), with the reference's PointCloudBVH closestPoints (k = 1, 5)
   and the same traversal with (d2, index) ordering.
+* ``grid2000.npz``       -- Tests/TestPointCloudHashGrid.cpp's clouds: the 2000-point cloud (seed
+  20260708) with 200 external queries (seed 99), the reference's PointCloudHashGrid closestPoints
+  (k = 1, 8) and allNearestNeighbors (k = 1, 5); its edge-case clouds (a planar cloud, a cluster with
+  a distant outlier, 16 coincident points, cell-size targets 1e-6 and 1000) with allNearestNeighbors
+  (k = 1).  Indices are the reference's own (ties in its visiting order).
 * ``csg_small.npz``      -- a union of 40 spheres and 3 posed displaced icospheres evaluated by the
   reference's BVHUnion over Translate(Rotate(TriMeshSDF)) and SphereSDF at 1000 points.
 """
@@ -109,6 +114,27 @@ def main(reference: str) -> None:
     sl8, tl8 = c.self_knn(8, lex=True)
     np.savez(os.path.join(HERE, "cloud2000.npz"), points=pts, queries=qs, idx1=i1, d1=d1, idx5=i5, d5=d5, lex1=l1,
              lexd1=e1, lex8=l8, lexd8=e8, self1=s1, selfd1=t1, self5=s5, selfd5=t5, selflex8=sl8, selflexd8=tl8)
+
+    # --- uniform-grid cloud (TestPointCloudHashGrid.cpp:60-330) ----------------------------------------
+    g = R.grid(pts)
+    gi1, gd1 = g.knn(qs, 1)
+    gi8, gd8 = g.knn(qs, 8)
+    gs1, gt1 = g.all_nn(1)
+    gs5, gt5 = g.all_nn(5)
+    planar = R.make_cloud_mt19937(500, 7)
+    planar[:, 2] = 0
+    ps1, pt1 = R.grid(planar).all_nn(1)
+    outl = np.concatenate([R.make_cloud_mt19937(999, 12), np.array([[1e6, 0.5, 0.5]], np.float32)])
+    os1, ot1 = R.grid(outl).all_nn(1)
+    coinc = np.tile(np.array([[1, 2, 3]], np.float32), (16, 1))
+    cs1, ct1 = R.grid(coinc).all_nn(1)
+    c800 = R.make_cloud_mt19937(800, 9)
+    tiny1, tinyd1 = R.grid(c800, 1e-6).all_nn(1)
+    huge1, huged1 = R.grid(c800, 1000.0).all_nn(1)
+    np.savez(os.path.join(HERE, "grid2000.npz"), points=pts, queries=qs, idx1=gi1, d1=gd1, idx8=gi8, d8=gd8,
+             self1=gs1, selfd1=gt1, self5=gs5, selfd5=gt5, planar=planar, planar1=ps1, planard1=pt1,
+             outlier=outl, outlier1=os1, outlierd1=ot1, coincident=coinc, coincident1=cs1,
+             coincidentd1=ct1, c800=c800, tiny1=tiny1, tinyd1=tinyd1, huge1=huge1, huged1=huged1)
 
     # --- small CSG union --------------------------------------------------------------------------------
     sc = W.csg_scene(77, n_spheres=40, n_meshes=3, levels=(1, 3), mesh_radius=(0.15, 0.3))

@@ -104,3 +104,21 @@ def test_self_knn_brute_matches_reference(port, golden):
         idx, d2 = port.knn_brute_self(g["points"], k)
         assert np.array_equal(d2, g[d2_key])
         assert np.array_equal(idx, g[idx_key].astype(np.int32))
+
+
+def test_grid_fixture_brute(port, golden):
+    """The reference's PointCloudHashGrid answers on its own test clouds equal brute force (the C
+    restatement): distances exactly, indices up to the order of equal distances."""
+    from _knn import assert_knn_equiv
+    g = golden("grid2000.npz")
+    for k, ik, dk in ((1, "idx1", "d1"), (8, "idx8", "d8")):
+        idx, d2 = port.knn_brute(g["points"], g["queries"], k)
+        assert_knn_equiv(g["points"], g["queries"], g[ik], g[dk], idx, d2)
+    for k, ik, dk in ((1, "self1", "selfd1"), (5, "self5", "selfd5")):
+        idx, d2 = port.knn_brute_self(g["points"], k)
+        assert_knn_equiv(g["points"], None, g[ik], g[dk], idx, d2)
+    for cloud, ik, dk in (("planar", "planar1", "planard1"), ("outlier", "outlier1", "outlierd1"),
+                          ("coincident", "coincident1", "coincidentd1"), ("c800", "tiny1", "tinyd1"),
+                          ("c800", "huge1", "huged1")):
+        idx, d2 = port.knn_brute_self(g[cloud], 1)
+        assert_knn_equiv(g[cloud], None, g[ik], g[dk], idx, d2)
