@@ -96,16 +96,35 @@ class TriMeshSDF:
                                       C.byref(h)))
         self._h = h
         self.num_triangles = f.shape[0]
-        inf = _capi.MeshInfo()
-        check(lib.ebg_mesh_get_info(self._h, C.byref(inf)))
-        self.info = {k: (list(getattr(inf, k)) if k in ("lo", "hi") else getattr(inf, k))
-                     for k, _ in _capi.MeshInfo._fields_}
+        self._refresh_info()
 
     @classmethod
     def from_file(cls, path, **kw):
         """Parser::readIntoTriangleBVH: the mesh of a .stl / .obj / .ply / .vtk file."""
         v, f = read_soup(path)
         return cls(v, f, **kw)
+
+    def _refresh_info(self):
+        inf = _capi.MeshInfo()
+        check(lib.ebg_mesh_get_info(self._h, C.byref(inf)))
+        self.info = {k: (list(getattr(inf, k)) if k in ("lo", "hi") else getattr(inf, k))
+                     for k, _ in _capi.MeshInfo._fields_}
+
+    def refit(self, vertices, stream=None):
+        """PackedBVH::refit for moved vertices: ``vertices`` (V,3) float64 -- numpy, or a CUDA
+        tensor -- are the new positions of the same vertices.  The tree keeps its topology; normals,
+        records and boxes are recomputed on the device, so later queries are exact for the moved
+        mesh.  Synchronous."""
+        if isinstance(vertices, np.ndarray) or not hasattr(vertices, "is_cuda"):
+            v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+            check(lib.ebg_mesh_refit(self._h, _ptr(v), v.shape[0], _stream_ptr(stream)))
+        else:
+            import torch
+            if not (vertices.is_cuda and vertices.dtype == torch.float64 and vertices.is_contiguous()):
+                raise ValueError("vertices must be a contiguous float64 CUDA tensor of shape (V,3)")
+            check(lib.ebg_mesh_refit_device(self._h, C.c_void_p(vertices.data_ptr()), vertices.numel() // 3,
+                                            _stream_ptr(stream)))
+        self._refresh_info()
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -77,6 +77,8 @@ SIGNATURES = {
                                                C.POINTER(_P)]),
     "ebg_compute_pseudonormals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _P]),
     "ebg_mesh_destroy": (C.c_int, [_P]),
+    "ebg_mesh_refit": (C.c_int, [_P, _P, _I64, _P]),
+    "ebg_mesh_refit_device": (C.c_int, [_P, _P, _I64, _P]),
     "ebg_mesh_get_info": (C.c_int, [_P, C.POINTER(MeshInfo)]),
     "ebg_mesh_get_normals": (C.c_int, [_P, _P, _P, _P]),
     "ebg_mesh_signed_distance": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),

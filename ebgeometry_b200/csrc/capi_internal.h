@@ -27,7 +27,15 @@ struct ebg_mesh
   void* dNodeObb = nullptr;
   void* dDcelN   = nullptr;
   int*  dStatus = nullptr;
-  // host copies of the pseudonormals (soup order) and the cumulative triangle area (leaf order)
+  // kept for refitting moved vertices: the soup's triangles, and each leaf's and each interior
+  // node's range of leaf positions
+  int32_t*  dF         = nullptr;
+  uint32_t* dLeafFirst = nullptr;
+  uint32_t* dLeafCount = nullptr;
+  uint32_t* dNodeFirst = nullptr;
+  uint32_t* dNodeEnd   = nullptr;
+  // the pseudonormals (soup order) during a host build only -- afterwards they live in the FP64
+  // records on the device -- and the cumulative triangle area (leaf order)
   std::vector<double> triN, cornerVN, edgeN;
   std::vector<double> areaCdf;
   // launch shape chosen by ebg_mesh_autotune (0 = library defaults)

@@ -179,6 +179,28 @@ void computeObbs(const double* V, const int32_t* F, Bvh4& bvh, std::vector<EbgOb
   }
 }
 
+// The mesh's bounding box in its view (FP32 root box, query-ordering domain) and summary.
+void setMeshBounds(ebg_mesh* m, const double* lo, const double* hi)
+{
+  EbgMeshView& v = m->view;
+  for (int a = 0; a < 3; a++) {
+    v.root_lo[a] = roundDown(lo[a]);
+    v.root_hi[a] = roundUp(hi[a]);
+    // Morton domain for query ordering: the mesh box grown to twice its extent about its centre
+    const double c    = 0.5 * (lo[a] + hi[a]);
+    const double ext  = std::max(hi[a] - lo[a], 1e-30);
+    v.morton_lo[a]    = float(c - ext);
+    v.morton_scale[a] = float(1024.0 / (2.0 * ext));
+  }
+  double d2 = 0;
+  for (int a = 0; a < 3; a++) {
+    m->info.lo[a] = lo[a];
+    m->info.hi[a] = hi[a];
+    d2 += (hi[a] - lo[a]) * (hi[a] - lo[a]);
+  }
+  m->info.diagonal = std::sqrt(d2);
+}
+
 // The device view and the summary of a mesh whose device arrays are in place (either build).
 ebg_status finishMesh(ebg_mesh* m, int64_t nv, int64_t nt, int leafSize, const double* lo, const double* hi,
                       ebg_mesh** out)
@@ -198,30 +220,15 @@ ebg_status finishMesh(ebg_mesh* m, int64_t nv, int64_t nt, int leafSize, const d
   v.obb          = static_cast<const EbgObb*>(m->dObb);
   v.node_obb     = static_cast<const EbgObb*>(m->dNodeObb);
   v.dcel_n       = static_cast<const double*>(m->dDcelN);
-  for (int a = 0; a < 3; a++) {
-    v.root_lo[a] = roundDown(lo[a]);
-    v.root_hi[a] = roundUp(hi[a]);
-    // Morton domain for query ordering: the mesh box grown to twice its extent about its centre
-    const double c    = 0.5 * (lo[a] + hi[a]);
-    const double ext  = std::max(hi[a] - lo[a], 1e-30);
-    v.morton_lo[a]    = float(c - ext);
-    v.morton_scale[a] = float(1024.0 / (2.0 * ext));
-  }
+  setMeshBounds(m, lo, hi);
   ebg_mesh_info& inf = m->info;
   inf.num_triangles  = nt;
   inf.num_vertices   = nv;
   inf.leaf_size      = leafSize;
-  double d2          = 0;
-  for (int a = 0; a < 3; a++) {
-    inf.lo[a] = lo[a];
-    inf.hi[a] = hi[a];
-    d2 += (hi[a] - lo[a]) * (hi[a] - lo[a]);
-  }
-  inf.diagonal     = std::sqrt(d2);
-  const size_t N   = size_t(nt);
-  inf.device_bytes = int64_t(size_t(std::max<int64_t>(inf.num_nodes, 1)) * (sizeof(EbgNode4) + sizeof(EbgObb)) +
-                             size_t(inf.num_leaves) * sizeof(EbgObb) +
-                             N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 33 * sizeof(double) + 4));
+  const size_t N     = size_t(nt);
+  inf.device_bytes = int64_t(size_t(std::max<int64_t>(inf.num_nodes, 1)) * (sizeof(EbgNode4) + sizeof(EbgObb) + 8) +
+                             size_t(inf.num_leaves) * (sizeof(EbgObb) + 8) +
+                             N * (sizeof(EbgTriHot) + sizeof(EbgTriSign) + 33 * sizeof(double) + 4 + 12));
   *out             = m;
   return EBG_OK;
 }
@@ -328,6 +335,9 @@ ebg_status buildMesh(const double*         V,
     double           lo[3], hi[3];
     const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, leafSize, lo, hi, bs, !givenNormal);
     cudaStreamDestroy(bs);
+    std::vector<double>().swap(m->triN);
+    std::vector<double>().swap(m->cornerVN);
+    std::vector<double>().swap(m->edgeN);
     if (rc != EBG_OK) {
       const std::string keep = ebg_last_error();
       ebg_mesh_destroy(m);
@@ -437,12 +447,21 @@ ebg_status buildMesh(const double*         V,
       !up(&m->dTriId, triId.data(), N * sizeof(int32_t)) ||
       !up(&m->dObb, obb.data(), obb.size() * sizeof(EbgObb)) ||
       !up(&m->dNodeObb, nodeObb.data(), nodeObb.size() * sizeof(EbgObb)) ||
-      !up(&m->dDcelN, dcelN.data(), dcelN.size() * sizeof(double))) {
+      !up(&m->dDcelN, dcelN.data(), dcelN.size() * sizeof(double)) ||
+      !up((void**)&m->dF, F, 3 * N * sizeof(int32_t)) ||
+      !up((void**)&m->dLeafFirst, bvh.leafFirst.data(), bvh.leafFirst.size() * sizeof(uint32_t)) ||
+      !up((void**)&m->dLeafCount, bvh.leafCount.data(), bvh.leafCount.size() * sizeof(uint32_t)) ||
+      !up((void**)&m->dNodeFirst, bvh.nodeFirst.data(), bvh.nodeFirst.size() * sizeof(uint32_t)) ||
+      !up((void**)&m->dNodeEnd, bvh.nodeEnd.data(), bvh.nodeEnd.size() * sizeof(uint32_t))) {
     cudaGetLastError();
     ebg_mesh_destroy(m);
     return setError(EBG_ERR_NO_MEMORY, "device allocation or upload failed for the mesh");
   }
 
+  // every normal now lives in the FP64 records on the device (ebg_mesh_get_normals reads them there)
+  std::vector<double>().swap(m->triN);
+  std::vector<double>().swap(m->cornerVN);
+  std::vector<double>().swap(m->edgeN);
   m->info.num_nodes  = int64_t(bvh.nodes.size());
   m->info.num_leaves = bvh.numLeaves;
   m->info.depth      = bvh.depth;
@@ -694,8 +713,44 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dNodeObb);
   cudaFree(m->dDcelN);
   cudaFree(m->dStatus);
+  cudaFree(m->dF);
+  cudaFree(m->dLeafFirst);
+  cudaFree(m->dLeafCount);
+  cudaFree(m->dNodeFirst);
+  cudaFree(m->dNodeEnd);
   delete m;
   return EBG_OK;
+}
+
+static ebg_status meshRefit(ebg_mesh* m, const double* vertices, bool onDevice, int64_t nv, void* stream)
+{
+  if (m == nullptr || vertices == nullptr) {
+    return setError(EBG_ERR_INVALID, "null mesh or vertex array");
+  }
+  if (nv != m->info.num_vertices) {
+    return setError(EBG_ERR_INVALID, "refit needs the mesh's own vertex count (" + std::to_string(m->info.num_vertices) +
+                                         "), got " + std::to_string(nv));
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double       lo[3], hi[3];
+  const ebg_status rc = refitMeshOnDevice(m, vertices, onDevice, nv, lo, hi, s);
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  setMeshBounds(m, lo, hi);
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_refit(ebg_mesh* m, const double* vertices_host, int64_t num_vertices, void* stream)
+{
+  return meshRefit(m, vertices_host, false, num_vertices, stream);
+}
+
+ebg_status ebg_mesh_refit_device(ebg_mesh* m, const double* vertices_dev, int64_t num_vertices, void* stream)
+{
+  return meshRefit(m, vertices_dev, true, num_vertices, stream);
 }
 
 ebg_status ebg_mesh_get_info(const ebg_mesh* m, ebg_mesh_info* info)
@@ -712,14 +767,27 @@ ebg_status ebg_mesh_get_normals(const ebg_mesh* m, double* fn, double* vn, doubl
   if (m == nullptr) {
     return setError(EBG_ERR_INVALID, "null mesh");
   }
-  if (fn) {
-    std::memcpy(fn, m->triN.data(), m->triN.size() * sizeof(double));
+  if (!fn && !vn && !en) {
+    return EBG_OK;
   }
-  if (vn) {
-    std::memcpy(vn, m->cornerVN.data(), m->cornerVN.size() * sizeof(double));
+  // the FP64 records hold every normal (leaf order); gather them into soup order on the device
+  DeviceGuard  guard;
+  cudaSetDevice(m->device);
+  const size_t N  = size_t(m->info.num_triangles);
+  double*      dN = nullptr;
+  if (cudaMalloc(&dN, 21 * 8 * N) != cudaSuccess) {
+    cudaGetLastError();
+    return setError(EBG_ERR_NO_MEMORY, "device buffer for the normals");
   }
-  if (en) {
-    std::memcpy(en, m->edgeN.data(), m->edgeN.size() * sizeof(double));
+  launchGatherNormals(static_cast<const double*>(m->dTri64), static_cast<const int32_t*>(m->dTriId), int64_t(N), dN,
+                      nullptr);
+  bool ok = cudaGetLastError() == cudaSuccess;
+  ok      = ok && (!fn || cudaMemcpy(fn, dN, 24 * N, cudaMemcpyDeviceToHost) == cudaSuccess);
+  ok      = ok && (!vn || cudaMemcpy(vn, dN + 3 * N, 72 * N, cudaMemcpyDeviceToHost) == cudaSuccess);
+  ok      = ok && (!en || cudaMemcpy(en, dN + 12 * N, 72 * N, cudaMemcpyDeviceToHost) == cudaSuccess);
+  cudaFree(dN);
+  if (!ok) {
+    return setError(EBG_ERR_CUDA, std::string("reading the normals: ") + cudaGetErrorString(cudaGetLastError()));
   }
   return EBG_OK;
 }

@@ -15,8 +15,11 @@
 //      up to four, as the host does; leaves and nodes get their indices from atomic counters;
 //   5. leaf-ordered triangle records (the FP32 hot and sign records, the FP64 lane records, the DCEL
 //      normals, areas), and the oriented box of every leaf and node (one block per range).
-// The pseudonormals come from the host (bit-identical to the reference's DCEL).  Results do not
-// depend on the tree's shape, so a mesh built here answers exactly as a host-built one.
+// The pseudonormals come from the host build's routine or from normals_gpu.cu (both bit-identical
+// to the reference's DCEL).  Results do not depend on the tree's shape, so a mesh built here
+// answers exactly as a host-built one.
+// 6. Refit (moved vertices, either build's tree): pseudonormals, records and oriented boxes again,
+//    and every node's child boxes from its children's ranges of leaf positions.
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -632,6 +635,86 @@ __global__ void kNodeObbFlags(const uint8_t* __restrict__ useful, const uint32_t
   }
 }
 
+// 6. refit (moved vertices, same tree): one block per node; each slot gets the FP64 box of its
+// range of leaf positions (a leaf slot: its triangles; an interior slot: the child's subtree),
+// rounded outward to FP32, and an interior slot's oriented-box flag from `useful`.
+__global__ void __launch_bounds__(128) kSlotBoxes(const double* __restrict__ tri64, const uint32_t* __restrict__ nodeFirst,
+                                                  const uint32_t* __restrict__ nodeEnd,
+                                                  const uint8_t* __restrict__ useful, uint32_t numNodes,
+                                                  EbgNode4* __restrict__ nodes)
+{
+  __shared__ double red[4];
+  for (uint32_t j = blockIdx.x; j < numNodes; j += gridDim.x) {
+    EbgNode4& nd = nodes[j];
+    for (int k = 0; k < 4; k++) {
+      const uint32_t c   = nd.child[k];
+      const uint32_t cnt = nd.count[k];
+      uint32_t       b, e;
+      if (c & EBG_LEAF_BIT) {
+        b = c & ~EBG_LEAF_BIT;
+        e = b + (cnt & EBG_COUNT_MASK);
+      }
+      else if (c != 0 && c < numNodes) {
+        b = nodeFirst[c];
+        e = nodeEnd[c];
+      }
+      else {
+        continue; // an empty slot (node 0 is the root, never a child)
+      }
+      double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+      for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+        const double* t = tri64 + 30 * size_t(i);
+        for (int a = 0; a < 3; a++) {
+          lo[a] = fmin(lo[a], fmin(t[a], fmin(t[3 + a], t[6 + a])));
+          hi[a] = fmax(hi[a], fmax(t[a], fmax(t[3 + a], t[6 + a])));
+        }
+      }
+      for (int a = 0; a < 3; a++) {
+        lo[a] = blockMin(lo[a], red);
+        hi[a] = blockMax(hi[a], red);
+      }
+      if (threadIdx.x == 0) {
+        nd.lox[k] = rdown(lo[0]);
+        nd.loy[k] = rdown(lo[1]);
+        nd.loz[k] = rdown(lo[2]);
+        nd.hix[k] = rup(hi[0]);
+        nd.hiy[k] = rup(hi[1]);
+        nd.hiz[k] = rup(hi[2]);
+        if (!(c & EBG_LEAF_BIT)) {
+          nd.count[k] = useful[c] ? EBG_NODE_HAS_OBB : 0u;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// the normals of the FP64 records (leaf order) back in soup order: out = [face 3N | corner 9N | edge 9N]
+__global__ void kGatherNormals(const double* __restrict__ tri64, const int32_t* __restrict__ triId, int64_t n,
+                               double* __restrict__ out)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t f = triId[i];
+    const double* t = tri64 + 30 * i;
+    for (int k = 0; k < 3; k++) {
+      out[3 * f + k] = t[9 + k];
+    }
+    for (int k = 0; k < 9; k++) {
+      out[3 * n + 9 * f + k]  = t[12 + k];
+      out[12 * n + 9 * f + k] = t[21 + k];
+    }
+  }
+}
+
+__global__ void kAllFinite(const double* __restrict__ v, int64_t n, int* __restrict__ bad)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    if (!isfinite(v[i])) {
+      *bad = 1;
+    }
+  }
+}
+
 inline unsigned gridFor(int64_t n, int t, int64_t cap = 1 << 20)
 {
   int64_t g = (n + t - 1) / t;
@@ -699,13 +782,6 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
     if (rc != EBG_OK) {
       return rc;
     }
-    // the host keeps a copy (ebg_mesh_get_normals)
-    m->triN.resize(3 * N);
-    m->cornerVN.resize(9 * N);
-    m->edgeN.resize(9 * N);
-    cudaMemcpyAsync(m->triN.data(), dTriN, 24 * N, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(m->cornerVN.data(), dVN, 72 * N, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(m->edgeN.data(), dEN, 72 * N, cudaMemcpyDeviceToHost, s);
   }
   else {
     cudaMemcpyAsync(dTriN, m->triN.data(), 24 * N, cudaMemcpyHostToDevice, s);
@@ -833,9 +909,19 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
   if (!keep(&m->dNodes, sizeof(EbgNode4) * std::max<size_t>(numNodes, 1)) || !keep(&m->dHot, sizeof(EbgTriHot) * N) ||
       !keep(&m->dSign, sizeof(EbgTriSign) * N) || !keep(&m->dTri64, 240 * N) || !keep(&m->dTriId, 4 * N) ||
       !keep(&m->dObb, sizeof(EbgObb) * numLeaves) || !keep(&m->dNodeObb, sizeof(EbgObb) * std::max<size_t>(numNodes, 1)) ||
-      !keep(&m->dDcelN, 24 * N)) {
+      !keep(&m->dDcelN, 24 * N) || !keep((void**)&m->dF, 12 * N) || !keep((void**)&m->dLeafFirst, 4 * size_t(numLeaves)) ||
+      !keep((void**)&m->dLeafCount, 4 * size_t(numLeaves)) ||
+      !keep((void**)&m->dNodeFirst, 4 * std::max<size_t>(numNodes, 1)) ||
+      !keep((void**)&m->dNodeEnd, 4 * std::max<size_t>(numNodes, 1))) {
     cudaGetLastError();
     return setError(EBG_ERR_NO_MEMORY, "device allocation for the mesh");
+  }
+  cudaMemcpyAsync(m->dF, dF, 12 * N, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(m->dLeafFirst, leafFirst, 4 * size_t(numLeaves), cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(m->dLeafCount, leafCount, 4 * size_t(numLeaves), cudaMemcpyDeviceToDevice, s);
+  if (numNodes > 0) {
+    cudaMemcpyAsync(m->dNodeFirst, nodeFirst, 4 * size_t(numNodes), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(m->dNodeEnd, nodeEnd, 4 * size_t(numNodes), cudaMemcpyDeviceToDevice, s);
   }
   kRecords<<<gridFor(n, 256), 256, 0, s>>>(dV, dF, dTriN, dVN, dEN, ids, n, static_cast<EbgTriHot*>(m->dHot),
                                            static_cast<EbgTriSign*>(m->dSign), static_cast<double*>(m->dTri64),
@@ -870,6 +956,133 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
   m->view.root_ref   = n > leafSize ? 0u : (EBG_LEAF_BIT | 0u);
   m->view.root_count = n > leafSize ? 0u : uint32_t(n);
   return EBG_OK;
+}
+
+} // namespace ebg
+
+namespace ebg {
+
+ebg_status refitMeshOnDevice(ebg_mesh* m, const double* V, bool vOnDevice, int64_t nv, double* outLo, double* outHi,
+                             cudaStream_t s)
+{
+  const int64_t n = m->info.num_triangles;
+  const size_t  N = size_t(n);
+  if (m->dF == nullptr) {
+    return setError(EBG_ERR_INVALID, "mesh has no topology kept for refitting");
+  }
+  std::vector<void*> tmp;
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMallocAsync(p, std::max<size_t>(bytes, 16), s) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    tmp.push_back(*p);
+    return true;
+  };
+  struct Guard
+  {
+    std::vector<void*>& t;
+    cudaStream_t        st;
+    ~Guard()
+    {
+      for (void* p : t) {
+        cudaFreeAsync(p, st);
+      }
+      cudaStreamSynchronize(st);
+    }
+  } guard{tmp, s};
+  const uint32_t numNodes  = uint32_t(m->info.num_nodes);
+  const uint32_t numLeaves = uint32_t(m->info.num_leaves);
+  double *dV = nullptr, *dTriN = nullptr, *dVN = nullptr, *dEN = nullptr, *triLo = nullptr, *triHi = nullptr,
+         *cen = nullptr, *area = nullptr;
+  unsigned long long* bounds = nullptr;
+  uint8_t*            useful = nullptr;
+  int*                bad    = nullptr;
+  bool ok = alloc((void**)&dTriN, 24 * N) && alloc((void**)&dVN, 72 * N) && alloc((void**)&dEN, 72 * N) &&
+            alloc((void**)&triLo, 24 * N) && alloc((void**)&triHi, 24 * N) && alloc((void**)&cen, 24 * N) &&
+            alloc((void**)&area, 8 * N) && alloc((void**)&bounds, 12 * 8) &&
+            alloc((void**)&useful, std::max<size_t>(numNodes, 1)) && alloc((void**)&bad, 4);
+  if (ok && !vOnDevice) {
+    ok = alloc((void**)&dV, 24 * size_t(nv)) &&
+         cudaMemcpyAsync(dV, V, 24 * size_t(nv), cudaMemcpyHostToDevice, s) == cudaSuccess;
+  }
+  if (!ok) {
+    return setError(EBG_ERR_NO_MEMORY, "refit workspace");
+  }
+  const double* v = vOnDevice ? V : dV;
+  cudaMemsetAsync(bad, 0, 4, s);
+  cudaMemsetAsync(useful, 0, std::max<size_t>(numNodes, 1), s);
+  kAllFinite<<<gridFor(3 * nv, 256, 4096), 256, 0, s>>>(v, 3 * nv, bad);
+  int hbad = 0;
+  cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("refit: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  if (hbad != 0) {
+    return setError(EBG_ERR_INVALID, "non-finite vertex coordinate");
+  }
+  // the pseudonormals of the moved soup (fails, leaving the mesh untouched, on degenerate triangles)
+  const ebg_status rc = pseudonormalsOnDevice(v, nv, m->dF, n, dTriN, dVN, dEN, s);
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  {
+    unsigned long long init[12];
+    for (int j = 0; j < 12; j++) {
+      const bool isMin = (j < 3) || (j >= 6 && j < 9);
+      init[j]          = isMin ? ~0ull : 0ull;
+    }
+    cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  }
+  kTriBounds<<<gridFor(n, 256, 8192), 256, 0, s>>>(v, m->dF, n, triLo, triHi, cen, bounds);
+  unsigned long long hb[12];
+  cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("refit: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  for (int a = 0; a < 3; a++) {
+    outLo[a] = hostDval(hb[6 + a]);
+    outHi[a] = hostDval(hb[9 + a]);
+  }
+  kRecords<<<gridFor(n, 256), 256, 0, s>>>(v, m->dF, dTriN, dVN, dEN, reinterpret_cast<const uint32_t*>(m->dTriId), n,
+                                           static_cast<EbgTriHot*>(m->dHot), static_cast<EbgTriSign*>(m->dSign),
+                                           static_cast<double*>(m->dTri64), static_cast<int32_t*>(m->dTriId),
+                                           static_cast<double*>(m->dDcelN), area);
+  double scale = 0;
+  for (int a = 0; a < 3; a++) {
+    scale = std::max(scale, std::max(std::fabs(outLo[a]), std::fabs(outHi[a])));
+  }
+  const double pad = 2e-6 * std::max(scale, 1e-30);
+  kRangeObbs<<<gridFor(numLeaves, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dLeafFirst,
+                                                            nullptr, m->dLeafCount, numLeaves, pad,
+                                                            static_cast<EbgObb*>(m->dObb), nullptr);
+  if (numNodes > 0) {
+    kRangeObbs<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dNodeFirst,
+                                                             m->dNodeEnd, nullptr, numNodes, pad,
+                                                             static_cast<EbgObb*>(m->dNodeObb), useful);
+    kSlotBoxes<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dNodeFirst,
+                                                             m->dNodeEnd, useful, numNodes,
+                                                             static_cast<EbgNode4*>(m->dNodes));
+  }
+  std::vector<double> cdf(N);
+  cudaMemcpyAsync(cdf.data(), area, 8 * N, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("refit: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  for (size_t i = 1; i < N; i++) {
+    cdf[i] += cdf[i - 1];
+  }
+  m->areaCdf.swap(cdf);
+  return EBG_OK;
+}
+
+} // namespace ebg
+
+namespace ebg {
+
+void launchGatherNormals(const double* tri64, const int32_t* triId, int64_t n, double* out, cudaStream_t s)
+{
+  kGatherNormals<<<gridFor(n, 256), 256, 0, s>>>(tri64, triId, n, out);
 }
 
 } // namespace ebg

@@ -142,6 +142,13 @@ public:
     check(ebg_mesh_signed_distance_f64(m_mesh, a_pointsDev, int64_t(a_n), a_distDev, nullptr, &o, a_stream));
   }
 
+  // PackedBVH::refit (BVHImplem.hpp:1608-1652) for moved vertices: the same vertices' new
+  // positions; the tree keeps its topology, normals and boxes are recomputed on the device.
+  void refit(const std::vector<std::array<double, 3>>& a_vertices, void* a_stream = nullptr)
+  {
+    check(ebg_mesh_refit(m_mesh, &a_vertices[0][0], int64_t(a_vertices.size()), a_stream));
+  }
+
   ebg_mesh_info info() const
   {
     ebg_mesh_info i{};

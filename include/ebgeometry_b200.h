@@ -180,6 +180,18 @@ ebg_status ebg_compute_pseudonormals(const double*  vertices,
 
 ebg_status ebg_mesh_destroy(ebg_mesh* mesh);
 
+/* Moving geometry: PackedBVH::refit (BVHImplem.hpp:1608-1652) for a TriMeshSDF whose vertices have
+ * moved.  vertices: the new positions of the same num_vertices vertices (the soup's triangles stay).
+ * The tree keeps its topology and leaf order; on the device the pseudonormals (the reference's
+ * DCEL rules, as ebg_mesh_create computes them), every triangle record, every box and oriented box
+ * are recomputed, so queries after the call answer exactly for the moved mesh -- as fast as a
+ * fresh build while the motion keeps the tree's grouping sensible.  Normals given to
+ * ebg_mesh_create_with_normals are replaced by computed ones.  Synchronous; work of earlier calls
+ * on other streams that reads the mesh must be complete.  Non-finite coordinates or a triangle
+ * that became degenerate: EBG_ERR_INVALID, mesh unchanged. */
+ebg_status ebg_mesh_refit(ebg_mesh* mesh, const double* vertices_host, int64_t num_vertices, void* stream);
+ebg_status ebg_mesh_refit_device(ebg_mesh* mesh, const double* vertices_dev, int64_t num_vertices, void* stream);
+
 /* Mesh files (host only, no device needed): the reading half of Parser::readIntoDCEL
  * (ParserImplem.hpp:1752-1800) for .stl (ASCII or binary), .obj, .ply (ascii or binary, either byte
  * order) and legacy ASCII .vtk POLYDATA, with the reference's rules for which triangles a file
