@@ -23,7 +23,8 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["read_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PointCloudBVH", "PointCloudHashGrid",
+__all__ = ["read_soup", "read_polygon_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PolygonMeshSDF",
+           "PolygonFlatMeshSDF", "polygon_normals", "PointCloudBVH", "PointCloudHashGrid",
            "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
 BUILD_SAH = 0
@@ -52,6 +53,24 @@ def read_soup(path):
     finally:
         lib.ebg_soup_destroy(h)
     return v, f
+
+
+def read_polygon_soup(path):
+    """(vertices (V,3) float64, face offsets (F+1,) int64, face vertex indices int32) of a mesh file
+    of any faces, read and merged the way the reference's parser does (host only)."""
+    h = C.c_void_p()
+    check(lib.ebg_soup_read(str(path).encode(), C.byref(h)))
+    try:
+        nv, nf, nc = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.ebg_soup_sizes(h, C.byref(nv), C.byref(nf)))
+        check(lib.ebg_soup_num_corners(h, C.byref(nc)))
+        v = np.empty((nv.value, 3), np.float64)
+        off = np.empty(nf.value + 1, np.int64)
+        idx = np.empty(nc.value, np.int32)
+        check(lib.ebg_soup_copy_polygons(h, _ptr(v), _ptr(off), _ptr(idx)))
+    finally:
+        lib.ebg_soup_destroy(h)
+    return v, off, idx
 
 
 def _stream_ptr(stream):
@@ -272,6 +291,103 @@ class MeshSDF(TriMeshSDF):
 
     signedDistance = value
     __call__ = value
+
+
+def _faces_csr(faces):
+    """(offsets int64, indices int32) of faces given as a list of index sequences or as an
+    (offsets, indices) pair."""
+    if isinstance(faces, tuple) and len(faces) == 2 and np.ndim(faces[0]) == 1 and np.ndim(faces[1]) == 1:
+        return np.ascontiguousarray(faces[0], np.int64), np.ascontiguousarray(faces[1], np.int32)
+    if isinstance(faces, np.ndarray) and faces.ndim == 2:
+        off = np.arange(faces.shape[0] + 1, dtype=np.int64) * faces.shape[1]
+        return off, np.ascontiguousarray(faces, np.int32).ravel()
+    counts = np.array([len(f) for f in faces], np.int64)
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    idx = np.concatenate([np.asarray(f, np.int32) for f in faces]) if len(faces) else np.empty(0, np.int32)
+    return off, np.ascontiguousarray(idx, np.int32)
+
+
+def polygon_normals(vertices, faces):
+    """Host-only: (face normals (F,3), centroids (F,3), corner vertex normals (C,3), corner edge
+    normals (C,3)) of a polygon soup, the reference's DCEL quantities (no device needed)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+    off, idx = _faces_csr(faces)
+    nf, nc = off.size - 1, idx.size
+    fn, c, vn, en = np.empty((nf, 3)), np.empty((nf, 3)), np.empty((nc, 3)), np.empty((nc, 3))
+    check(lib.ebg_compute_polygon_normals(_ptr(v), v.shape[0], _ptr(off), _ptr(idx), nf, _ptr(fn), _ptr(c),
+                                          _ptr(vn), _ptr(en)))
+    return fn, c, vn, en
+
+
+class PolygonMeshSDF:
+    """The reference's MeshSDF over a DCEL of polygon faces (three or more vertices each): faces
+    given as a list of vertex-index sequences, an (F,k) array, or (offsets, indices).  The DCEL
+    normals, the face algorithm and the smallest-|d| rule are the reference's; FP64 end to end."""
+
+    _dev_fn = "ebg_polymesh_signed_distance"
+    _host_fn = "ebg_polymesh_signed_distance_host"
+
+    def __init__(self, vertices, faces, build="SAH", leaf_size=4, device=-1, _handle=None):
+        if _handle is None:
+            v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+            off, idx = _faces_csr(faces)
+            b = {"SAH": BUILD_SAH, "MORTON": BUILD_MORTON}[str(build).upper()] if isinstance(build, str) else int(build)
+            opts = _capi.BuildOpts(b, int(leaf_size), int(device), 0)
+            _handle = C.c_void_p()
+            check(lib.ebg_polymesh_create(_ptr(v), v.shape[0], _ptr(off), _ptr(idx), off.size - 1, C.byref(opts),
+                                          C.byref(_handle)))
+        self._h = _handle
+        inf = _capi.MeshInfo()
+        nc = C.c_int64()
+        check(lib.ebg_polymesh_get_info(self._h, C.byref(inf), C.byref(nc)))
+        self.num_faces = int(inf.num_triangles)
+        self.num_corners = int(nc.value)
+        self.diagonal = float(inf.diagonal)
+
+    @classmethod
+    def from_file(cls, path, build="SAH", leaf_size=4, device=-1):
+        """Parser::readIntoDCEL + MeshSDF: the polygon mesh of a .stl / .obj / .ply / .vtk file."""
+        b = {"SAH": BUILD_SAH, "MORTON": BUILD_MORTON}[str(build).upper()]
+        opts = _capi.BuildOpts(b, int(leaf_size), int(device), 0)
+        h = C.c_void_p()
+        check(lib.ebg_polymesh_create_from_file(str(path).encode(), C.byref(opts), C.byref(h)))
+        return cls(None, None, _handle=h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.ebg_polymesh_destroy(h)
+            self._h = None
+
+    def normals(self):
+        """(face normals (F,3), centroids (F,3), corner vertex normals (C,3), corner edge normals
+        (C,3)), corners face after face in soup order."""
+        fn, c = np.empty((self.num_faces, 3)), np.empty((self.num_faces, 3))
+        vn, en = np.empty((self.num_corners, 3)), np.empty((self.num_corners, 3))
+        check(lib.ebg_polymesh_get_normals(self._h, _ptr(fn), _ptr(c), _ptr(vn), _ptr(en)))
+        return fn, c, vn, en
+
+    def signed_distance(self, points, closest_face=None, stream=None):
+        """FP64 signed distances (numpy: synchronous host call; CUDA float64 tensor: asynchronous)."""
+        return _fp64_call(self, getattr(lib, self._dev_fn), getattr(lib, self._host_fn), points, closest_face,
+                          stream, False)
+
+    def check_status(self, stream=None):
+        check(lib.ebg_polymesh_check_status(self._h, _stream_ptr(stream)))
+
+    def value(self, point) -> float:
+        return float(self.signed_distance(np.asarray(point, np.float64).reshape(1, 3))[0])
+
+    signedDistance = value
+    __call__ = value
+
+
+class PolygonFlatMeshSDF(PolygonMeshSDF):
+    """The reference's FlatMeshSDF over polygon faces: every face for every point, the first face
+    in soup order with the smallest unsigned distance."""
+
+    _dev_fn = "ebg_polymesh_signed_distance_flat"
+    _host_fn = "ebg_polymesh_signed_distance_flat_host"
 
 
 class FlatMeshSDF(TriMeshSDF):

@@ -86,6 +86,19 @@ SIGNATURES = {
     "ebg_soup_sizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64)]),
     "ebg_soup_copy": (C.c_int, [_P, _P, _P]),
     "ebg_soup_destroy": (C.c_int, [_P]),
+    "ebg_soup_num_corners": (C.c_int, [_P, C.POINTER(_I64)]),
+    "ebg_soup_copy_polygons": (C.c_int, [_P, _P, _P, _P]),
+    "ebg_polymesh_create": (C.c_int, [_P, _I64, _P, _P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "ebg_polymesh_create_from_file": (C.c_int, [C.c_char_p, C.POINTER(BuildOpts), C.POINTER(_P)]),
+    "ebg_polymesh_destroy": (C.c_int, [_P]),
+    "ebg_compute_polygon_normals": (C.c_int, [_P, _I64, _P, _P, _I64, _P, _P, _P, _P]),
+    "ebg_polymesh_get_info": (C.c_int, [_P, C.POINTER(MeshInfo), C.POINTER(_I64)]),
+    "ebg_polymesh_get_normals": (C.c_int, [_P, _P, _P, _P, _P]),
+    "ebg_polymesh_signed_distance": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "ebg_polymesh_signed_distance_host": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "ebg_polymesh_signed_distance_flat": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "ebg_polymesh_signed_distance_flat_host": (C.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "ebg_polymesh_check_status": (C.c_int, [_P, _P]),
     "ebg_mesh_create_from_file": (C.c_int, [C.c_char_p, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_mesh_signed_distance_host": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_mesh_signed_distance_noalloc": (C.c_int, [_P, _P, _I64, _P, _P, C.POINTER(QueryOpts), _P]),

@@ -203,6 +203,155 @@ bool computePseudonormals(const double*        V,
 }
 
 // ---------------------------------------------------------------------------------------------
+// Polygon faces: the same DCEL rules for faces of any vertex count.
+
+bool computePolygonNormals(const double*        V,
+                           int64_t              nv,
+                           const int64_t*       off,
+                           const int32_t*       idx,
+                           int64_t              nf,
+                           std::vector<double>& faceN,
+                           std::vector<double>& centroid,
+                           std::vector<double>& cornerVN,
+                           std::vector<double>& edgeN,
+                           std::string&         msg)
+{
+  const int64_t nc = off[nf];
+  faceN.assign(3 * nf, 0.0);
+  centroid.assign(3 * nf, 0.0);
+  cornerVN.assign(3 * nc, 0.0);
+  edgeN.assign(3 * nc, 0.0);
+  auto vx = [&](int64_t corner) { return ld3(V + 3 * int64_t(idx[corner])); };
+
+  // face normal: (x2 - x0) x (x2 - x1) of the first vertex triple (i, i+1, i+2) that spans a plane,
+  // normalised twice (FaceT::computeNormal, then reconcile's normalizeNormalVector); centroid: the
+  // vertex sum times 1/N (DCEL_FaceImplem.hpp:71-79,121-166)
+  bool degenerate = false;
+#pragma omp parallel for schedule(static) reduction(|| : degenerate)
+  for (int64_t f = 0; f < nf; f++) {
+    const int64_t b = off[f], N = off[f + 1] - off[f];
+    V3            c{0, 0, 0};
+    double        l = 0;
+    for (int64_t i = 0; i < N; i++) {
+      const V3 x0 = vx(b + i), x1 = vx(b + (i + 1) % N), x2 = vx(b + (i + 2) % N);
+      c = cross(sub(x2, x0), sub(x2, x1));
+      l = len(c);
+      if (l > 0.0) {
+        break;
+      }
+    }
+    if (!(l > 0.0)) {
+      degenerate = true;
+      continue;
+    }
+    const V3 once = divs(c, l);
+    st3(&faceN[3 * f], divs(once, len(once)));
+    V3 s{0, 0, 0};
+    for (int64_t i = 0; i < N; i++) {
+      const V3 x = vx(b + i);
+      s          = {s.x + x.x, s.y + x.y, s.z + x.z};
+    }
+    st3(&centroid[3 * f], divs(s, double(N)));
+  }
+  if (degenerate) {
+    msg = "degenerate face (no three vertices span a plane)";
+    return false;
+  }
+
+  // faces around each vertex in facet order (soupToDCEL adds them facet by facet)
+  std::vector<int64_t> start(nv + 1, 0);
+  for (int64_t i = 0; i < nc; i++) {
+    start[int64_t(idx[i]) + 1]++;
+  }
+  for (int64_t v = 0; v < nv; v++) {
+    start[v + 1] += start[v];
+  }
+  std::vector<int64_t> fill(start.begin(), start.end() - 1);
+  std::vector<int64_t> around(nc); // entries: the corner
+  std::vector<int64_t> faceOf(nc);
+  for (int64_t f = 0; f < nf; f++) {
+    for (int64_t k = off[f]; k < off[f + 1]; k++) {
+      around[fill[idx[k]]++] = k;
+      faceOf[k]              = f;
+    }
+  }
+
+  // edge normals: the pair of half-edge (a -> b) is a half-edge (b -> a) of a face around a
+  // (Soup::reconcilePairEdgesDCEL, SoupImplem.hpp:229-262); normalize(n_face + n_pair)
+  bool nonManifold = false;
+#pragma omp parallel for schedule(static) reduction(|| : nonManifold)
+  for (int64_t f = 0; f < nf; f++) {
+    const int64_t b = off[f], N = off[f + 1] - off[f];
+    for (int64_t i = 0; i < N; i++) {
+      const int32_t a = idx[b + i], e = idx[b + (i + 1) % N];
+      int64_t       pair = -1, found = 0;
+      for (int64_t s2 = start[a]; s2 < start[a + 1]; s2++) {
+        const int64_t g = faceOf[around[s2]];
+        const int64_t gb = off[g], gn = off[g + 1] - off[g];
+        for (int64_t j = 0; j < gn; j++) {
+          if (idx[gb + j] == e && idx[gb + (j + 1) % gn] == a) {
+            found++;
+            pair = g;
+          }
+        }
+      }
+      if (found > 1) {
+        nonManifold = true;
+      }
+      V3 n = ld3(&faceN[3 * f]);
+      if (pair >= 0) {
+        n = {n.x + faceN[3 * pair], n.y + faceN[3 * pair + 1], n.z + faceN[3 * pair + 2]};
+      }
+      const double l = len(n);
+      st3(&edgeN[3 * (b + i)], (l > std::numeric_limits<double>::epsilon()) ? divs(n, l) : V3{0, 0, 0});
+    }
+  }
+  if (nonManifold) {
+    msg = "non-manifold edge (shared by more than two faces)";
+    return false;
+  }
+
+  // angle-weighted vertex normals: the angle at each corner between its two neighbours in the
+  // face's loop, alpha * n_face summed over the vertex's faces in facet order, then normalised
+  std::vector<double> contrib(3 * nc);
+#pragma omp parallel for schedule(static)
+  for (int64_t f = 0; f < nf; f++) {
+    const int64_t b = off[f], N = off[f + 1] - off[f];
+    const V3      fn = ld3(&faceN[3 * f]);
+    for (int64_t k = 0; k < N; k++) {
+      const V3 x0 = vx(b + k);
+      V3       e1 = sub(vx(b + (k + N - 1) % N), x0);
+      V3       e2 = sub(vx(b + (k + 1) % N), x0);
+      e1          = divs(e1, len(e1));
+      e2          = divs(e2, len(e2));
+      const double alpha = std::acos(std::clamp(dot(e1, e2), -1.0, 1.0));
+      contrib[3 * (b + k) + 0] = alpha * fn.x;
+      contrib[3 * (b + k) + 1] = alpha * fn.y;
+      contrib[3 * (b + k) + 2] = alpha * fn.z;
+    }
+  }
+  std::vector<double> vn(3 * nv, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t v = 0; v < nv; v++) {
+    double x = 0.0, y = 0.0, z = 0.0;
+    for (int64_t e = start[v]; e < start[v + 1]; e++) {
+      const double* c = &contrib[3 * around[e]];
+      x += c[0];
+      y += c[1];
+      z += c[2];
+    }
+    const V3     n = {x, y, z};
+    const double l = len(n);
+    st3(&vn[3 * v], (l > std::numeric_limits<double>::epsilon()) ? divs(n, l) : n);
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < nc; k++) {
+    std::memcpy(&cornerVN[3 * k], &vn[3 * int64_t(idx[k])], 3 * sizeof(double));
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------------
 // 4-wide BVH build
 
 namespace {

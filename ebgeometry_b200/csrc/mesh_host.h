@@ -36,6 +36,22 @@ struct Bvh4
   double                lo[3], hi[3];
 };
 
+// The DCEL quantities of a polygon soup (faces: vertex lists idx[off[f] .. off[f+1]), each of at
+// least three distinct vertices), as the reference's soupToDCEL + reconcile computes them: per face
+// the DCEL normal (3) and centroid (3); per corner the vertex's pseudonormal (3) and the
+// pseudonormal of the edge from that corner to the next (3).  Returns false (with msg) on a face
+// whose vertices span no plane or an edge shared by more than two faces.
+bool computePolygonNormals(const double*        V,
+                           int64_t              nv,
+                           const int64_t*       off,
+                           const int32_t*       idx,
+                           int64_t              nf,
+                           std::vector<double>& faceN,
+                           std::vector<double>& centroid,
+                           std::vector<double>& cornerVN,
+                           std::vector<double>& edgeN,
+                           std::string&         msg);
+
 // Builds a 4-wide BVH over primitives given by FP64 boxes (lo/hi, 3 per primitive) and
 // centroids.  build: 0 = binned SAH, 1 = Morton.  leafSize: max primitives per leaf.
 bool buildBvh4(const std::vector<double>& boxLo,

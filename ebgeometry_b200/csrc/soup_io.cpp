@@ -13,8 +13,8 @@
 //   VTK  legacy ASCII POLYDATA: POINTS, then POLYGONS as count-prefixed lists or as OFFSETS /
 //        CONNECTIVITY arrays (:906-1645).
 // Vertex merging: the soup's positions are sorted lexicographically (x, then y, then z) and equal
-// positions become one vertex; facets keep their order.  Polygons of more than three vertices are
-// rejected (the mesh path takes triangles).
+// positions become one vertex; facets keep their order and their vertex count (a triangle mesh
+// takes triangles only; a polygon mesh takes any face of three or more vertices).
 #include <algorithm>
 #include <cctype>
 #include <cstdint>
@@ -30,8 +30,10 @@
 
 struct ebg_soup
 {
-  std::vector<double>  v; // 3 per vertex
-  std::vector<int32_t> f; // 3 per triangle
+  std::vector<double>  v;   // 3 per vertex
+  std::vector<int32_t> f;   // the faces' vertex indices, face after face
+  std::vector<int64_t> off; // face k is f[off[k] .. off[k + 1])
+  bool                 triangles = true;
 };
 
 namespace {
@@ -498,7 +500,7 @@ bool readVtk(const std::string& data, RawSoup& s, std::string& msg)
 }
 
 // ---- merging (Soup::compress) ---------------------------------------------------------------------
-bool compressToTriangles(const RawSoup& raw, ebg_soup& out, std::string& msg)
+bool compressSoup(const RawSoup& raw, ebg_soup& out, std::string& msg)
 {
   const int64_t nv = int64_t(raw.v.size() / 3);
   std::vector<int64_t> order(static_cast<size_t>(nv));
@@ -531,13 +533,15 @@ bool compressToTriangles(const RawSoup& raw, ebg_soup& out, std::string& msg)
   }
   out.f.clear();
   out.f.reserve(raw.f.size() * 3);
+  out.off.assign(1, 0);
+  out.triangles = true;
   for (size_t t = 0; t < raw.f.size(); t++) {
     const auto& facet = raw.f[t];
-    if (facet.size() != 3) {
-      msg = "face " + std::to_string(t) + " has " + std::to_string(facet.size()) +
-            " vertices: only triangle meshes are supported";
+    if (facet.size() < 3) {
+      msg = "face " + std::to_string(t) + " has fewer than three vertices";
       return false;
     }
+    out.triangles = out.triangles && facet.size() == 3;
     for (int64_t i : facet) {
       if (i < 0 || i >= nv) {
         msg = "face " + std::to_string(t) + " references vertex " + std::to_string(i) + " of " + std::to_string(nv);
@@ -545,6 +549,7 @@ bool compressToTriangles(const RawSoup& raw, ebg_soup& out, std::string& msg)
       }
       out.f.push_back(int32_t(remap[size_t(i)]));
     }
+    out.off.push_back(int64_t(out.f.size()));
   }
   return true;
 }
@@ -586,7 +591,7 @@ ebg_status ebg_soup_read(const char* path, ebg_soup** out)
     return ebg::setError(EBG_ERR_INVALID, std::string(path) + ": " + msg);
   }
   auto* s = new ebg_soup;
-  if (!compressToTriangles(raw, *s, msg)) {
+  if (!compressSoup(raw, *s, msg)) {
     delete s;
     return ebg::setError(EBG_ERR_INVALID, std::string(path) + ": " + msg);
   }
@@ -600,7 +605,7 @@ ebg_status ebg_soup_sizes(const ebg_soup* s, int64_t* num_vertices, int64_t* num
     return ebg::setError(EBG_ERR_INVALID, "null argument");
   }
   *num_vertices  = int64_t(s->v.size() / 3);
-  *num_triangles = int64_t(s->f.size() / 3);
+  *num_triangles = int64_t(s->off.size()) - 1;
   return EBG_OK;
 }
 
@@ -609,8 +614,33 @@ ebg_status ebg_soup_copy(const ebg_soup* s, double* vertices, int32_t* triangles
   if (s == nullptr || vertices == nullptr || triangles == nullptr) {
     return ebg::setError(EBG_ERR_INVALID, "null argument");
   }
+  if (!s->triangles) {
+    return ebg::setError(EBG_ERR_INVALID,
+                         "the file has faces of more than three vertices: read it with ebg_soup_copy_polygons "
+                         "(a triangle mesh takes triangles only)");
+  }
   std::memcpy(vertices, s->v.data(), s->v.size() * sizeof(double));
   std::memcpy(triangles, s->f.data(), s->f.size() * sizeof(int32_t));
+  return EBG_OK;
+}
+
+ebg_status ebg_soup_num_corners(const ebg_soup* s, int64_t* num_corners)
+{
+  if (s == nullptr || num_corners == nullptr) {
+    return ebg::setError(EBG_ERR_INVALID, "null argument");
+  }
+  *num_corners = int64_t(s->f.size());
+  return EBG_OK;
+}
+
+ebg_status ebg_soup_copy_polygons(const ebg_soup* s, double* vertices, int64_t* face_offsets, int32_t* face_vertices)
+{
+  if (s == nullptr || vertices == nullptr || face_offsets == nullptr || face_vertices == nullptr) {
+    return ebg::setError(EBG_ERR_INVALID, "null argument");
+  }
+  std::memcpy(vertices, s->v.data(), s->v.size() * sizeof(double));
+  std::memcpy(face_offsets, s->off.data(), s->off.size() * sizeof(int64_t));
+  std::memcpy(face_vertices, s->f.data(), s->f.size() * sizeof(int32_t));
   return EBG_OK;
 }
 
@@ -626,6 +656,12 @@ ebg_status ebg_mesh_create_from_file(const char* path, const ebg_build_opts* opt
   const ebg_status rc = ebg_soup_read(path, &s);
   if (rc != EBG_OK) {
     return rc;
+  }
+  if (!s->triangles) {
+    delete s;
+    return ebg::setError(EBG_ERR_INVALID, std::string(path) +
+                                              ": faces of more than three vertices (a triangle mesh takes triangles "
+                                              "only; ebg_polymesh_create_from_file takes polygons)");
   }
   const ebg_status rc2 = ebg_mesh_create(s->v.data(), int64_t(s->v.size() / 3), s->f.data(), int64_t(s->f.size() / 3),
                                          opts, out);

@@ -68,11 +68,21 @@ int main()
   PointCloudBVH::Hit one[4];
   same = same && pc.nearestNeighbors(77, 4, one) == 4 && one[0].index == nnB[77 * 4].index &&
          grid.nearestNeighbor(77).index == one[0].index;
+  // a unit cube of quad faces through the polygon-face MeshSDF and FlatMeshSDF
+  const std::vector<std::array<double, 3>> cv = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                                 {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  const std::vector<std::vector<int32_t>>  cf = {{0, 3, 2, 1}, {4, 5, 6, 7}, {0, 1, 5, 4},
+                                                 {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
+  PolygonMeshSDF     cube(cv, cf);
+  PolygonFlatMeshSDF cubeFlat(cv, cf);
+  const bool cubeOk = cube.value(Vec3(0.5, 0.5, 0.5)) == -0.5 && cube.value(Vec3(2.0, 0.5, 0.5)) == 1.0 &&
+                      cubeFlat.value(Vec3(0.5, 0.5, -1.0)) == 1.0;
   std::printf("batch/single max diff %.3g (FP64 batch: %.3g), centre %.6f (expect %.6f), nearest of point 123: "
-              "%zu (d2 %g), grid == BVH: %d\n",
-              maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared), int(same));
+              "%zu (d2 %g), grid == BVH: %d, quad cube: %d\n",
+              maxDiff, maxDiff64, centre, -1.0 / std::sqrt(3.0), hit.index, double(hit.distanceSquared), int(same),
+              int(cubeOk));
   const bool ok = maxDiff <= 1e-6 && maxDiff64 == 0.0 && maxDcel == 0.0 && std::fabs(centre + 1.0 / std::sqrt(3.0)) < 1e-12 &&
-                  hit.index == 123 && hit.distanceSquared == 0.f && same;
+                  hit.index == 123 && hit.distanceSquared == 0.f && same && cubeOk;
   std::printf("%s\n", ok ? "ok" : "FAILED");
   return ok ? 0 : 1;
 }

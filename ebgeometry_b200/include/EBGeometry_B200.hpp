@@ -206,6 +206,70 @@ public:
   }
 };
 
+// MeshSDF<double,short,K> over a DCEL of polygon faces (three or more vertices each; face f is
+// a_faces[f], counter-clockwise = outward).  The reference's DCEL normals and face algorithm, FP64.
+class PolygonMeshSDF : public ImplicitBase
+{
+public:
+  PolygonMeshSDF(const std::vector<std::array<double, 3>>& a_vertices, const std::vector<std::vector<int32_t>>& a_faces,
+                 Build a_build = Build::SAH, int a_leafSize = 4, int a_device = -1)
+  {
+    std::vector<int64_t> off(1, 0);
+    std::vector<int32_t> idx;
+    for (const auto& f : a_faces) {
+      idx.insert(idx.end(), f.begin(), f.end());
+      off.push_back(int64_t(idx.size()));
+    }
+    ebg_build_opts o{static_cast<int32_t>(a_build), a_leafSize, a_device, 0};
+    check(ebg_polymesh_create(&a_vertices[0][0], int64_t(a_vertices.size()), off.data(), idx.data(),
+                              int64_t(a_faces.size()), &o, &m_mesh));
+  }
+  // Parser::readIntoDCEL + MeshSDF: a .stl / .obj / .ply / .vtk file of any faces.
+  explicit PolygonMeshSDF(const std::string& a_file, Build a_build = Build::SAH, int a_leafSize = 4, int a_device = -1)
+  {
+    ebg_build_opts o{static_cast<int32_t>(a_build), a_leafSize, a_device, 0};
+    check(ebg_polymesh_create_from_file(a_file.c_str(), &o, &m_mesh));
+  }
+  PolygonMeshSDF(const PolygonMeshSDF&) = delete;
+  PolygonMeshSDF& operator=(const PolygonMeshSDF&) = delete;
+  ~PolygonMeshSDF() override { ebg_polymesh_destroy(m_mesh); }
+
+  double signedDistance(const Vec3& a_point) const noexcept override
+  {
+    const double p[3] = {x(a_point), y(a_point), z(a_point)};
+    double       d    = std::numeric_limits<double>::quiet_NaN();
+    return evalHost(p, 1, &d) == EBG_OK ? d : std::numeric_limits<double>::quiet_NaN();
+  }
+  // Batched, host buffers (xyz interleaved), synchronous.
+  void signedDistances(const double* a_pointsHost, size_t a_n, double* a_distHost) const
+  {
+    check(evalHost(a_pointsHost, int64_t(a_n), a_distHost));
+  }
+  const ebg_polymesh* handle() const noexcept { return m_mesh; }
+
+protected:
+  virtual ebg_status evalHost(const double* a_p, int64_t a_n, double* a_d) const
+  {
+    return ebg_polymesh_signed_distance_host(m_mesh, a_p, a_n, a_d, nullptr, nullptr);
+  }
+
+private:
+  ebg_polymesh* m_mesh = nullptr;
+};
+
+// FlatMeshSDF<double,short> over polygon faces: every face for every point.
+class PolygonFlatMeshSDF : public PolygonMeshSDF
+{
+public:
+  using PolygonMeshSDF::PolygonMeshSDF;
+
+protected:
+  ebg_status evalHost(const double* a_p, int64_t a_n, double* a_d) const override
+  {
+    return ebg_polymesh_signed_distance_flat_host(handle(), a_p, a_n, a_d, nullptr, nullptr);
+  }
+};
+
 // The learned pruning radius (trained on the device from the mesh's own exact distances).
 class SeedModel
 {

@@ -7,6 +7,11 @@ PCG64 generator, so the same seed gives the same arrays in every process.
   4-to-1 midpoint subdivision, vertices projected to the sphere; 20 * 4**level triangles) whose
   vertices are moved radially by a seeded sum of 8 sinusoids of total amplitude <= 0.08.  The
   result is watertight, with counter-clockwise (outward) triangles.
+* ``displaced_quad_sphere(n, seed)`` -- a cube subdivided into n x n quads per side, projected to
+  the sphere and displaced the same way (6 n^2 outward quads, slightly non-planar);
+  ``polygon_prism(k)`` -- a prism over a regular k-gon (two planar k-gon caps, k quads);
+  ``mixed_polygon_sphere(n, seed)`` -- the quad sphere with every other quad split into two
+  triangles.  Faces are (offsets, indices) pairs.
 * ``uniform_points``, ``grid_points`` (cell centres, x fastest), ``band_points`` (within +-w of the
   surface along the face normal, triangles drawn by area).
 * ``point_cloud`` -- half uniform in the unit cube, half from anisotropic Gaussian clusters.
@@ -65,6 +70,66 @@ def displaced_icosphere(level: int, seed: int, radius: float = 1.0, amplitude: f
     a, w, phi = radial_field(seed, 8, amplitude)
     r = 1.0 + (np.sin(v @ w.T + phi) * a).sum(axis=1)
     return (radius * r)[:, None] * v + np.asarray(center, np.float64), f
+
+
+def _cube_quads(n: int):
+    """Integer lattice points (coordinates in -n..n, step 2) and outward quads of a subdivided cube."""
+    key, verts, quads = {}, [], []
+
+    def vid(p):
+        if p not in key:
+            key[p] = len(verts)
+            verts.append(p)
+        return key[p]
+
+    # (axis, sign) -> in-plane axes (b, c) with e_b x e_c = sign * e_axis (counter-clockwise outside)
+    for a, s_, b, c in ((0, 1, 1, 2), (0, -1, 2, 1), (1, 1, 2, 0), (1, -1, 0, 2), (2, 1, 0, 1), (2, -1, 1, 0)):
+        for i in range(n):
+            for j in range(n):
+                q = []
+                for di, dj in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                    p = [0, 0, 0]
+                    p[a] = s_ * n
+                    p[b] = 2 * (i + di) - n
+                    p[c] = 2 * (j + dj) - n
+                    q.append(vid(tuple(p)))
+                quads.append(q)
+    return np.array(verts, np.float64), np.array(quads, np.int64)
+
+
+def displaced_quad_sphere(n: int, seed: int, radius: float = 1.0, amplitude: float = 0.08):
+    """Quad sphere with seeded radial displacement: (vertices (V,3), (offsets, indices))."""
+    v, q = _cube_quads(n)
+    u = v / np.linalg.norm(v, axis=1, keepdims=True)
+    a, w, phi = radial_field(seed, 8, amplitude)
+    r = 1.0 + (np.sin(u @ w.T + phi) * a).sum(axis=1)
+    off = np.arange(q.shape[0] + 1, dtype=np.int64) * 4
+    return (radius * r)[:, None] * u, (off, q.ravel().astype(np.int32))
+
+
+def mixed_polygon_sphere(n: int, seed: int):
+    """The displaced quad sphere with every other quad split into two triangles."""
+    v, (off, idx) = displaced_quad_sphere(n, seed)
+    faces = []
+    for k, qd in enumerate(idx.reshape(-1, 4)):
+        if k % 2:
+            faces += [[qd[0], qd[1], qd[2]], [qd[0], qd[2], qd[3]]]
+        else:
+            faces.append(list(qd))
+    counts = np.array([len(f) for f in faces], np.int64)
+    return v, (np.concatenate([[0], np.cumsum(counts)]).astype(np.int64),
+               np.concatenate(faces).astype(np.int32))
+
+
+def polygon_prism(k: int, radius: float = 1.0, height: float = 1.0):
+    """A prism over a regular k-gon, centred at the origin: two k-gon caps and k side quads."""
+    t = 2.0 * np.pi * np.arange(k) / k
+    ring = np.stack([radius * np.cos(t), radius * np.sin(t)], 1)
+    v = np.concatenate([np.c_[ring, np.full(k, -0.5 * height)], np.c_[ring, np.full(k, 0.5 * height)]])
+    faces = [list(range(k - 1, -1, -1)), list(range(k, 2 * k))]
+    faces += [[i, (i + 1) % k, k + (i + 1) % k, k + i] for i in range(k)]
+    counts = np.array([len(f) for f in faces], np.int64)
+    return v, (np.concatenate([[0], np.cumsum(counts)]).astype(np.int64), np.concatenate(faces).astype(np.int32))
 
 
 def uniform_points(n: int, seed: int, lo=-1.5, hi=1.5) -> np.ndarray:

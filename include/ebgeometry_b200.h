@@ -61,6 +61,7 @@ typedef struct ebg_build_opts
 } ebg_build_opts;
 
 typedef struct ebg_soup  ebg_soup;
+typedef struct ebg_polymesh ebg_polymesh;
 typedef struct ebg_mesh  ebg_mesh;
 typedef struct ebg_cloud ebg_cloud;
 typedef struct ebg_grid  ebg_grid;
@@ -196,15 +197,68 @@ ebg_status ebg_mesh_refit_device(ebg_mesh* mesh, const double* vertices_dev, int
  * (ParserImplem.hpp:1752-1800) for .stl (ASCII or binary), .obj, .ply (ascii or binary, either byte
  * order) and legacy ASCII .vtk POLYDATA, with the reference's rules for which triangles a file
  * yields, then its vertex merging (Soup::compress, SoupImplem.hpp:78-145: equal positions become
- * one vertex, vertices in lexicographic order, facets in file order).  Only triangle faces are
- * accepted.  ebg_soup_sizes / ebg_soup_copy hand the soup out (vertices 3 doubles, triangles 3
- * int32 per entry). */
+ * one vertex, vertices in lexicographic order, facets in file order).  Faces keep their vertex
+ * count.  ebg_soup_sizes gives the vertex and face counts; ebg_soup_copy hands a triangle soup out
+ * (vertices 3 doubles, triangles 3 int32; EBG_ERR_INVALID when some face is not a triangle);
+ * ebg_soup_copy_polygons hands any soup out as face offsets (num_faces + 1 int64, starting at 0)
+ * into a list of ebg_soup_num_corners vertex indices. */
 ebg_status ebg_soup_read(const char* path, ebg_soup** soup);
-ebg_status ebg_soup_sizes(const ebg_soup* soup, int64_t* num_vertices, int64_t* num_triangles);
+ebg_status ebg_soup_sizes(const ebg_soup* soup, int64_t* num_vertices, int64_t* num_faces);
 ebg_status ebg_soup_copy(const ebg_soup* soup, double* vertices, int32_t* triangles);
+ebg_status ebg_soup_num_corners(const ebg_soup* soup, int64_t* num_corners);
+ebg_status ebg_soup_copy_polygons(const ebg_soup* soup, double* vertices, int64_t* face_offsets, int32_t* face_vertices);
 ebg_status ebg_soup_destroy(ebg_soup* soup);
 /* Parser::readIntoTriangleBVH (ParserImplem.hpp:1893-1903): read + merge + ebg_mesh_create. */
 ebg_status ebg_mesh_create_from_file(const char* path, const ebg_build_opts* opts, ebg_mesh** mesh);
+
+/* ---- meshes of polygon faces: MeshSDF / FlatMeshSDF over a DCEL of any faces -------------------
+ *
+ * ebg_polymesh_create replaces Soup::soupToDCEL + MeshSDF<double, Meta, 4>(mesh, build)
+ * (SoupImplem.hpp:149-227, MeshDistanceFunctionsImplem.hpp:249-295) for faces of three or more
+ * vertices: face f is face_vertices[face_offsets[f] .. face_offsets[f + 1]) (counter-clockwise =
+ * outward; no vertex twice in one face).  The DCEL quantities are the reference's (face normal from
+ * the first vertex triple that spans a plane, centroid, angle-weighted vertex and edge
+ * pseudonormals); the 4-wide tree (opts: SAH or Morton, leaf_size default 4) is built on the host.
+ * Queries are FP64: the DCEL face algorithm (projection into the face plane, crossing-number inside
+ * test, else the nearest edge or vertex with its pseudonormal's sign).  closest_face (nullable)
+ * receives the winner's soup index.  A face whose vertices span no plane, or an edge of more than
+ * two faces: EBG_ERR_INVALID. */
+ebg_status ebg_polymesh_create(const double*         vertices,
+                               int64_t               num_vertices,
+                               const int64_t*        face_offsets,
+                               const int32_t*        face_vertices,
+                               int64_t               num_faces,
+                               const ebg_build_opts* opts,
+                               ebg_polymesh**        out);
+/* Host-only: the DCEL quantities ebg_polymesh_create computes (no device needed), in soup order
+ * as ebg_polymesh_get_normals gives them.  Any output may be null. */
+ebg_status ebg_compute_polygon_normals(const double* vertices, int64_t num_vertices, const int64_t* face_offsets,
+                                       const int32_t* face_vertices, int64_t num_faces, double* face_normals,
+                                       double* centroids, double* corner_vertex_normals, double* edge_normals);
+/* Parser::readIntoDCEL + MeshSDF: read + merge (polygon faces kept) + ebg_polymesh_create. */
+ebg_status ebg_polymesh_create_from_file(const char* path, const ebg_build_opts* opts, ebg_polymesh** out);
+ebg_status ebg_polymesh_destroy(ebg_polymesh* mesh);
+/* info->num_triangles holds the face count; num_corners (nullable) the number of face corners. */
+ebg_status ebg_polymesh_get_info(const ebg_polymesh* mesh, ebg_mesh_info* info, int64_t* num_corners);
+/* The DCEL quantities in soup order: per face normal (3) and centroid (3); per corner (face after
+ * face) the vertex pseudonormal (3) and the pseudonormal of the edge to the next corner (3).  Any
+ * output may be null. */
+ebg_status ebg_polymesh_get_normals(const ebg_polymesh* mesh, double* face_normals, double* centroids,
+                                    double* corner_vertex_normals, double* edge_normals);
+/* MeshSDF::signedDistance (MeshDistanceFunctionsImplem.hpp:269-295) for n FP64 points; device
+ * arrays, asynchronous on stream. */
+ebg_status ebg_polymesh_signed_distance(const ebg_polymesh* mesh, const double* points_dev, int64_t n,
+                                        double* out_dev, int32_t* closest_face_dev, void* stream);
+ebg_status ebg_polymesh_signed_distance_host(const ebg_polymesh* mesh, const double* points_host, int64_t n,
+                                             double* out_host, int32_t* closest_face_host, void* stream);
+/* FlatMeshSDF::signedDistance (MeshDistanceFunctionsImplem.hpp:219-229, DCEL_MeshImplem.hpp:574-595):
+ * every face for every point; the first face in soup order with the smallest unsigned distance. */
+ebg_status ebg_polymesh_signed_distance_flat(const ebg_polymesh* mesh, const double* points_dev, int64_t n,
+                                             double* out_dev, int32_t* closest_face_dev, void* stream);
+ebg_status ebg_polymesh_signed_distance_flat_host(const ebg_polymesh* mesh, const double* points_host, int64_t n,
+                                                  double* out_host, int32_t* closest_face_host, void* stream);
+/* Synchronises stream; reports a non-finite query point (EBG_ERR_INVALID) or a traversal bound. */
+ebg_status ebg_polymesh_check_status(const ebg_polymesh* mesh, void* stream);
 ebg_status ebg_mesh_get_info(const ebg_mesh* mesh, ebg_mesh_info* info);
 
 /* Pseudonormals the handle computed (per triangle: face normal 3, vertex normals 9, edge normals 9

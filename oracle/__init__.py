@@ -63,6 +63,9 @@ class _Ref:
         sig = {
             "ref_omp_max_threads": (C.c_int, []),
             "ref_mesh_create": (_P, [_P, _I64, _P, _I64, C.c_int, C.c_int, C.c_int]),
+            "ref_polymesh_create": (_P, [_P, _I64, _P, _P, _I64, C.c_int]),
+            "ref_polymesh_normals": (C.c_int, [_P, _P, _P, _P, _P]),
+            "ref_read_polysoup": (C.c_int, [C.c_char_p, _P, _P, _P, _P, _P, _P]),
             "ref_mesh_destroy": (None, [_P]),
             "ref_mesh_sdf": (C.c_int, [_P, _P, _I64, _P, C.c_int, C.c_int]),
             "ref_mesh_value1": (_D, [_P, _D, _D, _D]),
@@ -131,6 +134,38 @@ class _Ref:
 
     def mesh(self, v, f, kind=0, build=0, max_leaf_groups=4):
         return _Ref.Mesh(self, v, f, kind, build, max_leaf_groups)
+
+    class PolyMesh(Mesh):
+        """Reference MeshSDF<double,short,4> and FlatMeshSDF over a polygon soup (faces: offsets,
+        indices).  sdf(p, dcel=True) is the MeshSDF, sdf(p, flat=True) the FlatMeshSDF."""
+
+        def __init__(self, ref, v, off, idx, build=0):
+            self.ref = ref
+            self.v = np.ascontiguousarray(v, np.float64)
+            self.off = np.ascontiguousarray(off, np.int64)
+            self.idx = np.ascontiguousarray(idx, np.int64)
+            self.h = ref.lib.ref_polymesh_create(_ptr(self.v), self.v.shape[0], _ptr(self.off), _ptr(self.idx),
+                                                 self.off.size - 1, build)
+
+        def polygon_normals(self):
+            nf, nc = self.off.size - 1, self.idx.size
+            fn, c, vn, en = np.empty((nf, 3)), np.empty((nf, 3)), np.empty((nc, 3)), np.empty((nc, 3))
+            assert self.ref.lib.ref_polymesh_normals(self.h, _ptr(fn), _ptr(c), _ptr(vn), _ptr(en)) == 0
+            return fn, c, vn, en
+
+    def polymesh(self, v, off, idx, build=0):
+        return _Ref.PolyMesh(self, v, off, idx, build)
+
+    def read_polysoup(self, path):
+        nv, nf, nc = (C.c_int64(), C.c_int64(), C.c_int64())
+        assert self.lib.ref_read_polysoup(str(path).encode(), None, C.byref(nv), None, None, C.byref(nf),
+                                          C.byref(nc)) == 0
+        v = np.empty((nv.value, 3))
+        off = np.empty(nf.value + 1, np.int64)
+        idx = np.empty(nc.value, np.int64)
+        assert self.lib.ref_read_polysoup(str(path).encode(), _ptr(v), C.byref(nv), _ptr(off), _ptr(idx),
+                                          C.byref(nf), C.byref(nc)) == 0
+        return v, off, idx
 
     def triangle_sd(self, v, vn, en, p) -> float:
         a = [np.ascontiguousarray(x, np.float64).ravel() for x in (v, vn, en, p)]

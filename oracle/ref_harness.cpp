@@ -19,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <memory>
 #include <random>
 #include <string>
@@ -60,6 +61,25 @@ makeMesh(const double* V, int64_t nv, const int64_t* F, int64_t nf)
   std::vector<std::vector<size_t>> facets(nf);
   for (int64_t f = 0; f < nf; f++) {
     facets[f] = {size_t(F[3 * f + 0]), size_t(F[3 * f + 1]), size_t(F[3 * f + 2])};
+  }
+  auto mesh = std::make_shared<MeshD>();
+  Soup::soupToDCEL(*mesh, verts, facets, "oracle");
+  return mesh;
+}
+
+// The same from a polygon soup: face f is idx[off[f] .. off[f+1]).
+std::shared_ptr<MeshD>
+makePolyMesh(const double* V, int64_t nv, const int64_t* off, const int64_t* idx, int64_t nf)
+{
+  std::vector<Vec3d> verts(nv);
+  for (int64_t i = 0; i < nv; i++) {
+    verts[i] = Vec3d(V[3 * i + 0], V[3 * i + 1], V[3 * i + 2]);
+  }
+  std::vector<std::vector<size_t>> facets(nf);
+  for (int64_t f = 0; f < nf; f++) {
+    for (int64_t k = off[f]; k < off[f + 1]; k++) {
+      facets[f].push_back(size_t(idx[k]));
+    }
   }
   auto mesh = std::make_shared<MeshD>();
   Soup::soupToDCEL(*mesh, verts, facets, "oracle");
@@ -111,6 +131,89 @@ ref_mesh_create(const double* V, int64_t nv, const int64_t* F, int64_t nf, int a
   }
   h->flat = std::make_shared<FlatMeshSDF<double, short>>(h->mesh);
   return h;
+}
+
+// MeshSDF<double, short, 4> (a_build) and FlatMeshSDF<double, short> over a polygon soup; query
+// them with ref_mesh_sdf (a_which 2 and 1).
+void*
+ref_polymesh_create(const double* V, int64_t nv, const int64_t* off, const int64_t* idx, int64_t nf, int a_build)
+{
+  auto* h = new RefMesh;
+  h->mesh = makePolyMesh(V, nv, off, idx, nf);
+  h->dcel = std::make_shared<MeshSDF<double, short, 4>>(h->mesh, buildOf(a_build));
+  h->flat = std::make_shared<FlatMeshSDF<double, short>>(h->mesh);
+  return h;
+}
+
+// The DCEL quantities of a mesh in face order: normal and centroid per face; per corner in
+// gatherVertices() order the vertex normal, and in gatherEdges() order the half-edge normal.
+int
+ref_polymesh_normals(void* a_h, double* faceN, double* centroid, double* vertN, double* edgeN)
+{
+  auto*       h     = static_cast<RefMesh*>(a_h);
+  const auto& faces = h->mesh->getFaces();
+  int64_t     at    = 0;
+  for (size_t f = 0; f < faces.size(); f++) {
+    const auto& n = faces[f]->getNormal();
+    const auto& c = faces[f]->getCentroid();
+    for (int a = 0; a < 3; a++) {
+      faceN[3 * f + a]    = n[a];
+      centroid[3 * f + a] = c[a];
+    }
+    const auto verts = faces[f]->gatherVertices();
+    const auto edges = faces[f]->gatherEdges();
+    for (size_t k = 0; k < verts.size(); k++, at++) {
+      const auto& vn = verts[k]->getNormal();
+      const auto& en = edges[k]->getNormal();
+      for (int a = 0; a < 3; a++) {
+        vertN[3 * at + a] = vn[a];
+        edgeN[3 * at + a] = en[a];
+      }
+    }
+  }
+  return 0;
+}
+
+// Parser::readIntoDCEL of a file of any faces: vertices, face offsets and vertex indices.  Call
+// with null buffers first for the counts.
+int
+ref_read_polysoup(const char* a_file, double* V, int64_t* nv, int64_t* off, int64_t* idx, int64_t* nf, int64_t* nc)
+{
+  auto mesh = Parser::readIntoDCEL<double, short>(std::string(a_file));
+  if (!mesh) {
+    return -1;
+  }
+  const auto& verts = mesh->getVertices();
+  const auto& faces = mesh->getFaces();
+  std::map<const void*, int64_t> index;
+  for (size_t i = 0; i < verts.size(); i++) {
+    index[verts[i].get()] = int64_t(i);
+    if (V != nullptr) {
+      for (int c = 0; c < 3; c++) {
+        V[3 * i + c] = verts[i]->getPosition()[c];
+      }
+    }
+  }
+  int64_t at = 0;
+  if (off != nullptr) {
+    off[0] = 0;
+  }
+  for (size_t f = 0; f < faces.size(); f++) {
+    const auto fv = faces[f]->gatherVertices();
+    for (const auto& v : fv) {
+      if (idx != nullptr) {
+        idx[at] = index[v.get()];
+      }
+      at++;
+    }
+    if (off != nullptr) {
+      off[f + 1] = at;
+    }
+  }
+  *nv = int64_t(verts.size());
+  *nf = int64_t(faces.size());
+  *nc = at;
+  return 0;
 }
 
 void

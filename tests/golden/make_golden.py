@@ -25,6 +25,10 @@ It builds nothing but the oracle (``make -C oracle``) and writes small .npz file
   (k = 1, 8) and allNearestNeighbors (k = 1, 5); its edge-case clouds (a planar cloud, a cluster with
   a distant outlier, 16 coincident points, cell-size targets 1e-6 and 1000) with allNearestNeighbors
   (k = 1).  Indices are the reference's own (ties in its visiting order).
+* ``polygons.npz``       -- polygon meshes (a heptagonal prism, a displaced 4x4 quad sphere, a 6x6
+  quad sphere with every other quad split into triangles) with the reference's DCEL normals
+  (soupToDCEL) and its MeshSDF<double,short,4> (SAH) and FlatMeshSDF values at 1000 points each
+  (uniform, plus points near the faces).
 * ``csg_small.npz``      -- a union of 40 spheres and 3 posed displaced icospheres evaluated by the
   reference's BVHUnion over Translate(Rotate(TriMeshSDF)) and SphereSDF at 1000 points.
 """
@@ -135,6 +139,29 @@ def main(reference: str) -> None:
              self1=gs1, selfd1=gt1, self5=gs5, selfd5=gt5, planar=planar, planar1=ps1, planard1=pt1,
              outlier=outl, outlier1=os1, outlierd1=ot1, coincident=coinc, coincident1=cs1,
              coincidentd1=ct1, c800=c800, tiny1=tiny1, tinyd1=tinyd1, huge1=huge1, huged1=huged1)
+
+    # --- polygon meshes (MeshSDF / FlatMeshSDF over DCEL polygon faces) --------------------------------
+    out = {}
+    for name, (pv, (off, idx)) in (("prism", W.polygon_prism(7)), ("quad", W.displaced_quad_sphere(4, 3)),
+                                   ("mixed", W.mixed_polygon_sphere(6, 5))):
+        rng = np.random.default_rng(len(name))
+        pts = [rng.uniform(-1.6, 1.6, (700, 3))]
+        # near the faces: a random convex combination of a face's vertices, moved along its normal
+        pm = R.polymesh(pv, off, idx)
+        fn, _, _, _ = pm.polygon_normals()
+        fsel = rng.integers(0, off.size - 1, 300)
+        near = []
+        for f in fsel:
+            cv = pv[idx[off[f]:off[f + 1]]]
+            w = rng.dirichlet(np.ones(len(cv)))
+            near.append(w @ cv + rng.uniform(-1e-3, 1e-3) * fn[f])
+        pts.append(np.array(near))
+        pq = np.concatenate(pts)
+        fnn, cen, vn, en = pm.polygon_normals()
+        out.update({f"{name}_v": pv, f"{name}_off": off, f"{name}_idx": idx, f"{name}_p": pq,
+                    f"{name}_ref": pm.sdf(pq, dcel=True), f"{name}_flat": pm.sdf(pq, flat=True),
+                    f"{name}_face_n": fnn, f"{name}_centroid": cen, f"{name}_vert_n": vn, f"{name}_edge_n": en})
+    np.savez(os.path.join(HERE, "polygons.npz"), **out)
 
     # --- small CSG union --------------------------------------------------------------------------------
     sc = W.csg_scene(77, n_spheres=40, n_meshes=3, levels=(1, 3), mesh_radius=(0.15, 0.3))
