@@ -147,7 +147,7 @@ class TriMeshSDF:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_mesh_destroy(h)
             self._h = None
 
@@ -355,7 +355,7 @@ class PolygonMeshSDF:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_polymesh_destroy(h)
             self._h = None
 
@@ -432,7 +432,7 @@ class PointCloudBVH:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_cloud_destroy(h)
             self._h = None
 
@@ -537,7 +537,7 @@ class PointCloudHashGrid:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_grid_destroy(h)
             self._h = None
 
@@ -663,7 +663,7 @@ class SeedModel:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_seed_destroy(h)
             self._h = None
 
@@ -731,7 +731,7 @@ class BVHUnion:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.ebg_scene_destroy(h)
             self._h = None
 

@@ -268,6 +268,9 @@ ebg_status buildMesh(const double*         V,
   if (build != EBG_BUILD_SAH && build != EBG_BUILD_MORTON) {
     return setError(EBG_ERR_INVALID, "unknown build method");
   }
+  if (leafSize > int(EBG_MAX_LEAF)) {
+    return setError(EBG_ERR_INVALID, "leaf_size must be at most " + std::to_string(EBG_MAX_LEAF));
+  }
   DeviceGuard guard;
   if (device >= 0) {
     if (cudaSetDevice(device) != cudaSuccess) {

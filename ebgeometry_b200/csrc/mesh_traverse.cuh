@@ -83,6 +83,15 @@ __device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, cons
 
 __device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
 
+// Quotients by a leaf's triangle count c (1..32) without integer division: 32 / c, and
+// ceil(4096 / c), with which (a * ceil(4096 / c)) >> 12 == a / c for every 0 <= a < 64.
+static __constant__ uint16_t c_lanesPer[33] = {0, 32, 16, 10, 8, 6, 5, 4, 4, 3, 3, 2, 2, 2, 2, 2, 2,
+                                               1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+static __constant__ uint16_t c_recip12[33] = {0,   4096, 2048, 1366, 1024, 820, 683, 586, 512, 456, 410,
+                                              373, 342,  316,  293,  274,  256, 241, 228, 216, 205, 196,
+                                              187, 179,  171,  164,  158,  152, 147, 142, 137, 133, 128};
+__device__ __forceinline__ int divSmall(int a, int c) { return (a * int(c_recip12[c])) >> 12; }
+
 // Squared distance from p to an oriented box (EbgObb as four float4: n|dn, u|du, v|dv, h), scaled
 // down by 4e-6 relative.  The FP32 error of each plane distance n . p - dn is about 1e-7 of |p|,
 // which the padding of the half-extents (2e-6 of the mesh's extent) covers near the mesh and the
@@ -150,6 +159,8 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
                                              TraversalCounters& cnt_)
 {
   const int lane = threadIdx.x & 31;
+      // a finite bound keeps empty child slots (infinite box distance) off the stack
+      best = fminf(best, FLT_MAX);
       int sp = 1;
       if (lane == 0) {
         stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
@@ -192,8 +203,8 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           // lanes per pass, instead of every lane testing every triangle.  A pass costs about two
           // triangle tests, so this runs when it needs fewer passes than cnt - 1.
           const int nNeed  = __popc(needMask);
-          const int lpp    = 32 / int(cnt);
-          const int passes = (nNeed + lpp - 1) / lpp;
+          const int lpp    = int(c_lanesPer[cnt]);
+          const int passes = divSmall(nNeed + lpp - 1, lpp);
           if (STATS && needObb) {
             cnt_.leaf++;
             cnt_.tri += cnt;
@@ -208,7 +219,7 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
               pts[rank] = make_float4(px, py, pz, 0.f);
             }
             __syncwarp();
-            const int     li = lane / int(cnt), ti = lane - li * int(cnt);
+            const int     li = divSmall(lane, int(cnt)), ti = lane - li * int(cnt);
             const float4* h  = reinterpret_cast<const float4*>(m.hot + t0 + uint32_t(ti));
 #pragma unroll 1
             for (int ps = 0; ps < passes; ps++) {
@@ -299,8 +310,8 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             // lanes that ruled the node out cannot gain from its children
             const float dk = needN ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz)
                                    : __int_as_float(0x7f800000);
-            // an empty slot (child 0, count 0: node 0 is the root, never a child) is never pushed
-            const bool  nk = __any_sync(FULL, dk <= best) && (cref[k] | ccnt[k]) != 0u;
+            // an empty slot (child 0, count 0) has an empty box, at +inf: never within the finite bound
+            const bool  nk = __any_sync(FULL, dk <= best);
             // uniform ordering key: the child's smallest distance over the packet's lanes (one
             // warp min-reduction; non-negative floats order like their bit patterns); children
             // nobody needs get -1 and are not pushed
