@@ -277,8 +277,6 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
           const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
           const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
-          const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
-          const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
           // lanes for which the node's own oriented box (all triangles below it) is within bound
           bool needN = need;
           if (cntw & EBG_NODE_HAS_OBB) {
@@ -303,7 +301,6 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
                       clz[4] = {lz.x, lz.y, lz.z, lz.w};
           const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
                       chz[4] = {hz.x, hz.y, hz.z, hz.w};
-          const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
           float key[4];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
@@ -323,7 +320,9 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             break;
           }
           // lane k (< 4) writes child k straight into its slot: farther children sit deeper, so the
-          // nearest is popped first; ties go by slot index (a total order, so slots are distinct)
+          // nearest is popped first; ties go by slot index (a total order, so slots are distinct).
+          // The child's box and words come again from the node's line (an L1 hit), which is cheaper
+          // than selecting them out of the registers.
           if (lane < 4) {
             const float kk = sel4(key, lane);
             if (kk >= 0.f) {
@@ -332,9 +331,10 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
               for (int j = 0; j < 4; j++) {
                 rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
               }
-              float4* e = stk + 2 * (sp + rank);
-              e[0]      = make_float4(sel4(clx, lane), sel4(cly, lane), sel4(clz, lane), __uint_as_float(sel4u(cref, lane)));
-              e[1]      = make_float4(sel4(chx, lane), sel4(chy, lane), sel4(chz, lane), __uint_as_float(sel4u(ccnt, lane)));
+              const float* nf = reinterpret_cast<const float*>(nd) + lane;
+              float4*      e  = stk + 2 * (sp + rank);
+              e[0]            = make_float4(__ldg(nf), __ldg(nf + 4), __ldg(nf + 8), __ldg(nf + 24));
+              e[1]            = make_float4(__ldg(nf + 12), __ldg(nf + 16), __ldg(nf + 20), __ldg(nf + 28));
             }
           }
           sp += np;
