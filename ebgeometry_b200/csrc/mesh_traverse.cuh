@@ -234,9 +234,12 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
                 dd = triDist2<false>(h0, h1, h2, q.x, q.y, q.z, s, t, r);
               }
               // minimum of (d2, triangle) over the cnt threads serving one lane; the first thread
-              // of the segment ends with it
+              // of the segment ends with it (offsets of cnt or more reach no segment partner)
 #pragma unroll
               for (int off = 16; off > 0; off >>= 1) {
+                if (off >= int(cnt)) {
+                  continue;
+                }
                 const float od = __shfl_down_sync(FULL, dd, off);
                 const int   oi = __shfl_down_sync(FULL, bi, off);
                 if (ti + off < int(cnt) && (od < dd || (od == dd && oi < bi))) {
