@@ -238,12 +238,16 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
       py = __ldg(a.queries + 3 * size_t(id) + 1);
       pz = __ldg(a.queries + 3 * size_t(id) + 2);
     }
-    float    kd[K];
-    uint32_t ki[K];
+    // The k best sit in the LAST k of the K slots, in (d2, index) order, so slot K - 1 is the k-th
+    // best (the pruning bound); the first K - k slots hold d2 = -1, below any distance, and never
+    // move.  Unfilled slots are +inf: every finite point beats them.
+    const int pad = K - a.k;
+    float     kd[K];
+    uint32_t  ki[K];
 #pragma unroll
     for (int j = 0; j < K; j++) {
-      kd[j] = __int_as_float(0x7f800000);  // +inf: every finite point beats it
-      ki[j] = 0xffffffffu;
+      kd[j] = j < pad ? -1.f : __int_as_float(0x7f800000);
+      ki[j] = j < pad ? 0u : 0xffffffffu;
     }
     uint32_t iters = 0;
     int      err   = 0;
@@ -324,18 +328,12 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
             for (int j = 0; j < 4; j++) {
               rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
             }
-            const int k   = lane;
-            float4*   e   = stk + 2 * (sp + rank);
-            const float lxk = k == 0 ? clx[0] : (k == 1 ? clx[1] : (k == 2 ? clx[2] : clx[3]));
-            const float lyk = k == 0 ? cly[0] : (k == 1 ? cly[1] : (k == 2 ? cly[2] : cly[3]));
-            const float lzk = k == 0 ? clz[0] : (k == 1 ? clz[1] : (k == 2 ? clz[2] : clz[3]));
-            const float hxk = k == 0 ? chx[0] : (k == 1 ? chx[1] : (k == 2 ? chx[2] : chx[3]));
-            const float hyk = k == 0 ? chy[0] : (k == 1 ? chy[1] : (k == 2 ? chy[2] : chy[3]));
-            const float hzk = k == 0 ? chz[0] : (k == 1 ? chz[1] : (k == 2 ? chz[2] : chz[3]));
-            const uint32_t rk = k == 0 ? cref[0] : (k == 1 ? cref[1] : (k == 2 ? cref[2] : cref[3]));
-            const uint32_t nn = k == 0 ? ccnt[0] : (k == 1 ? ccnt[1] : (k == 2 ? ccnt[2] : ccnt[3]));
-            e[0] = make_float4(lxk, lyk, lzk, __uint_as_float(rk));
-            e[1] = make_float4(hxk, hyk, hzk, __uint_as_float(nn));
+            // the child's box and words again from the node's line (an L1 hit), cheaper than
+            // selecting them out of the registers
+            const float* nf = reinterpret_cast<const float*>(nd) + lane;
+            float4*      e  = stk + 2 * (sp + rank);
+            e[0]            = make_float4(__ldg(nf), __ldg(nf + 4), __ldg(nf + 8), __ldg(nf + 24));
+            e[1]            = make_float4(__ldg(nf + 12), __ldg(nf + 16), __ldg(nf + 20), __ldg(nf + 28));
           }
         }
         sp += np;
@@ -351,10 +349,11 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
     if (valid) {
 #pragma unroll
       for (int j = 0; j < K; j++) {
-        if (j < a.k) {
-          const bool found = ki[j] != 0xffffffffu;
-          a.out_idx[size_t(id) * a.k + j] = found ? int32_t(ki[j]) : -1;
-          a.out_d2[size_t(id) * a.k + j]  = found ? kd[j] : __int_as_float(0x7f800000);
+        if (j >= pad) {
+          const bool   found = ki[j] != 0xffffffffu;
+          const size_t o     = size_t(id) * a.k + (j - pad);
+          a.out_idx[o]       = found ? int32_t(ki[j]) : -1;
+          a.out_d2[o]        = found ? kd[j] : __int_as_float(0x7f800000);
         }
       }
     }
