@@ -271,9 +271,9 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
       }
       const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
       if (ref & EBG_LEAF_BIT) {
-        const uint32_t p0 = ref & ~EBG_LEAF_BIT;
-        for (uint32_t t = p0; t < p0 + cnt; ++t) {
-          const float4   q  = __ldg(c.points + t);
+        const uint32_t p0 = ref & ~EBG_LEAF_BIT, pe = p0 + cnt;
+        // one point into the sorted k-best list (lowest index on equal distances)
+        auto consider = [&](const float4 q) {
           const float    dd = d2exact(px - q.x, py - q.y, pz - q.z);
           const uint32_t ii = __float_as_uint(q.w);
           if ((!SELF || ii != self) && lexLess(dd, ii, kd[K - 1], ki[K - 1])) {
@@ -290,6 +290,26 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
                 ki[j - 1]         = ti;
               }
             }
+          }
+        };
+        if constexpr (K >= 4) {
+          // a longer insertion per point: four points' loads go out at a time
+          uint32_t t = p0;
+          for (; t + 4 <= pe; t += 4) {
+            const float4 q0 = __ldg(c.points + t), q1 = __ldg(c.points + t + 1), q2 = __ldg(c.points + t + 2),
+                         q3 = __ldg(c.points + t + 3);
+            consider(q0);
+            consider(q1);
+            consider(q2);
+            consider(q3);
+          }
+          for (; t < pe; ++t) {
+            consider(__ldg(c.points + t));
+          }
+        }
+        else {
+          for (uint32_t t = p0; t < pe; ++t) {
+            consider(__ldg(c.points + t));
           }
         }
       }
