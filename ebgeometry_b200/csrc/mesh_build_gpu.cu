@@ -451,175 +451,376 @@ __global__ void kRecords(const double* __restrict__ V, const int32_t* __restrict
   }
 }
 
-// 5b. oriented box of the triangles at sorted positions [first, end): one block per range.  The
-// same construction as the host build (area-weighted mean normal, in-plane principal axis, padded
-// extents) in FP64 block reductions.
-__device__ double blockSum(double v, double* red)
-{
-  for (int off = 16; off > 0; off >>= 1) {
-    v += __shfl_xor_sync(FULL, v, off);
-  }
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-    red[threadIdx.x >> 5] = v;
-  }
-  __syncthreads();
-  double s = 0.0;
-  for (int w = 0; w < int(blockDim.x >> 5); w++) {
-    s += red[w];
-  }
-  return s;
-}
-__device__ double blockMin(double v, double* red)
-{
-  for (int off = 16; off > 0; off >>= 1) {
-    v = fmin(v, __shfl_xor_sync(FULL, v, off));
-  }
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) {
-    red[threadIdx.x >> 5] = v;
-  }
-  __syncthreads();
-  double s = DBL_MAX;
-  for (int w = 0; w < int(blockDim.x >> 5); w++) {
-    s = fmin(s, red[w]);
-  }
-  return s;
-}
-__device__ double blockMax(double v, double* red) { return -blockMin(-v, red); }
+// 5b. oriented box of the triangles at sorted positions [first, end).  The same construction as
+// the host build (area-weighted mean normal, in-plane principal axis, padded extents) in FP64, in
+// three passes over the range's vertices: (1) normal sum, area and axis-aligned box; (2) in-plane
+// mean and covariance; (3) extents along the box's axes.  A range of at most SMALL_RANGE triangles
+// (every leaf, most nodes) is one warp's; a larger one is cut into CHUNK-triangle pieces spread over
+// blocks, whose partial results are combined per range in chunk order.  Every range's axis-aligned
+// box is kept too (the child boxes of a refit come from it).
+constexpr uint32_t SMALL_RANGE = 2048;
+constexpr uint32_t CHUNK       = 4096;
 
-__global__ void __launch_bounds__(128) kRangeObbs(const double* __restrict__ tri64, const uint32_t* __restrict__ rFirst,
-                                                  const uint32_t* __restrict__ rEnd, const uint32_t* __restrict__ rCount,
-                                                  int64_t numRanges, double pad, EbgObb* __restrict__ out,
-                                                  uint8_t* __restrict__ useful)
+struct WarpGroup
 {
-  __shared__ double red[4];
-  for (int64_t r = blockIdx.x; r < numRanges; r += gridDim.x) {
+  __device__ int    rank() const { return threadIdx.x & 31; }
+  __device__ int    size() const { return 32; }
+  __device__ double sum(double v) const
+  {
+    for (int off = 16; off > 0; off >>= 1) {
+      v += __shfl_xor_sync(FULL, v, off);
+    }
+    return v;
+  }
+  __device__ double min(double v) const
+  {
+    for (int off = 16; off > 0; off >>= 1) {
+      v = fmin(v, __shfl_xor_sync(FULL, v, off));
+    }
+    return v;
+  }
+  __device__ double max(double v) const { return -min(-v); }
+};
+
+struct BlockGroup
+{
+  double*           red; // one slot per warp
+  __device__ int    rank() const { return threadIdx.x; }
+  __device__ int    size() const { return blockDim.x; }
+  __device__ double combine(double v, bool isMin) const
+  {
+    v = isMin ? WarpGroup().min(v) : WarpGroup().sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+      red[threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    double r = isMin ? DBL_MAX : 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); w++) {
+      r = isMin ? fmin(r, red[w]) : r + red[w];
+    }
+    return r;
+  }
+  __device__ double sum(double v) const { return combine(v, false); }
+  __device__ double min(double v) const { return combine(v, true); }
+  __device__ double max(double v) const { return -combine(-v, true); }
+};
+
+// pass 1 over [b, e) of this thread's share: normal sum, area, axis-aligned box
+template <class G>
+__device__ void obbPass1(const double* __restrict__ tri64, uint32_t b, uint32_t e, const G& g, double n[3],
+                         double& area, double lo[3], double hi[3])
+{
+  n[0] = n[1] = n[2] = 0;
+  area               = 0;
+  for (int a = 0; a < 3; a++) {
+    lo[a] = DBL_MAX;
+    hi[a] = -DBL_MAX;
+  }
+  for (uint32_t i = b + g.rank(); i < e; i += g.size()) {
+    const double* t     = tri64 + 30 * size_t(i);
+    const double  e1[3] = {t[3] - t[0], t[4] - t[1], t[5] - t[2]};
+    const double  e2[3] = {t[6] - t[0], t[7] - t[1], t[8] - t[2]};
+    const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    for (int a = 0; a < 3; a++) {
+      n[a] += cr[a];
+      for (int c = 0; c < 3; c++) {
+        lo[a] = fmin(lo[a], t[3 * c + a]);
+        hi[a] = fmax(hi[a], t[3 * c + a]);
+      }
+    }
+    area += sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+  }
+  for (int a = 0; a < 3; a++) {
+    n[a]  = g.sum(n[a]);
+    lo[a] = g.min(lo[a]);
+    hi[a] = g.max(hi[a]);
+  }
+  area = g.sum(area);
+}
+
+// the box normal n (the mean normal, or the box's thinnest axis when the normals nearly cancel)
+// and an in-plane frame t1, t2
+__device__ void obbFrame(double n[3], double area, const double lo[3], const double hi[3], double t1[3], double t2[3])
+{
+  double ln = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  if (!(ln > 0.5 * area) || !(ln > 0)) {
+    int ax = 0;
+    for (int a = 1; a < 3; a++) {
+      if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
+        ax = a;
+      }
+    }
+    n[0] = n[1] = n[2] = 0;
+    n[ax]              = 1;
+    ln                 = 1;
+  }
+  for (int a = 0; a < 3; a++) {
+    n[a] /= ln;
+  }
+  if (fabs(n[0]) < 0.9) {
+    t1[0] = 0;
+    t1[1] = n[2];
+    t1[2] = -n[1];
+  }
+  else {
+    t1[0] = -n[2];
+    t1[1] = 0;
+    t1[2] = n[0];
+  }
+  const double l1 = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+  for (int a = 0; a < 3; a++) {
+    t1[a] /= l1;
+  }
+  t2[0] = n[1] * t1[2] - n[2] * t1[1];
+  t2[1] = n[2] * t1[0] - n[0] * t1[2];
+  t2[2] = n[0] * t1[1] - n[1] * t1[0];
+}
+
+// pass 2: vertex sums in the frame, about (ox, oy) for accuracy: sx, sy, sxx, syy, sxy
+template <class G>
+__device__ void obbPass2(const double* __restrict__ tri64, uint32_t b, uint32_t e, const G& g, const double t1[3],
+                         const double t2[3], double ox, double oy, double m[5])
+{
+  double sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
+  for (uint32_t i = b + g.rank(); i < e; i += g.size()) {
+    const double* t = tri64 + 30 * size_t(i);
+    for (int c = 0; c < 3; c++) {
+      const double* p = t + 3 * c;
+      const double  x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - ox;
+      const double  y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - oy;
+      sx += x;
+      sy += y;
+      sxx += x * x;
+      syy += y * y;
+      sxy += x * y;
+    }
+  }
+  m[0] = g.sum(sx);
+  m[1] = g.sum(sy);
+  m[2] = g.sum(sxx);
+  m[3] = g.sum(syy);
+  m[4] = g.sum(sxy);
+}
+
+// the in-plane principal axis u and w = n x u from pass 2's sums over cn vertices
+__device__ void obbPrincipal(const double m[5], double cn, const double n[3], const double t1[3], const double t2[3],
+                             double u[3], double w[3])
+{
+  const double mx = m[0] / cn, my = m[1] / cn;
+  const double cxx = m[2] / cn - mx * mx, cyy = m[3] / cn - my * my, cxy = m[4] / cn - mx * my;
+  const double th  = 0.5 * atan2(2 * cxy, cxx - cyy);
+  for (int a = 0; a < 3; a++) {
+    u[a] = cos(th) * t1[a] + sin(th) * t2[a];
+  }
+  w[0] = n[1] * u[2] - n[2] * u[1];
+  w[1] = n[2] * u[0] - n[0] * u[2];
+  w[2] = n[0] * u[1] - n[1] * u[0];
+}
+
+// pass 3: extents of the vertices along n, u, w
+template <class G>
+__device__ void obbPass3(const double* __restrict__ tri64, uint32_t b, uint32_t e, const G& g, const double n[3],
+                         const double u[3], const double w[3], double mn[3], double mx[3])
+{
+  for (int a = 0; a < 3; a++) {
+    mn[a] = DBL_MAX;
+    mx[a] = -DBL_MAX;
+  }
+  for (uint32_t i = b + g.rank(); i < e; i += g.size()) {
+    const double* t = tri64 + 30 * size_t(i);
+    for (int c = 0; c < 3; c++) {
+      const double* p     = t + 3 * c;
+      const double  pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
+                             p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
+      for (int a = 0; a < 3; a++) {
+        mn[a] = fmin(mn[a], pr[a]);
+        mx[a] = fmax(mx[a], pr[a]);
+      }
+    }
+  }
+  for (int a = 0; a < 3; a++) {
+    mn[a] = g.min(mn[a]);
+    mx[a] = g.max(mx[a]);
+  }
+}
+
+// the padded box, whether it is worth testing (at most half the axis-aligned box's volume), and the
+// axis-aligned box itself
+__device__ void obbStore(const double n[3], const double u[3], const double w[3], const double mn[3],
+                         const double mx[3], const double lo[3], const double hi[3], double pad, EbgObb* out,
+                         uint8_t* useful, double* aabb)
+{
+  EbgObb o;
+  o.nx  = float(n[0]);
+  o.ny  = float(n[1]);
+  o.nz  = float(n[2]);
+  o.dn  = float(0.5 * (mn[0] + mx[0]));
+  o.ux  = float(u[0]);
+  o.uy  = float(u[1]);
+  o.uz  = float(u[2]);
+  o.du  = float(0.5 * (mn[1] + mx[1]));
+  o.vx  = float(w[0]);
+  o.vy  = float(w[1]);
+  o.vz  = float(w[2]);
+  o.dv  = float(0.5 * (mn[2] + mx[2]));
+  o.hn  = rup(0.5 * (mx[0] - mn[0]) + pad);
+  o.hu  = rup(0.5 * (mx[1] - mn[1]) + pad);
+  o.hv  = rup(0.5 * (mx[2] - mn[2]) + pad);
+  o.pad = 0.f;
+  *out  = o;
+  if (useful) {
+    const double obbVol  = 8.0 * double(o.hn) * double(o.hu) * double(o.hv);
+    const double aabbVol = (hi[0] - lo[0] + 2 * pad) * (hi[1] - lo[1] + 2 * pad) * (hi[2] - lo[2] + 2 * pad);
+    *useful              = (aabbVol > 0 ? obbVol / aabbVol : 1.0) <= 0.5 ? 1 : 0;
+  }
+  if (aabb) {
+    for (int a = 0; a < 3; a++) {
+      aabb[a]     = lo[a];
+      aabb[3 + a] = hi[a];
+    }
+  }
+}
+
+// the ranges of at most SMALL_RANGE triangles, [rFirst[r], rEnd[r]) or rFirst[r] + rCount[r]: a warp each
+__global__ void __launch_bounds__(128) kRangeObbsSmall(const double* __restrict__ tri64,
+                                                       const uint32_t* __restrict__ rFirst,
+                                                       const uint32_t* __restrict__ rEnd,
+                                                       const uint32_t* __restrict__ rCount, int64_t numRanges,
+                                                       double pad, EbgObb* __restrict__ out,
+                                                       uint8_t* __restrict__ useful, double* __restrict__ aabb)
+{
+  const int64_t   nWarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const WarpGroup g;
+  for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < numRanges; r += nWarps) {
     const uint32_t b = rFirst[r];
     const uint32_t e = rEnd ? rEnd[r] : b + rCount[r];
-    // pass 1: normal sum, area, AABB
-    double n[3] = {0, 0, 0}, area = 0, lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-      const double* t  = tri64 + 30 * size_t(i);
-      const double  e1[3] = {t[3] - t[0], t[4] - t[1], t[5] - t[2]};
-      const double  e2[3] = {t[6] - t[0], t[7] - t[1], t[8] - t[2]};
-      const double  cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-      for (int a = 0; a < 3; a++) {
-        n[a] += cr[a];
-        for (int c = 0; c < 3; c++) {
-          lo[a] = fmin(lo[a], t[3 * c + a]);
-          hi[a] = fmax(hi[a], t[3 * c + a]);
+    if (e - b > SMALL_RANGE) {
+      continue;
+    }
+    double n[3], area, lo[3], hi[3], t1[3], t2[3], m[5], u[3], w[3], mn[3], mx[3];
+    obbPass1(tri64, b, e, g, n, area, lo, hi);
+    obbFrame(n, area, lo, hi, t1, t2);
+    const double* t0 = tri64 + 30 * size_t(b);
+    const double  ox = t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2], oy = t0[0] * t2[0] + t0[1] * t2[1] + t0[2] * t2[2];
+    obbPass2(tri64, b, e, g, t1, t2, ox, oy, m);
+    obbPrincipal(m, 3.0 * double(e - b), n, t1, t2, u, w);
+    obbPass3(tri64, b, e, g, n, u, w, mn, mx);
+    if (g.rank() == 0) {
+      obbStore(n, u, w, mn, mx, lo, hi, pad, out + r, useful ? useful + r : nullptr, aabb ? aabb + 6 * r : nullptr);
+    }
+  }
+}
+
+// the larger ranges: one entry per range, one per CHUNK-triangle piece of it
+struct ObbRange
+{
+  uint32_t r, b, e, c0, nc; // range index, its span, its first chunk and chunk count
+};
+struct ObbChunk
+{
+  uint32_t lr, b, e; // large-range entry, the piece's span
+};
+struct ObbFrameState
+{
+  double n[3], t1[3], t2[3], u[3], w[3], lo[3], hi[3], ox, oy;
+};
+
+template <int PASS>
+__global__ void __launch_bounds__(128) kObbChunks(const double* __restrict__ tri64, const ObbChunk* __restrict__ chunks,
+                                                  uint32_t numChunks, const ObbFrameState* __restrict__ frames,
+                                                  double* __restrict__ part)
+{
+  __shared__ double red[4];
+  const BlockGroup  g{red};
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const ObbChunk ch = chunks[c];
+    double*        pc = part + 10 * size_t(c);
+    if (PASS == 1) {
+      double n[3], area, lo[3], hi[3];
+      obbPass1(tri64, ch.b, ch.e, g, n, area, lo, hi);
+      if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; a++) {
+          pc[a]     = n[a];
+          pc[4 + a] = lo[a];
+          pc[7 + a] = hi[a];
+        }
+        pc[3] = area;
+      }
+    }
+    else if (PASS == 2) {
+      const ObbFrameState& f = frames[ch.lr];
+      double               m[5];
+      obbPass2(tri64, ch.b, ch.e, g, f.t1, f.t2, f.ox, f.oy, m);
+      if (threadIdx.x == 0) {
+        for (int k = 0; k < 5; k++) {
+          pc[k] = m[k];
         }
       }
-      area += sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-    }
-    for (int a = 0; a < 3; a++) {
-      n[a]  = blockSum(n[a], red);
-      lo[a] = blockMin(lo[a], red);
-      hi[a] = blockMax(hi[a], red);
-    }
-    area      = blockSum(area, red);
-    double ln = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-    if (!(ln > 0.5 * area) || !(ln > 0)) {
-      int ax = 0;
-      for (int a = 1; a < 3; a++) {
-        if (hi[a] - lo[a] < hi[ax] - lo[ax]) {
-          ax = a;
-        }
-      }
-      n[0] = n[1] = n[2] = 0;
-      n[ax]              = 1;
-      ln                 = 1;
-    }
-    for (int a = 0; a < 3; a++) {
-      n[a] /= ln;
-    }
-    double t1[3];
-    if (fabs(n[0]) < 0.9) {
-      t1[0] = 0;
-      t1[1] = n[2];
-      t1[2] = -n[1];
     }
     else {
-      t1[0] = -n[2];
-      t1[1] = 0;
-      t1[2] = n[0];
-    }
-    const double l1 = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
-    for (int a = 0; a < 3; a++) {
-      t1[a] /= l1;
-    }
-    const double t2[3] = {n[1] * t1[2] - n[2] * t1[1], n[2] * t1[0] - n[0] * t1[2], n[0] * t1[1] - n[1] * t1[0]};
-    // pass 2: in-plane mean and covariance of the vertices (about the first vertex, for accuracy)
-    const double* t0  = tri64 + 30 * size_t(b);
-    const double  ox = t0[0] * t1[0] + t0[1] * t1[1] + t0[2] * t1[2], oy = t0[0] * t2[0] + t0[1] * t2[1] + t0[2] * t2[2];
-    double        sx = 0, sy = 0, sxx = 0, syy = 0, sxy = 0;
-    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-      const double* t = tri64 + 30 * size_t(i);
-      for (int c = 0; c < 3; c++) {
-        const double* p = t + 3 * c;
-        const double  x = p[0] * t1[0] + p[1] * t1[1] + p[2] * t1[2] - ox;
-        const double  y = p[0] * t2[0] + p[1] * t2[1] + p[2] * t2[2] - oy;
-        sx += x;
-        sy += y;
-        sxx += x * x;
-        syy += y * y;
-        sxy += x * y;
-      }
-    }
-    sx              = blockSum(sx, red);
-    sy              = blockSum(sy, red);
-    sxx             = blockSum(sxx, red);
-    syy             = blockSum(syy, red);
-    sxy             = blockSum(sxy, red);
-    const double cn = 3.0 * double(e - b);
-    const double mx = sx / cn, my = sy / cn;
-    const double cxx = sxx / cn - mx * mx, cyy = syy / cn - my * my, cxy = sxy / cn - mx * my;
-    const double th  = 0.5 * atan2(2 * cxy, cxx - cyy);
-    const double u[3] = {cos(th) * t1[0] + sin(th) * t2[0], cos(th) * t1[1] + sin(th) * t2[1],
-                         cos(th) * t1[2] + sin(th) * t2[2]};
-    const double w[3] = {n[1] * u[2] - n[2] * u[1], n[2] * u[0] - n[0] * u[2], n[0] * u[1] - n[1] * u[0]};
-    // pass 3: extents along n, u, w
-    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mxx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-      const double* t = tri64 + 30 * size_t(i);
-      for (int c = 0; c < 3; c++) {
-        const double* p     = t + 3 * c;
-        const double  pr[3] = {p[0] * n[0] + p[1] * n[1] + p[2] * n[2], p[0] * u[0] + p[1] * u[1] + p[2] * u[2],
-                               p[0] * w[0] + p[1] * w[1] + p[2] * w[2]};
+      const ObbFrameState& f = frames[ch.lr];
+      double               mn[3], mx[3];
+      obbPass3(tri64, ch.b, ch.e, g, f.n, f.u, f.w, mn, mx);
+      if (threadIdx.x == 0) {
         for (int a = 0; a < 3; a++) {
-          mn[a]  = fmin(mn[a], pr[a]);
-          mxx[a] = fmax(mxx[a], pr[a]);
+          pc[a]     = mn[a];
+          pc[3 + a] = mx[a];
         }
       }
     }
-    for (int a = 0; a < 3; a++) {
-      mn[a]  = blockMin(mn[a], red);
-      mxx[a] = blockMax(mxx[a], red);
-    }
-    if (threadIdx.x == 0) {
-      EbgObb& o = out[r];
-      o.nx      = float(n[0]);
-      o.ny      = float(n[1]);
-      o.nz      = float(n[2]);
-      o.dn      = float(0.5 * (mn[0] + mxx[0]));
-      o.ux      = float(u[0]);
-      o.uy      = float(u[1]);
-      o.uz      = float(u[2]);
-      o.du      = float(0.5 * (mn[1] + mxx[1]));
-      o.vx      = float(w[0]);
-      o.vy      = float(w[1]);
-      o.vz      = float(w[2]);
-      o.dv      = float(0.5 * (mn[2] + mxx[2]));
-      o.hn      = rup(0.5 * (mxx[0] - mn[0]) + pad);
-      o.hu      = rup(0.5 * (mxx[1] - mn[1]) + pad);
-      o.hv      = rup(0.5 * (mxx[2] - mn[2]) + pad);
-      o.pad     = 0.f;
-      if (useful) {
-        const double obbVol  = 8.0 * double(o.hn) * double(o.hu) * double(o.hv);
-        const double aabbVol = (hi[0] - lo[0] + 2 * pad) * (hi[1] - lo[1] + 2 * pad) * (hi[2] - lo[2] + 2 * pad);
-        useful[r]            = (aabbVol > 0 ? obbVol / aabbVol : 1.0) <= 0.5 ? 1 : 0;
+    __syncthreads();
+  }
+}
+
+template <int PASS>
+__global__ void kObbRanges(const double* __restrict__ tri64, const ObbRange* __restrict__ ranges, uint32_t numLarge,
+                           const double* __restrict__ part, ObbFrameState* __restrict__ frames, double pad,
+                           EbgObb* __restrict__ out, uint8_t* __restrict__ useful, double* __restrict__ aabb)
+{
+  for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < numLarge; l += gridDim.x * blockDim.x) {
+    const ObbRange rg = ranges[l];
+    ObbFrameState& f  = frames[l];
+    if (PASS == 1) {
+      double n[3] = {0, 0, 0}, area = 0, lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+      for (uint32_t c = rg.c0; c < rg.c0 + rg.nc; c++) {
+        const double* pc = part + 10 * size_t(c);
+        for (int a = 0; a < 3; a++) {
+          n[a] += pc[a];
+          lo[a] = fmin(lo[a], pc[4 + a]);
+          hi[a] = fmax(hi[a], pc[7 + a]);
+        }
+        area += pc[3];
       }
+      obbFrame(n, area, lo, hi, f.t1, f.t2);
+      for (int a = 0; a < 3; a++) {
+        f.n[a]  = n[a];
+        f.lo[a] = lo[a];
+        f.hi[a] = hi[a];
+      }
+      const double* t0 = tri64 + 30 * size_t(rg.b);
+      f.ox             = t0[0] * f.t1[0] + t0[1] * f.t1[1] + t0[2] * f.t1[2];
+      f.oy             = t0[0] * f.t2[0] + t0[1] * f.t2[1] + t0[2] * f.t2[2];
+    }
+    else if (PASS == 2) {
+      double m[5] = {0, 0, 0, 0, 0};
+      for (uint32_t c = rg.c0; c < rg.c0 + rg.nc; c++) {
+        for (int k = 0; k < 5; k++) {
+          m[k] += part[10 * size_t(c) + k];
+        }
+      }
+      obbPrincipal(m, 3.0 * double(rg.e - rg.b), f.n, f.t1, f.t2, f.u, f.w);
+    }
+    else {
+      double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+      for (uint32_t c = rg.c0; c < rg.c0 + rg.nc; c++) {
+        for (int a = 0; a < 3; a++) {
+          mn[a] = fmin(mn[a], part[10 * size_t(c) + a]);
+          mx[a] = fmax(mx[a], part[10 * size_t(c) + 3 + a]);
+        }
+      }
+      obbStore(f.n, f.u, f.w, mn, mx, f.lo, f.hi, pad, out + rg.r, useful ? useful + rg.r : nullptr,
+               aabb ? aabb + 6 * size_t(rg.r) : nullptr);
     }
   }
 }
@@ -635,57 +836,39 @@ __global__ void kNodeObbFlags(const uint8_t* __restrict__ useful, const uint32_t
   }
 }
 
-// 6. refit (moved vertices, same tree): one block per node; each slot gets the FP64 box of its
-// range of leaf positions (a leaf slot: its triangles; an interior slot: the child's subtree),
-// rounded outward to FP32, and an interior slot's oriented-box flag from `useful`.
-__global__ void __launch_bounds__(128) kSlotBoxes(const double* __restrict__ tri64, const uint32_t* __restrict__ nodeFirst,
-                                                  const uint32_t* __restrict__ nodeEnd,
-                                                  const uint8_t* __restrict__ useful, uint32_t numNodes,
-                                                  EbgNode4* __restrict__ nodes)
+// 6. refit (moved vertices, same tree): each node's four child boxes, rounded outward to FP32, from
+// the axis-aligned boxes of the children's ranges (leafAabb per leaf id, nodeAabb per node; 6 doubles
+// each), and an interior slot's oriented-box flag from `useful`.
+__global__ void kSlotBoxes(const double* __restrict__ leafAabb, const double* __restrict__ nodeAabb,
+                           const uint8_t* __restrict__ useful, uint32_t numNodes, uint32_t numLeaves,
+                           EbgNode4* __restrict__ nodes)
 {
-  __shared__ double red[4];
-  for (uint32_t j = blockIdx.x; j < numNodes; j += gridDim.x) {
-    EbgNode4& nd = nodes[j];
-    for (int k = 0; k < 4; k++) {
-      const uint32_t c   = nd.child[k];
-      const uint32_t cnt = nd.count[k];
-      uint32_t       b, e;
-      if (c & EBG_LEAF_BIT) {
-        b = c & ~EBG_LEAF_BIT;
-        e = b + (cnt & EBG_COUNT_MASK);
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < 4 * numNodes; q += gridDim.x * blockDim.x) {
+    EbgNode4&      nd  = nodes[q >> 2];
+    const int      k   = int(q & 3u);
+    const uint32_t c   = nd.child[k];
+    const uint32_t cnt = nd.count[k];
+    const double*  bx;
+    if (c & EBG_LEAF_BIT) {
+      const uint32_t leaf = cnt >> EBG_COUNT_BITS;
+      if (leaf >= numLeaves) {
+        continue;
       }
-      else if (c != 0 && c < numNodes) {
-        b = nodeFirst[c];
-        e = nodeEnd[c];
-      }
-      else {
-        continue; // an empty slot (node 0 is the root, never a child)
-      }
-      double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-      for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
-        const double* t = tri64 + 30 * size_t(i);
-        for (int a = 0; a < 3; a++) {
-          lo[a] = fmin(lo[a], fmin(t[a], fmin(t[3 + a], t[6 + a])));
-          hi[a] = fmax(hi[a], fmax(t[a], fmax(t[3 + a], t[6 + a])));
-        }
-      }
-      for (int a = 0; a < 3; a++) {
-        lo[a] = blockMin(lo[a], red);
-        hi[a] = blockMax(hi[a], red);
-      }
-      if (threadIdx.x == 0) {
-        nd.lox[k] = rdown(lo[0]);
-        nd.loy[k] = rdown(lo[1]);
-        nd.loz[k] = rdown(lo[2]);
-        nd.hix[k] = rup(hi[0]);
-        nd.hiy[k] = rup(hi[1]);
-        nd.hiz[k] = rup(hi[2]);
-        if (!(c & EBG_LEAF_BIT)) {
-          nd.count[k] = useful[c] ? EBG_NODE_HAS_OBB : 0u;
-        }
-      }
-      __syncthreads();
+      bx = leafAabb + 6 * size_t(leaf);
     }
+    else if (c != 0 && c < numNodes) {
+      bx                  = nodeAabb + 6 * size_t(c);
+      nd.count[k]         = useful[c] ? EBG_NODE_HAS_OBB : 0u;
+    }
+    else {
+      continue; // an empty slot (node 0 is the root, never a child)
+    }
+    nd.lox[k] = rdown(bx[0]);
+    nd.loy[k] = rdown(bx[1]);
+    nd.loz[k] = rdown(bx[2]);
+    nd.hix[k] = rup(bx[3]);
+    nd.hiy[k] = rup(bx[4]);
+    nd.hiz[k] = rup(bx[5]);
   }
 }
 
@@ -720,6 +903,77 @@ inline unsigned gridFor(int64_t n, int t, int64_t cap = 1 << 20)
   int64_t g = (n + t - 1) / t;
   g         = g < cap ? g : cap;
   return unsigned(g < 1 ? 1 : g);
+}
+
+// Oriented boxes (and, with aabb, the axis-aligned boxes) of nr ranges of leaf positions,
+// [first[r], end[r]) or first[r] + count[r], device arrays.  With mayBeLong the range arrays are
+// read back once to find the ranges of more than SMALL_RANGE triangles and cut them into chunks
+// (the call then synchronises s).
+ebg_status rangeObbs(const double* tri64, const uint32_t* first, const uint32_t* end, const uint32_t* count,
+                     uint32_t nr, bool mayBeLong, double pad, EbgObb* out, uint8_t* useful, double* aabb, int numSms,
+                     cudaStream_t s)
+{
+  if (nr == 0) {
+    return EBG_OK;
+  }
+  kRangeObbsSmall<<<gridFor(nr, 4, 1 << 20), 128, 0, s>>>(tri64, first, end, count, nr, pad, out, useful, aabb);
+  if (!mayBeLong) {
+    return EBG_OK;
+  }
+  std::vector<uint32_t> hf(nr), he(nr);
+  cudaMemcpyAsync(hf.data(), first, 4 * size_t(nr), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(he.data(), end ? end : count, 4 * size_t(nr), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("oriented boxes: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  std::vector<ObbRange> lr;
+  std::vector<ObbChunk> ch;
+  for (uint32_t r = 0; r < nr; r++) {
+    const uint32_t b = hf[r], e = end ? he[r] : hf[r] + he[r];
+    if (e - b <= SMALL_RANGE) {
+      continue;
+    }
+    ObbRange x{r, b, e, uint32_t(ch.size()), 0u};
+    for (uint32_t c = b; c < e; c += CHUNK) {
+      ch.push_back(ObbChunk{uint32_t(lr.size()), c, std::min(c + CHUNK, e)});
+      x.nc++;
+    }
+    lr.push_back(x);
+  }
+  if (lr.empty()) {
+    return EBG_OK;
+  }
+  const uint32_t nl = uint32_t(lr.size()), nc = uint32_t(ch.size());
+  ObbRange*      dR = nullptr;
+  ObbChunk*      dC = nullptr;
+  ObbFrameState* dF = nullptr;
+  double*        dP = nullptr;
+  const bool ok = cudaMallocAsync((void**)&dR, sizeof(ObbRange) * nl, s) == cudaSuccess &&
+                  cudaMallocAsync((void**)&dC, sizeof(ObbChunk) * nc, s) == cudaSuccess &&
+                  cudaMallocAsync((void**)&dF, sizeof(ObbFrameState) * nl, s) == cudaSuccess &&
+                  cudaMallocAsync((void**)&dP, 80 * size_t(nc), s) == cudaSuccess;
+  if (ok) {
+    cudaMemcpyAsync(dR, lr.data(), sizeof(ObbRange) * nl, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dC, ch.data(), sizeof(ObbChunk) * nc, cudaMemcpyHostToDevice, s);
+    const unsigned gc = gridFor(nc, 1, int64_t(numSms) * 8), gr = gridFor(nl, 128);
+    kObbChunks<1><<<gc, 128, 0, s>>>(tri64, dC, nc, dF, dP);
+    kObbRanges<1><<<gr, 128, 0, s>>>(tri64, dR, nl, dP, dF, pad, out, useful, aabb);
+    kObbChunks<2><<<gc, 128, 0, s>>>(tri64, dC, nc, dF, dP);
+    kObbRanges<2><<<gr, 128, 0, s>>>(tri64, dR, nl, dP, dF, pad, out, useful, aabb);
+    kObbChunks<3><<<gc, 128, 0, s>>>(tri64, dC, nc, dF, dP);
+    kObbRanges<3><<<gr, 128, 0, s>>>(tri64, dR, nl, dP, dF, pad, out, useful, aabb);
+  }
+  for (void* p : {(void*)dR, (void*)dC, (void*)dF, (void*)dP}) {
+    if (p) {
+      cudaFreeAsync(p, s);
+    }
+  }
+  if (!ok) {
+    cudaGetLastError();
+    return setError(EBG_ERR_NO_MEMORY, "oriented-box workspace");
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? EBG_OK : setError(EBG_ERR_CUDA, std::string("oriented boxes: ") + cudaGetErrorString(e));
 }
 
 } // namespace
@@ -931,13 +1185,18 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
     scale = std::max(scale, std::max(std::fabs(outLo[a]), std::fabs(outHi[a])));
   }
   const double pad = 2e-6 * std::max(scale, 1e-30);
-  kRangeObbs<<<gridFor(numLeaves, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), leafFirst, nullptr,
-                                                            leafCount, numLeaves, pad,
-                                                            static_cast<EbgObb*>(m->dObb), nullptr);
+  // leaves hold at most EBG_MAX_LEAF triangles; nodes near the root span most of the mesh
+  const double* t64 = static_cast<const double*>(m->dTri64);
+  ebg_status    orc = rangeObbs(t64, leafFirst, nullptr, leafCount, numLeaves, false, pad,
+                                static_cast<EbgObb*>(m->dObb), nullptr, nullptr, m->numSms, s);
+  if (orc == EBG_OK && numNodes > 0) {
+    orc = rangeObbs(t64, nodeFirst, nodeEnd, nullptr, numNodes, true, pad, static_cast<EbgObb*>(m->dNodeObb), useful,
+                    nullptr, m->numSms, s);
+  }
+  if (orc != EBG_OK) {
+    return orc;
+  }
   if (numNodes > 0) {
-    kRangeObbs<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), nodeFirst, nodeEnd,
-                                                             nullptr, numNodes, pad,
-                                                             static_cast<EbgObb*>(m->dNodeObb), useful);
     kNodeObbFlags<<<gridFor(numNodes, 256), 256, 0, s>>>(useful, nodeParent, numNodes, dNodesTmp);
     cudaMemcpyAsync(m->dNodes, dNodesTmp, sizeof(EbgNode4) * size_t(numNodes), cudaMemcpyDeviceToDevice, s);
   }
@@ -998,10 +1257,12 @@ ebg_status refitMeshOnDevice(ebg_mesh* m, const double* V, bool vOnDevice, int64
   unsigned long long* bounds = nullptr;
   uint8_t*            useful = nullptr;
   int*                bad    = nullptr;
+  double *            leafAabb = nullptr, *nodeAabb = nullptr;
   bool ok = alloc((void**)&dTriN, 24 * N) && alloc((void**)&dVN, 72 * N) && alloc((void**)&dEN, 72 * N) &&
             alloc((void**)&triLo, 24 * N) && alloc((void**)&triHi, 24 * N) && alloc((void**)&cen, 24 * N) &&
             alloc((void**)&area, 8 * N) && alloc((void**)&bounds, 12 * 8) &&
-            alloc((void**)&useful, std::max<size_t>(numNodes, 1)) && alloc((void**)&bad, 4);
+            alloc((void**)&useful, std::max<size_t>(numNodes, 1)) && alloc((void**)&bad, 4) &&
+            alloc((void**)&leafAabb, 48 * size_t(numLeaves)) && alloc((void**)&nodeAabb, 48 * size_t(numNodes));
   if (ok && !vOnDevice) {
     ok = alloc((void**)&dV, 24 * size_t(nv)) &&
          cudaMemcpyAsync(dV, V, 24 * size_t(nv), cudaMemcpyHostToDevice, s) == cudaSuccess;
@@ -1053,16 +1314,19 @@ ebg_status refitMeshOnDevice(ebg_mesh* m, const double* V, bool vOnDevice, int64
     scale = std::max(scale, std::max(std::fabs(outLo[a]), std::fabs(outHi[a])));
   }
   const double pad = 2e-6 * std::max(scale, 1e-30);
-  kRangeObbs<<<gridFor(numLeaves, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dLeafFirst,
-                                                            nullptr, m->dLeafCount, numLeaves, pad,
-                                                            static_cast<EbgObb*>(m->dObb), nullptr);
+  const double* t64 = static_cast<const double*>(m->dTri64);
+  ebg_status    orc = rangeObbs(t64, m->dLeafFirst, nullptr, m->dLeafCount, numLeaves, false, pad,
+                                static_cast<EbgObb*>(m->dObb), nullptr, leafAabb, m->numSms, s);
+  if (orc == EBG_OK && numNodes > 0) {
+    orc = rangeObbs(t64, m->dNodeFirst, m->dNodeEnd, nullptr, numNodes, true, pad, static_cast<EbgObb*>(m->dNodeObb),
+                    useful, nodeAabb, m->numSms, s);
+  }
+  if (orc != EBG_OK) {
+    return orc;
+  }
   if (numNodes > 0) {
-    kRangeObbs<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dNodeFirst,
-                                                             m->dNodeEnd, nullptr, numNodes, pad,
-                                                             static_cast<EbgObb*>(m->dNodeObb), useful);
-    kSlotBoxes<<<gridFor(numNodes, 1, 1 << 20), 128, 0, s>>>(static_cast<const double*>(m->dTri64), m->dNodeFirst,
-                                                             m->dNodeEnd, useful, numNodes,
-                                                             static_cast<EbgNode4*>(m->dNodes));
+    kSlotBoxes<<<gridFor(4 * int64_t(numNodes), 256), 256, 0, s>>>(leafAabb, nodeAabb, useful, numNodes, numLeaves,
+                                                                   static_cast<EbgNode4*>(m->dNodes));
   }
   std::vector<double> cdf(N);
   cudaMemcpyAsync(cdf.data(), area, 8 * N, cudaMemcpyDeviceToHost, s);
