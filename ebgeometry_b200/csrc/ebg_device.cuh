@@ -34,6 +34,15 @@ __device__ __forceinline__ float boxDist2(float lx, float ly, float lz, float hx
 
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 
+// Quotients by a leaf's primitive count c (1..32) without integer division: 32 / c, and
+// ceil(4096 / c), with which (a * ceil(4096 / c)) >> 12 == a / c for every 0 <= a < 64.
+static __constant__ uint16_t c_lanesPer[33] = {0, 32, 16, 10, 8, 6, 5, 4, 4, 3, 3, 2, 2, 2, 2, 2, 2,
+                                               1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
+static __constant__ uint16_t c_recip12[33] = {0,   4096, 2048, 1366, 1024, 820, 683, 586, 512, 456, 410,
+                                              373, 342,  316,  293,  274,  256, 241, 228, 216, 205, 196,
+                                              187, 179,  171,  164,  158,  152, 147, 142, 137, 133, 128};
+__device__ __forceinline__ int divSmall(int a, int c) { return (a * int(c_recip12[c])) >> 12; }
+
 // 10 bits per axis -> 30-bit Morton code.
 __device__ __forceinline__ uint32_t spread10(uint32_t x)
 {

@@ -83,14 +83,6 @@ __device__ __forceinline__ float triDist2(const float4 h0, const float4 h1, cons
 
 __device__ __forceinline__ float signOf(float x) { return signbit(x) ? -1.f : 1.f; }
 
-// Quotients by a leaf's triangle count c (1..32) without integer division: 32 / c, and
-// ceil(4096 / c), with which (a * ceil(4096 / c)) >> 12 == a / c for every 0 <= a < 64.
-static __constant__ uint16_t c_lanesPer[33] = {0, 32, 16, 10, 8, 6, 5, 4, 4, 3, 3, 2, 2, 2, 2, 2, 2,
-                                               1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1};
-static __constant__ uint16_t c_recip12[33] = {0,   4096, 2048, 1366, 1024, 820, 683, 586, 512, 456, 410,
-                                              373, 342,  316,  293,  274,  256, 241, 228, 216, 205, 196,
-                                              187, 179,  171,  164,  158,  152, 147, 142, 137, 133, 128};
-__device__ __forceinline__ int divSmall(int a, int c) { return (a * int(c_recip12[c])) >> 12; }
 
 // Squared distance from p to an oriented box (EbgObb as four float4: n|dn, u|du, v|dv, h), scaled
 // down by 4e-6 relative.  The FP32 error of each plane distance n . p - dn is about 1e-7 of |p|,
