@@ -326,17 +326,13 @@ ebg_status buildMesh(const double*         V,
   }
 
   if (onDevice) {
-    if (build != EBG_BUILD_MORTON) {
-      delete m;
-      return setError(EBG_ERR_INVALID, "the device build makes Morton trees only");
-    }
     cudaStream_t bs = nullptr;
     if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) {
       delete m;
       return setError(EBG_ERR_CUDA, "stream for the device build");
     }
     double           lo[3], hi[3];
-    const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, leafSize, lo, hi, bs, !givenNormal);
+    const ebg_status rc = buildMeshOnDevice(m, V, nv, F, nt, build, leafSize, lo, hi, bs, !givenNormal);
     cudaStreamDestroy(bs);
     std::vector<double>().swap(m->triN);
     std::vector<double>().swap(m->cornerVN);

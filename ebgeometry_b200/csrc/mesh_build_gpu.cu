@@ -29,6 +29,7 @@
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
+#include <math_constants.h>
 
 #include "capi_common.h"
 #include "capi_internal.h"
@@ -60,6 +61,53 @@ __host__ double hostDval(unsigned long long k)
   std::memcpy(&d, &b, sizeof(d));
   return d;
 }
+
+// FP64 reductions over a warp or a block (one shared slot per warp)
+struct WarpGroup
+{
+  __device__ int    rank() const { return threadIdx.x & 31; }
+  __device__ int    size() const { return 32; }
+  __device__ double sum(double v) const
+  {
+    for (int off = 16; off > 0; off >>= 1) {
+      v += __shfl_xor_sync(FULL, v, off);
+    }
+    return v;
+  }
+  __device__ double min(double v) const
+  {
+    for (int off = 16; off > 0; off >>= 1) {
+      v = fmin(v, __shfl_xor_sync(FULL, v, off));
+    }
+    return v;
+  }
+  __device__ double max(double v) const { return -min(-v); }
+};
+
+struct BlockGroup
+{
+  double*           red; // one slot per warp
+  __device__ int    rank() const { return threadIdx.x; }
+  __device__ int    size() const { return blockDim.x; }
+  __device__ double combine(double v, bool isMin) const
+  {
+    v = isMin ? WarpGroup().min(v) : WarpGroup().sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+      red[threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    double r = isMin ? DBL_MAX : 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); w++) {
+      r = isMin ? fmin(r, red[w]) : r + red[w];
+    }
+    return r;
+  }
+  __device__ double sum(double v) const { return combine(v, false); }
+  __device__ double min(double v) const { return combine(v, true); }
+  __device__ double max(double v) const { return -combine(-v, true); }
+};
+
 
 __device__ __forceinline__ uint64_t spread21(uint64_t x)
 {
@@ -286,12 +334,17 @@ __device__ __forceinline__ uint32_t refCount(const TreeView& t, uint32_t ref)
 {
   return (ref & EBG_LEAF_BIT) ? 1u : t.last[ref] - t.first[ref] + 1u;
 }
+// 2 (dx dy + dy dz + dz dx) with every operation rounded on its own, as the host build computes it
+__device__ __forceinline__ double boxArea(const double* lo, const double* hi)
+{
+  const double dx = __dsub_rn(hi[0], lo[0]), dy = __dsub_rn(hi[1], lo[1]), dz = __dsub_rn(hi[2], lo[2]);
+  return __dmul_rn(2.0, __dadd_rn(__dadd_rn(__dmul_rn(dx, dy), __dmul_rn(dy, dz)), __dmul_rn(dz, dx)));
+}
 __device__ __forceinline__ double refArea(const TreeView& t, uint32_t ref)
 {
   double lo[3], hi[3];
   childBox(ref, t.leafLo, t.leafHi, t.nodeLo, t.nodeHi, lo, hi);
-  const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
-  return 2.0 * (dx * dy + dy * dz + dz * dx);
+  return boxArea(lo, hi);
 }
 
 __device__ __forceinline__ float rdown(double x) { return __double2float_rd(x); }
@@ -388,6 +441,263 @@ __global__ void kCollapse(const TreeView t, const uint2* __restrict__ frontier, 
   }
 }
 
+// 2-3 (SAH).  The binary tree of the host's binned-SAH build, level by level, one block per node
+// range [b, e) of the current order: its FP64 box and centroid bounds; for each axis with extent,
+// 32 centroid bins holding counts and FP64 triangle boxes (per-warp copies merged in warp order); the
+// split of least cost A_L N_L + A_R N_R (the first minimum over axis, then bin); a stable partition
+// of the range by bin.  Host and device compute the same doubles, so the tree is the host's.  A range
+// of at most leafSize triangles keeps no children (the collapse makes it a leaf); a single triangle is
+// a leaf reference.
+struct SahTask
+{
+  uint32_t node, b, e;
+};
+
+constexpr int SAH_BINS    = 32;
+constexpr int SAH_THREADS = 128;
+constexpr int SAH_WARPS   = SAH_THREADS / 32;
+
+__device__ __forceinline__ int sahBin(double c, double cl, double k)
+{
+  const int bi = int(__dmul_rn(__dsub_rn(c, cl), k));
+  return bi < 0 ? 0 : (bi > SAH_BINS - 1 ? SAH_BINS - 1 : bi);
+}
+
+__global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restrict__ tasks, uint32_t numTasks,
+                                                         uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp,
+                                                         const double* __restrict__ triLo,
+                                                         const double* __restrict__ triHi,
+                                                         const double* __restrict__ cen, int leafSize,
+                                                         uint32_t* __restrict__ left, uint32_t* __restrict__ right,
+                                                         uint32_t* __restrict__ first, uint32_t* __restrict__ last,
+                                                         double* __restrict__ nodeLo, double* __restrict__ nodeHi,
+                                                         SahTask* __restrict__ next, uint32_t* __restrict__ counters,
+                                                         uint32_t maxNodes, int* __restrict__ err)
+{
+  // per warp, axis and bin: count, and the bin's box as order-preserving keys (3 lo, 3 hi)
+  __shared__ uint32_t           bcnt[SAH_WARPS][3][SAH_BINS];
+  __shared__ unsigned long long bbox[SAH_WARPS][3][SAH_BINS][6];
+  __shared__ double             red[SAH_WARPS];
+  __shared__ int                sAxis, sBin;
+  __shared__ uint32_t           wl[SAH_WARPS], wr[SAH_WARPS];
+  const BlockGroup              g{red};
+  const int                     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  for (uint32_t t = blockIdx.x; t < numTasks; t += gridDim.x) {
+    const SahTask tk = tasks[t];
+    const uint32_t b = tk.b, e = tk.e, n = e - b;
+    // the range's box and its centroids' bounds
+    double lo[3], hi[3], cl[3], ch[3];
+    for (int a = 0; a < 3; a++) {
+      lo[a] = cl[a] = DBL_MAX;
+      hi[a] = ch[a] = -DBL_MAX;
+    }
+    for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
+      const size_t p = ids[i];
+      for (int a = 0; a < 3; a++) {
+        lo[a] = fmin(lo[a], triLo[3 * p + a]);
+        hi[a] = fmax(hi[a], triHi[3 * p + a]);
+        cl[a] = fmin(cl[a], cen[3 * p + a]);
+        ch[a] = fmax(ch[a], cen[3 * p + a]);
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      lo[a] = g.min(lo[a]);
+      hi[a] = g.max(hi[a]);
+      cl[a] = g.min(cl[a]);
+      ch[a] = g.max(ch[a]);
+    }
+    if (threadIdx.x == 0) {
+      for (int a = 0; a < 3; a++) {
+        nodeLo[3 * size_t(tk.node) + a] = lo[a];
+        nodeHi[3 * size_t(tk.node) + a] = hi[a];
+      }
+      first[tk.node] = b;
+      last[tk.node]  = e - 1;
+    }
+    if (n <= uint32_t(leafSize)) {
+      continue;
+    }
+    // bins
+    for (int q = threadIdx.x; q < SAH_WARPS * 3 * SAH_BINS; q += SAH_THREADS) {
+      const int w = q / (3 * SAH_BINS), r = q % (3 * SAH_BINS), a = r / SAH_BINS, bi = r % SAH_BINS;
+      bcnt[w][a][bi] = 0;
+      for (int c = 0; c < 3; c++) {
+        bbox[w][a][bi][c]     = ~0ull;
+        bbox[w][a][bi][3 + c] = 0ull;
+      }
+    }
+    __syncthreads();
+    double k[3];
+    for (int a = 0; a < 3; a++) {
+      const double ext = __dsub_rn(ch[a], cl[a]);
+      k[a]             = ext > 0.0 ? __ddiv_rn(double(SAH_BINS), ext) : 0.0;
+    }
+    for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
+      const size_t p = ids[i];
+      for (int a = 0; a < 3; a++) {
+        if (k[a] == 0.0) {
+          continue;
+        }
+        const int bi = sahBin(cen[3 * p + a], cl[a], k[a]);
+        atomicAdd(&bcnt[warp][a][bi], 1u);
+        for (int c = 0; c < 3; c++) {
+          atomicMin(&bbox[warp][a][bi][c], dkey(triLo[3 * p + c]));
+          atomicMax(&bbox[warp][a][bi][3 + c], dkey(triHi[3 * p + c]));
+        }
+      }
+    }
+    __syncthreads();
+    // merge the warps' bins into warp 0's
+    for (int q = threadIdx.x; q < 3 * SAH_BINS; q += SAH_THREADS) {
+      const int a = q / SAH_BINS, bi = q % SAH_BINS;
+      for (int w = 1; w < SAH_WARPS; w++) {
+        bcnt[0][a][bi] += bcnt[w][a][bi];
+        for (int c = 0; c < 3; c++) {
+          bbox[0][a][bi][c]     = min(bbox[0][a][bi][c], bbox[w][a][bi][c]);
+          bbox[0][a][bi][3 + c] = max(bbox[0][a][bi][3 + c], bbox[w][a][bi][3 + c]);
+        }
+      }
+    }
+    __syncthreads();
+    // the cheapest split: thread 0 scans the axes in order, as the host does
+    if (threadIdx.x == 0) {
+      double bestCost = CUDART_INF;
+      int    bestAxis = -1, bestBin = -1;
+      for (int a = 0; a < 3; a++) {
+        if (k[a] == 0.0) {
+          continue;
+        }
+        double   rightArea[SAH_BINS];
+        uint32_t rightCnt[SAH_BINS];
+        double   al[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, ah[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        uint32_t c     = 0;
+        for (int i = SAH_BINS - 1; i > 0; i--) {
+          if (bcnt[0][a][i] > 0) {
+            for (int x = 0; x < 3; x++) {
+              al[x] = fmin(al[x], dval(bbox[0][a][i][x]));
+              ah[x] = fmax(ah[x], dval(bbox[0][a][i][3 + x]));
+            }
+          }
+          c += bcnt[0][a][i];
+          rightArea[i] = c > 0 ? boxArea(al, ah) : 0.0;
+          rightCnt[i]  = c;
+        }
+        double   ll[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, lh[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        uint32_t lc    = 0;
+        for (int i = 0; i < SAH_BINS - 1; i++) {
+          if (bcnt[0][a][i] > 0) {
+            for (int x = 0; x < 3; x++) {
+              ll[x] = fmin(ll[x], dval(bbox[0][a][i][x]));
+              lh[x] = fmax(lh[x], dval(bbox[0][a][i][3 + x]));
+            }
+          }
+          lc += bcnt[0][a][i];
+          if (lc == 0 || rightCnt[i + 1] == 0) {
+            continue;
+          }
+          const double cost = __dadd_rn(__dmul_rn(boxArea(ll, lh), double(lc)),
+                                        __dmul_rn(rightArea[i + 1], double(rightCnt[i + 1])));
+          if (cost < bestCost) {
+            bestCost = cost;
+            bestAxis = a;
+            bestBin  = i;
+          }
+        }
+      }
+      sAxis = bestAxis;
+      sBin  = bestBin;
+    }
+    __syncthreads();
+    const int ax = sAxis, bin = sBin;
+    uint32_t  m  = b + n / 2; // every centroid the same point: halve
+    if (ax >= 0) {
+      // stable partition into tmp, then back
+      uint32_t nl = 0;
+      for (int i = 0; i <= bin; i++) {
+        nl += bcnt[0][ax][i];
+      }
+      uint32_t offL = 0, offR = 0;
+      for (uint32_t base = b; base < e; base += SAH_THREADS) {
+        const uint32_t i     = base + threadIdx.x;
+        const bool     valid = i < e;
+        const uint32_t p     = valid ? ids[i] : 0u;
+        const bool     isL   = valid && sahBin(cen[3 * size_t(p) + ax], cl[ax], k[ax]) <= bin;
+        const unsigned bl    = __ballot_sync(FULL, isL);
+        const unsigned br    = __ballot_sync(FULL, valid && !isL);
+        if (lane == 0) {
+          wl[warp] = __popc(bl);
+          wr[warp] = __popc(br);
+        }
+        __syncthreads();
+        uint32_t pl = offL, pr = offR, tl = 0, tr = 0;
+        for (int w = 0; w < SAH_WARPS; w++) {
+          if (w < warp) {
+            pl += wl[w];
+            pr += wr[w];
+          }
+          tl += wl[w];
+          tr += wr[w];
+        }
+        const unsigned below = (1u << lane) - 1u;
+        if (valid) {
+          tmp[isL ? b + pl + __popc(bl & below) : b + nl + pr + __popc(br & below)] = p;
+        }
+        offL += tl;
+        offR += tr;
+        __syncthreads();
+      }
+      for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
+        ids[i] = tmp[i];
+      }
+      m = b + nl;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t ref[2];
+      const uint32_t cb[2] = {b, m}, ce[2] = {m, e};
+      for (int c = 0; c < 2; c++) {
+        if (ce[c] - cb[c] == 1) {
+          ref[c] = EBG_LEAF_BIT | cb[c];
+        }
+        else {
+          const uint32_t id = atomicAdd(counters + 0, 1u);
+          if (id >= maxNodes) {
+            atomicOr(err, 32);
+            ref[c] = EBG_LEAF_BIT | cb[c];
+            continue;
+          }
+          ref[c]                               = id;
+          next[atomicAdd(counters + 1, 1u)]    = SahTask{id, cb[c], ce[c]};
+        }
+      }
+      left[tk.node]  = ref[0];
+      right[tk.node] = ref[1];
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void kIota(uint32_t* __restrict__ ids, int64_t n)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    ids[i] = uint32_t(i);
+  }
+}
+
+__global__ void kGatherLeafBoxes(int64_t n, const uint32_t* __restrict__ ids, const double* __restrict__ triLo,
+                                 const double* __restrict__ triHi, double* __restrict__ leafLo,
+                                 double* __restrict__ leafHi)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const uint32_t f = ids[i];
+    for (int a = 0; a < 3; a++) {
+      leafLo[3 * i + a] = triLo[3 * size_t(f) + a];
+      leafHi[3 * i + a] = triHi[3 * size_t(f) + a];
+    }
+  }
+}
+
 // 5a. leaf-ordered records
 __global__ void kRecords(const double* __restrict__ V, const int32_t* __restrict__ F,
                          const double* __restrict__ triN, const double* __restrict__ cornerVN,
@@ -460,51 +770,6 @@ __global__ void kRecords(const double* __restrict__ V, const int32_t* __restrict
 // box is kept too (the child boxes of a refit come from it).
 constexpr uint32_t SMALL_RANGE = 2048;
 constexpr uint32_t CHUNK       = 4096;
-
-struct WarpGroup
-{
-  __device__ int    rank() const { return threadIdx.x & 31; }
-  __device__ int    size() const { return 32; }
-  __device__ double sum(double v) const
-  {
-    for (int off = 16; off > 0; off >>= 1) {
-      v += __shfl_xor_sync(FULL, v, off);
-    }
-    return v;
-  }
-  __device__ double min(double v) const
-  {
-    for (int off = 16; off > 0; off >>= 1) {
-      v = fmin(v, __shfl_xor_sync(FULL, v, off));
-    }
-    return v;
-  }
-  __device__ double max(double v) const { return -min(-v); }
-};
-
-struct BlockGroup
-{
-  double*           red; // one slot per warp
-  __device__ int    rank() const { return threadIdx.x; }
-  __device__ int    size() const { return blockDim.x; }
-  __device__ double combine(double v, bool isMin) const
-  {
-    v = isMin ? WarpGroup().min(v) : WarpGroup().sum(v);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) {
-      red[threadIdx.x >> 5] = v;
-    }
-    __syncthreads();
-    double r = isMin ? DBL_MAX : 0.0;
-    for (int w = 0; w < int(blockDim.x >> 5); w++) {
-      r = isMin ? fmin(r, red[w]) : r + red[w];
-    }
-    return r;
-  }
-  __device__ double sum(double v) const { return combine(v, false); }
-  __device__ double min(double v) const { return combine(v, true); }
-  __device__ double max(double v) const { return -combine(-v, true); }
-};
 
 // pass 1 over [b, e) of this thread's share: normal sum, area, axis-aligned box
 template <class G>
@@ -978,8 +1243,8 @@ ebg_status rangeObbs(const double* tri64, const uint32_t* first, const uint32_t*
 
 } // namespace
 
-ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int leafSize,
-                             double* outLo, double* outHi, cudaStream_t s, bool normalsOnDevice)
+ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int build,
+                             int leafSize, double* outLo, double* outHi, cudaStream_t s, bool normalsOnDevice)
 {
   const int64_t n = nt;
   std::vector<void*> tmp;
@@ -1061,6 +1326,41 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
 
   // 1. boxes, bounds, codes, sort
   kTriBounds<<<gridFor(n, 256, 8192), 256, 0, s>>>(dV, dF, n, triLo, triHi, cen, bounds);
+  if (build == EBG_BUILD_SAH) {
+    // 2-3 (SAH): the binary tree top-down, one launch per level, in place of codes, sort and refit
+    const size_t maxTasks = N / 2 + 1;
+    SahTask*     tasks[2] = {nullptr, nullptr};
+    if (!alloc((void**)&tasks[0], sizeof(SahTask) * maxTasks) || !alloc((void**)&tasks[1], sizeof(SahTask) * maxTasks)) {
+      return setError(EBG_ERR_NO_MEMORY, "device build workspace");
+    }
+    kIota<<<gridFor(n, 256), 256, 0, s>>>(ids, n);
+    if (n > leafSize) {
+      const SahTask  root{0u, 0u, uint32_t(n)};
+      const uint32_t init[2] = {1u, 0u};
+      cudaMemcpyAsync(tasks[0], &root, sizeof(root), cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
+      uint32_t count = 1;
+      int      cur   = 0;
+      for (int level = 0; count > 0; level++) {
+        if (level > 256) {
+          return setError(EBG_ERR_INVALID, "device SAH build: tree deeper than 256 levels");
+        }
+        cudaMemsetAsync(counters + 1, 0, 4, s);
+        kSahLevel<<<gridFor(count, 1, 1 << 16), SAH_THREADS, 0, s>>>(
+          tasks[cur], count, ids, idsIn, triLo, triHi, cen, leafSize, left, right, first, last, nodeLo, nodeHi,
+          tasks[1 - cur], counters, uint32_t(NI), overflow);
+        uint32_t hc[2];
+        cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+          return setError(EBG_ERR_CUDA, std::string("device SAH build: ") + cudaGetErrorString(cudaGetLastError()));
+        }
+        count = hc[1];
+        cur   = 1 - cur;
+      }
+    }
+    kGatherLeafBoxes<<<gridFor(n, 256), 256, 0, s>>>(n, ids, triLo, triHi, leafLo, leafHi);
+  }
+  else {
   kTriMorton<<<gridFor(n, 256), 256, 0, s>>>(cen, n, bounds, codesIn, idsIn);
   size_t sortBytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, codesIn, codesOut, idsIn, ids, int(n), 0, 63, s);
@@ -1079,6 +1379,7 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
   }
   kRefit<<<gridFor(n, 256), 256, 0, s>>>(n, ids, triLo, triHi, leafLo, leafHi, left, right, parentI, parentL, nodeLo,
                                          nodeHi, arrivals, overflow);
+  }
 
   // root box (the whole mesh)
   unsigned long long hb[12];

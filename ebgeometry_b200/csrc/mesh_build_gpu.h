@@ -10,13 +10,14 @@
 
 namespace ebg {
 
-// Builds the tree and every device array of m (nodes, records, oriented boxes, DCEL normals) from
-// the soup (V, F on the host) and m's pseudonormals (m->triN, cornerVN, edgeN, soup order; with
-// normalsOnDevice they are computed here instead, and the records are their only copy); fills
-// m->areaCdf and m->info's num_nodes / num_leaves / depth, m->view's root reference, and the
-// triangles' bounding box (outLo / outHi).  Synchronous on s.
-ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int leafSize,
-                             double* outLo, double* outHi, cudaStream_t s, bool normalsOnDevice = false);
+// Builds the tree (build: EBG_BUILD_MORTON or EBG_BUILD_SAH, the host build's tree in either case)
+// and every device array of m (nodes, records, oriented boxes, DCEL normals) from the soup (V, F on
+// the host) and m's pseudonormals (m->triN, cornerVN, edgeN, soup order; with normalsOnDevice they
+// are computed here instead, and the records are their only copy); fills m->areaCdf and m->info's
+// num_nodes / num_leaves / depth, m->view's root reference, and the triangles' bounding box (outLo /
+// outHi).  Synchronous on s.
+ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int32_t* F, int64_t nt, int build,
+                             int leafSize, double* outLo, double* outHi, cudaStream_t s, bool normalsOnDevice = false);
 
 // Refits m to moved vertices (same count, same triangles; V on the host, or on the device with
 // vOnDevice): the pseudonormals, every triangle record, every leaf's and node's oriented box and

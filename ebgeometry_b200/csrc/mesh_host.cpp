@@ -494,7 +494,9 @@ struct Builder
     if (bestAxis >= 0) {
       const double ext = ch[bestAxis] - cl[bestAxis];
       const double k   = NB / ext;
-      auto         mid = std::partition(idx.begin() + b, idx.begin() + e, [&](uint32_t p) {
+      // stable, so the order inside each side (and with it every leaf's triangle order) is the
+      // order it had, exactly as the device build's partition keeps it
+      auto         mid = std::stable_partition(idx.begin() + b, idx.begin() + e, [&](uint32_t p) {
         int bi = int((cen[3 * size_t(p) + bestAxis] - cl[bestAxis]) * k);
         bi     = std::min(std::max(bi, 0), NB - 1);
         return bi <= bestBin;
@@ -504,20 +506,9 @@ struct Builder
         return m;
       }
     }
-    // Fallback: median along the widest centroid axis.
-    int    axis = 0;
-    double w    = -1;
-    for (int a = 0; a < 3; a++) {
-      if (ch[a] - cl[a] > w) {
-        w    = ch[a] - cl[a];
-        axis = a;
-      }
-    }
-    const uint32_t m = b + n / 2;
-    std::nth_element(idx.begin() + b, idx.begin() + m, idx.begin() + e, [&](uint32_t p, uint32_t q) {
-      return cen[3 * size_t(p) + axis] < cen[3 * size_t(q) + axis];
-    });
-    return m;
+    // No SAH split has both sides non-empty only when every centroid is the same point (on any
+    // axis with extent, the lowest and highest centroids fall in the first and last bins): halve.
+    return b + n / 2;
   }
 
   // Builds the interior node for [b,e) into nodes[self] (count > leafSize).
