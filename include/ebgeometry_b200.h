@@ -49,8 +49,8 @@ typedef enum ebg_build
 } ebg_build;
 
 /* ebg_build_opts.flags */
-#define EBG_BUILD_ON_DEVICE 1 /* meshes, Morton build: build the tree, records and boxes on the GPU
-                                 (the pseudonormals stay on the host, bit-identical to the DCEL) */
+#define EBG_BUILD_ON_DEVICE 1 /* meshes: build the tree (Morton or SAH, the host build's tree), the
+                                 pseudonormals (bit-identical to the DCEL), records and boxes on the GPU */
 
 typedef struct ebg_build_opts
 {
