@@ -93,7 +93,8 @@ class TriMeshSDF:
     from outside.  Pseudonormals are computed the way the reference's DCEL computes them unless
     ``vertex_normals`` (per corner, (T,3,3)) and ``edge_normals`` ((T,3,3), edge i from corner i to
     i+1) are given.  ``build``: "SAH" or "Morton"; ``leaf_size``: max triangles per leaf;
-    ``on_device``: build the (Morton) tree, records and boxes on the GPU.
+    ``on_device``: build the tree (either method; the host build's tree), pseudonormals, records and
+    boxes on the GPU.
     """
 
     def __init__(self, vertices, triangles, build="SAH", leaf_size=8, device=-1,
