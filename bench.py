@@ -629,7 +629,7 @@ def run_csg(args, rank, world, local_rank):
     stream = torch.cuda.current_stream(dev)
     t0 = time.time()
     sc = W.csg_scene(11, n_spheres=args.csg_spheres, n_meshes=args.csg_meshes)
-    tms = [TriMeshSDF(v, f, device=local_rank) for v, f in sc["meshes"]]
+    tms = [TriMeshSDF(v, f, device=local_rank, on_device=True) for v, f in sc["meshes"]]
     scene = BVHUnion(sc["spheres"], tms, sc["poses"], device=local_rank)
     t_build = time.time() - t0
     rng = np.random.default_rng(12)
