@@ -463,6 +463,169 @@ __device__ __forceinline__ int sahBin(double c, double cl, double k)
   return bi < 0 ? 0 : (bi > SAH_BINS - 1 ? SAH_BINS - 1 : bi);
 }
 
+// The split of least SAH cost over the merged bins (cnt[axis][bin], box keys[axis][bin][6]): the first
+// minimum over axis, then bin, among splits with both sides non-empty; axis -1 if none.
+__device__ void sahBestSplit(const uint32_t (&cnt)[3][SAH_BINS], const unsigned long long (&box)[3][SAH_BINS][6],
+                             const double k[3], int& outAxis, int& outBin)
+{
+  double bestCost = CUDART_INF;
+  int    bestAxis = -1, bestBin = -1;
+  for (int a = 0; a < 3; a++) {
+    if (k[a] == 0.0) {
+      continue;
+    }
+    double   rightArea[SAH_BINS];
+    uint32_t rightCnt[SAH_BINS];
+    double   al[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, ah[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    uint32_t c     = 0;
+    for (int i = SAH_BINS - 1; i > 0; i--) {
+      if (cnt[a][i] > 0) {
+        for (int x = 0; x < 3; x++) {
+          al[x] = fmin(al[x], dval(box[a][i][x]));
+          ah[x] = fmax(ah[x], dval(box[a][i][3 + x]));
+        }
+      }
+      c += cnt[a][i];
+      rightArea[i] = c > 0 ? boxArea(al, ah) : 0.0;
+      rightCnt[i]  = c;
+    }
+    double   ll[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, lh[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    uint32_t lc    = 0;
+    for (int i = 0; i < SAH_BINS - 1; i++) {
+      if (cnt[a][i] > 0) {
+        for (int x = 0; x < 3; x++) {
+          ll[x] = fmin(ll[x], dval(box[a][i][x]));
+          lh[x] = fmax(lh[x], dval(box[a][i][3 + x]));
+        }
+      }
+      lc += cnt[a][i];
+      if (lc == 0 || rightCnt[i + 1] == 0) {
+        continue;
+      }
+      const double cost =
+        __dadd_rn(__dmul_rn(boxArea(ll, lh), double(lc)), __dmul_rn(rightArea[i + 1], double(rightCnt[i + 1])));
+      if (cost < bestCost) {
+        bestCost = cost;
+        bestAxis = a;
+        bestBin  = i;
+      }
+    }
+  }
+  outAxis = bestAxis;
+  outBin  = bestBin;
+}
+
+// The two children of node `node` over [b, m) and [m, e): a single triangle is a leaf reference, a
+// longer range a new internal node and a task of the next level.
+__device__ void sahEmitChildren(uint32_t node, uint32_t b, uint32_t m, uint32_t e, uint32_t* left, uint32_t* right,
+                                SahTask* next, uint32_t* counters, uint32_t maxNodes, int* err)
+{
+  uint32_t       ref[2];
+  const uint32_t cb[2] = {b, m}, ce[2] = {m, e};
+  for (int c = 0; c < 2; c++) {
+    if (ce[c] - cb[c] == 1) {
+      ref[c] = EBG_LEAF_BIT | cb[c];
+    }
+    else {
+      const uint32_t id = atomicAdd(counters + 0, 1u);
+      if (id >= maxNodes) {
+        atomicOr(err, 32);
+        ref[c] = EBG_LEAF_BIT | cb[c];
+        continue;
+      }
+      ref[c]                            = id;
+      next[atomicAdd(counters + 1, 1u)] = SahTask{id, cb[c], ce[c]};
+    }
+  }
+  left[node]  = ref[0];
+  right[node] = ref[1];
+}
+
+// Block-level binning of [b, e) (centroid bins along every axis with k != 0): per-warp bins in
+// shared memory, merged in warp order into bcnt[0] / bbox[0].  Ends synchronised.
+__device__ void sahBinRange(const uint32_t* __restrict__ ids, uint32_t b, uint32_t e, const double* __restrict__ cen,
+                            const double* __restrict__ triLo, const double* __restrict__ triHi, const double cl[3],
+                            const double k[3], uint32_t (&bcnt)[SAH_WARPS][3][SAH_BINS],
+                            unsigned long long (&bbox)[SAH_WARPS][3][SAH_BINS][6])
+{
+  const int warp = threadIdx.x >> 5;
+  for (int q = threadIdx.x; q < SAH_WARPS * 3 * SAH_BINS; q += SAH_THREADS) {
+    const int w = q / (3 * SAH_BINS), r = q % (3 * SAH_BINS), a = r / SAH_BINS, bi = r % SAH_BINS;
+    bcnt[w][a][bi] = 0;
+    for (int c = 0; c < 3; c++) {
+      bbox[w][a][bi][c]     = ~0ull;
+      bbox[w][a][bi][3 + c] = 0ull;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
+    const size_t p = ids[i];
+    for (int a = 0; a < 3; a++) {
+      if (k[a] == 0.0) {
+        continue;
+      }
+      const int bi = sahBin(cen[3 * p + a], cl[a], k[a]);
+      atomicAdd(&bcnt[warp][a][bi], 1u);
+      for (int c = 0; c < 3; c++) {
+        atomicMin(&bbox[warp][a][bi][c], dkey(triLo[3 * p + c]));
+        atomicMax(&bbox[warp][a][bi][3 + c], dkey(triHi[3 * p + c]));
+      }
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < 3 * SAH_BINS; q += SAH_THREADS) {
+    const int a = q / SAH_BINS, bi = q % SAH_BINS;
+    for (int w = 1; w < SAH_WARPS; w++) {
+      bcnt[0][a][bi] += bcnt[w][a][bi];
+      for (int c = 0; c < 3; c++) {
+        bbox[0][a][bi][c]     = min(bbox[0][a][bi][c], bbox[w][a][bi][c]);
+        bbox[0][a][bi][3 + c] = max(bbox[0][a][bi][3 + c], bbox[w][a][bi][3 + c]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Block-level stable partition of ids[b, e) by (bin along ax <= bin): the left elements to
+// tmp[dstL ...], the right ones to tmp[dstR ...], each side in its original order.  wl, wr: one
+// shared slot per warp.  Ends synchronised.
+__device__ void sahPartitionRange(const uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp, uint32_t b,
+                                  uint32_t e, uint32_t dstL, uint32_t dstR, const double* __restrict__ cen, double cla,
+                                  double ka, int ax, int bin, uint32_t* wl, uint32_t* wr)
+{
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint32_t  offL = 0, offR = 0;
+  for (uint32_t base = b; base < e; base += SAH_THREADS) {
+    const uint32_t i     = base + threadIdx.x;
+    const bool     valid = i < e;
+    const uint32_t p     = valid ? ids[i] : 0u;
+    const bool     isL   = valid && sahBin(cen[3 * size_t(p) + ax], cla, ka) <= bin;
+    const unsigned bl    = __ballot_sync(FULL, isL);
+    const unsigned br    = __ballot_sync(FULL, valid && !isL);
+    if (lane == 0) {
+      wl[warp] = __popc(bl);
+      wr[warp] = __popc(br);
+    }
+    __syncthreads();
+    uint32_t pl = offL, pr = offR, tl = 0, tr = 0;
+    for (int w = 0; w < SAH_WARPS; w++) {
+      if (w < warp) {
+        pl += wl[w];
+        pr += wr[w];
+      }
+      tl += wl[w];
+      tr += wr[w];
+    }
+    const unsigned below = (1u << lane) - 1u;
+    if (valid) {
+      tmp[isL ? dstL + pl + __popc(bl & below) : dstR + pr + __popc(br & below)] = p;
+    }
+    offL += tl;
+    offR += tr;
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restrict__ tasks, uint32_t numTasks,
                                                          uint32_t* __restrict__ ids, uint32_t* __restrict__ tmp,
                                                          const double* __restrict__ triLo,
@@ -472,7 +635,7 @@ __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restri
                                                          uint32_t* __restrict__ first, uint32_t* __restrict__ last,
                                                          double* __restrict__ nodeLo, double* __restrict__ nodeHi,
                                                          SahTask* __restrict__ next, uint32_t* __restrict__ counters,
-                                                         uint32_t maxNodes, int* __restrict__ err)
+                                                         uint32_t maxNodes, uint32_t bigMin, int* __restrict__ err)
 {
   // per warp, axis and bin: count, and the bin's box as order-preserving keys (3 lo, 3 hi)
   __shared__ uint32_t           bcnt[SAH_WARPS][3][SAH_BINS];
@@ -481,11 +644,13 @@ __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restri
   __shared__ int                sAxis, sBin;
   __shared__ uint32_t           wl[SAH_WARPS], wr[SAH_WARPS];
   const BlockGroup              g{red};
-  const int                     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   for (uint32_t t = blockIdx.x; t < numTasks; t += gridDim.x) {
     const SahTask tk = tasks[t];
     const uint32_t b = tk.b, e = tk.e, n = e - b;
+    if (n > bigMin) {
+      continue; // a long range: the chunked kernels below take it
+    }
     // the range's box and its centroids' bounds
     double lo[3], hi[3], cl[3], ch[3];
     for (int a = 0; a < 3; a++) {
@@ -518,95 +683,15 @@ __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restri
     if (n <= uint32_t(leafSize)) {
       continue;
     }
-    // bins
-    for (int q = threadIdx.x; q < SAH_WARPS * 3 * SAH_BINS; q += SAH_THREADS) {
-      const int w = q / (3 * SAH_BINS), r = q % (3 * SAH_BINS), a = r / SAH_BINS, bi = r % SAH_BINS;
-      bcnt[w][a][bi] = 0;
-      for (int c = 0; c < 3; c++) {
-        bbox[w][a][bi][c]     = ~0ull;
-        bbox[w][a][bi][3 + c] = 0ull;
-      }
-    }
-    __syncthreads();
     double k[3];
     for (int a = 0; a < 3; a++) {
       const double ext = __dsub_rn(ch[a], cl[a]);
       k[a]             = ext > 0.0 ? __ddiv_rn(double(SAH_BINS), ext) : 0.0;
     }
-    for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
-      const size_t p = ids[i];
-      for (int a = 0; a < 3; a++) {
-        if (k[a] == 0.0) {
-          continue;
-        }
-        const int bi = sahBin(cen[3 * p + a], cl[a], k[a]);
-        atomicAdd(&bcnt[warp][a][bi], 1u);
-        for (int c = 0; c < 3; c++) {
-          atomicMin(&bbox[warp][a][bi][c], dkey(triLo[3 * p + c]));
-          atomicMax(&bbox[warp][a][bi][3 + c], dkey(triHi[3 * p + c]));
-        }
-      }
-    }
-    __syncthreads();
-    // merge the warps' bins into warp 0's
-    for (int q = threadIdx.x; q < 3 * SAH_BINS; q += SAH_THREADS) {
-      const int a = q / SAH_BINS, bi = q % SAH_BINS;
-      for (int w = 1; w < SAH_WARPS; w++) {
-        bcnt[0][a][bi] += bcnt[w][a][bi];
-        for (int c = 0; c < 3; c++) {
-          bbox[0][a][bi][c]     = min(bbox[0][a][bi][c], bbox[w][a][bi][c]);
-          bbox[0][a][bi][3 + c] = max(bbox[0][a][bi][3 + c], bbox[w][a][bi][3 + c]);
-        }
-      }
-    }
-    __syncthreads();
+    sahBinRange(ids, b, e, cen, triLo, triHi, cl, k, bcnt, bbox);
     // the cheapest split: thread 0 scans the axes in order, as the host does
     if (threadIdx.x == 0) {
-      double bestCost = CUDART_INF;
-      int    bestAxis = -1, bestBin = -1;
-      for (int a = 0; a < 3; a++) {
-        if (k[a] == 0.0) {
-          continue;
-        }
-        double   rightArea[SAH_BINS];
-        uint32_t rightCnt[SAH_BINS];
-        double   al[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, ah[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        uint32_t c     = 0;
-        for (int i = SAH_BINS - 1; i > 0; i--) {
-          if (bcnt[0][a][i] > 0) {
-            for (int x = 0; x < 3; x++) {
-              al[x] = fmin(al[x], dval(bbox[0][a][i][x]));
-              ah[x] = fmax(ah[x], dval(bbox[0][a][i][3 + x]));
-            }
-          }
-          c += bcnt[0][a][i];
-          rightArea[i] = c > 0 ? boxArea(al, ah) : 0.0;
-          rightCnt[i]  = c;
-        }
-        double   ll[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, lh[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        uint32_t lc    = 0;
-        for (int i = 0; i < SAH_BINS - 1; i++) {
-          if (bcnt[0][a][i] > 0) {
-            for (int x = 0; x < 3; x++) {
-              ll[x] = fmin(ll[x], dval(bbox[0][a][i][x]));
-              lh[x] = fmax(lh[x], dval(bbox[0][a][i][3 + x]));
-            }
-          }
-          lc += bcnt[0][a][i];
-          if (lc == 0 || rightCnt[i + 1] == 0) {
-            continue;
-          }
-          const double cost = __dadd_rn(__dmul_rn(boxArea(ll, lh), double(lc)),
-                                        __dmul_rn(rightArea[i + 1], double(rightCnt[i + 1])));
-          if (cost < bestCost) {
-            bestCost = cost;
-            bestAxis = a;
-            bestBin  = i;
-          }
-        }
-      }
-      sAxis = bestAxis;
-      sBin  = bestBin;
+      sahBestSplit(bcnt[0], bbox[0], k, sAxis, sBin);
     }
     __syncthreads();
     const int ax = sAxis, bin = sBin;
@@ -617,36 +702,7 @@ __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restri
       for (int i = 0; i <= bin; i++) {
         nl += bcnt[0][ax][i];
       }
-      uint32_t offL = 0, offR = 0;
-      for (uint32_t base = b; base < e; base += SAH_THREADS) {
-        const uint32_t i     = base + threadIdx.x;
-        const bool     valid = i < e;
-        const uint32_t p     = valid ? ids[i] : 0u;
-        const bool     isL   = valid && sahBin(cen[3 * size_t(p) + ax], cl[ax], k[ax]) <= bin;
-        const unsigned bl    = __ballot_sync(FULL, isL);
-        const unsigned br    = __ballot_sync(FULL, valid && !isL);
-        if (lane == 0) {
-          wl[warp] = __popc(bl);
-          wr[warp] = __popc(br);
-        }
-        __syncthreads();
-        uint32_t pl = offL, pr = offR, tl = 0, tr = 0;
-        for (int w = 0; w < SAH_WARPS; w++) {
-          if (w < warp) {
-            pl += wl[w];
-            pr += wr[w];
-          }
-          tl += wl[w];
-          tr += wr[w];
-        }
-        const unsigned below = (1u << lane) - 1u;
-        if (valid) {
-          tmp[isL ? b + pl + __popc(bl & below) : b + nl + pr + __popc(br & below)] = p;
-        }
-        offL += tl;
-        offR += tr;
-        __syncthreads();
-      }
+      sahPartitionRange(ids, tmp, b, e, b, b + nl, cen, cl[ax], k[ax], ax, bin, wl, wr);
       for (uint32_t i = b + threadIdx.x; i < e; i += SAH_THREADS) {
         ids[i] = tmp[i];
       }
@@ -654,27 +710,257 @@ __global__ void __launch_bounds__(SAH_THREADS) kSahLevel(const SahTask* __restri
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      uint32_t ref[2];
-      const uint32_t cb[2] = {b, m}, ce[2] = {m, e};
-      for (int c = 0; c < 2; c++) {
-        if (ce[c] - cb[c] == 1) {
-          ref[c] = EBG_LEAF_BIT | cb[c];
-        }
-        else {
-          const uint32_t id = atomicAdd(counters + 0, 1u);
-          if (id >= maxNodes) {
-            atomicOr(err, 32);
-            ref[c] = EBG_LEAF_BIT | cb[c];
-            continue;
-          }
-          ref[c]                               = id;
-          next[atomicAdd(counters + 1, 1u)]    = SahTask{id, cb[c], ce[c]};
-        }
-      }
-      left[tk.node]  = ref[0];
-      right[tk.node] = ref[1];
+      sahEmitChildren(tk.node, b, m, e, left, right, next, counters, maxNodes, err);
     }
     __syncthreads();
+  }
+}
+
+// The ranges longer than SAH_BIG triangles: one entry per range, one per SAH_CHUNK-triangle piece,
+// the same steps spread over many blocks (bounds, bins, split, stable partition by piece offsets);
+// merged piece results are exact (sums of counts, minima and maxima), so the split is the single
+// block's.
+constexpr uint32_t SAH_BIG   = 32768;
+constexpr uint32_t SAH_CHUNK = 8192;
+
+struct SahBig
+{
+  uint32_t node, b, e, c0, nc; // the task, its span, its first piece and piece count
+  int      ax, bin;
+  uint32_t nl;
+  double   cl[3], k[3];
+};
+struct SahChunk
+{
+  uint32_t big, b, e;
+};
+struct SahBins
+{
+  uint32_t           cnt[3][SAH_BINS];
+  unsigned long long box[3][SAH_BINS][6];
+};
+
+__global__ void __launch_bounds__(SAH_THREADS) kSahChunkBounds(const SahChunk* __restrict__ chunks, uint32_t numChunks,
+                                                               const uint32_t* __restrict__ ids,
+                                                               const double* __restrict__ triLo,
+                                                               const double* __restrict__ triHi,
+                                                               const double* __restrict__ cen, double* __restrict__ part)
+{
+  __shared__ double red[SAH_WARPS];
+  const BlockGroup  g{red};
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const SahChunk ck = chunks[c];
+    double         v[12];
+    for (int a = 0; a < 3; a++) {
+      v[a] = v[6 + a] = DBL_MAX;
+      v[3 + a] = v[9 + a] = -DBL_MAX;
+    }
+    for (uint32_t i = ck.b + threadIdx.x; i < ck.e; i += SAH_THREADS) {
+      const size_t p = ids[i];
+      for (int a = 0; a < 3; a++) {
+        v[a]     = fmin(v[a], triLo[3 * p + a]);
+        v[3 + a] = fmax(v[3 + a], triHi[3 * p + a]);
+        v[6 + a] = fmin(v[6 + a], cen[3 * p + a]);
+        v[9 + a] = fmax(v[9 + a], cen[3 * p + a]);
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      v[a]     = g.min(v[a]);
+      v[3 + a] = g.max(v[3 + a]);
+      v[6 + a] = g.min(v[6 + a]);
+      v[9 + a] = g.max(v[9 + a]);
+    }
+    if (threadIdx.x == 0) {
+      for (int q = 0; q < 12; q++) {
+        part[12 * size_t(c) + q] = v[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void kSahBigBounds(SahBig* __restrict__ bigs, uint32_t numBig, const double* __restrict__ part,
+                              uint32_t* __restrict__ first, uint32_t* __restrict__ last, double* __restrict__ nodeLo,
+                              double* __restrict__ nodeHi)
+{
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < numBig; t += gridDim.x * blockDim.x) {
+    SahBig& bg = bigs[t];
+    double  v[12];
+    for (int a = 0; a < 3; a++) {
+      v[a] = v[6 + a] = DBL_MAX;
+      v[3 + a] = v[9 + a] = -DBL_MAX;
+    }
+    for (uint32_t c = bg.c0; c < bg.c0 + bg.nc; c++) {
+      const double* pc = part + 12 * size_t(c);
+      for (int a = 0; a < 3; a++) {
+        v[a]     = fmin(v[a], pc[a]);
+        v[3 + a] = fmax(v[3 + a], pc[3 + a]);
+        v[6 + a] = fmin(v[6 + a], pc[6 + a]);
+        v[9 + a] = fmax(v[9 + a], pc[9 + a]);
+      }
+    }
+    for (int a = 0; a < 3; a++) {
+      nodeLo[3 * size_t(bg.node) + a] = v[a];
+      nodeHi[3 * size_t(bg.node) + a] = v[3 + a];
+      bg.cl[a]                        = v[6 + a];
+      const double ext                = __dsub_rn(v[9 + a], v[6 + a]);
+      bg.k[a]                         = ext > 0.0 ? __ddiv_rn(double(SAH_BINS), ext) : 0.0;
+    }
+    first[bg.node] = bg.b;
+    last[bg.node]  = bg.e - 1;
+  }
+}
+
+__global__ void __launch_bounds__(SAH_THREADS) kSahChunkBins(const SahChunk* __restrict__ chunks, uint32_t numChunks,
+                                                             const SahBig* __restrict__ bigs,
+                                                             const uint32_t* __restrict__ ids,
+                                                             const double* __restrict__ triLo,
+                                                             const double* __restrict__ triHi,
+                                                             const double* __restrict__ cen, SahBins* __restrict__ out)
+{
+  __shared__ uint32_t           bcnt[SAH_WARPS][3][SAH_BINS];
+  __shared__ unsigned long long bbox[SAH_WARPS][3][SAH_BINS][6];
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const SahChunk ck = chunks[c];
+    const SahBig&  bg = bigs[ck.big];
+    const double   cl[3] = {bg.cl[0], bg.cl[1], bg.cl[2]}, k[3] = {bg.k[0], bg.k[1], bg.k[2]};
+    sahBinRange(ids, ck.b, ck.e, cen, triLo, triHi, cl, k, bcnt, bbox);
+    for (int q = threadIdx.x; q < 3 * SAH_BINS; q += SAH_THREADS) {
+      const int a = q / SAH_BINS, bi = q % SAH_BINS;
+      out[c].cnt[a][bi] = bcnt[0][a][bi];
+      for (int x = 0; x < 6; x++) {
+        out[c].box[a][bi][x] = bbox[0][a][bi][x];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(SAH_THREADS) kSahBigSplit(SahBig* __restrict__ bigs, uint32_t numBig,
+                                                            const SahBins* __restrict__ bins)
+{
+  __shared__ uint32_t           cnt[3][SAH_BINS];
+  __shared__ unsigned long long box[3][SAH_BINS][6];
+  __shared__ int                sAxis, sBin;
+  for (uint32_t t = blockIdx.x; t < numBig; t += gridDim.x) {
+    SahBig& bg = bigs[t];
+    for (int q = threadIdx.x; q < 3 * SAH_BINS; q += SAH_THREADS) {
+      const int          a = q / SAH_BINS, bi = q % SAH_BINS;
+      uint32_t           n = 0;
+      unsigned long long v[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+      for (uint32_t c = bg.c0; c < bg.c0 + bg.nc; c++) {
+        n += bins[c].cnt[a][bi];
+        for (int x = 0; x < 3; x++) {
+          v[x]     = min(v[x], bins[c].box[a][bi][x]);
+          v[3 + x] = max(v[3 + x], bins[c].box[a][bi][3 + x]);
+        }
+      }
+      cnt[a][bi] = n;
+      for (int x = 0; x < 6; x++) {
+        box[a][bi][x] = v[x];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const double k[3] = {bg.k[0], bg.k[1], bg.k[2]};
+      sahBestSplit(cnt, box, k, sAxis, sBin);
+      uint32_t nl = 0;
+      if (sAxis >= 0) {
+        for (int i = 0; i <= sBin; i++) {
+          nl += cnt[sAxis][i];
+        }
+      }
+      bg.ax  = sAxis;
+      bg.bin = sBin;
+      bg.nl  = nl;
+    }
+    __syncthreads();
+  }
+}
+
+// each piece's left-element count, then each range's pieces' offsets in piece order
+__global__ void __launch_bounds__(SAH_THREADS) kSahChunkCount(const SahChunk* __restrict__ chunks, uint32_t numChunks,
+                                                              const SahBig* __restrict__ bigs,
+                                                              const uint32_t* __restrict__ ids,
+                                                              const double* __restrict__ cen,
+                                                              uint32_t* __restrict__ chunkL)
+{
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const SahChunk ck = chunks[c];
+    const SahBig&  bg = bigs[ck.big];
+    uint32_t       nL = 0;
+    if (bg.ax >= 0) {
+      for (uint32_t base = ck.b; base < ck.e; base += SAH_THREADS) {
+        const uint32_t i   = base + threadIdx.x;
+        const bool     isL = i < ck.e && sahBin(cen[3 * size_t(ids[i]) + bg.ax], bg.cl[bg.ax], bg.k[bg.ax]) <= bg.bin;
+        nL += uint32_t(__syncthreads_count(isL));
+      }
+    }
+    if (threadIdx.x == 0) {
+      chunkL[c] = nL;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void kSahBigOffsets(const SahBig* __restrict__ bigs, uint32_t numBig, const SahChunk* __restrict__ chunks,
+                               const uint32_t* __restrict__ chunkL, uint32_t* __restrict__ offL,
+                               uint32_t* __restrict__ offR)
+{
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < numBig; t += gridDim.x * blockDim.x) {
+    const SahBig& bg = bigs[t];
+    uint32_t      l = 0, r = 0;
+    for (uint32_t c = bg.c0; c < bg.c0 + bg.nc; c++) {
+      offL[c] = l;
+      offR[c] = r;
+      l += chunkL[c];
+      r += (chunks[c].e - chunks[c].b) - chunkL[c];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SAH_THREADS) kSahChunkScatter(const SahChunk* __restrict__ chunks,
+                                                                uint32_t numChunks, const SahBig* __restrict__ bigs,
+                                                                const uint32_t* __restrict__ ids,
+                                                                uint32_t* __restrict__ tmp,
+                                                                const double* __restrict__ cen,
+                                                                const uint32_t* __restrict__ offL,
+                                                                const uint32_t* __restrict__ offR)
+{
+  __shared__ uint32_t wl[SAH_WARPS], wr[SAH_WARPS];
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const SahChunk ck = chunks[c];
+    const SahBig&  bg = bigs[ck.big];
+    if (bg.ax < 0) {
+      continue;
+    }
+    sahPartitionRange(ids, tmp, ck.b, ck.e, bg.b + offL[c], bg.b + bg.nl + offR[c], cen, bg.cl[bg.ax], bg.k[bg.ax],
+                      bg.ax, bg.bin, wl, wr);
+  }
+}
+
+__global__ void kSahChunkCopy(const SahChunk* __restrict__ chunks, uint32_t numChunks, const SahBig* __restrict__ bigs,
+                              uint32_t* __restrict__ ids, const uint32_t* __restrict__ tmp)
+{
+  for (uint32_t c = blockIdx.x; c < numChunks; c += gridDim.x) {
+    const SahChunk ck = chunks[c];
+    if (bigs[ck.big].ax < 0) {
+      continue;
+    }
+    for (uint32_t i = ck.b + threadIdx.x; i < ck.e; i += blockDim.x) {
+      ids[i] = tmp[i];
+    }
+  }
+}
+
+__global__ void kSahBigChildren(const SahBig* __restrict__ bigs, uint32_t numBig, uint32_t* __restrict__ left,
+                                uint32_t* __restrict__ right, SahTask* __restrict__ next,
+                                uint32_t* __restrict__ counters, uint32_t maxNodes, int* __restrict__ err)
+{
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < numBig; t += gridDim.x * blockDim.x) {
+    const SahBig&  bg = bigs[t];
+    const uint32_t m  = bg.ax >= 0 ? bg.b + bg.nl : bg.b + (bg.e - bg.b) / 2;
+    sahEmitChildren(bg.node, bg.b, m, bg.e, left, right, next, counters, maxNodes, err);
   }
 }
 
@@ -1339,16 +1625,70 @@ ebg_status buildMeshOnDevice(ebg_mesh* m, const double* V, int64_t nv, const int
       const uint32_t init[2] = {1u, 0u};
       cudaMemcpyAsync(tasks[0], &root, sizeof(root), cudaMemcpyHostToDevice, s);
       cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
-      uint32_t count = 1;
-      int      cur   = 0;
+      uint32_t count  = 1;
+      int      cur    = 0;
+      bool     mayBig = uint64_t(n) > SAH_BIG;
       for (int level = 0; count > 0; level++) {
         if (level > 256) {
           return setError(EBG_ERR_INVALID, "device SAH build: tree deeper than 256 levels");
         }
+        // the level's long ranges (only the first few levels have any), cut into pieces
+        std::vector<SahBig>   bigs;
+        std::vector<SahChunk> chunks;
+        if (mayBig) {
+          std::vector<SahTask> ht(count);
+          cudaMemcpyAsync(ht.data(), tasks[cur], sizeof(SahTask) * count, cudaMemcpyDeviceToHost, s);
+          if (cudaStreamSynchronize(s) != cudaSuccess) {
+            return setError(EBG_ERR_CUDA, std::string("device SAH build: ") + cudaGetErrorString(cudaGetLastError()));
+          }
+          for (const SahTask& t : ht) {
+            if (t.e - t.b <= SAH_BIG) {
+              continue;
+            }
+            SahBig bg{};
+            bg.node = t.node;
+            bg.b    = t.b;
+            bg.e    = t.e;
+            bg.c0   = uint32_t(chunks.size());
+            for (uint32_t c = t.b; c < t.e; c += SAH_CHUNK) {
+              chunks.push_back(SahChunk{uint32_t(bigs.size()), c, std::min(c + SAH_CHUNK, t.e)});
+              bg.nc++;
+            }
+            bg.ax = -1;
+            bigs.push_back(bg);
+          }
+          mayBig = !bigs.empty(); // ranges only shrink
+        }
         cudaMemsetAsync(counters + 1, 0, 4, s);
         kSahLevel<<<gridFor(count, 1, 1 << 16), SAH_THREADS, 0, s>>>(
           tasks[cur], count, ids, idsIn, triLo, triHi, cen, leafSize, left, right, first, last, nodeLo, nodeHi,
-          tasks[1 - cur], counters, uint32_t(NI), overflow);
+          tasks[1 - cur], counters, uint32_t(NI), bigs.empty() ? UINT32_MAX : SAH_BIG, overflow);
+        if (!bigs.empty()) {
+          const uint32_t nb = uint32_t(bigs.size()), nc = uint32_t(chunks.size());
+          SahBig*        dBig = nullptr;
+          SahChunk*      dCh  = nullptr;
+          double*        part = nullptr;
+          SahBins*       bins = nullptr;
+          uint32_t *     cL = nullptr, *oL = nullptr, *oR = nullptr;
+          if (!alloc((void**)&dBig, sizeof(SahBig) * nb) || !alloc((void**)&dCh, sizeof(SahChunk) * nc) ||
+              !alloc((void**)&part, 96 * size_t(nc)) || !alloc((void**)&bins, sizeof(SahBins) * nc) ||
+              !alloc((void**)&cL, 4 * size_t(nc)) || !alloc((void**)&oL, 4 * size_t(nc)) ||
+              !alloc((void**)&oR, 4 * size_t(nc))) {
+            return setError(EBG_ERR_NO_MEMORY, "device SAH build workspace");
+          }
+          cudaMemcpyAsync(dBig, bigs.data(), sizeof(SahBig) * nb, cudaMemcpyHostToDevice, s);
+          cudaMemcpyAsync(dCh, chunks.data(), sizeof(SahChunk) * nc, cudaMemcpyHostToDevice, s);
+          const unsigned gb = gridFor(nb, 128);
+          kSahChunkBounds<<<nc, SAH_THREADS, 0, s>>>(dCh, nc, ids, triLo, triHi, cen, part);
+          kSahBigBounds<<<gb, 128, 0, s>>>(dBig, nb, part, first, last, nodeLo, nodeHi);
+          kSahChunkBins<<<nc, SAH_THREADS, 0, s>>>(dCh, nc, dBig, ids, triLo, triHi, cen, bins);
+          kSahBigSplit<<<nb, SAH_THREADS, 0, s>>>(dBig, nb, bins);
+          kSahChunkCount<<<nc, SAH_THREADS, 0, s>>>(dCh, nc, dBig, ids, cen, cL);
+          kSahBigOffsets<<<gb, 128, 0, s>>>(dBig, nb, dCh, cL, oL, oR);
+          kSahChunkScatter<<<nc, SAH_THREADS, 0, s>>>(dCh, nc, dBig, ids, idsIn, cen, oL, oR);
+          kSahChunkCopy<<<nc, 256, 0, s>>>(dCh, nc, dBig, ids, idsIn);
+          kSahBigChildren<<<gb, 128, 0, s>>>(dBig, nb, left, right, tasks[1 - cur], counters, uint32_t(NI), overflow);
+        }
         uint32_t hc[2];
         cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
         if (cudaStreamSynchronize(s) != cudaSuccess) {

@@ -24,7 +24,7 @@ def query(m, p, **kw):
 
 
 @pytest.mark.parametrize("build", ["Morton", "SAH"])
-@pytest.mark.parametrize("level,leaf", [(3, 8), (5, 8), (5, 1), (5, 32)])
+@pytest.mark.parametrize("level,leaf", [(3, 8), (5, 8), (5, 1), (5, 32), (6, 8), (7, 4)])
 def test_device_build_equals_host_build(level, leaf, build):
     v, f = W.displaced_icosphere(level, 3)
     p = np.concatenate([W.uniform_points(100000, 4), W.band_points(v, f, 30000, 5)])
