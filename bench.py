@@ -471,7 +471,11 @@ def run_ours(args, rank, world, local_rank):
                      "kernel": "kMeshSdf32 (FP32 packet traversal" + (", seeded)" if seed is not None else ")"),
                      "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit): 16 B query in/out + 128 B per node + "
                                     "64 B per oriented box + 48 B per triangle",
-                     "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs},
+                     "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs,
+                     # the floor: every byte the step must touch once (the mesh's device arrays, the
+                     # points in, the distances out) at the measured HBM rate
+                     "unique_bytes_per_step": int(mesh.info["device_bytes"]) + 16 * n,
+                     "unique_floor_ms": (int(mesh.info["device_bytes"]) + 16 * n) / (hbm_peak * 1e6)},
         "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                 "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},
         "gpu_launches": (4 if seed is not None else 3) * args.steps,
