@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--build", default="Morton")
     ap.add_argument("--leaf", type=int, default=8)
     ap.add_argument("--host-build", action="store_true",
-                    help="build the tree on the host (default: on the GPU for Morton builds)")
+                    help="build the tree on the host (default: on the GPU, for Morton and SAH builds alike)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU work of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -286,7 +286,7 @@ def run_ours(args, rank, world, local_rank):
     n = pts.shape[0]
     n_grid, n_band = args.grid ** 3, args.band_points
     t0 = time.time()
-    on_device = args.build.upper() == "MORTON" and not args.host_build
+    on_device = not args.host_build
     mesh = TriMeshSDF(v, f, build=args.build, leaf_size=args.leaf, device=local_rank, on_device=on_device)
     t_build = time.time() - t0
     log(f"[rank {rank}] mesh {f.shape[0]} tris built in {t_build:.2f}s: {mesh.info}")
