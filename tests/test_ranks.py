@@ -6,7 +6,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-from ebgeometry_b200.ranks import max_over_ranks, shard_range
+from ebgeometry_b200.ranks import max_over_ranks, shard_range, sharded_query
 
 
 def _free_port():
@@ -22,8 +22,15 @@ def _worker(rank, world, port, q):
     import datetime
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
+        import torch
         ms = 10.0 + 5.0 * rank
-        q.put((rank, max_over_ranks(ms), shard_range(1001, rank, world)))
+        # a stand-in query (sum of coordinates, tagged with the rank that evaluated it) over a
+        # point set that does not divide evenly: every rank ends with every point's answer
+        pts = torch.arange(3 * 1001, dtype=torch.float64).reshape(1001, 3)
+        full, span = sharded_query(lambda x: torch.stack([x.sum(1), torch.full((x.shape[0],), float(rank),
+                                                                             dtype=torch.float64)], 1), pts)
+        local, lspan = sharded_query(lambda x: x[:, 0], pts, gather=False)
+        q.put((rank, max_over_ranks(ms), shard_range(1001, rank, world), full.numpy(), span, local.numpy(), lspan))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -41,10 +48,18 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    got.sort()
-    assert all(m == 15.0 for _, m, _ in got)
-    spans = [s for _, _, s in got]
+    got.sort(key=lambda g: g[0])
+    assert all(g[1] == 15.0 for g in got)
+    spans = [g[2] for g in got]
     assert spans[0][0] == 0 and spans[-1][1] == 1001 and spans[0][1] == spans[1][0]
+    import numpy as np
+    pts = np.arange(3 * 1001, dtype=np.float64).reshape(1001, 3)
+    for rank, _, _, full, span, local, lspan in got:
+        assert span == (0, 1001) and full.shape == (1001, 2)
+        assert np.array_equal(full[:, 0], pts.sum(1))
+        # the first ceil(1001/2) answers came from rank 0, the rest from rank 1
+        assert np.array_equal(full[:, 1], (np.arange(1001) >= spans[0][1]).astype(np.float64))
+        assert lspan == spans[rank] and np.array_equal(local, pts[lspan[0]:lspan[1], 0])
 
 
 @pytest.mark.parametrize("n,world", [(0, 3), (10, 4), (1000003, 8)])
