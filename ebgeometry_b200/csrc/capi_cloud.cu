@@ -59,6 +59,7 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
   }
   int device = 0;
   cudaGetDevice(&device);
+  keepPoolMemory();
   auto* c   = new ebg_cloud;
   c->device = device;
   c->n      = n;

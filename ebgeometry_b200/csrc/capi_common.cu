@@ -18,6 +18,17 @@ ebg_status setError(ebg_status code, const std::string& msg)
   return code;
 }
 
+void keepPoolMemory()
+{
+  int           device = 0;
+  cudaMemPool_t pool;
+  if (cudaGetDevice(&device) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+}
+
 namespace {
 
 // Streams float4 loads over a buffer (grid-stride, 4 independent loads in flight per thread) and

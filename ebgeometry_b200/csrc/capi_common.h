@@ -13,6 +13,12 @@ namespace ebg {
 // Records msg as the calling thread's last error and returns code.
 ebg_status setError(ebg_status code, const std::string& msg);
 
+// Keeps freed stream-ordered allocations in the current device's default memory pool.  Query calls
+// take their workspace from that pool; with the driver's default release threshold (0) the pool
+// returns its memory at every synchronisation and the next call maps it again, which costs
+// milliseconds per call and varies from call to call.  Called by every create entry point.
+void keepPoolMemory();
+
 // Restores the caller's current CUDA device on scope exit (entry points switch to the handle's).
 struct DeviceGuard
 {

@@ -281,16 +281,7 @@ ebg_status buildMesh(const double*         V,
     return setError(EBG_ERR_NOT_FOUND, "no CUDA device");
   }
 
-  // Keep freed stream-ordered allocations in the device's default pool: every query call takes its
-  // workspace from it, and returning the memory to the driver at each synchronisation would make
-  // the next call map it again.
-  {
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-      uint64_t keep = UINT64_MAX;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-  }
+  keepPoolMemory();
   auto* m   = new ebg_mesh;
   m->device = device;
   cudaDeviceGetAttribute(&m->numSms, cudaDevAttrMultiProcessorCount, device);

@@ -108,6 +108,7 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
   if (cudaSetDevice(device) != cudaSuccess) {
     return setError(EBG_ERR_NOT_FOUND, "cannot select CUDA device");
   }
+  keepPoolMemory();
   const int64_t            no = num_spheres + num_meshes;
   std::vector<SceneObject> objs(no);
   std::vector<double>      lo(3 * no), hi(3 * no), cen(3 * no);

@@ -365,6 +365,7 @@ ebg_status ebg_grid_create(const float* points_host, int64_t n, double target_pe
   if (device >= 0 && cudaSetDevice(device) != cudaSuccess) {
     return setError(EBG_ERR_NOT_FOUND, "cannot select CUDA device " + std::to_string(device));
   }
+  keepPoolMemory();
   auto* G   = new ebg_grid;
   G->target = target_per_cell > 0 ? target_per_cell : 1.0;
   cudaGetDevice(&G->device);

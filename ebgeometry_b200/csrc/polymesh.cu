@@ -395,6 +395,7 @@ ebg_status buildPoly(const double* V, int64_t nv, const int64_t* off, const int3
   else if (cudaGetDevice(&device) != cudaSuccess) {
     return setError(EBG_ERR_NOT_FOUND, "no CUDA device");
   }
+  keepPoolMemory();
   std::string         msg;
   std::vector<double> faceN, cen, cornerVN, edgeN;
   if (!computePolygonNormals(V, nv, off, idx, nf, faceN, cen, cornerVN, edgeN, msg)) {
