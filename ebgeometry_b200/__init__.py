@@ -413,10 +413,13 @@ class PointCloudBVH:
     ``points``: (n,3) float32, a numpy array (built after a host->device copy) or a CUDA tensor
     (built in place).  Neighbours come in increasing (squared distance, index) order, so equal
     distances resolve to the lowest index; squared distances are the reference's float arithmetic.
+    ``leaf_size``: at most that many points per leaf (<= 32).  The tree divides the Morton-ordered
+    points where the Morton curve jumps; ``balanced=True`` groups fixed runs of ``leaf_size`` points
+    four at a time instead (the same answers, more work per query on clustered clouds).
     """
 
-    def __init__(self, points, leaf_size=16, device=-1, stream=None):
-        opts = _capi.BuildOpts(0, int(leaf_size), int(device), 0)
+    def __init__(self, points, leaf_size=16, device=-1, stream=None, balanced=False):
+        opts = _capi.BuildOpts(0, int(leaf_size), int(device), 2 if balanced else 0)
         h = C.c_void_p()
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
@@ -436,6 +439,12 @@ class PointCloudBVH:
         if h is not None and h.value and lib is not None:
             lib.ebg_cloud_destroy(h)
             self._h = None
+
+    def tree_info(self):
+        """{"nodes": 4-wide nodes, "depth": node levels, "radix": False for the balanced tree}."""
+        nn, d, r = C.c_int64(), C.c_int32(), C.c_int32()
+        check(lib.ebg_cloud_tree_info(self._h, C.byref(nn), C.byref(d), C.byref(r)))
+        return {"nodes": nn.value, "depth": d.value, "radix": bool(r.value)}
 
     def numPoints(self) -> int:
         return int(lib.ebg_cloud_size(self._h))

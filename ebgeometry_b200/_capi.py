@@ -117,6 +117,7 @@ SIGNATURES = {
     "ebg_cloud_create_device": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P), _P]),
     "ebg_cloud_destroy": (C.c_int, [_P]),
     "ebg_cloud_size": (_I64, [_P]),
+    "ebg_cloud_tree_info": (C.c_int, [_P, _P, _P, _P]),
     "ebg_cloud_knn": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_knn_host": (C.c_int, [_P, _P, _I64, _I32, _P, _P, C.POINTER(QueryOpts), _P]),
     "ebg_cloud_self_knn": (C.c_int, [_P, _I32, _P, _P, _P]),

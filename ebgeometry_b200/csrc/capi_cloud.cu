@@ -22,7 +22,9 @@ struct ebg_cloud
   int          numSms  = 148;
   int64_t      n       = 0;
   int          leaf    = 16;
-  int          levels  = 0;
+  int          levels  = 0;     // node levels of the tree (0: the root is one leaf)
+  int64_t      numNodes = 0;
+  bool         radixTree = false; // false: the balanced fallback tree
   EbgCloudView view{};
   void*        dNodes  = nullptr;
   void*        dPoints = nullptr;
@@ -66,15 +68,7 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
   c->leaf   = L;
   cudaDeviceGetAttribute(&c->numSms, cudaDevAttrMultiProcessorCount, device);
 
-  const int64_t nLeaves = (n + L - 1) / L;
-  int64_t       levelNodes[64];
-  c->levels           = cloudLevels(nLeaves, levelNodes, 64);
-  int64_t totalNodes  = 0;
-  for (int l = 0; l < c->levels; l++) {
-    totalNodes += levelNodes[l];
-  }
-  if (cudaMalloc(&c->dNodes, std::max<int64_t>(totalNodes, 1) * sizeof(EbgNode4)) != cudaSuccess ||
-      cudaMalloc(&c->dPoints, size_t(n) * sizeof(float4)) != cudaSuccess ||
+  if (cudaMalloc(&c->dPoints, size_t(n) * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&c->dInv), size_t(n) * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(reinterpret_cast<void**>(&c->dStatus), sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
@@ -82,35 +76,29 @@ ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* 
     return setError(EBG_ERR_NO_MEMORY, "device allocation for the point cloud");
   }
   cudaMemsetAsync(c->dStatus, 0, sizeof(int), s);
-
-  std::vector<void*> ws;
-  CloudBuildBuffers  b{};
-  b.box           = devAlloc<uint32_t>(6, s, ws);
-  b.keysIn        = devAlloc<uint32_t>(n, s, ws);
-  b.keysOut       = devAlloc<uint32_t>(n, s, ws);
-  b.idsIn         = devAlloc<uint32_t>(n, s, ws);
-  b.idsOut        = devAlloc<uint32_t>(n, s, ws);
-  b.sortTempBytes = cloudSortTempBytes(n);
-  b.sortTemp      = devAlloc<char>(b.sortTempBytes, s, ws);
-  b.boxA          = devAlloc<float>(6 * nLeaves, s, ws);
-  b.boxB          = devAlloc<float>(6 * std::max<int64_t>(levelNodes[0], 1), s, ws);
-  if (!b.box || !b.keysIn || !b.keysOut || !b.idsIn || !b.idsOut || !b.sortTemp || !b.boxA || !b.boxB) {
-    freeAll(ws, s);
-    ebg_cloud_destroy(c);
-    return setError(EBG_ERR_NO_MEMORY, "build workspace for the point cloud");
-  }
-  float rootBox[6];
-  cudaError_t e = buildCloud(pointsDev, n, L, b, static_cast<EbgNode4*>(c->dNodes), static_cast<float4*>(c->dPoints),
-                             levelNodes, c->levels, rootBox, s);
-  freeAll(ws, s);
+  CloudTree   tree;
+  const bool  balanced = opts && (opts->flags & EBG_CLOUD_BALANCED);
+  cudaError_t e        = buildCloud(pointsDev, n, L, balanced, static_cast<float4*>(c->dPoints), tree, s);
+  c->dNodes     = tree.nodes;
   if (e == cudaSuccess) {
     launchInvertOrder(static_cast<const float4*>(c->dPoints), n, c->dInv, s);
     e = cudaGetLastError();
   }
-  if (e != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
-    ebg_cloud_destroy(c);
-    return setError(EBG_ERR_CUDA, std::string("point cloud build failed: ") + cudaGetErrorString(cudaGetLastError()));
+  if (e == cudaSuccess) {
+    e = cudaStreamSynchronize(s);
   }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ebg_cloud_destroy(c);
+    if (e == cudaErrorMemoryAllocation) {
+      return setError(EBG_ERR_NO_MEMORY, "build workspace for the point cloud");
+    }
+    return setError(EBG_ERR_CUDA, std::string("point cloud build failed: ") + cudaGetErrorString(e));
+  }
+  c->levels      = tree.depth;
+  c->numNodes    = tree.numNodes;
+  c->radixTree   = tree.radix;
+  const float* rootBox = tree.rootBox;
   EbgCloudView& v = c->view;
   v.nodes         = static_cast<const EbgNode4*>(c->dNodes);
   v.points        = static_cast<const float4*>(c->dPoints);
@@ -276,6 +264,23 @@ ebg_status ebg_cloud_destroy(ebg_cloud* c)
 }
 
 int64_t ebg_cloud_size(const ebg_cloud* c) { return c ? c->n : 0; }
+
+ebg_status ebg_cloud_tree_info(const ebg_cloud* c, int64_t* num_nodes, int32_t* depth, int32_t* radix)
+{
+  if (c == nullptr) {
+    return setError(EBG_ERR_INVALID, "null cloud");
+  }
+  if (num_nodes) {
+    *num_nodes = c->numNodes;
+  }
+  if (depth) {
+    *depth = c->levels;
+  }
+  if (radix) {
+    *radix = c->radixTree ? 1 : 0;
+  }
+  return EBG_OK;
+}
 
 ebg_status ebg_cloud_knn(const ebg_cloud*      c,
                          const float*          queries_dev,

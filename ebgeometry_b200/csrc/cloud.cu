@@ -5,12 +5,17 @@
 // queried by pruneTraverse with a {d2, index} state for k = 1 and an insertion-sorted Hit[k] for
 // k > 1 (PointCloudBVHImplem.hpp:263-427).
 //
-// Build here (all on the device, a few kernels):
+// Build here (all on the device):
 //   1. bounding box of the points; 2. 30-bit Morton key of each point in that box; 3. radix sort
-//   of (key, index); 4. leaves = runs of L consecutive sorted points, stored as float4
-//   (x, y, z, original index) -- one or two 128-byte lines per leaf; 5. an implicit 4-ary tree over
-//   the leaves in Morton order, level by level (node j of a level owns children 4j..4j+3 of the level
-//   below), written as 128-byte EbgNode4 records with the root at index 0.
+//   of (key, index); 4. the points gathered into that order as float4 (x, y, z, original index);
+//   5. a 4-wide tree built top-down, one launch per level: a node owns a range of sorted points,
+//   divided at the highest bit in which the range's first and last keys differ (the middle when all
+//   its keys are equal), and its largest part divided again, until it has four parts or none holds
+//   more than L points; a part of at most L points is a leaf (a run of consecutive points);
+//   6. node boxes bottom-up, one launch per level.  Cutting where the Morton curve jumps keeps
+//   every box spatially compact.  (Fixed runs of L points grouped four at a time in Morton order --
+//   the balanced tree kept as the fallback for clouds whose radix tree is too deep for the
+//   traversal stack -- make long, thin boxes across those jumps that every nearby query opens.)
 // Query: Morton-sorted queries in packets of 32 per warp with a shared stack (as the mesh kernel);
 // each lane keeps its k best (d2, index) pairs sorted in registers.  Order is lexicographic on
 // (d2, index), so equal distances resolve to the lowest index, and d2 is the reference's float
@@ -21,6 +26,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstdint>
+#include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -187,6 +193,159 @@ __global__ void kTreeLevel(int64_t nNodes, int64_t nChild, const float* __restri
   for (int a = 0; a < 3; a++) {
     outBoxes[6 * j + a]     = lo[a];
     outBoxes[6 * j + 3 + a] = hi[a];
+  }
+}
+
+// ---- top-down radix build ----------------------------------------------------------------------
+
+struct CloudTask
+{
+  uint32_t b, e, node; // sorted point range [b, e) of node `node`
+};
+
+// The first position of [b, e) (e - b >= 2) whose key differs from keys[b] in the highest bit where
+// keys[b] and keys[e - 1] differ; the middle when the range's keys are all equal.
+__device__ __forceinline__ uint32_t radixSplit(const uint32_t* __restrict__ keys, uint32_t b, uint32_t e)
+{
+  const uint32_t x = keys[b] ^ keys[e - 1];
+  if (x == 0u) {
+    return b + (e - b) / 2;
+  }
+  const int      bit = 31 - __clz(int(x));
+  const uint32_t pre = keys[b] >> bit;
+  uint32_t       lo = b + 1, hi = e - 1; // keys[e - 1] >> bit != pre: the answer lies in [b + 1, e - 1]
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if ((keys[mid] >> bit) == pre) {
+      lo = mid + 1;
+    }
+    else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// One level: each task's node gets 2-4 parts (the largest part of more than L points is divided
+// until there are four, ties to the lowest slot); leaf parts get their boxes here, interior parts a
+// node index (counters[0]), a task for the next level (counters[1]) and an empty box that the box
+// pass fills.  A node index at or above maxNodes sets *overflow and leaves the slot empty.
+__global__ void kCloudSplit(const CloudTask* __restrict__ tasks, uint32_t count, const uint32_t* __restrict__ keys,
+                            const float4* __restrict__ pts, int L, EbgNode4* __restrict__ nodes,
+                            CloudTask* __restrict__ next, uint32_t* __restrict__ counters,
+                            uint32_t* __restrict__ parentSlot, uint32_t maxNodes, int* __restrict__ overflow)
+{
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < count; w += gridDim.x * blockDim.x) {
+    const CloudTask t = tasks[w];
+    uint32_t        pb[4], pe[4];
+    int             nc = 1;
+    pb[0]              = t.b;
+    pe[0]              = t.e;
+    while (nc < 4) {
+      int      pick = -1;
+      uint32_t most = uint32_t(L);
+      for (int i = 0; i < nc; i++) {
+        if (pe[i] - pb[i] > most) {
+          most = pe[i] - pb[i];
+          pick = i;
+        }
+      }
+      if (pick < 0) {
+        break;
+      }
+      const uint32_t m = radixSplit(keys, pb[pick], pe[pick]);
+      for (int i = nc; i > pick + 1; i--) {
+        pb[i] = pb[i - 1];
+        pe[i] = pe[i - 1];
+      }
+      pb[pick + 1] = m;
+      pe[pick + 1] = pe[pick];
+      pe[pick]     = m;
+      nc++;
+    }
+    EbgNode4 nd;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float    lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+      uint32_t child = 0, cnt = 0;
+      bool     leafBox = false;
+      if (k < nc) {
+        const uint32_t c = pe[k] - pb[k];
+        if (c <= uint32_t(L)) {
+          for (uint32_t i = pb[k]; i < pe[k]; i++) {
+            const float4 q = pts[i];
+            lo[0]          = fminf(lo[0], q.x);
+            lo[1]          = fminf(lo[1], q.y);
+            lo[2]          = fminf(lo[2], q.z);
+            hi[0]          = fmaxf(hi[0], q.x);
+            hi[1]          = fmaxf(hi[1], q.y);
+            hi[2]          = fmaxf(hi[2], q.z);
+          }
+          child   = EBG_LEAF_BIT | pb[k];
+          cnt     = c;
+          leafBox = true;
+        }
+        else {
+          const uint32_t id = atomicAdd(counters, 1u);
+          if (id >= maxNodes) {
+            atomicOr(overflow, 1);
+          }
+          else {
+            child            = id;
+            parentSlot[id]   = t.node * 4u + uint32_t(k);
+            const uint32_t q = atomicAdd(counters + 1, 1u);
+            next[q]          = CloudTask{pb[k], pe[k], id};
+          }
+        }
+      }
+      nd.lox[k]   = leafBox ? lo[0] : __int_as_float(0x7f800000);
+      nd.loy[k]   = leafBox ? lo[1] : __int_as_float(0x7f800000);
+      nd.loz[k]   = leafBox ? lo[2] : __int_as_float(0x7f800000);
+      nd.hix[k]   = leafBox ? hi[0] : __int_as_float(0xff800000);
+      nd.hiy[k]   = leafBox ? hi[1] : __int_as_float(0xff800000);
+      nd.hiz[k]   = leafBox ? hi[2] : __int_as_float(0xff800000);
+      nd.child[k] = child;
+      nd.count[k] = cnt;
+    }
+    nodes[t.node] = nd;
+  }
+}
+
+// Boxes of one level's nodes [begin, end) (every deeper level done): the union of the node's
+// occupied slots, written into its parent's slot (the root's into rootBox).
+__global__ void kCloudBoxes(EbgNode4* __restrict__ nodes, uint32_t begin, uint32_t end,
+                            const uint32_t* __restrict__ parentSlot, float* __restrict__ rootBox)
+{
+  for (uint32_t id = begin + blockIdx.x * blockDim.x + threadIdx.x; id < end; id += gridDim.x * blockDim.x) {
+    const EbgNode4 nd    = nodes[id];
+    float          lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if ((nd.child[k] | nd.count[k]) != 0u) {
+        lo[0] = fminf(lo[0], nd.lox[k]);
+        lo[1] = fminf(lo[1], nd.loy[k]);
+        lo[2] = fminf(lo[2], nd.loz[k]);
+        hi[0] = fmaxf(hi[0], nd.hix[k]);
+        hi[1] = fmaxf(hi[1], nd.hiy[k]);
+        hi[2] = fmaxf(hi[2], nd.hiz[k]);
+      }
+    }
+    if (id == 0u) {
+      for (int a = 0; a < 3; a++) {
+        rootBox[a]     = lo[a];
+        rootBox[3 + a] = hi[a];
+      }
+      continue;
+    }
+    const uint32_t ps = parentSlot[id];
+    EbgNode4&      p  = nodes[ps >> 2];
+    const int      k  = int(ps & 3u);
+    p.lox[k]          = lo[0];
+    p.loy[k]          = lo[1];
+    p.loz[k]          = lo[2];
+    p.hix[k]          = hi[0];
+    p.hiy[k]          = hi[1];
+    p.hiz[k]          = hi[2];
   }
 }
 
@@ -428,63 +587,197 @@ inline unsigned blocksFor(int64_t n, int t) { return unsigned((n + t - 1) / t); 
 
 } // namespace
 
-int cloudLevels(int64_t nLeaves, int64_t* levelNodes, int maxLevels)
+namespace {
+
+// 3 x depth + 1 stack entries: a 4-wide node pushes at most 3 siblings per level besides the one
+// the packet descends into
+constexpr int kMaxCloudDepth = (EBG_STACK_DEPTH - 1) / 3;
+
+// stream-ordered build workspace, released in order on the stream when the build returns
+struct Workspace
 {
-  int     nl = 0;
-  int64_t c  = nLeaves;
-  while (c > 1 && nl < maxLevels) {
+  cudaStream_t       s;
+  std::vector<void*> held;
+  explicit Workspace(cudaStream_t st) : s(st) {}
+  ~Workspace()
+  {
+    for (void* p : held) {
+      cudaFreeAsync(p, s);
+    }
+  }
+  template <class T>
+  T* get(size_t count)
+  {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, std::max<size_t>(count * sizeof(T), 16), s) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    held.push_back(p);
+    return static_cast<T*>(p);
+  }
+};
+
+// The balanced tree: runs of L sorted points, grouped four at a time, level by level.
+cudaError_t buildBalanced(const float4* leafPts, int64_t n, int L, Workspace& ws, CloudTree& tree, cudaStream_t s)
+{
+  const int     T       = 256;
+  const int64_t nLeaves = (n + L - 1) / L;
+  int64_t       levelNodes[64];
+  int           nl = 0;
+  for (int64_t c = nLeaves; c > 1 && nl < 64;) {
     c                = (c + 3) / 4;
     levelNodes[nl++] = c;
   }
-  return nl;
-}
-
-cudaError_t buildCloud(const float* points, int64_t n, int L, const CloudBuildBuffers& b, EbgNode4* nodes,
-                       float4* leafPts, const int64_t* levelNodes, int nLevels, float* rootBox, cudaStream_t s)
-{
-  const int T = 256;
-  // box init: lo = fkey(+max) (atomicMin), hi = fkey(-max) (atomicMax)
-  {
-    const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-    cudaMemcpyAsync(b.box, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  int64_t total = 0;
+  for (int l = 0; l < nl; l++) {
+    total += levelNodes[l];
   }
-  kBounds<<<unsigned(std::min<int64_t>(blocksFor(n, T), 4096)), T, 0, s>>>(points, n, b.box);
-  kCloudKeys<<<blocksFor(n, T), T, 0, s>>>(points, n, b.box, b.keysIn, b.idsIn);
-  size_t tb = b.sortTempBytes;
-  cub::DeviceRadixSort::SortPairs(b.sortTemp, tb, b.keysIn, b.keysOut, b.idsIn, b.idsOut, int(n), 0, 30, s);
-  kGatherLeaves<<<blocksFor(n, T), T, 0, s>>>(points, b.idsOut, n, leafPts);
-  const int64_t nLeaves = (n + L - 1) / L;
-  kLeafBoxes<<<blocksFor(nLeaves, T), T, 0, s>>>(leafPts, n, L, nLeaves, b.boxA);
-  // levels bottom-up; node index base of level l (1..nLevels) counts the levels above it
-  int64_t base[64];
+  float* boxA = ws.get<float>(6 * size_t(nLeaves));
+  float* boxB = ws.get<float>(6 * size_t(nl > 0 ? levelNodes[0] : 1));
+  if (!boxA || !boxB) {
+    return cudaErrorMemoryAllocation;
+  }
+  if (cudaMalloc(reinterpret_cast<void**>(&tree.nodes), size_t(std::max<int64_t>(total, 1)) * sizeof(EbgNode4)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    tree.nodes = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  kLeafBoxes<<<blocksFor(nLeaves, T), T, 0, s>>>(leafPts, n, L, nLeaves, boxA);
+  // node index base of level l (1..nl) counts the levels above it
+  int64_t base[65];
   int64_t acc = 0;
-  for (int l = nLevels; l >= 1; l--) {
+  for (int l = nl; l >= 1; l--) {
     base[l] = acc;
     acc += levelNodes[l - 1];
   }
-  float*  cur    = b.boxA;
-  float*  nxt    = b.boxB;
+  float*  cur    = boxA;
+  float*  nxt    = boxB;
   int64_t nChild = nLeaves;
-  for (int l = 1; l <= nLevels; l++) {
+  for (int l = 1; l <= nl; l++) {
     const int64_t nn = levelNodes[l - 1];
-    kTreeLevel<<<blocksFor(nn, T), T, 0, s>>>(nn, nChild, cur, l == 1 ? 1 : 0, l == 1 ? 0 : base[l - 1], L, n, nodes,
-                                             base[l], nxt);
-    float* t = cur;
-    cur      = nxt;
-    nxt      = t;
-    nChild   = nn;
+    kTreeLevel<<<blocksFor(nn, T), T, 0, s>>>(nn, nChild, cur, l == 1 ? 1 : 0, l == 1 ? 0 : base[l - 1], L, n,
+                                             tree.nodes, base[l], nxt);
+    std::swap(cur, nxt);
+    nChild = nn;
   }
-  // root box (6 floats) for the traversal's first stack entry
-  cudaMemcpyAsync(rootBox, cur, 6 * sizeof(float), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(tree.rootBox, cur, 6 * sizeof(float), cudaMemcpyDeviceToHost, s);
+  tree.numNodes = total;
+  tree.depth    = nl;
+  tree.radix    = false;
   return cudaGetLastError();
 }
 
-size_t cloudSortTempBytes(int64_t n)
+// The radix tree (kCloudSplit, kCloudBoxes).  Sets fallback (and builds nothing) when the tree
+// would need more than kMaxCloudDepth levels or more nodes than the workspace holds: n / max(1,
+// L / 4) + 64.  A node has at least two children, so a tree never has more than n - 1 nodes (the
+// bound for L < 8); Morton-ordered clouds need about n / (1.4 L) (leaves average about 0.7 L
+// points, two to four per node), a fifth of the workspace.
+cudaError_t buildRadix(const float4* leafPts, const uint32_t* keys, int64_t n, int L, Workspace& ws, CloudTree& tree,
+                       cudaStream_t s, bool& fallback)
 {
-  size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
-                                  static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr), int(n), 0, 30);
-  return tb;
+  const int64_t  per        = std::max(1, L / 4);
+  const uint32_t cap        = uint32_t(std::min<int64_t>(n / per + 64, int64_t(1) << 29));
+  CloudTask*     tasks[2]   = {ws.get<CloudTask>(cap), ws.get<CloudTask>(cap)};
+  uint32_t*      parentSlot = ws.get<uint32_t>(cap);
+  EbgNode4*      built      = ws.get<EbgNode4>(cap);
+  uint32_t*      counters   = ws.get<uint32_t>(4); // nodes, next tasks, overflow
+  float*         rootDev    = ws.get<float>(6);
+  if (!tasks[0] || !tasks[1] || !parentSlot || !built || !counters || !rootDev) {
+    fallback = true;
+    return cudaSuccess;
+  }
+  const CloudTask root{0u, uint32_t(n), 0u};
+  const uint32_t  init[4] = {1u, 0u, 0u, 0u};
+  cudaMemcpyAsync(tasks[0], &root, sizeof(root), cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  // level l holds nodes [start[l], start[l + 1])
+  std::vector<uint32_t> start = {0u, 1u};
+  uint32_t              count = 1;
+  int                   cur   = 0;
+  while (count > 0) {
+    if (int(start.size()) - 1 > kMaxCloudDepth) {
+      fallback = true;
+      return cudaSuccess;
+    }
+    cudaMemsetAsync(counters + 1, 0, sizeof(uint32_t), s);
+    kCloudSplit<<<blocksFor(count, 128), 128, 0, s>>>(tasks[cur], count, keys, leafPts, L, built, tasks[1 - cur],
+                                                      counters, parentSlot, cap,
+                                                      reinterpret_cast<int*>(counters + 2));
+    uint32_t hc[3];
+    cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      return e;
+    }
+    if (hc[2] != 0u) {
+      fallback = true;
+      return cudaSuccess;
+    }
+    count = hc[1];
+    if (count > 0) {
+      start.push_back(hc[0]);
+    }
+    cur = 1 - cur;
+  }
+  const int depth = int(start.size()) - 1;
+  for (int l = depth - 1; l >= 0; l--) {
+    const uint32_t b = start[l], e = start[l + 1];
+    kCloudBoxes<<<blocksFor(e - b, 128), 128, 0, s>>>(built, b, e, parentSlot, rootDev);
+  }
+  const int64_t total = start.back();
+  if (cudaMalloc(reinterpret_cast<void**>(&tree.nodes), size_t(total) * sizeof(EbgNode4)) != cudaSuccess) {
+    cudaGetLastError();
+    tree.nodes = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  cudaMemcpyAsync(tree.nodes, built, size_t(total) * sizeof(EbgNode4), cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(tree.rootBox, rootDev, 6 * sizeof(float), cudaMemcpyDeviceToHost, s);
+  tree.numNodes = total;
+  tree.depth    = depth;
+  tree.radix    = true;
+  return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t buildCloud(const float* points, int64_t n, int L, bool balanced, float4* leafPts, CloudTree& tree,
+                       cudaStream_t s)
+{
+  const int T = 256;
+  Workspace ws(s);
+  uint32_t* box     = ws.get<uint32_t>(6);
+  uint32_t* keysIn  = ws.get<uint32_t>(size_t(n));
+  uint32_t* keysOut = ws.get<uint32_t>(size_t(n));
+  uint32_t* idsIn   = ws.get<uint32_t>(size_t(n));
+  uint32_t* idsOut  = ws.get<uint32_t>(size_t(n));
+  size_t    tb      = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, keysIn, keysOut, idsIn, idsOut, int(n), 0, 30, s);
+  void* sortTemp = ws.get<char>(tb);
+  if (!box || !keysIn || !keysOut || !idsIn || !idsOut || !sortTemp) {
+    return cudaErrorMemoryAllocation;
+  }
+  // box init: lo = fkey(+max) (atomicMin), hi = fkey(-max) (atomicMax)
+  const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  cudaMemcpyAsync(box, init, sizeof(init), cudaMemcpyHostToDevice, s);
+  kBounds<<<unsigned(std::min<int64_t>(blocksFor(n, T), 4096)), T, 0, s>>>(points, n, box);
+  kCloudKeys<<<blocksFor(n, T), T, 0, s>>>(points, n, box, keysIn, idsIn);
+  cub::DeviceRadixSort::SortPairs(sortTemp, tb, keysIn, keysOut, idsIn, idsOut, int(n), 0, 30, s);
+  kGatherLeaves<<<blocksFor(n, T), T, 0, s>>>(points, idsOut, n, leafPts);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    return e;
+  }
+  if (n > L && !balanced) {
+    bool fallback = false;
+    e             = buildRadix(leafPts, keysOut, n, L, ws, tree, s, fallback);
+    if (e != cudaSuccess || !fallback) {
+      return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
+  }
+  e = buildBalanced(leafPts, n, L, ws, tree, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
 }
 
 cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s, bool self)

@@ -36,24 +36,22 @@ struct CloudQueryArgs
   int*                status;
 };
 
-struct CloudBuildBuffers
+// A cloud's tree: 4-wide nodes (cudaMalloc'd by buildCloud, freed by the caller) and the root's box.
+struct CloudTree
 {
-  uint32_t* box;      // 6 words
-  uint32_t* keysIn;
-  uint32_t* keysOut;
-  uint32_t* idsIn;
-  uint32_t* idsOut;
-  void*     sortTemp;
-  size_t    sortTempBytes;
-  float*    boxA;     // 6 floats per leaf
-  float*    boxB;
+  EbgNode4* nodes    = nullptr;
+  int64_t   numNodes = 0;
+  int       depth    = 0;     // node levels; 0 when the root is a single leaf (n <= L)
+  bool      radix    = false; // false: the balanced tree (fallback)
+  float     rootBox[6]{};
 };
 
-// Node counts of the levels above nLeaves leaves (bottom-up); returns the number of levels.
-int         cloudLevels(int64_t nLeaves, int64_t* levelNodes, int maxLevels);
-size_t      cloudSortTempBytes(int64_t n);
-cudaError_t buildCloud(const float* points, int64_t n, int L, const CloudBuildBuffers& b, EbgNode4* nodes,
-                       float4* leafPts, const int64_t* levelNodes, int nLevels, float* rootBoxHost, cudaStream_t s);
+// Builds the tree of n points on stream s and synchronises s: leafPts (n float4, the caller's)
+// receives the points in Morton order, tree the nodes (the balanced tree when asked for, or when
+// the radix tree would be too deep or too large).  Returns cudaErrorMemoryAllocation when
+// device memory runs out, else the first failing call's error or cudaSuccess.
+cudaError_t buildCloud(const float* points, int64_t n, int L, bool balanced, float4* leafPts, CloudTree& tree,
+                       cudaStream_t s);
 cudaError_t launchCloudKnn(const CloudQueryArgs& a, int kTemplate, int numSms, cudaStream_t s, bool self = false);
 
 // inv[cloud index] = leaf position, from the leaf points' index words.

@@ -51,6 +51,8 @@ typedef enum ebg_build
 /* ebg_build_opts.flags */
 #define EBG_BUILD_ON_DEVICE 1 /* meshes: build the tree (Morton or SAH, the host build's tree), the
                                  pseudonormals (bit-identical to the DCEL), records and boxes on the GPU */
+#define EBG_CLOUD_BALANCED 2  /* point clouds: fixed runs of leaf_size Morton-ordered points grouped four
+                                 at a time (a balanced tree) instead of the radix tree; same answers */
 
 typedef struct ebg_build_opts
 {
@@ -401,14 +403,19 @@ ebg_status ebg_check_status(const ebg_mesh* mesh, void* stream);
 /* ---- point clouds: PointCloudBVH (PointCloudBVH.hpp:56-350) --------------------------------
  *
  * ebg_cloud_create replaces PointCloudBVH(positions, meta) (PointCloudBVHImplem.hpp:27-57): the
- * tree is built on the device (Morton order, leaves of opts->leaf_size points, default 16, and a
- * 4-wide tree above them).  The cloud index of a point is its position in the input array. */
+ * tree is built on the device (the points in Morton order, a 4-wide tree whose nodes divide their
+ * range where the Morton curve jumps, leaves of at most opts->leaf_size points, default 16).  The
+ * cloud index of a point is its position in the input array. */
 ebg_status ebg_cloud_create(const float* points_host, int64_t n, const ebg_build_opts* opts, ebg_cloud** out);
 /* The same from a device array (no host copy); the build runs on stream and is complete on return. */
 ebg_status ebg_cloud_create_device(const float* points_dev, int64_t n, const ebg_build_opts* opts, ebg_cloud** out,
                                    void* stream);
 ebg_status ebg_cloud_destroy(ebg_cloud* cloud);
 int64_t    ebg_cloud_size(const ebg_cloud* cloud);
+/* The tree's shape: 4-wide nodes, node levels (0 when the root is a single leaf) and whether it is
+ * the radix tree (1) or the balanced tree of fixed runs of leaf_size points (0), which the build
+ * falls back to when the radix tree would be deeper than the traversal stack allows. */
+ebg_status ebg_cloud_tree_info(const ebg_cloud* cloud, int64_t* num_nodes, int32_t* depth, int32_t* radix);
 
 /* Batched PointCloudBVH::closestPoints (PointCloudBVHImplem.hpp:441-453) / closestPoint (k = 1):
  * for each query the k nearest points in increasing (squared distance, index) order -- equal

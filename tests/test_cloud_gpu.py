@@ -37,13 +37,15 @@ def test_reference_cloud_fixture(golden):
         assert j == i and dd == 0.0
 
 
+@pytest.mark.parametrize("balanced", [False, True])
 @pytest.mark.parametrize("k", [1, 2, 3, 8, 17, 32])
 @pytest.mark.parametrize("leaf", [1, 7, 16, 32])
-def test_against_brute_force(k, leaf):
+def test_against_brute_force(k, leaf, balanced):
     pts = W.point_cloud(20000, 3)
     q = np.concatenate([W.uniform_points(3000, 4, 0, 1), pts[:500]])  # includes exact hits
     ref_idx, ref_d2 = oracle.port().knn_brute(pts, q, k)
-    c = PointCloudBVH(pts, leaf_size=leaf)
+    c = PointCloudBVH(pts, leaf_size=leaf, balanced=balanced)
+    assert c.tree_info()["radix"] == (not balanced)
     idx, d2 = knn_gpu(c, q, k)
     assert np.array_equal(idx, ref_idx)
     assert np.array_equal(d2, ref_d2)
@@ -66,6 +68,44 @@ def test_ties_lowest_index():
     ref_idx, _ = oracle.port().knn_brute(g, qq, 8)
     idx, _ = knn_gpu(PointCloudBVH(g), qq, 8)
     assert np.array_equal(idx, ref_idx)
+
+
+def test_tree_shapes():
+    """The radix tree divides where the Morton curve jumps: leaves of at most leaf_size points, a
+    depth the traversal stack holds, and far fewer nodes than points; a cloud of at most leaf_size
+    points is one leaf."""
+    pts = W.point_cloud(200000, 21)
+    for leaf in (1, 8, 16, 32):
+        info = PointCloudBVH(pts, leaf_size=leaf).tree_info()
+        assert info["radix"] and 1 <= info["depth"] <= 31
+        assert info["nodes"] <= max(1, len(pts) // max(1, leaf // 4))
+    bal = PointCloudBVH(pts, leaf_size=16, balanced=True).tree_info()
+    assert not bal["radix"] and bal["nodes"] == sum(-(-len(pts) // (16 * 4 ** j)) for j in range(1, bal["depth"] + 1))
+    one = PointCloudBVH(pts[:16], leaf_size=16).tree_info()
+    assert one["depth"] == 0
+
+
+@pytest.mark.parametrize("leaf", [1, 16])
+def test_degenerate_clouds(leaf):
+    """Inputs whose Morton keys say little: one point repeated (every key equal: middle splits), points
+    on a line at geometric spacing (most keys equal, a few far apart), two far clusters.  The answers
+    are brute force's, lowest index first on ties."""
+    rng = np.random.default_rng(22)
+    same = np.tile(np.array([[0.25, 0.5, 0.75]], np.float32), (3000, 1))
+    line = np.zeros((120, 3), np.float32)
+    line[:, 0] = np.float32(2.0) ** -np.arange(120, dtype=np.float32)
+    far = np.concatenate([rng.random((2000, 3), dtype=np.float32) * 1e-3,
+                          1e4 + rng.random((2000, 3), dtype=np.float32)]).astype(np.float32)
+    for pts, q in ((same, W.uniform_points(500, 23, 0, 1)),
+                   (line, np.concatenate([line[::7], W.uniform_points(200, 24, -0.5, 1.5)])),
+                   (far, np.concatenate([far[::50], W.uniform_points(200, 25, -1, 2)]))):
+        c = PointCloudBVH(pts, leaf_size=leaf)
+        info = c.tree_info()
+        assert info["depth"] <= 31
+        for k in (1, 8):
+            ref_idx, ref_d2 = oracle.port().knn_brute(pts, q, k)
+            idx, d2 = knn_gpu(c, q, k)
+            assert np.array_equal(idx, ref_idx) and np.array_equal(d2, ref_d2)
 
 
 def test_small_and_edge_cases():
