@@ -524,7 +524,7 @@ def run_knn(args, rank, world, local_rank):
     for k in (1, 8):
         ms = device_timed(lambda: cloud.knn(qd, k), args.steps, args.warmup, torch, dev, stream)
         res[f"k{k}"] = {"ms_per_step": ms, "value": q.shape[0] * world / (ms * 1e-3)}
-    # the same queries on the balanced tree (fixed runs of 16 points grouped four at a time)
+    # the same queries on the balanced tree (fixed runs of 8 points grouped four at a time)
     bal_cloud = PointCloudBVH(pd, balanced=True)
     balanced = {"tree": bal_cloud.tree_info()}
     for k in (1, 8):
@@ -554,7 +554,7 @@ def run_knn(args, rank, world, local_rank):
                                           f"(build {tb:.1f}s)",
                                 "d2_equal_fraction": float(np.mean(gd.cpu().numpy() == rd))}
     print(json.dumps({"metric": "k-NN queries/s on 1 B200", "workload": "knn", "n_gpus": world,
-                      "config": {"points": int(pts.shape[0]), "queries": int(q.shape[0]), "leaf": 16,
+                      "config": {"points": int(pts.shape[0]), "queries": int(q.shape[0]), "leaf": 8,
                                  "tree": cloud.tree_info()},
                       "build_ms_device": build_dev, "results": res, "balanced_tree": balanced,
                       "cpu_baseline": cpu}), flush=True)

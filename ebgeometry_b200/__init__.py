@@ -418,7 +418,7 @@ class PointCloudBVH:
     four at a time instead (the same answers, more work per query on clustered clouds).
     """
 
-    def __init__(self, points, leaf_size=16, device=-1, stream=None, balanced=False):
+    def __init__(self, points, leaf_size=8, device=-1, stream=None, balanced=False):
         opts = _capi.BuildOpts(0, int(leaf_size), int(device), 2 if balanced else 0)
         h = C.c_void_p()
         if isinstance(points, np.ndarray):

@@ -55,7 +55,7 @@ void freeAll(std::vector<void*>& list, cudaStream_t s)
 
 ebg_status createCloud(const float* pointsDev, int64_t n, const ebg_build_opts* opts, cudaStream_t s, ebg_cloud** out)
 {
-  const int L = (opts && opts->leaf_size > 0) ? opts->leaf_size : 16;
+  const int L = (opts && opts->leaf_size > 0) ? opts->leaf_size : 8;
   if (L > EBG_MAX_LEAF) {
     return setError(EBG_ERR_INVALID, "leaf size must be in [1, 32]");
   }

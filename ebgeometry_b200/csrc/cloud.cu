@@ -1,4 +1,4 @@
-// Point-cloud nearest-neighbour search (sm_100a): GPU build + packet k-NN traversal.
+// Point-cloud nearest-neighbour search (sm_100a): GPU build + per-lane k-NN traversal.
 //
 // Reference: PointCloudBVH (PointCloudBVH.hpp:56-350, PointCloudBVHImplem.hpp:59-610): a K-wide
 // packed BVH over SoA groups of W points, built by recursive longest-axis midpoint partitioning,
@@ -16,8 +16,8 @@
 //   every box spatially compact.  (Fixed runs of L points grouped four at a time in Morton order --
 //   the balanced tree kept as the fallback for clouds whose radix tree is too deep for the
 //   traversal stack -- make long, thin boxes across those jumps that every nearby query opens.)
-// Query: Morton-sorted queries in packets of 32 per warp with a shared stack (as the mesh kernel);
-// each lane keeps its k best (d2, index) pairs sorted in registers.  Order is lexicographic on
+// Query: Morton-sorted queries, one per lane, each walking the tree with its own stack and keeping
+// its k best (d2, index) pairs sorted in registers.  Order is lexicographic on
 // (d2, index), so equal distances resolve to the lowest index, and d2 is the reference's float
 // arithmetic (PointSoAImplem.hpp:214-230): dx = q - p, d2 = (dx*dx + dy*dy) + dz*dz, each operation
 // rounded separately (no fused multiply-add).  Box distances use the same association, which makes
@@ -356,17 +356,21 @@ __device__ __forceinline__ bool lexLess(float da, uint32_t ia, float db, uint32_
   return da < db || (da == db && ia < ib);
 }
 
+// One query per lane.  Each lane walks the tree on its own, nearest child first, with a private
+// stack of (ref, count, box distance) entries (in local memory: at most 3 x depth + 1 of them); a
+// popped entry whose distance exceeds the lane's k-th best is skipped.  Warps take packets of 32
+// consecutive (Morton-ordered) queries from the work counter, so a warp's lanes walk nearby paths
+// and mostly read the same node and point lines.  (A warp walking one shared stack for its 32
+// queries opens every node any lane needs -- about four times what each lane needs on the k-NN
+// workloads -- and costs more than the divergence of separate walks.)
 // SELF: the queries are cloud points (self_pos), each excluded from its own neighbours
 // (nearestNeighbors / allNearestNeighbors, PointCloudBVHImplem.hpp:455-507).
 template <int K, bool SELF>
 __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
 {
-  __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
-  const int          lane = threadIdx.x & 31;
-  float4*            stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
-  const EbgCloudView& c   = a.cloud;
-  const uint64_t     numPackets = (uint64_t(a.n) + 31) / 32;
-
+  const int           lane       = threadIdx.x & 31;
+  const EbgCloudView& c          = a.cloud;
+  const uint64_t      numPackets = (uint64_t(a.n) + 31) / 32;
   while (true) {
     unsigned long long pk = 0;
     if (lane == 0) {
@@ -376,30 +380,27 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
     if (pk >= numPackets) {
       break;
     }
-    const int64_t  pos   = int64_t(pk) * 32 + lane;
-    const bool     valid = pos < a.n;
-    const int64_t  src   = valid ? pos : a.n - 1;
-    uint32_t       id, self = 0xffffffffu;
-    float          px, py, pz;
+    const int64_t pos = int64_t(pk) * 32 + lane;
+    if (pos >= a.n) {
+      continue;
+    }
+    uint32_t id, self = 0xffffffffu;
+    float    px, py, pz;
     if (SELF) {
-      // the query point comes from the cloud's own leaf array, which carries its index
-      const uint32_t lp = a.self_pos ? __ldg(a.self_pos + src) : uint32_t(src);
+      const uint32_t lp = a.self_pos ? __ldg(a.self_pos + pos) : uint32_t(pos);
       const float4   qp = __ldg(c.points + lp);
       px                = qp.x;
       py                = qp.y;
       pz                = qp.z;
       self              = __float_as_uint(qp.w);
-      id                = a.order ? __ldg(a.order + src) : self;
+      id                = a.order ? __ldg(a.order + pos) : self;
     }
     else {
-      id = a.order ? __ldg(a.order + src) : uint32_t(src);
+      id = a.order ? __ldg(a.order + pos) : uint32_t(pos);
       px = __ldg(a.queries + 3 * size_t(id));
       py = __ldg(a.queries + 3 * size_t(id) + 1);
       pz = __ldg(a.queries + 3 * size_t(id) + 2);
     }
-    // The k best sit in the LAST k of the K slots, in (d2, index) order, so slot K - 1 is the k-th
-    // best (the pruning bound); the first K - k slots hold d2 = -1, below any distance, and never
-    // move.  Unfilled slots are +inf: every finite point beats them.
     const int pad = K - a.k;
     float     kd[K];
     uint32_t  ki[K];
@@ -408,31 +409,27 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
       kd[j] = j < pad ? -1.f : __int_as_float(0x7f800000);
       ki[j] = j < pad ? 0u : 0xffffffffu;
     }
+    uint4    stk[EBG_STACK_DEPTH];
+    int      sp    = 1;
     uint32_t iters = 0;
     int      err   = 0;
-    int      sp    = 1;
-    if (lane == 0) {
-      stk[0] = make_float4(c.root_lo[0], c.root_lo[1], c.root_lo[2], __uint_as_float(c.root_ref));
-      stk[1] = make_float4(c.root_hi[0], c.root_hi[1], c.root_hi[2], __uint_as_float(c.root_count));
-    }
-    __syncwarp();
+    stk[0]         = make_uint4(c.root_ref, c.root_count,
+                                __float_as_uint(boxD2exact(c.root_lo[0], c.root_lo[1], c.root_lo[2], c.root_hi[0],
+                                                           c.root_hi[1], c.root_hi[2], px, py, pz)),
+                                0u);
     while (sp > 0) {
       if (++iters > MAX_ITERS) {
         err |= ST_ITERS;
         break;
       }
-      --sp;
-      const float4 A = stk[2 * sp], B = stk[2 * sp + 1];
-      const float  bound = kd[K - 1];
-      const float  d2    = boxD2exact(A.x, A.y, A.z, B.x, B.y, B.z, px, py, pz);
-      if (!__any_sync(FULL, d2 <= bound)) {
+      const uint4 e = stk[--sp];
+      if (__uint_as_float(e.z) > kd[K - 1]) {
         continue;
       }
-      const uint32_t ref = __float_as_uint(A.w), cnt = __float_as_uint(B.w);
-      if (ref & EBG_LEAF_BIT) {
-        const uint32_t p0 = ref & ~EBG_LEAF_BIT, pe = p0 + cnt;
-        // one point into the sorted k-best list (lowest index on equal distances)
-        auto consider = [&](const float4 q) {
+      if (e.x & EBG_LEAF_BIT) {
+        const uint32_t p0 = e.x & ~EBG_LEAF_BIT, pe = p0 + e.y;
+        for (uint32_t t = p0; t < pe; ++t) {
+          const float4   q  = __ldg(c.points + t);
           const float    dd = d2exact(px - q.x, py - q.y, pz - q.z);
           const uint32_t ii = __float_as_uint(q.w);
           if ((!SELF || ii != self) && lexLess(dd, ii, kd[K - 1], ki[K - 1])) {
@@ -450,90 +447,68 @@ __global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
               }
             }
           }
-        };
-        if constexpr (K >= 4) {
-          // a longer insertion per point: four points' loads go out at a time
-          uint32_t t = p0;
-          for (; t + 4 <= pe; t += 4) {
-            const float4 q0 = __ldg(c.points + t), q1 = __ldg(c.points + t + 1), q2 = __ldg(c.points + t + 2),
-                         q3 = __ldg(c.points + t + 3);
-            consider(q0);
-            consider(q1);
-            consider(q2);
-            consider(q3);
-          }
-          for (; t < pe; ++t) {
-            consider(__ldg(c.points + t));
-          }
         }
-        else {
-          for (uint32_t t = p0; t < pe; ++t) {
-            consider(__ldg(c.points + t));
-          }
+        continue;
+      }
+      const float4* nd    = reinterpret_cast<const float4*>(c.nodes + e.x);
+      const float4  lx    = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+      const float4  hx    = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+      const uint4   ch    = __ldg(reinterpret_cast<const uint4*>(nd + 6));
+      const uint4   cn    = __ldg(reinterpret_cast<const uint4*>(nd + 7));
+      const float   bound = kd[K - 1];
+      // (distance, ref, count) of each child; -1 marks an empty slot or a child beyond the bound
+      float    d[4]  = {boxD2exact(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, px, py, pz),
+                        boxD2exact(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, px, py, pz),
+                        boxD2exact(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, px, py, pz),
+                        boxD2exact(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, px, py, pz)};
+      uint32_t r[4]  = {ch.x, ch.y, ch.z, ch.w};
+      uint32_t n4[4] = {cn.x, cn.y, cn.z, cn.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (!(d[k] <= bound) || (r[k] | n4[k]) == 0u) {
+          d[k] = -1.f;
         }
       }
-      else {
-        const float4* nd = reinterpret_cast<const float4*>(c.nodes + ref);
-        const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
-        const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
-        const uint4   ch = __ldg(reinterpret_cast<const uint4*>(nd + 6));
-        const uint4   cn = __ldg(reinterpret_cast<const uint4*>(nd + 7));
-        const float   clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
-                    clz[4] = {lz.x, lz.y, lz.z, lz.w};
-        const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
-                    chz[4] = {hz.x, hz.y, hz.z, hz.w};
-        const uint32_t cref[4] = {ch.x, ch.y, ch.z, ch.w}, ccnt[4] = {cn.x, cn.y, cn.z, cn.w};
-        float key[4];
+      // farthest first onto the stack, so the nearest is popped next (ties by slot)
+      auto cswap = [&](int i, int j) {
+        if (d[i] < d[j]) {
+          const float    td = d[i];
+          const uint32_t tr = r[i], tn = n4[i];
+          d[i]              = d[j];
+          r[i]              = r[j];
+          n4[i]             = n4[j];
+          d[j]              = td;
+          r[j]              = tr;
+          n4[j]             = tn;
+        }
+      };
+      cswap(0, 1);
+      cswap(2, 3);
+      cswap(0, 2);
+      cswap(1, 3);
+      cswap(1, 2);
+      const int np = int(d[0] >= 0.f) + int(d[1] >= 0.f) + int(d[2] >= 0.f) + int(d[3] >= 0.f);
+      if (sp + np > EBG_STACK_DEPTH) {
+        err |= ST_STACK;
+        break;
+      }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const float dk = boxD2exact(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz);
-          // an empty slot (child 0 = the root, count 0) has an infinite box distance, which an
-          // unfilled k-best list (bound +inf) would admit: it is never pushed
-          const bool nk = __any_sync(FULL, dk <= bound) && (cref[k] | ccnt[k]) != 0u;
-          // ordering key: the child's smallest distance over the lanes (finite: nk excludes empty)
-          key[k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
-        }
-        const int np = int(key[0] >= 0.f) + int(key[1] >= 0.f) + int(key[2] >= 0.f) + int(key[3] >= 0.f);
-        if (sp + np > EBG_STACK_DEPTH) {
-          err |= ST_STACK;
-          break;
-        }
-        // lane k (< 4) writes child k into its slot, farther children deeper (ties by slot index)
-        if (lane < 4) {
-          const float kk = lane == 0 ? key[0] : (lane == 1 ? key[1] : (lane == 2 ? key[2] : key[3]));
-          if (kk >= 0.f) {
-            int rank = 0;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
-            }
-            // the child's box and words again from the node's line (an L1 hit), cheaper than
-            // selecting them out of the registers
-            const float* nf = reinterpret_cast<const float*>(nd) + lane;
-            float4*      e  = stk + 2 * (sp + rank);
-            e[0]            = make_float4(__ldg(nf), __ldg(nf + 4), __ldg(nf + 8), __ldg(nf + 24));
-            e[1]            = make_float4(__ldg(nf + 12), __ldg(nf + 16), __ldg(nf + 20), __ldg(nf + 28));
-          }
-        }
-        sp += np;
-        __syncwarp();
-        if (err) {
-          break;
+      for (int k = 0; k < 4; k++) {
+        if (d[k] >= 0.f) {
+          stk[sp++] = make_uint4(r[k], n4[k], __float_as_uint(d[k]), 0u);
         }
       }
     }
-    if (err && lane == 0) {
+    if (err) {
       atomicOr(a.status, err);
     }
-    if (valid) {
 #pragma unroll
-      for (int j = 0; j < K; j++) {
-        if (j >= pad) {
-          const bool   found = ki[j] != 0xffffffffu;
-          const size_t o     = size_t(id) * a.k + (j - pad);
-          a.out_idx[o]       = found ? int32_t(ki[j]) : -1;
-          a.out_d2[o]        = found ? kd[j] : __int_as_float(0x7f800000);
-        }
+    for (int j = 0; j < K; j++) {
+      if (j >= pad) {
+        const bool   found = ki[j] != 0xffffffffu;
+        const size_t o     = size_t(id) * a.k + (j - pad);
+        a.out_idx[o]       = found ? int32_t(ki[j]) : -1;
+        a.out_d2[o]        = found ? kd[j] : __int_as_float(0x7f800000);
       }
     }
   }
@@ -590,7 +565,7 @@ inline unsigned blocksFor(int64_t n, int t) { return unsigned((n + t - 1) / t); 
 namespace {
 
 // 3 x depth + 1 stack entries: a 4-wide node pushes at most 3 siblings per level besides the one
-// the packet descends into
+// the walk descends into
 constexpr int kMaxCloudDepth = (EBG_STACK_DEPTH - 1) / 3;
 
 // stream-ordered build workspace, released in order on the stream when the build returns

@@ -327,7 +327,7 @@ public:
     float  distanceSquared;
   };
 
-  explicit PointCloudBVH(const std::vector<std::array<float, 3>>& a_points, int a_leafSize = 16, int a_device = -1)
+  explicit PointCloudBVH(const std::vector<std::array<float, 3>>& a_points, int a_leafSize = 8, int a_device = -1)
   {
     ebg_build_opts o{0, a_leafSize, a_device, 0};
     check(ebg_cloud_create(&a_points[0][0], int64_t(a_points.size()), &o, &m_cloud));

@@ -404,7 +404,7 @@ ebg_status ebg_check_status(const ebg_mesh* mesh, void* stream);
  *
  * ebg_cloud_create replaces PointCloudBVH(positions, meta) (PointCloudBVHImplem.hpp:27-57): the
  * tree is built on the device (the points in Morton order, a 4-wide tree whose nodes divide their
- * range where the Morton curve jumps, leaves of at most opts->leaf_size points, default 16).  The
+ * range where the Morton curve jumps, leaves of at most opts->leaf_size points, default 8).  The
  * cloud index of a point is its position in the input array. */
 ebg_status ebg_cloud_create(const float* points_host, int64_t n, const ebg_build_opts* opts, ebg_cloud** out);
 /* The same from a device array (no host copy); the build runs on stream and is complete on return. */
