@@ -366,7 +366,7 @@ __device__ __forceinline__ bool lexLess(float da, uint32_t ia, float db, uint32_
 // SELF: the queries are cloud points (self_pos), each excluded from its own neighbours
 // (nearestNeighbors / allNearestNeighbors, PointCloudBVHImplem.hpp:455-507).
 template <int K, bool SELF>
-__global__ void __launch_bounds__(128) kCloudKnn(const CloudQueryArgs a)
+__global__ void __launch_bounds__(128, (K <= 2 ? 16 : (K <= 8 ? 10 : 1))) kCloudKnn(const CloudQueryArgs a)
 {
   const int           lane       = threadIdx.x & 31;
   const EbgCloudView& c          = a.cloud;
