@@ -196,8 +196,87 @@ __global__ void __launch_bounds__(128) kGridKnn(const GridQueryArgs a)
     const int    cy = cellCoord(Qy, g.lo[1], g.invH, g.n[1]);
     const int    cz = cellCoord(Qz, g.lo[2], g.invH, g.n[2]);
     const int    rMax = max(max(max(cx, g.n[0] - 1 - cx), max(cy, g.n[1] - 1 - cy)), max(cz, g.n[2] - 1 - cz));
+    // one point into the sorted k-best list (lowest index on equal distances)
+    auto scan = [&](uint32_t b, uint32_t e) {
 #pragma unroll 1
-    for (int r = 0; r <= rMax; r++) {
+      for (uint32_t s = b; s < e; s++) {
+        const float4   p  = __ldg(g.points + s);
+        const uint32_t ii = __float_as_uint(p.w);
+        const float    dd = gridD2(p.x, p.y, p.z, qx, qy, qz);
+        if (ii != self && lexLessG(dd, ii, kd[K - 1], ki[K - 1])) {
+          kd[K - 1] = dd;
+          ki[K - 1] = ii;
+#pragma unroll
+          for (int j = K - 1; j > 0; j--) {
+            if (lexLessG(kd[j], ki[j], kd[j - 1], ki[j - 1])) {
+              const float    td = kd[j];
+              const uint32_t ti = ki[j];
+              kd[j]             = kd[j - 1];
+              ki[j]             = ki[j - 1];
+              kd[j - 1]         = td;
+              ki[j - 1]         = ti;
+            }
+          }
+        }
+      }
+    };
+    // After shell r: stop once the k-th best is below every distance a later shell can hold (a point
+    // in a cell outside [c - r, c + r] on some axis lies beyond that side's plane, at least lb away;
+    // the comparison leaves room for the rounding of the float squared distances, a relative 1e-6
+    // against their 3e-7), or when no side is open.
+    auto done = [&](int r) {
+      if (ki[K - 1] == 0xffffffffu) {
+        return false;
+      }
+      double lb   = DBL_MAX;
+      bool   open = false;
+      sideBound(Qx, cx, r, g.n[0], g.lo[0], g.h, lb, open);
+      sideBound(Qy, cy, r, g.n[1], g.lo[1], g.h, lb, open);
+      sideBound(Qz, cz, r, g.n[2], g.lo[2], g.h, lb, open);
+      if (!open) {
+        return true;
+      }
+      lb = fmax(0.0, lb);
+      return double(kd[K - 1]) < lb * lb * (1.0 - 1e-6);
+    };
+    // Shells 0 and 1: the query's cell, then the rest of the 3 x 3 rows around it, x from cx - 1 to
+    // cx + 1 (each row a contiguous range of sorted points).  The bounds of all nine rows and of the
+    // query's cell are loaded before any point, so those reads overlap instead of following one
+    // another; the check after shell 0 keeps dense cells from scanning their neighbours.
+    bool stop;
+    {
+      const int      xlo = max(0, cx - 1), xhi = min(g.n[0] - 1, cx + 1);
+      uint32_t       rb[9], re[9];
+      const uint32_t rowc = (uint32_t(cz) * uint32_t(g.n[1]) + uint32_t(cy)) * uint32_t(g.n[0]);
+      const uint32_t cb = __ldg(g.cellStart + rowc + cx), ce = __ldg(g.cellStart + rowc + cx + 1);
+#pragma unroll
+      for (int j = 0; j < 9; j++) {
+        const int iz = cz - 1 + j / 3, iy = cy - 1 + j % 3;
+        rb[j] = re[j] = 0;
+        if (iz >= 0 && iz < g.n[2] && iy >= 0 && iy < g.n[1]) {
+          const uint32_t row0 = (uint32_t(iz) * uint32_t(g.n[1]) + uint32_t(iy)) * uint32_t(g.n[0]);
+          rb[j]               = __ldg(g.cellStart + row0 + xlo);
+          re[j]               = __ldg(g.cellStart + row0 + xhi + 1);
+        }
+      }
+      scan(cb, ce);
+      stop = done(0);
+      if (!stop) {
+#pragma unroll
+        for (int j = 0; j < 9; j++) {
+          if (j == 4) {
+            scan(rb[4], cb); // the query's row without its cell
+            scan(ce, re[4]);
+          }
+          else {
+            scan(rb[j], re[j]);
+          }
+        }
+        stop = done(1);
+      }
+    }
+#pragma unroll 1
+    for (int r = 2; !stop && r <= rMax; r++) {
       // the shell at Chebyshev radius r: on its two z faces and two y faces a whole x row of cells
       // (contiguous in the sorted points), elsewhere the two cells at x = cx -/+ r
       const int xlo = max(0, cx - r), xhi = min(g.n[0] - 1, cx + r);
@@ -210,74 +289,20 @@ __global__ void __launch_bounds__(128) kGridKnn(const GridQueryArgs a)
         for (int iy = ylo; iy <= yhi; iy++) {
           const bool     yEdge = (iy == cy - r) || (iy == cy + r);
           const uint32_t row0  = (uint32_t(iz) * uint32_t(g.n[1]) + uint32_t(iy)) * uint32_t(g.n[0]);
-          // up to two ranges of sorted points: [b0, e0) and [b1, e1)
-          uint32_t b0, e0, b1 = 0, e1 = 0;
           if (zEdge || yEdge) {
-            b0 = g.cellStart[row0 + xlo];
-            e0 = g.cellStart[row0 + xhi + 1];
+            scan(g.cellStart[row0 + xlo], g.cellStart[row0 + xhi + 1]);
           }
           else {
-            b0 = e0 = 0;
             if (cx - r >= 0) {
-              b0 = g.cellStart[row0 + cx - r];
-              e0 = g.cellStart[row0 + cx - r + 1];
+              scan(g.cellStart[row0 + cx - r], g.cellStart[row0 + cx - r + 1]);
             }
             if (cx + r < g.n[0]) {
-              b1 = g.cellStart[row0 + cx + r];
-              e1 = g.cellStart[row0 + cx + r + 1];
-            }
-          }
-          uint32_t sEnd = e0;
-#pragma unroll 1
-          for (uint32_t s = b0;; s++) {
-            if (s >= sEnd) {
-              if (b1 >= e1) {
-                break;
-              }
-              s    = b1;
-              sEnd = e1;
-              b1   = e1;
-            }
-            const float4   p  = __ldg(g.points + s);
-            const uint32_t ii = __float_as_uint(p.w);
-            const float    dd = gridD2(p.x, p.y, p.z, qx, qy, qz);
-            if (ii != self && lexLessG(dd, ii, kd[K - 1], ki[K - 1])) {
-              kd[K - 1] = dd;
-              ki[K - 1] = ii;
-#pragma unroll
-              for (int j = K - 1; j > 0; j--) {
-                if (lexLessG(kd[j], ki[j], kd[j - 1], ki[j - 1])) {
-                  const float    td = kd[j];
-                  const uint32_t ti = ki[j];
-                  kd[j]             = kd[j - 1];
-                  ki[j]             = ki[j - 1];
-                  kd[j - 1]         = td;
-                  ki[j - 1]         = ti;
-                }
-              }
+              scan(g.cellStart[row0 + cx + r], g.cellStart[row0 + cx + r + 1]);
             }
           }
         }
       }
-      // Stop once the k-th best is below every distance a later shell can hold: a point in a cell
-      // outside [c - r, c + r] on some axis lies beyond that side's plane, at least lb away; the
-      // comparison leaves room for the rounding of the float squared distances (a relative 1e-6
-      // against their 3e-7).
-      if (ki[K - 1] == 0xffffffffu) {
-        continue;
-      }
-      double lb   = DBL_MAX;
-      bool   open = false;
-      sideBound(Qx, cx, r, g.n[0], g.lo[0], g.h, lb, open);
-      sideBound(Qy, cy, r, g.n[1], g.lo[1], g.h, lb, open);
-      sideBound(Qz, cz, r, g.n[2], g.lo[2], g.h, lb, open);
-      if (!open) {
-        break;
-      }
-      lb = fmax(0.0, lb);
-      if (double(kd[K - 1]) < lb * lb * (1.0 - 1e-6)) {
-        break;
-      }
+      stop = done(r);
     }
 #pragma unroll
     for (int j = 0; j < K; j++) {
