@@ -857,9 +857,36 @@ ebg_status ebg_mesh_signed_distance_host(const ebg_mesh*       m,
         cudaEventRecord(ev[0], s);
         cudaStreamWaitEvent(aux[0], ev[0], 0);
         cudaStreamWaitEvent(aux[1], ev[0], 0);
-        const int64_t chunk = ((n + pieces - 1) / pieces + 31) / 32 * 32;
-        for (int64_t off = 0, c = 0; off < n && rc == EBG_OK; off += chunk, c++) {
-          const int64_t  cnt = std::min(chunk, n - off);
+        // Chunk sizes: equal pieces, or for calls of at least 64 M points a ramp -- 1, 2 and 4 units,
+        // pieces of about 8 units, then 4, 2 and 1 units (a unit is 1/64 of the call) -- so that the
+        // first chunk's copy in and the last chunk's copy out, which nothing overlaps, are short.
+        // Every chunk but the last is a multiple of 32 points.
+        std::vector<int64_t> sizes;
+        auto round32 = [](int64_t x) { return (x + 31) / 32 * 32; };
+        if (n >= (int64_t(1) << 26)) {
+          const int64_t u = round32((n + 63) / 64);
+          for (int64_t f : {1, 2, 4}) {
+            sizes.push_back(f * u);
+          }
+          const int64_t mid   = (n - 14 * u) / 32 * 32;
+          const int64_t m     = std::max<int64_t>(1, (mid + 8 * u - 1) / (8 * u));
+          const int64_t piece = round32((mid + m - 1) / m);
+          for (int64_t left = mid; left > 0; left -= piece) {
+            sizes.push_back(std::min(piece, left));
+          }
+          sizes.push_back(4 * u);
+          sizes.push_back(2 * u);
+          sizes.push_back(n - 13 * u - mid);
+        }
+        else {
+          const int64_t chunk = round32((n + pieces - 1) / pieces);
+          for (int64_t left = n; left > 0; left -= chunk) {
+            sizes.push_back(std::min(chunk, left));
+          }
+        }
+        int64_t off = 0;
+        for (size_t c = 0; c < sizes.size() && rc == EBG_OK; off += sizes[c], c++) {
+          const int64_t  cnt = sizes[c];
           cudaStream_t   st  = aux[c & 1];
           ebg_query_opts o   = opts ? *opts : ebg_query_opts{};
           if (o.radius_hint) {

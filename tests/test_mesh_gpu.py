@@ -220,3 +220,20 @@ def test_chunked_host_call_matches_device_path():
     hint = (d_dev.abs() * 1.01 + 1e-3).contiguous()
     d_hint = m.signed_distance(p, radius_hint=hint)
     assert np.array_equal(d_hint, d_host)
+
+
+def test_ramped_host_call_matches_device_path():
+    """Host calls of at least 64M points use ramped chunks (1, 2, 4 units, pieces of about 8, then
+    4, 2, 1; a unit is 1/64 of the call) with a last chunk that is not a multiple of 32 points: the
+    results are still those of the one-piece device call."""
+    v, f = W.displaced_icosphere(2, 43)
+    m = TriMeshSDF(v, f)
+    n = (1 << 26) + 45
+    p = np.random.default_rng(44).uniform(-1.5, 1.5, size=(n, 3)).astype(np.float32)
+    pd = torch.from_numpy(p).cuda()
+    tri_d = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_dev, _ = m.signed_distance(pd, closest_tri=tri_d)
+    torch.cuda.synchronize()
+    d_host, tri_h = m.signed_distance(p, closest_tri=np.empty(n, np.int32))
+    assert np.array_equal(d_host, d_dev.cpu().numpy())
+    assert np.array_equal(tri_h, tri_d.cpu().numpy())
