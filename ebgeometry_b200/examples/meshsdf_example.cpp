@@ -68,6 +68,13 @@ int main()
   PointCloudBVH::Hit one[4];
   same = same && pc.nearestNeighbors(77, 4, one) == 4 && one[0].index == nnB[77 * 4].index &&
          grid.nearestNeighbor(77).index == one[0].index;
+  // the balanced tree (fixed runs of points) gives the same answers as the default radix tree
+  PointCloudBVH balanced(cloud, 8, -1, true);
+  const auto    nnBal = balanced.allNearestNeighbors(4);
+  for (size_t i = 0; i < nnB.size(); i++) {
+    same = same && nnB[i].index == nnBal[i].index && nnB[i].distanceSquared == nnBal[i].distanceSquared;
+  }
+  same = same && pc.treeInfo().radix && !balanced.treeInfo().radix && pc.treeInfo().depth <= 31;
   // a unit cube of quad faces through the polygon-face MeshSDF and FlatMeshSDF
   const std::vector<std::array<double, 3>> cv = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                                                  {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};

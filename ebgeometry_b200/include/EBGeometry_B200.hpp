@@ -327,9 +327,20 @@ public:
     float  distanceSquared;
   };
 
-  explicit PointCloudBVH(const std::vector<std::array<float, 3>>& a_points, int a_leafSize = 8, int a_device = -1)
+  // Shape of the cloud's tree (ebg_cloud_tree_info).
+  struct TreeInfo
   {
-    ebg_build_opts o{0, a_leafSize, a_device, 0};
+    int64_t nodes;
+    int     depth;
+    bool    radix; // false: the balanced tree
+  };
+
+  // a_balanced: fixed runs of a_leafSize Morton-ordered points grouped four at a time instead of
+  // the radix tree (EBG_CLOUD_BALANCED); the answers are the same.
+  explicit PointCloudBVH(const std::vector<std::array<float, 3>>& a_points, int a_leafSize = 8, int a_device = -1,
+                         bool a_balanced = false)
+  {
+    ebg_build_opts o{0, a_leafSize, a_device, a_balanced ? EBG_CLOUD_BALANCED : 0};
     check(ebg_cloud_create(&a_points[0][0], int64_t(a_points.size()), &o, &m_cloud));
   }
   PointCloudBVH(const PointCloudBVH&) = delete;
@@ -337,6 +348,14 @@ public:
   ~PointCloudBVH() { ebg_cloud_destroy(m_cloud); }
 
   size_t numPoints() const noexcept { return size_t(ebg_cloud_size(m_cloud)); }
+
+  TreeInfo treeInfo() const
+  {
+    int64_t n = 0;
+    int32_t d = 0, r = 0;
+    check(ebg_cloud_tree_info(m_cloud, &n, &d, &r));
+    return TreeInfo{n, int(d), r != 0};
+  }
 
   // PointCloudBVH::closestPoint / closestPoints for one query (PointCloudBVHImplem.hpp:429-453);
   // returns how many neighbours were found (< k only if the cloud has fewer points).
