@@ -9,6 +9,8 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
 
 #include "capi_common.h"
@@ -569,9 +571,20 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
       return setError(EBG_ERR_NO_MEMORY, "seed workspace allocation failed");
     }
   }
+  // The band list: the traversal flags each sorted position, and a compaction of the flags gives
+  // the list in position (Morton) order, so that each FP64 packet holds 32 neighbouring queries.
+  // (Appending from the traversal lists them in completion order, which interleaves thousands of
+  // packets in flight.)
   unsigned long long* counters = ws.get<unsigned long long>(2); // [0] packets, [1] band count (u32)
   uint32_t*           bandList = band64 ? ws.get<uint32_t>(n) : nullptr;
-  float*              bandD    = band64 ? ws.get<float>(n) : nullptr;
+  uint8_t*            bandFlag = band64 ? ws.get<uint8_t>(n) : nullptr;
+  size_t              selBytes = 0;
+  void*               selTemp  = nullptr;
+  if (band64) {
+    cub::DeviceSelect::Flagged(nullptr, selBytes, thrust::counting_iterator<uint32_t>(0u), bandFlag, bandList,
+                               reinterpret_cast<uint32_t*>(counters + 1), int(n), s);
+    selTemp = ws.get<char>(selBytes);
+  }
   if (!ws.ok) {
     return setError(EBG_ERR_NO_MEMORY, "query workspace allocation failed");
   }
@@ -598,7 +611,8 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.band       = float(band);
   a.band_list  = bandList;
   a.band_count = reinterpret_cast<uint32_t*>(counters + 1);
-  a.band_d32   = bandD;
+  a.band_d32   = nullptr;
+  a.band_flag  = bandFlag;
   a.work       = counters;
   a.status     = m->dStatus;
   a.stats      = statsDev;
@@ -609,6 +623,10 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
     cudaEventRecord(ev[2], s);
   }
   if (band64) {
+    if (cub::DeviceSelect::Flagged(selTemp, selBytes, thrust::counting_iterator<uint32_t>(0u), bandFlag, bandList,
+                                   a.band_count, int(n), s) != cudaSuccess) {
+      return setError(EBG_ERR_CUDA, "band list compaction failed");
+    }
     // delta bounds the FP32 distance error (relative 1e-6 of the box diagonal)
     const float delta = float(2e-6 * m->info.diagonal) + 1e-30f;
     if (launchMeshBand64(a, delta, m->numSms, s) != cudaSuccess) {

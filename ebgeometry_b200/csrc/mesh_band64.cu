@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(128, 8) kMeshBand64(const MeshQueryArgs a, flo
                                       : D3{double(a.points[3 * size_t(id)]), double(a.points[3 * size_t(id) + 1]),
                                            double(a.points[3 * size_t(id) + 2])};
     const float    px = a.points[3 * size_t(id)], py = a.points[3 * size_t(id) + 1], pz = a.points[3 * size_t(id) + 2];
-    const float    d32 = a.band_d32[jj];
+    const float    d32 = a.band_d32 ? a.band_d32[jj] : a.out_d[id]; // the FP32 pass's distance
     // Boxes are tested at the FP32 point, `shift` from the FP64 point.  The mesh is within
     // |d32| + delta of the FP32 point (delta covers the FP32 distance error near the surface, the
     // relative term far from it), so the FP64 winner is within |d32| + delta + shift of the FP64

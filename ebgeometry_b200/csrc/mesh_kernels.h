@@ -26,7 +26,9 @@ struct MeshQueryArgs
   float              band;       // |d| <= band -> FP64 re-evaluation list
   uint32_t*          band_list;  // sorted positions needing FP64 (nullable = no band pass)
   uint32_t*          band_count;
-  float*             band_d32;   // FP32 distance of each band entry
+  float*             band_d32;   // FP32 distance of each band entry (nullable: read out_d instead)
+  uint8_t*           band_flag;  // per sorted position, 1 = needs FP64 (nullable: the traversal
+                                 // appends to band_list itself, in completion order)
   unsigned long long* work;      // packet counter (zeroed before the launch)
   int*               status;     // device status word (ST_* bits)
   unsigned long long* stats;     // 12 counters (nullable): 6 per query, 6 per packet

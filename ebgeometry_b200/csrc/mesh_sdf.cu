@@ -134,7 +134,13 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         a.out_tri[id] = besttri >= 0 ? __ldg(m.tri_id + besttri) : -1;
       }
     }
-    if (a.band_list) {
+    if (a.band_flag) {
+      // one flag per sorted position; the list is compacted from them in position order
+      if (valid) {
+        a.band_flag[pos] = uint8_t(besttri >= 0 && fabsf(dist) <= a.band);
+      }
+    }
+    else if (a.band_list) {
       const bool     inb  = valid && besttri >= 0 && fabsf(dist) <= a.band;
       const unsigned mask = __ballot_sync(FULL, inb);
       if (mask) {
