@@ -34,7 +34,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from ebgeometry_b200.ranks import max_over_ranks  # noqa: E402  (pure Python, no library load)
+
+def _module(name):
+    """A pure-Python module of the package, loaded from its file without running the package's
+    __init__ (which loads the CUDA library): the reference arm maps only the oracle's libraries."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(f"_bench_{name}", os.path.join(ROOT, "ebgeometry_b200", f"{name}.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+max_over_ranks = _module("ranks").max_over_ranks
 
 METRIC = "SDF queries/s on 1 B200: learned-seeded vs plain GPU BVH at equal accuracy"
 UNIT = "queries/s"
@@ -46,8 +57,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["mesh", "knn", "grid", "csg"], default="mesh",
-                    help="mesh: the headline mesh-SDF configuration; knn: 16M-point cloud, 4M queries, k=1 and 8; "
+    ap.add_argument("--workload", choices=["mesh", "fp64", "knn", "grid", "csg"], default="mesh",
+                    help="mesh: the headline mesh-SDF configuration; fp64: the level-5 mesh, 1M FP64 queries; "
+                         "knn: 16M-point cloud, 4M queries, k=1 and 8; "
                          "grid: the uniform-grid cloud against the BVH cloud on a uniform and a clustered 16M-point "
                          "cloud; csg: 4,096 spheres + 256 posed meshes, 2,048 query batches in one launch")
     ap.add_argument("--knn-points", type=int, default=16 * 1024 * 1024)
@@ -70,6 +82,17 @@ def parse():
                     help="also time the traversal seeded with the exact distances (the bound any seed can reach)")
     ap.add_argument("--hint-slack", default="0.02:4e-4,0.005:1e-4",
                     help="with --perfect-seed: also time radius hints |d|(1+a)+b for these a:b pairs")
+    ap.add_argument("--cells", type=int, default=0, help="seed attach: cells per axis (0 = the library default)")
+    ap.add_argument("--cut-entries", type=int, default=0, help="seed attach: subtrees per cell (0 = default)")
+    ap.add_argument("--cell-margin", type=float, default=0.0, help="seed attach: cell growth in cells (0 = default)")
+    ap.add_argument("--seed-ablation", action="store_true",
+                    help="also time the seeded traversal with no radius, with the exact cell radius and without "
+                         "anchors (what each part of the seed buys)")
+    ap.add_argument("--traffic-csv", default=None,
+                    help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum of the traversal kernel) captured "
+                         "from this same command; fills roofline.traffic")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the FP64 level-5 and k-NN configurations measured beside the headline line")
     ap.add_argument("--seed-samples", type=int, default=1 << 25)
     ap.add_argument("--seed-steps", type=int, default=2000)
     ap.add_argument("--seed-batch", type=int, default=1 << 18)
@@ -83,7 +106,7 @@ def log(*a):
 
 
 def workload(args):
-    from ebgeometry_b200 import workloads as W
+    W = _module("workloads")
     v, f = W.displaced_icosphere(args.level, 1)
     grid = W.grid_points(args.grid, -1.25, 1.25)
     band = W.band_points(v, f, args.band_points, 2, 1e-3)
@@ -101,11 +124,13 @@ def sample_indices(n_grid, n_band, n, seed=17):
 
 
 # --- reference CPU implementation -----------------------------------------------------------------
-def reference_mesh(v, f):
+def reference_mesh(v, f, kind=0, timing=True):
+    """The reference's TriMeshSDF (Morton build): kind 0 <double,short,4,4>, kind 1 the ISA-default
+    K/W; from the timing build (or the parity build with timing=False)."""
     import oracle
-    R = oracle.ref()
+    R = oracle.ref(timing=timing)
     t0 = time.time()
-    m = R.mesh(v, f, kind=0, build=1, max_leaf_groups=4)  # TriMeshSDF<double,short,4,4>, Morton
+    m = R.mesh(v, f, kind=kind, build=1, max_leaf_groups=4)
     return R, m, time.time() - t0
 
 
@@ -201,13 +226,67 @@ def measured_peaks():
 
 
 def l2_read_bandwidth():
-    """Read bandwidth of a 48 MB L2-resident buffer streamed by the library's own kernel."""
+    """Read bandwidth of a 48 MB L2-resident buffer streamed by the bench's probe kernel
+    (ebgeometry_b200/libebgprobe.so, built beside the library, outside its C ABI)."""
     import ctypes as C
-
-    from ebgeometry_b200 import _capi
+    lib = C.CDLL(os.path.join(ROOT, "ebgeometry_b200", "libebgprobe.so"))
+    lib.ebgprobe_read_bandwidth.restype = C.c_int
+    lib.ebgprobe_read_bandwidth.argtypes = [C.c_int64, C.c_int32, C.POINTER(C.c_double)]
     out = C.c_double()
-    _capi.check(_capi.lib.ebg_measure_read_bandwidth(48 << 20, 20, C.byref(out)))
-    return out.value
+    rc = lib.ebgprobe_read_bandwidth(48 << 20, 20, C.byref(out))
+    return out.value if rc == 0 else None
+
+
+def traffic_from_csv(path, kernel="kMeshSdf32"):
+    """DRAM bytes (read + write) per launch of `kernel`, averaged over the launches an ncu CSV
+    (--metrics dram__bytes_read.sum,dram__bytes_write.sum --csv) recorded."""
+    import csv
+    if not path or not os.path.exists(path):
+        return None
+    per = {}
+    with open(path) as fh:
+        rows = [ln for ln in fh if ln.startswith('"')]
+    for r in csv.DictReader(rows):
+        if kernel not in r.get("Kernel Name", ""):
+            continue
+        name, unit, val = r.get("Metric Name"), r.get("Metric Unit", ""), r.get("Metric Value", "0")
+        if name not in ("dram__bytes_read.sum", "dram__bytes_write.sum"):
+            continue
+        scale = {"byte": 1, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "KB": 1e3, "MB": 1e6, "GB": 1e9}.get(unit, 1)
+        per.setdefault(r.get("ID"), 0.0)
+        per[r.get("ID")] += float(val.replace(",", "")) * scale
+    return (sum(per.values()) / len(per)) if per else None
+
+
+def packet_bytes(st, n):
+    """Bytes the traversal's warps load per call, counted per packet (each distinct line once per
+    packet: the packet is what a warp executes): 128 B per interior node opened, 64 B per oriented
+    box tested, 48 B per triangle record of an opened leaf, 32 B per entry of a cell's cut plus the
+    cell's count, radius, anchor index and anchor record; and per query its 12-B point, 4-B order
+    index, 4-B result and the winner's 96-B sign record."""
+    return (128 * st["packet_nodes"] + 64 * st["packet_boxes"] + 48 * st["packet_triangle_records"] +
+            32 * st["cut_entries"] + 60 * st["cut_packets"] + n * (12 + 4 + 4 + 96))
+
+
+def reference_rates(v, f, pts, n_grid, n_band, build=1, cpu_seconds=12.0):
+    """The reference's TriMeshSDF<double,short,4,4> and its ISA-default K/W, from the timing build
+    (oracle/_ref, -O3 -march=sapphirerapids with fused multiply-adds) on all host threads, on one
+    seeded stratified sample of the workload sized for about cpu_seconds of work in total.  Returns
+    (queries/s by kind, sample indices, build seconds by kind, library, threads)."""
+    import oracle
+    R = oracle.ref(timing=True)
+    rates, builds, sidx = {}, {}, None
+    for kind in (0, 1):
+        t0 = time.time()
+        m = R.mesh(v, f, kind=kind, build=build, max_leaf_groups=4)
+        builds[kind] = time.time() - t0
+        if sidx is None:
+            probe = sample_indices(n_grid, n_band, 16384, seed=5)
+            qps0 = probe.shape[0] / max(time_reference(m, pts[probe]), 1e-6)
+            sidx = sample_indices(n_grid, n_band, int(min(max(qps0 * cpu_seconds / 2, 16384), 8_000_000)))
+        rates[kind] = sidx.shape[0] / time_reference(m, pts[sidx])
+        del m
+    return rates, sidx, builds, os.path.basename(R.path), R.max_threads()
 
 
 # --- arms -------------------------------------------------------------------------------------------
@@ -220,9 +299,17 @@ def run_reference(args, rank, world):
         return 0
     v, f, pts = workload(args)
     n_grid, n_band = args.grid ** 3, args.band_points
-    R, m, tbuild = reference_mesh(v, f)
+    # the faster of the reference's 4-wide and ISA-default trees on a short probe
+    best = None
+    for kind in (0, 1):
+        R, m, tbuild = reference_mesh(v, f, kind)
+        _, qps0 = calibrated_sample(m, pts, n_grid, n_band, 1.0)
+        if best is None or qps0 > best[3]:
+            best = (R, m, tbuild, qps0, kind)
+        else:
+            del m
+    R, m, tbuild, qps0, kind = best
     # each step: a fresh stratified sample sized for ~4 s of CPU work
-    _, qps0 = calibrated_sample(m, pts, n_grid, n_band, 1.0)
     n = int(min(max(qps0 * 4.0, 16384), 4_000_000))
     for s in range(args.warmup):
         time_reference(m, pts[sample_indices(n_grid, n_band, n, seed=100 + s)])
@@ -232,15 +319,19 @@ def run_reference(args, rank, world):
     tot = sum(times)
     qps = n * args.steps / tot
     cores = R.max_threads()
+    impl = ("reference TriMeshSDF<double,short,4,4>" if kind == 0 else
+            "reference TriMeshSDF<double,short> with the ISA-default branching and SoA width")
     sample = (f"{n} points per step: a seeded stratified sample of the {n_grid + n_band} workload points "
-              f"({n_grid} grid + {n_band} band in proportion)")
+              f"({n_grid} grid + {n_band} band in proportion); {impl}, Morton build, "
+              f"{os.path.basename(R.path)} (-O3 -march=sapphirerapids with fused multiply-adds)")
     line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"mesh SDF, displaced icosphere level {args.level} ({f.shape[0]} triangles), "
                                    f"{args.grid}^3 grid + {n_band} band points",
-                       "implementation": "reference TriMeshSDF<double,short,4,4> (Morton build), value() per "
-                                         "point in an OpenMP parallel-for", "build_s": tbuild,
+                       "implementation": impl + " (Morton build), value() per point in an OpenMP parallel-for, "
+                                                "the faster of the 4-wide and ISA-default configurations",
+                       "build_s": tbuild,
                        "cpu": cpu_info()},
             "cpu_baseline": {"value": qps, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": qps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -335,20 +426,25 @@ def run_ours(args, rank, world, local_rank):
         perfect["slack"] = slack
         del hout, hint
 
-    seed, rep, st_seed = None, None, None
+    seed, rep, att, st_seed, ablation = None, None, None, None, None
     if not args.no_seed:
         t0 = time.time()
         if args.seed_load:
             seed = SeedModel.load(args.seed_load, device=local_rank)
         else:
             seed = SeedModel.train(mesh, num_samples=args.seed_samples, steps=args.seed_steps,
-                                   batch=args.seed_batch, rng_seed=7, lo=[-1.25] * 3, hi=[1.25] * 3)
+                                   batch=args.seed_batch, rng_seed=7, lo=[-1.25] * 3, hi=[1.25] * 3, attach=False)
         rep = seed.report()
         rep["wall_s"] = time.time() - t0
         rep["loaded_from"] = args.seed_load
         if args.seed_save:
             seed.save(args.seed_save)
         log(f"[rank {rank}] seed trained: {rep}")
+        attach_kw = dict(cells_per_axis=args.cells, max_entries=args.cut_entries, margin_cells=args.cell_margin)
+        t0 = time.time()
+        att = mesh.attach_seed(seed, **attach_kw)
+        att["wall_s"] = time.time() - t0
+        log(f"[rank {rank}] seed attached: {att}")
         _, st_seed = mesh.stats(pd, seed=seed)
         log(f"[rank {rank}] seeded stats {st_seed}")
         for _ in range(args.warmup):
@@ -356,9 +452,24 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         ms_seed, tms_seed, ck_seed = timed_steps(*tsteps, seed, *tctx)
         log(f"[rank {rank}] seeded {ms_seed:.1f} ms/step")
-        diff = (out - plain_ref).abs()
         same_frac = float((out == plain_ref).float().mean().item())
-        max_diff = float(diff.max().item())
+        max_diff = float((out - plain_ref).abs().max().item())
+        if args.seed_ablation:
+            # what each part of the seed buys: no radius (cuts by distance order only), the exact
+            # distance at the cell centres instead of the model's radius, no anchor triangles
+            ablation = []
+            aout = torch.empty_like(out)
+            for mode, anchors, what in ((1, True, "no radius (cuts by distance order only)"),
+                                        (2, True, "exact cell-centre distance instead of the model"),
+                                        (0, False, "model radius, no anchor triangles")):
+                mesh.attach_seed(seed, radius_mode=mode, anchors=anchors, **attach_kw)
+                mesh.signed_distance(pd, out=aout, seed=seed)
+                ms_a, _, _ = timed_steps(mesh, pd, aout, max(2, args.steps // 2), seed, *tctx)
+                ablation.append({"variant": what, "ms_per_step": ms_a, "speedup_vs_plain": ms_plain / ms_a,
+                                 "equal_to_plain": bool(torch.equal(aout, plain_ref))})
+                log(f"[rank {rank}] ablation {what}: {ms_a:.1f} ms/step")
+            del aout
+            mesh.attach_seed(seed, **attach_kw)
     ms_step, tms, ck = (ms_seed, tms_seed, ck_seed) if seed is not None else (ms_plain, tms_plain, ck_plain)
     value = n * world / (ms_step * 1e-3)
     plain_value = n * world / (ms_plain * 1e-3)
@@ -392,46 +503,40 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return 0
 
-    # roofline of the traversal kernel: per-query algorithmic bytes of the PLAIN traversal (the
-    # equal work unit for both runs) over the traversal phase's event-timed duration
+    # roofline of the traversal kernel (the launch timed as the "traverse" phase): the bytes its warps
+    # load per call, counted per packet from the measured run's own counters, over the phase's
+    # event-timed duration, against the measured HBM copy roof and the measured L2 read roof
     hbm_peak, peak_kind = measured_peaks()
     l2_gbs = l2_read_bandwidth()
-    node_b, box_b, tri_b = 128, 64, 48
+    st_run = st_seed if seed is not None else st
     nq = float(n)
-    bq = (12 + 4 + st["nodes_visited"] / nq * node_b + st["boxes_tested"] / nq * box_b +
-          st["triangles_tested"] / nq * tri_b)
+    bytes_call = float(packet_bytes(st_run, n))
     trav_ms = float(tms[:, 1].mean())
-    achieved = nq * bq / (trav_ms * 1e-3) / 1e9
-    # DRAM bytes of one traversal launch on this workload, from a single-pass ncu capture recorded
-    # in the profile summaries as "traffic <workload key> <bytes>" lines
-    traffic = None
-    key = f"L{args.level}_g{args.grid}_b{args.band_points}_{args.build}_leaf{args.leaf}"
-    for fn in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
-        if fn.endswith(".md"):
-            with open(os.path.join(ROOT, "profiles", fn)) as fh:
-                for ln in fh:
-                    parts = ln.split()
-                    if len(parts) >= 3 and parts[0] == "traffic" and parts[1] == key:
-                        traffic = int(parts[2])
+    achieved = bytes_call / (trav_ms * 1e-3) / 1e9
+    traffic = traffic_from_csv(args.traffic_csv)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         import oracle
         if oracle.ref_available():
-            R, m, tb = reference_mesh(v, f)
-            # bounded sample: probe the reference's rate, then size the sample to ~cpu_seconds
-            sidx, qps_probe = calibrated_sample(m, pts, n_grid, n_band, args.cpu_seconds)
-            ns = len(sidx)
-            dt = time_reference(m, pts[sidx])
-            # parity on that sample while it is at hand (reported, not asserted)
-            d_ref = m.sdf(pts[sidx].astype(np.float64))
+            rates, sidx, builds, lib_name, threads = reference_rates(v, f, pts, n_grid, n_band, build=1,
+                                                                     cpu_seconds=args.cpu_seconds)
+            kind = max(rates, key=rates.get)
+            # parity on that sample against the parity build of the reference (reported here; the
+            # gpu tests assert it)
+            _, mref, _ = reference_mesh(v, f, 0, timing=False)
+            d_ref = mref.sdf(pts[sidx].astype(np.float64))
+            del mref
             d_gpu = out.index_select(0, torch.from_numpy(sidx).to(dev)).cpu().numpy().astype(np.float64)
             err = np.abs(d_gpu - d_ref)
             bandm = np.abs(d_ref) > 1e-4 * mesh.diagonal
-            cpu = {"value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
-                   "sample": f"{ns} seeded stratified points of the workload ({n_grid} grid : {n_band} band), "
-                             f"reference TriMeshSDF<double,short,4,4> Morton build ({tb:.1f}s), OpenMP over "
-                             f"value(); host CPU: {cpu_info()}",
+            cpu = {"value": rates[kind], "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{sidx.shape[0]} seeded stratified points of the workload ({n_grid} grid : {n_band} "
+                             f"band), reference TriMeshSDF Morton build, OpenMP over value(), {lib_name} "
+                             f"(-O3 -march=sapphirerapids, fused multiply-adds); host CPU: {cpu_info()}",
+                   "by_configuration": {"TriMeshSDF<double,short,4,4>": {"value": rates[0], "build_s": builds[0]},
+                                        "TriMeshSDF<double,short> (ISA-default K, W)": {"value": rates[1],
+                                                                                         "build_s": builds[1]}},
                    "parity_on_sample": {"max_abs_err": float(err.max()), "tol": 1e-6 * mesh.diagonal,
                                         "sign_mismatch_outside_band": int(np.sum(np.sign(d_gpu[bandm]) !=
                                                                                  np.sign(d_ref[bandm])))}}
@@ -443,6 +548,14 @@ def run_ours(args, rank, world, local_rank):
                                        "band_fraction": s["band_queries"] / nq,
                                        "seed_fallback_fraction": s["seed_fallbacks"] / nq}
 
+    def per_packet(s):
+        pk = max(s["packets"], 1)
+        return {"pops": s["packet_pops"] / pk, "nodes": s["packet_nodes"] / pk, "leaves": s["packet_leaves"] / pk,
+                "triangle_passes": s["packet_triangles"] / pk, "oriented_boxes": s["packet_boxes"] / pk,
+                "triangle_records": s["packet_triangle_records"] / pk,
+                "cut_packet_fraction": s["cut_packets"] / pk,
+                "cut_entries_per_cut_packet": s["cut_entries"] / max(s["cut_packets"], 1)}
+
     phases = lambda t: {"order": float(t[:, 0].mean()), "traverse": float(t[:, 1].mean()),
                         "band64": float(t[:, 2].mean()), "total": float(t[:, 3].mean())}
     line = {
@@ -453,39 +566,146 @@ def run_ours(args, rank, world, local_rank):
                                f"{args.build} 4-wide BVH, leaf {args.leaf}), {args.grid}^3 grid over [-1.25,1.25]^3 "
                                f"+ {n_band} points within 1e-3 of the surface = {n} queries/step; FP32 traversal, "
                                f"FP64 band |d| <= 1e-4 diag",
-                   "seed": ("learned pruning radius (16-level hash grid + 3x64 BF16 MLP, trained on the GPU)"
+                   "seed": ("learned pruning radius (16-level hash grid + 3x64 BF16 MLP, trained on the GPU) "
+                            "attached as per-cell entry cuts of the tree with anchor triangles"
                             if seed is not None else "none (plain traversal)"),
                    "build_on_device": bool(on_device),
                    "queries_per_step": n, "l2": "inputs larger than L2 "
                    f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
                    "plain": {"value": plain_value, "ms_per_step": ms_plain, "phase_ms_mean": phases(tms_plain),
-                             "per_query": per_query(st), "clocks": ck_plain},
+                             "per_query": per_query(st), "per_packet": per_packet(st), "clocks": ck_plain},
                    "perfect_radius_bound": perfect,
                    "seeded": None if seed is None else {
                        "value": value, "ms_per_step": ms_seed, "speedup_vs_plain": value / plain_value,
                        "phase_ms_mean": phases(tms_seed), "per_query": per_query(st_seed),
-                       "equal_to_plain_fraction": same_frac, "max_abs_diff_vs_plain": max_diff,
-                       "training": rep}},
+                       "per_packet": per_packet(st_seed), "equal_to_plain_fraction": same_frac,
+                       "max_abs_diff_vs_plain": max_diff, "training": rep, "attach": att,
+                       "ablation": ablation}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic_source": (f"ncu capture {os.path.basename(args.traffic_csv)}" if traffic is not None
+                                        else "none in this run (pass --traffic-csv from an ncu capture of it)"),
                      "kernel": "kMeshSdf32 (FP32 packet traversal" + (", seeded)" if seed is not None else ")"),
-                     "bytes_per_query": bq, "bytes_basis": "plain traversal visit counts (equal work unit): 16 B query in/out + 128 B per node + "
-                                    "64 B per oriented box + 48 B per triangle",
-                     "l2_read_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs,
+                     "bytes_per_query": bytes_call / nq,
+                     "bytes_basis": "per packet: 128 B per interior node opened + 64 B per oriented box + 48 B per "
+                                    "triangle record of an opened leaf + 32 B per cut entry (+60 B per cut); per "
+                                    "query: 12 B point + 4 B order + 4 B result + 96 B sign record",
+                     "l2_read_gbs_measured": l2_gbs, "frac_of_l2": (achieved / l2_gbs) if l2_gbs else None,
+                     "limiter": "instruction issue and L1/L2 latency on the SMs (ncu: issue-active ~75 %, about "
+                                "2 eligible warps per cycle, L2 throughput a few %), not DRAM or L2 bandwidth",
                      # the floor: every byte the step must touch once (the mesh's device arrays, the
                      # points in, the distances out) at the measured HBM rate
                      "unique_bytes_per_step": int(mesh.info["device_bytes"]) + 16 * n,
                      "unique_floor_ms": (int(mesh.info["device_bytes"]) + 16 * n) / (hbm_peak * 1e6)},
         "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(pts.nbytes),
                 "d2h_bytes_per_step": int(n * 4), "ms_per_step": e2e_ms, "matches_device_path": same},
-        "gpu_launches": (4 if seed is not None else 3) * args.steps,
-        "gpu_launches_note": "per step: Morton-key kernel, " + ("seed inference, " if seed is not None else "") +
-                             "FP32 traversal, FP64 band pass (plus the CUB radix-sort passes of the point ordering)",
+        "gpu_launches": 3 * args.steps,
+        "gpu_launches_note": "per step: Morton-key kernel, FP32 traversal, FP64 band pass (plus the CUB radix-sort "
+                             "and band-list compaction passes)",
         "clocks": ck,
         "cpu_baseline": cpu,
     }
+    if world == 1 and not args.no_extra:
+        # the other configurations' device throughput, end-to-end throughput and CPU baseline
+        del pd, out, plain_ref
+        torch.cuda.empty_cache()
+        line["other_configurations"] = {"fp64_level5": measure_fp64(args, torch, dev, stream,
+                                                                    cpu=not args.no_cpu_baseline),
+                                        "knn": measure_knn(args, torch, dev, stream, cpu=not args.no_cpu_baseline)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_fp64(args, torch, dev, stream, cpu=True):
+    """The CPU-runnable configuration: level-5 displaced icosphere (20,480 triangles, 4-wide SAH
+    tree), 1,048,576 FP64 points uniform in [-1.5,1.5]^3, FP64 signed distance end to end."""
+    from ebgeometry_b200 import TriMeshSDF
+    W = _module("workloads")
+    v, f = W.displaced_icosphere(5, 1)
+    p = np.random.default_rng(3).uniform(-1.5, 1.5, size=(1 << 20, 3))
+    mesh = TriMeshSDF(v, f, build="SAH", leaf_size=8)
+    pd = torch.from_numpy(p).to(dev)
+    out = torch.empty(p.shape[0], dtype=torch.float64, device=dev)
+    ms = device_timed(lambda: mesh.signed_distance(pd, out=out), max(3, args.steps), 3, torch, dev, stream)
+    ph = torch.from_numpy(p).pin_memory()
+    oh = torch.empty(p.shape[0], dtype=torch.float64).pin_memory()
+    hn = ph.numpy()
+    ohn = oh.numpy()
+    mesh.signed_distance(hn, out=ohn)
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        mesh.signed_distance(hn, out=ohn)  # the host entry point: H2D, query, D2H (synchronous)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / reps
+    res = {"workload": "level-5 displaced icosphere (20,480 triangles, SAH), 1,048,576 FP64 points uniform in "
+                       "[-1.5,1.5]^3, FP64 signed distance", "unit": UNIT,
+           "value": p.shape[0] / (ms * 1e-3), "ms_per_step": ms,
+           "e2e": {"value": p.shape[0] / (e2e_ms * 1e-3), "ms_per_step": e2e_ms, "h2d_bytes_per_step": int(p.nbytes),
+                   "d2h_bytes_per_step": int(p.shape[0] * 8), "timer": "host wall clock around the synchronous "
+                                                                       "host entry point"}}
+    if cpu:
+        import oracle
+        if oracle.ref_available():
+            d = out.cpu().numpy()
+            rates = {}
+            for kind, name in ((0, "TriMeshSDF<double,short,4,4>"), (1, "TriMeshSDF<double,short> (ISA-default K, W)")):
+                R = oracle.ref(timing=True)
+                m = R.mesh(v, f, kind=kind, build=0, max_leaf_groups=4)
+                m.sdf(p[:20000])
+                t0 = time.perf_counter()
+                m.sdf(p)
+                rates[name] = p.shape[0] / (time.perf_counter() - t0)
+                del m
+            best = max(rates, key=rates.get)
+            ref = oracle.ref().mesh(v, f, kind=0, build=0, max_leaf_groups=4).sdf(p)
+            res["cpu_baseline"] = {"value": rates[best], "unit": UNIT, "cores": oracle.ref(timing=True).max_threads(),
+                                   "kind": "reference", "sample": f"all {p.shape[0]} points, reference {best} SAH "
+                                   "(the faster configuration), -O3 -march=sapphirerapids",
+                                   "by_configuration": rates}
+            res["parity"] = {"bit_identical_fraction": float(np.mean(d == ref)),
+                             "max_abs_err": float(np.abs(d - ref).max()), "tol": 1e-6 * mesh.diagonal}
+    return res
+
+
+def measure_knn(args, torch, dev, stream, cpu=True):
+    """Point-cloud nearest neighbours: 16M FP32 points (half uniform, half in 64 anisotropic
+    clusters), 4M uniform queries, k = 1 and 8; int32 indices, ties to the lowest index."""
+    from ebgeometry_b200 import PointCloudBVH
+    W = _module("workloads")
+    pts = W.point_cloud(args.knn_points, 1)
+    q = W.uniform_points(args.knn_queries, 2, 0.0, 1.0)
+    cloud = PointCloudBVH(torch.from_numpy(pts).to(dev))
+    qd = torch.from_numpy(q).to(dev)
+    res = {"workload": f"{pts.shape[0]} points (half uniform, half in 64 anisotropic clusters), {q.shape[0]} uniform "
+                       "queries; int32 indices", "unit": UNIT}
+    for k in (1, 8):
+        ms = device_timed(lambda: cloud.knn(qd, k), max(3, args.steps), 3, torch, dev, stream)
+        cloud.knn(q[:1000], k)
+        t0 = time.perf_counter()
+        cloud.knn(q, k)  # the host entry point: H2D, query, D2H (synchronous)
+        e2e_ms = (time.perf_counter() - t0) * 1e3
+        res[f"k{k}"] = {"value": q.shape[0] / (ms * 1e-3), "ms_per_step": ms,
+                        "e2e": {"value": q.shape[0] / (e2e_ms * 1e-3), "ms_per_step": e2e_ms,
+                                "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(q.shape[0] * k * 8)}}
+    if cpu:
+        import oracle
+        if oracle.ref_available():
+            R = oracle.ref(timing=True)
+            t0 = time.time()
+            rc = R.cloud(pts)
+            tb = time.time() - t0
+            ns = 200000
+            for k in (1, 8):
+                t0 = time.perf_counter()
+                ri, rd = rc.knn(q[:ns], k, lex=False)
+                dt = time.perf_counter() - t0
+                gi, gd = cloud.knn(q[:ns], k)
+                res[f"k{k}"]["cpu_baseline"] = {
+                    "value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
+                    "sample": f"first {ns} queries, reference PointCloudBVH<float> closestPoints (build {tb:.1f}s), "
+                              "-O3 -march=sapphirerapids"}
+                res[f"k{k}"]["d2_equal_fraction"] = float(np.mean(gd == rd))
+    return res
 
 
 def device_timed(fn, steps, warmup, torch, dev, stream):
@@ -631,12 +851,13 @@ def run_grid(args, rank, world, local_rank):
 
 
 def run_csg(args, rank, world, local_rank):
-    """Batched CSG union: spheres + posed displaced icospheres (levels 3-7), batches of log-uniform
-    length 1k-1M concatenated into one call (one persistent launch)."""
+    """Batched CSG union: 4,096 spheres + 256 posed displaced icospheres (levels 3-7), 2,048 query
+    batches of log-uniform length 1k-1M points, all in one call (ebg_scene_eval_batches: one
+    persistent launch over all batches, then the FP64 near-surface pass)."""
     import torch
 
     from ebgeometry_b200 import BVHUnion, TriMeshSDF
-    from ebgeometry_b200 import workloads as W
+    W = _module("workloads")
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream(dev)
@@ -651,17 +872,78 @@ def run_csg(args, rank, world, local_rank):
     lo = np.minimum(sc["spheres"][:, :3].min(0), sc["poses"][:, 2:5].min(0)) - 0.2
     hi = np.maximum(sc["spheres"][:, :3].max(0), sc["poses"][:, 2:5].max(0)) + 0.2
     pts = (rng.random((n, 3), dtype=np.float32) * (hi - lo).astype(np.float32) + lo.astype(np.float32))
+    starts = np.concatenate([[0], np.cumsum(lens)])
     pd = torch.from_numpy(pts).to(dev)
     out = torch.empty(n, dtype=torch.float32, device=dev)
-    ms = device_timed(lambda: scene.values(pd, out=out), args.steps, args.warmup, torch, dev, stream)
+    batches = [pd[starts[i]:starts[i + 1]] for i in range(len(lens))]
+    outs = [out[starts[i]:starts[i + 1]] for i in range(len(lens))]
+    ms = device_timed(lambda: scene.values_batches(batches, outs=outs), args.steps, args.warmup, torch, dev, stream)
     scene.check_status()
+    # end to end: every step copies each batch in from pinned host memory, evaluates all of them in
+    # one call and copies the results out
+    ph = torch.from_numpy(pts).pin_memory()
+    oh = torch.empty(n, dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        for i in range(len(lens)):
+            batches[i].copy_(ph[starts[i]:starts[i + 1]], non_blocking=True)
+        scene.values_batches(batches, outs=outs)
+        oh.copy_(out, non_blocking=True)
+
+    e2e_ms = device_timed(e2e_step, max(2, min(args.steps, 3)), 1, torch, dev, stream)
+    same = bool(torch.equal(oh, out.cpu()))
     if rank != 0:
         return 0
     ntris = int(sum(f.shape[0] for _, f in sc["meshes"]))
+    mesh_bytes = int(sum(t.info["device_bytes"] for t in tms))
+    hbm_peak, peak_kind = measured_peaks()
+    unique = mesh_bytes + 16 * n
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.ref_available():
+            bb = []
+            for (v, f), ps in zip(sc["meshes"], sc["poses"]):
+                w = W.rotate_points(v, -ps[0], int(ps[1])) + ps[2:5]
+                bb.append(np.concatenate([w.min(0) - 1e-9, w.max(0) + 1e-9]))
+            R = oracle.ref(timing=True)
+            t0 = time.time()
+            rs = R.scene(sc["spheres"], sc["meshes"], sc["poses"], np.array(bb))
+            tb = time.time() - t0
+            sidx = np.sort(rng.choice(n, size=min(n, 200000), replace=False))
+            sp = pts[sidx].astype(np.float64)
+            rs.value(sp[:5000])
+            t0 = time.perf_counter()
+            ref = rs.value(sp)
+            dt = time.perf_counter() - t0
+            d = out.index_select(0, torch.from_numpy(sidx).to(dev)).cpu().numpy().astype(np.float64)
+            diag = float(np.linalg.norm(hi - lo))
+            outside = np.abs(ref) > 1e-4 * diag
+            cpu = {"value": sidx.shape[0] / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
+                   "sample": f"{sidx.shape[0]} seeded points of the batches, reference BVHUnion<double, "
+                             f"ImplicitFunction<double>, AABB, 4> over SphereSDF and Translate(Rotate(TriMeshSDF"
+                             f"<double,short,4,4>)) (build {tb:.1f}s on all threads), -O3 -march=sapphirerapids",
+                   "parity_on_sample": {"max_abs_err": float(np.abs(d - ref).max()), "tol": 1e-6 * diag,
+                                        "sign_mismatch_outside_band": int(np.sum(np.sign(d[outside]) !=
+                                                                                 np.sign(ref[outside])))}}
     print(json.dumps({"metric": "CSG union queries/s on 1 B200", "workload": "csg", "n_gpus": world,
-                      "value": n * world / (ms * 1e-3), "ms_per_step": ms,
-                      "config": {"spheres": args.csg_spheres, "meshes": args.csg_meshes, "mesh_triangles": ntris,
-                                 "batches": args.csg_batches, "points": n, "build_s": t_build}}), flush=True)
+                      "value": n * world / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "steps": args.steps,
+                      "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": f"{args.csg_spheres} spheres + {args.csg_meshes} displaced icospheres "
+                                             f"(levels 3-7, {ntris} triangles) at random poses; {args.csg_batches} "
+                                             f"batches of log-uniform length 1k-1M = {n} points in one "
+                                             "ebg_scene_eval_batches call; FP32 with the FP64 near-surface pass",
+                                 "points": n, "build_s": t_build, "l2": "inputs larger than L2"},
+                      "roofline": {"bound": "hbm", "achieved": unique / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                                   "unit": "GB/s", "frac": unique / (ms * 1e-3) / 1e9 / hbm_peak, "traffic": None,
+                                   "peak_kind": peak_kind,
+                                   "bytes_basis": "unique bytes (the meshes' device arrays once, 16 B per query); "
+                                                  "the union kernel keeps no per-packet counters"},
+                      "e2e": {"value": n * world / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms,
+                              "h2d_bytes_per_step": int(pts.nbytes), "d2h_bytes_per_step": int(4 * n),
+                              "matches_device_path": same},
+                      "gpu_launches": 6 * args.steps,
+                      "cpu_baseline": cpu}), flush=True)
     return 0
 
 
@@ -680,6 +962,14 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, rank, world)
+        if args.workload == "fp64":
+            import torch
+            dev = torch.device("cuda", local_rank)
+            torch.cuda.set_device(dev)
+            r = measure_fp64(args, torch, dev, torch.cuda.current_stream(dev), cpu=not args.no_cpu_baseline)
+            if rank == 0:
+                print(json.dumps({"metric": "FP64 mesh SDF queries/s on 1 B200", "n_gpus": world, **r}), flush=True)
+            return 0
         if args.workload == "knn":
             return run_knn(args, rank, world, local_rank)
         if args.workload == "grid":

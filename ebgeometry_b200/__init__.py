@@ -168,12 +168,13 @@ class TriMeshSDF:
         return fn, vn, en
 
     @staticmethod
-    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None, occupancy=None):
+    def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None, occupancy=None,
+              queue_chunk=None):
         return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
                                seed.handle if seed is not None else None,
                                int(warps_per_block or 0), int(occupancy or 0),
                                C.pointer(timings) if timings is not None else None,
-                               radius_hint.data_ptr() if radius_hint is not None else None)
+                               radius_hint.data_ptr() if radius_hint is not None else None, int(queue_chunk or 0))
 
     # --- ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance -----------------
     def value(self, point) -> float:
@@ -188,7 +189,7 @@ class TriMeshSDF:
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
                         fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None,
-                        radius_hint=None, occupancy=None):
+                        radius_hint=None, occupancy=None, queue_chunk=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  Float64 points (numpy or CUDA) take the FP64 entry points: every
@@ -196,7 +197,7 @@ class TriMeshSDF:
         times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
         radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
         float32 tensor of per-point upper bounds on |d| that seed the bound the same way."""
-        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy)
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy, queue_chunk)
         if isinstance(points, np.ndarray) and points.dtype == np.float64:
             p = np.ascontiguousarray(points).reshape(-1, 3)
             n = p.shape[0]
@@ -249,13 +250,29 @@ class TriMeshSDF:
     def check_status(self, stream=None):
         check(lib.ebg_check_status(self._h, _stream_ptr(stream)))
 
-    def autotune(self, sample_points, stream=None):
-        """Times the traversal launch shapes on a CUDA tensor of sample points and keeps the fastest
-        as this mesh's default; returns {"occupancy", "warps_per_block", "ms"}."""
-        o, w, ms = C.c_int32(), C.c_int32(), C.c_float()
+    def attach_seed(self, seed, cells_per_axis=0, max_entries=0, margin_cells=0.0, radius_mode=0, anchors=True,
+                    stream=None):
+        """Builds this mesh's per-cell entry cuts from a :class:`SeedModel` (ebg_seed_attach);
+        queries passing ``seed=`` that model then start their packets from the cuts.  Returns the
+        attach report as a dict.  ``radius_mode``: 0 the model's radius, 1 none, 2 exact."""
+        o = _capi.AttachOpts(int(cells_per_axis), int(max_entries), float(margin_cells), int(radius_mode),
+                             0 if anchors else 1)
+        r = _capi.AttachReport()
+        check(lib.ebg_seed_attach(self._h, seed.handle, C.byref(o), C.byref(r), _stream_ptr(stream)))
+        return {k: getattr(r, k) for k, _ in _capi.AttachReport._fields_}
+
+    def detach_seed(self):
+        check(lib.ebg_seed_detach(self._h))
+
+    def autotune(self, sample_points, seed=None, stream=None):
+        """Times the traversal launch shapes and the work-queue chunk on a CUDA tensor of sample
+        points (seeded with an attached :class:`SeedModel` if given) and keeps the fastest as this
+        mesh's default; returns {"occupancy", "warps_per_block", "queue_chunk", "ms"}."""
+        o, w, c, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
         check(lib.ebg_mesh_autotune(self._h, C.c_void_p(sample_points.data_ptr()), sample_points.numel() // 3,
-                                    C.byref(o), C.byref(w), C.byref(ms), _stream_ptr(stream)))
-        return {"occupancy": o.value, "warps_per_block": w.value, "ms": ms.value}
+                                    seed.handle if seed is not None else None, C.byref(o), C.byref(w),
+                                    C.byref(c), C.byref(ms), _stream_ptr(stream)))
+        return {"occupancy": o.value, "warps_per_block": w.value, "queue_chunk": c.value, "ms": ms.value}
 
 
 def _fp64_call(mesh, dev_fn, host_fn, points, closest_tri, stream, with_opts):
@@ -630,7 +647,8 @@ class SeedModel:
     """Learned pruning radius for :class:`TriMeshSDF` queries (no counterpart in the reference).
 
     A 16-level hash-grid encoding with a 3-layer, 64-wide BF16 ReLU MLP, trained on the GPU by the
-    library's own kernels on exact signed distances the mesh path generates.  Use
+    library's own kernels on exact signed distances the mesh path generates.  Attach it to a mesh
+    (``mesh.attach_seed(model)``, done by :meth:`train`), then query with
     ``mesh.signed_distance(points, seed=model)``.
     """
 
@@ -648,14 +666,18 @@ class SeedModel:
         return o
 
     @classmethod
-    def train(cls, mesh, stream=None, **kw):
-        """Trains on ``mesh`` (see ebg_seed_opts for the keyword options)."""
+    def train(cls, mesh, stream=None, attach=True, **kw):
+        """Trains on ``mesh`` (see ebg_seed_opts for the keyword options) and, unless ``attach`` is
+        False, attaches the model to it with the default cells (:meth:`TriMeshSDF.attach_seed`)."""
         o = cls._opts(**kw)
         h = C.c_void_p()
         rep = _capi.SeedReport()
         check(lib.ebg_seed_train(mesh.handle, C.byref(o), C.byref(h), C.byref(rep),
                                  _stream_ptr(stream) if stream is not None else None))
-        return cls(h)
+        model = cls(h)
+        if attach:
+            mesh.attach_seed(model, stream=stream)
+        return model
 
     @classmethod
     def create(cls, **kw):
@@ -748,9 +770,9 @@ class BVHUnion:
     def num_objects(self) -> int:
         return int(lib.ebg_scene_num_objects(self._h))
 
-    def values(self, points, out=None, sort=True, stream=None):
+    def values(self, points, out=None, sort=True, fp64_band=True, stream=None):
         """Union value at (n,3) float32 points (CUDA tensor: asynchronous; numpy: synchronous)."""
-        opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0, None, 0, 0, None)
+        opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0 if fp64_band else 1, None, 0, 0, None)
         if isinstance(points, np.ndarray):
             p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
             d = out if out is not None else np.empty(p.shape[0], np.float32)
@@ -765,6 +787,36 @@ class BVHUnion:
 
     def value(self, point) -> float:
         return float(self.values(np.asarray(point, np.float32).reshape(1, 3))[0])
+
+    def values_batches(self, batches, outs=None, sort=True, fp64_band=True, stream=None):
+        """Union values of several batches of (n_i,3) float32 CUDA points in one call
+        (ebg_scene_eval_batches: one persistent launch for all of them).  Returns the list of
+        result tensors (``outs`` if given).  Asynchronous on ``stream``."""
+        import torch
+        if not batches:
+            return []
+        dev = batches[0].device
+        outs = outs if outs is not None else [torch.empty(b.numel() // 3, dtype=torch.float32, device=dev)
+                                              for b in batches]
+        desc = np.zeros((len(batches), 3), np.int64)  # ebg_batch: points, n, out
+        for i, (b, o) in enumerate(zip(batches, outs)):
+            if not (b.is_cuda and b.dtype == torch.float32 and b.is_contiguous()):
+                raise ValueError("batches must be contiguous float32 CUDA tensors of shape (n,3)")
+            desc[i] = (b.data_ptr(), b.numel() // 3, o.data_ptr())
+        d = torch.from_numpy(desc).to(dev, non_blocking=False)
+        self._last_batches = d  # the descriptors must outlive the asynchronous call
+        opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0 if fp64_band else 1, None, 0, 0, None)
+        check(lib.ebg_scene_eval_batches(self._h, C.c_void_p(d.data_ptr()), len(batches), int(desc[:, 1].sum()),
+                                         C.byref(opts), _stream_ptr(stream)))
+        return outs
+
+    def autotune(self, sample_points, stream=None):
+        """Times the work-queue chunk on a CUDA tensor of sample points and keeps the fastest as
+        this scene's default; returns {"queue_chunk", "ms"}."""
+        c, ms = C.c_int32(), C.c_float()
+        check(lib.ebg_scene_autotune(self._h, C.c_void_p(sample_points.data_ptr()), sample_points.numel() // 3,
+                                     C.byref(c), C.byref(ms), _stream_ptr(stream)))
+        return {"queue_chunk": c.value, "ms": ms.value}
 
     def check_status(self, stream=None):
         check(lib.ebg_scene_check_status(self._h, _stream_ptr(stream)))

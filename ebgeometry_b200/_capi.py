@@ -25,7 +25,7 @@ class PhaseTimings(C.Structure):
 class QueryOpts(C.Structure):
     _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
                 ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("occupancy", C.c_int32),
-                ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p)]
+                ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p), ("queue_chunk", C.c_int32)]
 
 
 class SeedOpts(C.Structure):
@@ -54,7 +54,19 @@ class QueryStats(C.Structure):
                 ("triangles_tested", C.c_int64), ("band_queries", C.c_int64),
                 ("seed_fallbacks", C.c_int64), ("packets", C.c_int64), ("packet_pops", C.c_int64),
                 ("packet_nodes", C.c_int64), ("packet_leaves", C.c_int64), ("packet_triangles", C.c_int64),
-                ("boxes_tested", C.c_int64), ("packet_boxes", C.c_int64)]
+                ("boxes_tested", C.c_int64), ("packet_boxes", C.c_int64), ("cut_packets", C.c_int64),
+                ("cut_entries", C.c_int64), ("packet_triangle_records", C.c_int64)]
+
+
+class AttachOpts(C.Structure):
+    _fields_ = [("cells_per_axis", C.c_int32), ("max_entries", C.c_int32), ("margin_cells", C.c_float),
+                ("radius_mode", C.c_int32), ("no_anchors", C.c_int32)]
+
+
+class AttachReport(C.Structure):
+    _fields_ = [("cells_per_axis", C.c_int32), ("max_entries", C.c_int32), ("cells", C.c_int64),
+                ("cut_entries", C.c_int64), ("empty_cells", C.c_int64), ("device_bytes", C.c_int64),
+                ("build_ms", C.c_float), ("mean_radius", C.c_float)]
 
 
 EBG_OK = 0
@@ -71,7 +83,6 @@ SIGNATURES = {
     "ebg_last_error": (C.c_char_p, []),
     "ebg_version": (C.c_char_p, []),
     "ebg_device_count": (C.c_int, []),
-    "ebg_measure_read_bandwidth": (C.c_int, [_I64, _I32, C.POINTER(_D)]),
     "ebg_mesh_create": (C.c_int, [_P, _I64, _P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_mesh_create_with_normals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, C.POINTER(BuildOpts),
                                                C.POINTER(_P)]),
@@ -111,7 +122,8 @@ SIGNATURES = {
     "ebg_mesh_signed_distance_stats": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts),
                                                  C.POINTER(QueryStats), _P]),
     "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),
-    "ebg_mesh_autotune": (C.c_int, [_P, _P, _I64, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_float), _P]),
+    "ebg_mesh_autotune": (C.c_int, [_P, _P, _I64, _P, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32),
+                                    C.POINTER(C.c_float), _P]),
     "ebg_check_status": (C.c_int, [_P, _P]),
     "ebg_cloud_create": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_cloud_create_device": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P), _P]),
@@ -142,6 +154,8 @@ SIGNATURES = {
     "ebg_scene_value": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts), _P]),
     "ebg_scene_value_host": (C.c_int, [_P, _P, _I64, _P, C.POINTER(QueryOpts), _P]),
     "ebg_scene_check_status": (C.c_int, [_P, _P]),
+    "ebg_scene_eval_batches": (C.c_int, [_P, _P, _I32, _I64, C.POINTER(QueryOpts), _P]),
+    "ebg_scene_autotune": (C.c_int, [_P, _P, _I64, C.POINTER(_I32), C.POINTER(C.c_float), _P]),
     "ebg_seed_create": (C.c_int, [C.POINTER(SeedOpts), C.POINTER(_P)]),
     "ebg_seed_train": (C.c_int, [_P, C.POINTER(SeedOpts), C.POINTER(_P), C.POINTER(SeedReport), _P]),
     "ebg_seed_destroy": (C.c_int, [_P]),
@@ -152,6 +166,8 @@ SIGNATURES = {
     "ebg_seed_get_params": (C.c_int, [_P, _P, _P]),
     "ebg_seed_set_params": (C.c_int, [_P, _P, _P]),
     "ebg_seed_gradients": (C.c_int, [_P, _P, _P, _I32, C.c_float, C.POINTER(C.c_float), _P, _P]),
+    "ebg_seed_attach": (C.c_int, [_P, _P, C.POINTER(AttachOpts), C.POINTER(AttachReport), _P]),
+    "ebg_seed_detach": (C.c_int, [_P]),
 }
 
 

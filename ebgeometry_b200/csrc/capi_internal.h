@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "cells_kernels.h"
 #include "ebg_layout.h"
 #include "ebgeometry_b200.h"
 #include "seed_kernels.h"
@@ -41,6 +42,16 @@ struct ebg_mesh
   // launch shape chosen by ebg_mesh_autotune (0 = library defaults)
   int tunedOccupancy = 0;
   int tunedWpb       = 0;
+  int tunedChunk     = 0;
+  // per-cell entry cuts built by ebg_seed_attach from `cellsSeed` (queries passing that model use
+  // them); a refit drops them
+  const ebg_seed*    cellsSeed    = nullptr;
+  float4*            dCellEntries = nullptr;
+  uint32_t*          dCellCount   = nullptr;
+  float*             dCellRadius  = nullptr;
+  int32_t*           dCellAnchor  = nullptr;
+  ebg::SeedCellsView cellsView{};
+  ebg_attach_report  cellsReport{};
 };
 
 struct ebg_seed
@@ -63,6 +74,9 @@ struct ebg_seed
 
 namespace ebg {
 
+// Frees a mesh's entry cuts (if any) and forgets the model they came from.
+void dropCells(ebg_mesh* m);
+
 // The mesh query pipeline (ordering, optional seed inference, FP32 traversal, FP64 band pass) on
 // device buffers, asynchronous on s.  With pts64/out64 (the caller's FP64 points, of which pts is
 // the FP32 rounding, and an FP64 result array) every query is re-evaluated in FP64, with the
@@ -77,7 +91,8 @@ ebg_status meshQuery(const ebg_mesh*       m,
                      cudaStream_t          s,
                      const double*         pts64    = nullptr,
                      double*               out64    = nullptr,
-                     int                   evalKind = 0);
+                     int                   evalKind = 0,
+                     bool                  triLeafOrder = false);
 
 } // namespace ebg
 

@@ -499,7 +499,8 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
                           cudaStream_t          s,
                           const double*         pts64,
                           double*               out64,
-                          int                   evalKind)
+                          int                   evalKind,
+                          bool                  triLeafOrder)
 {
   if (n > int64_t(INT32_MAX)) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
@@ -515,6 +516,10 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   const ebg_seed* seed = opts ? opts->seed : nullptr;
   if (seed && seed->device != m->device) {
     return setError(EBG_ERR_INVALID, "seed model lives on another device than the mesh");
+  }
+  // a model seeds the traversal through the entry cuts it was attached with (ebg_seed_attach)
+  if (seed && !(m->cellsSeed == seed && m->dCellCount != nullptr)) {
+    return setError(EBG_ERR_INVALID, "the seed model is not attached to this mesh (ebg_seed_attach)");
   }
 
   // optional per-phase events (ev[0] start, [1] after ordering, [2] after traversal, [3] end)
@@ -561,16 +566,6 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
       return setError(EBG_ERR_CUDA, "query sort failed");
     }
   }
-  // learned pruning radius per packet of 32 sorted queries, predicted at the packet's centre (the
-  // traversal widens it per lane by the distance to that centre, which keeps it an upper bound
-  // wherever it holds at the centre)
-  float4* seedPk = nullptr;
-  if (seed) {
-    seedPk = ws.get<float4>((n + 31) / 32);
-    if (!ws.ok) {
-      return setError(EBG_ERR_NO_MEMORY, "seed workspace allocation failed");
-    }
-  }
   // The band list: the traversal flags each sorted position, and a compaction of the flags gives
   // the list in position (Morton) order, so that each FP64 packet holds 32 neighbouring queries.
   // (Appending from the traversal lists them in completion order, which interleaves thousands of
@@ -592,9 +587,6 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   if (tm) {
     cudaEventRecord(ev[1], s);
   }
-  if (seed && launchSeedPackets(seed->view, pts, order, n, seedPk, m->numSms, s) != cudaSuccess) {
-    return setError(EBG_ERR_CUDA, "seed inference launch failed");
-  }
 
   MeshQueryArgs a{};
   a.mesh       = m->view;
@@ -603,11 +595,11 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.out_d64    = out64;
   a.eval       = evalKind;
   a.order      = order;
-  a.seed_pk    = seedPk;
   a.hint       = (seed == nullptr && opts) ? opts->radius_hint : nullptr;
   a.n          = n;
   a.out_d      = outD;
   a.out_tri    = outTri;
+  a.tri_leaf   = triLeafOrder ? 1 : 0;
   a.band       = float(band);
   a.band_list  = bandList;
   a.band_count = reinterpret_cast<uint32_t*>(counters + 1);
@@ -616,6 +608,10 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   a.work       = counters;
   a.status     = m->dStatus;
   a.stats      = statsDev;
+  a.chunk      = (opts && opts->queue_chunk > 0) ? opts->queue_chunk : (m->tunedChunk > 0 ? m->tunedChunk : 1);
+  if (seed) {
+    a.cells = m->cellsView;
+  }
   if (launchMeshSdf32(a, wpb, m->numSms, s, occ) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
   }
@@ -726,6 +722,7 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dLeafCount);
   cudaFree(m->dNodeFirst);
   cudaFree(m->dNodeEnd);
+  dropCells(m);
   delete m;
   return EBG_OK;
 }
@@ -742,6 +739,9 @@ static ebg_status meshRefit(ebg_mesh* m, const double* vertices, bool onDevice, 
   DeviceGuard guard;
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the entry cuts were cut from the old boxes; they would no longer hold every near triangle
+  cudaStreamSynchronize(s);
+  dropCells(m);
   double       lo[3], hi[3];
   const ebg_status rc = refitMeshOnDevice(m, vertices, onDevice, nv, lo, hi, s);
   if (rc != EBG_OK) {
@@ -1143,7 +1143,7 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   cudaSetDevice(m->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   ebg_status   rc;
-  constexpr int      NSTAT    = 12;
+  constexpr int      NSTAT    = 15;
   unsigned long long host[NSTAT] = {};
   {
     Workspace           ws(s);
@@ -1175,16 +1175,21 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       m,
   stats->packet_triangles = int64_t(host[9]);
   stats->boxes_tested     = int64_t(host[10]);
   stats->packet_boxes     = int64_t(host[11]);
+  stats->cut_packets      = int64_t(host[12]);
+  stats->cut_entries      = int64_t(host[13]);
+  stats->packet_triangle_records = int64_t(host[14]);
   return ebg_check_status(m, stream);
 }
 
-ebg_status ebg_mesh_autotune(ebg_mesh*    m,
-                             const float* sample_points_dev,
-                             int64_t      n,
-                             int32_t*     best_occupancy,
-                             int32_t*     best_warps_per_block,
-                             float*       best_ms,
-                             void*        stream)
+ebg_status ebg_mesh_autotune(ebg_mesh*       m,
+                             const float*    sample_points_dev,
+                             int64_t         n,
+                             const ebg_seed* seed,
+                             int32_t*        best_occupancy,
+                             int32_t*        best_warps_per_block,
+                             int32_t*        best_queue_chunk,
+                             float*          best_ms,
+                             void*           stream)
 {
   if (m == nullptr || sample_points_dev == nullptr || n < 32) {
     return setError(EBG_ERR_INVALID, "autotune needs a mesh and at least 32 sample points");
@@ -1197,8 +1202,30 @@ ebg_status ebg_mesh_autotune(ebg_mesh*    m,
     cudaGetLastError();
     return setError(EBG_ERR_NO_MEMORY, "autotune output buffer");
   }
+  // the traversal time of one candidate: the best of two timed runs after a warm-up run
+  auto timeOne = [&](int o, int w, int c, float& ms) -> ebg_status {
+    ebg_query_opts    q{};
+    ebg_phase_timings t{};
+    q.occupancy       = o;
+    q.warps_per_block = w;
+    q.queue_chunk     = c;
+    q.no_fp64_band    = 1;
+    q.seed            = seed;
+    ms                = INFINITY;
+    for (int rep = 0; rep < 3; rep++) {
+      q.timings           = &t;
+      const ebg_status rc = meshQuery(m, sample_points_dev, n, out, nullptr, &q, nullptr, s);
+      if (rc != EBG_OK) {
+        return rc;
+      }
+      if (rep > 0) {
+        ms = std::min(ms, t.traverse_ms);
+      }
+    }
+    return EBG_OK;
+  };
   float     bestMs = INFINITY;
-  int       bestO = 1, bestW = 4;
+  int       bestO = 1, bestW = 4, bestC = 1;
   const int occs[] = {1, 4, 2};
   const int wpbs[] = {2, 4, 8};
   for (int o : occs) {
@@ -1206,22 +1233,11 @@ ebg_status ebg_mesh_autotune(ebg_mesh*    m,
       if (o != 4 && w > 4) {
         continue;
       }
-      ebg_query_opts    q{};
-      ebg_phase_timings t{};
-      q.occupancy       = o;
-      q.warps_per_block = w;
-      q.no_fp64_band    = 1;
-      float ms          = INFINITY;
-      for (int rep = 0; rep < 3; rep++) {  // the first run warms caches and the pool
-        q.timings           = &t;
-        const ebg_status rc = meshQuery(m, sample_points_dev, n, out, nullptr, &q, nullptr, s);
-        if (rc != EBG_OK) {
-          cudaFreeAsync(out, s);
-          return rc;
-        }
-        if (rep > 0) {
-          ms = std::min(ms, t.traverse_ms);
-        }
+      float            ms = INFINITY;
+      const ebg_status rc = timeOne(o, w, 1, ms);
+      if (rc != EBG_OK) {
+        cudaFreeAsync(out, s);
+        return rc;
       }
       if (ms < bestMs) {
         bestMs = ms;
@@ -1230,15 +1246,31 @@ ebg_status ebg_mesh_autotune(ebg_mesh*    m,
       }
     }
   }
+  for (int c : {2, 4}) {
+    float            ms = INFINITY;
+    const ebg_status rc = timeOne(bestO, bestW, c, ms);
+    if (rc != EBG_OK) {
+      cudaFreeAsync(out, s);
+      return rc;
+    }
+    if (ms < bestMs) {
+      bestMs = ms;
+      bestC  = c;
+    }
+  }
   cudaFreeAsync(out, s);
   cudaStreamSynchronize(s);
   m->tunedOccupancy = bestO;
   m->tunedWpb       = bestW;
+  m->tunedChunk     = bestC;
   if (best_occupancy) {
     *best_occupancy = bestO;
   }
   if (best_warps_per_block) {
     *best_warps_per_block = bestW;
+  }
+  if (best_queue_chunk) {
+    *best_queue_chunk = bestC;
   }
   if (best_ms) {
     *best_ms = bestMs;

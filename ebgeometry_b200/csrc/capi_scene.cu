@@ -6,7 +6,9 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
 #include <cuda_runtime.h>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "capi_common.h"
 #include "capi_internal.h"
@@ -23,10 +25,13 @@ struct ebg_scene
   SceneView view{};
   void*     dNodes   = nullptr;
   void*     dObjects = nullptr;
+  void*     dObjects64 = nullptr;
   void*     dMeshes  = nullptr;
   int*      dStatus  = nullptr;
   int64_t   numObjects = 0;
   int       depth      = 0;
+  double    diagonal   = 0.0; // of the scene's box
+  int       tunedChunk = 0;   // work-queue chunk chosen by ebg_scene_autotune (0 = one packet)
 };
 
 namespace {
@@ -57,6 +62,148 @@ void rotationMatrix(double angleDeg, int axis, double R[9])
     R[3] = -s;
     R[4] = c;
   }
+}
+
+// The union query of one batch (points/out) or of several (batches), asynchronous on the stream:
+// ordering, the FP32 pass, the band compaction and the FP64 pass.
+ebg_status sceneQuery(const ebg_scene*      s,
+                      const float*          points,
+                      float*                out,
+                      const SceneBatch*     batches,
+                      int32_t               nb,
+                      int64_t               n,
+                      const ebg_query_opts* opts,
+                      void*                 stream)
+{
+  if (n > int64_t(INT32_MAX)) {
+    return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
+  }
+  if (n == 0) {
+    return EBG_OK;
+  }
+  DeviceGuard  guard;
+  cudaSetDevice(s->device);
+  cudaStream_t st     = static_cast<cudaStream_t>(stream);
+  const bool   sort   = !(opts && opts->no_sort);
+  const bool   band64 = !(opts && opts->no_fp64_band);
+  std::vector<void*> ws;
+  bool ok  = true;
+  auto get = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (!ok || cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st) != cudaSuccess) {
+      ok = false;
+      return nullptr;
+    }
+    ws.push_back(p);
+    return p;
+  };
+  auto release = [&]() {
+    for (void* p : ws) {
+      cudaFreeAsync(p, st);
+    }
+  };
+  SceneQueryArgs a{};
+  a.scene       = s->view;
+  a.points      = points;
+  a.out         = out;
+  a.batches     = batches;
+  a.num_batches = nb;
+  a.n           = n;
+  a.status      = s->dStatus;
+  a.band        = float((opts && opts->band > 0) ? opts->band : 1e-4 * s->diagonal);
+  auto* counters = static_cast<unsigned long long*>(get(2 * sizeof(unsigned long long))); // work, band count
+  int64_t* starts = batches ? static_cast<int64_t*>(get(size_t(nb + 1) * sizeof(int64_t))) : nullptr;
+  uint32_t* order = nullptr;
+  if (sort) {
+    order      = static_cast<uint32_t*>(get(n * 4));
+    auto* iin  = static_cast<uint32_t*>(get(n * 4));
+    size_t tb  = 0;
+    if (batches) {
+      auto* kin  = static_cast<uint64_t*>(get(n * 8));
+      auto* kout = static_cast<uint64_t*>(get(n * 8));
+      int   bits = 30;
+      while ((int64_t(1) << (bits - 30)) < nb) {
+        bits++;
+      }
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, iin, order, int(n), 0, bits, st);
+      void* tmp = get(tb);
+      if (!ok) {
+        release();
+        return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
+      }
+      a.batch_start = starts;
+      if (launchSceneBatchStarts(batches, nb, starts, s->dStatus, n, st) != cudaSuccess ||
+          launchSceneBatchKeys(a, kin, iin, st) != cudaSuccess ||
+          cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(n), 0, bits, st) != cudaSuccess) {
+        release();
+        return setError(EBG_ERR_CUDA, std::string("scene batch ordering: ") + cudaGetErrorString(cudaGetLastError()));
+      }
+    }
+    else {
+      auto* kin  = static_cast<uint32_t*>(get(n * 4));
+      auto* kout = static_cast<uint32_t*>(get(n * 4));
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, iin, order, int(n), 0, 30, st);
+      void* tmp = get(tb);
+      if (!ok) {
+        release();
+        return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
+      }
+      launchQueryKeys(points, n, s->view.morton_lo, s->view.morton_scale, kin, iin, st);
+      if (cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(n), 0, 30, st) != cudaSuccess) {
+        release();
+        return setError(EBG_ERR_CUDA, "scene query sort failed");
+      }
+    }
+  }
+  else if (batches) {
+    if (!ok) {
+      release();
+      return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
+    }
+    a.batch_start = starts;
+    if (launchSceneBatchStarts(batches, nb, starts, s->dStatus, n, st) != cudaSuccess) {
+      release();
+      return setError(EBG_ERR_CUDA, "scene batch starts launch failed");
+    }
+  }
+  uint8_t*  flags    = band64 ? static_cast<uint8_t*>(get(size_t(n))) : nullptr;
+  uint32_t* bandList = band64 ? static_cast<uint32_t*>(get(size_t(n) * 4)) : nullptr;
+  size_t    selBytes = 0;
+  void*     selTemp  = nullptr;
+  auto*     bandCnt  = counters ? reinterpret_cast<uint32_t*>(counters + 1) : nullptr;
+  if (band64 && ok) {
+    cub::DeviceSelect::Flagged(nullptr, selBytes, thrust::counting_iterator<uint32_t>(0u), flags, bandList, bandCnt,
+                               int(n), st);
+    selTemp = get(selBytes);
+  }
+  if (!ok) {
+    release();
+    return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
+  }
+  cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st);
+  a.order      = order;
+  a.work       = counters;
+  a.chunk      = (opts && opts->queue_chunk > 0) ? opts->queue_chunk : (s->tunedChunk > 0 ? s->tunedChunk : 1);
+  a.band_flag  = flags;
+  a.band_list  = bandList;
+  a.band_count = bandCnt;
+  cudaError_t e = launchSceneValue(a, s->numSms, st);
+  if (e == cudaSuccess && band64) {
+    if (cub::DeviceSelect::Flagged(selTemp, selBytes, thrust::counting_iterator<uint32_t>(0u), flags, bandList,
+                                   bandCnt, int(n), st) != cudaSuccess) {
+      e = cudaGetLastError();
+      e = e == cudaSuccess ? cudaErrorUnknown : e;
+    }
+    else {
+      // delta bounds the FP32 error of the union's value: the instance transform and the mesh distance
+      e = launchSceneBand64(a, float(4e-6 * s->diagonal) + 1e-30f, s->numSms, st);
+    }
+  }
+  release();
+  if (e != cudaSuccess) {
+    return setError(EBG_ERR_CUDA, std::string("scene launch failed: ") + cudaGetErrorString(e));
+  }
+  return EBG_OK;
 }
 
 } // namespace
@@ -111,6 +258,7 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
   keepPoolMemory();
   const int64_t            no = num_spheres + num_meshes;
   std::vector<SceneObject> objs(no);
+  std::vector<SceneObject64> objs64(no);
   std::vector<double>      lo(3 * no), hi(3 * no), cen(3 * no);
   for (int64_t i = 0; i < num_spheres; i++) {
     const double* s = spheres + 4 * i;
@@ -118,7 +266,12 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
     std::memset(&o, 0, sizeof(o));
     o.kind   = 0;
     o.radius = float(s[3]);
+    SceneObject64& o64 = objs64[i];
+    std::memset(&o64, 0, sizeof(o64));
+    o64.kind   = 0;
+    o64.radius = s[3];
     for (int a = 0; a < 3; a++) {
+      o64.t[a]          = s[a];
       o.t[a]            = float(s[a]);
       lo[3 * i + a]     = s[a] - std::fabs(s[3]);
       hi[3 * i + a]     = s[a] + std::fabs(s[3]);
@@ -137,8 +290,17 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
     for (int k = 0; k < 9; k++) {
       o.R[k] = float(R[k]);
     }
+    SceneObject64& o64 = objs64[i];
+    std::memset(&o64, 0, sizeof(o64));
+    o64.kind = 1;
+    o64.axis = int32_t(poses[5 * m + 1]);
+    // RotateIF's cosine and sine (TransformImplem.hpp:164-181): theta = angle * pi / 180
+    const double theta = poses[5 * m] * 3.14159265358979323846 / 180.0;
+    o64.c              = std::cos(theta);
+    o64.s              = std::sin(theta);
     for (int a = 0; a < 3; a++) {
-      o.t[a] = float(poses[5 * m + 2 + a]);
+      o.t[a]   = float(poses[5 * m + 2 + a]);
+      o64.t[a] = poses[5 * m + 2 + a];
     }
     views[m] = meshes[m]->view;
     // world box: the 8 corners of the local box mapped back (p = R^T local + t), grown by the
@@ -171,8 +333,10 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
     return setError(EBG_ERR_TOO_LARGE, "object hierarchy too deep for the traversal stack");
   }
   std::vector<SceneObject> ordered(no);
+  std::vector<SceneObject64> ordered64(no);
   for (int64_t i = 0; i < no; i++) {
-    ordered[i] = objs[bvh.order[i]];
+    ordered[i]   = objs[bvh.order[i]];
+    ordered64[i] = objs64[bvh.order[i]];
   }
   auto* s      = new ebg_scene;
   s->device    = device;
@@ -185,6 +349,7 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
   };
   if (!up(&s->dNodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(EbgNode4)) ||
       !up(&s->dObjects, ordered.data(), no * sizeof(SceneObject)) ||
+      !up(&s->dObjects64, ordered64.data(), no * sizeof(SceneObject64)) ||
       !up(&s->dMeshes, views.data(), views.size() * sizeof(EbgMeshView)) ||
       cudaMalloc(reinterpret_cast<void**>(&s->dStatus), sizeof(int)) != cudaSuccess ||
       cudaMemset(s->dStatus, 0, sizeof(int)) != cudaSuccess) {
@@ -195,9 +360,13 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
   SceneView& v = s->view;
   v.nodes      = static_cast<const EbgNode4*>(s->dNodes);
   v.objects    = static_cast<const SceneObject*>(s->dObjects);
+  v.objects64  = static_cast<const SceneObject64*>(s->dObjects64);
   v.meshes     = static_cast<const EbgMeshView*>(s->dMeshes);
   v.root_ref   = bvh.rootRef;
   v.root_count = bvh.rootCount;
+  s->diagonal = std::sqrt((bvh.hi[0] - bvh.lo[0]) * (bvh.hi[0] - bvh.lo[0]) +
+                          (bvh.hi[1] - bvh.lo[1]) * (bvh.hi[1] - bvh.lo[1]) +
+                          (bvh.hi[2] - bvh.lo[2]) * (bvh.hi[2] - bvh.lo[2]));
   for (int a = 0; a < 3; a++) {
     v.root_lo[a]      = roundDown(bvh.lo[a]);
     v.root_hi[a]      = roundUp(bvh.hi[a]);
@@ -219,6 +388,7 @@ ebg_status ebg_scene_destroy(ebg_scene* s)
   cudaSetDevice(s->device);
   cudaFree(s->dNodes);
   cudaFree(s->dObjects);
+  cudaFree(s->dObjects64);
   cudaFree(s->dMeshes);
   cudaFree(s->dStatus);
   delete s;
@@ -235,66 +405,28 @@ ebg_status ebg_scene_value(const ebg_scene*      s,
   if (s == nullptr || n < 0 || (n > 0 && (!points_dev || !out_dev))) {
     return setError(EBG_ERR_INVALID, "null scene/buffer or negative count");
   }
-  if (n > int64_t(INT32_MAX)) {
-    return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points per call");
+  return sceneQuery(s, points_dev, out_dev, nullptr, 0, n, opts, stream);
+}
+
+ebg_status ebg_scene_eval_batches(const ebg_scene*      s,
+                                  const ebg_batch*      batches_dev,
+                                  int32_t               num_batches,
+                                  int64_t               total_points,
+                                  const ebg_query_opts* opts,
+                                  void*                 stream)
+{
+  if (s == nullptr || num_batches < 0 || total_points < 0 || (num_batches > 0 && batches_dev == nullptr)) {
+    return setError(EBG_ERR_INVALID, "null scene/batches or negative count");
   }
-  if (n == 0) {
+  if (num_batches > (1 << 24)) {
+    return setError(EBG_ERR_TOO_LARGE, "at most 2^24 batches per call");
+  }
+  if (num_batches == 0 || total_points == 0) {
     return EBG_OK;
   }
-  DeviceGuard  guard;
-  cudaSetDevice(s->device);
-  cudaStream_t st   = static_cast<cudaStream_t>(stream);
-  const bool   sort = !(opts && opts->no_sort);
-  std::vector<void*> ws;
-  auto get = [&](size_t bytes) -> void* {
-    void* p = nullptr;
-    if (cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st) != cudaSuccess) {
-      return nullptr;
-    }
-    ws.push_back(p);
-    return p;
-  };
-  auto release = [&]() {
-    for (void* p : ws) {
-      cudaFreeAsync(p, st);
-    }
-  };
-  uint32_t* order = nullptr;
-  if (sort) {
-    auto* kin  = static_cast<uint32_t*>(get(n * 4));
-    auto* kout = static_cast<uint32_t*>(get(n * 4));
-    auto* iin  = static_cast<uint32_t*>(get(n * 4));
-    order      = static_cast<uint32_t*>(get(n * 4));
-    size_t tb  = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, iin, order, int(n), 0, 30, st);
-    void* tmp = get(tb);
-    if (!kin || !kout || !iin || !order || !tmp) {
-      release();
-      return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
-    }
-    launchQueryKeys(points_dev, n, s->view.morton_lo, s->view.morton_scale, kin, iin, st);
-    cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(n), 0, 30, st);
-  }
-  auto* work = static_cast<unsigned long long*>(get(sizeof(unsigned long long)));
-  if (!work) {
-    release();
-    return setError(EBG_ERR_NO_MEMORY, "scene query workspace");
-  }
-  cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
-  SceneQueryArgs a{};
-  a.scene  = s->view;
-  a.points = points_dev;
-  a.order  = order;
-  a.n      = n;
-  a.out    = out_dev;
-  a.work   = work;
-  a.status = s->dStatus;
-  const cudaError_t e = launchSceneValue(a, s->numSms, st);
-  release();
-  if (e != cudaSuccess) {
-    return setError(EBG_ERR_CUDA, std::string("scene launch failed: ") + cudaGetErrorString(e));
-  }
-  return EBG_OK;
+  static_assert(sizeof(ebg_batch) == sizeof(SceneBatch), "ebg_batch and SceneBatch must match");
+  return sceneQuery(s, nullptr, nullptr, reinterpret_cast<const SceneBatch*>(batches_dev), num_batches, total_points,
+                    opts, stream);
 }
 
 ebg_status ebg_scene_value_host(const ebg_scene*      s,
@@ -360,5 +492,67 @@ ebg_status ebg_scene_check_status(const ebg_scene* s, void* stream)
 }
 
 int64_t ebg_scene_num_objects(const ebg_scene* s) { return s ? s->numObjects : 0; }
+
+ebg_status ebg_scene_autotune(ebg_scene*   s,
+                              const float* sample_points_dev,
+                              int64_t      n,
+                              int32_t*     best_queue_chunk,
+                              float*       best_ms,
+                              void*        stream)
+{
+  if (s == nullptr || sample_points_dev == nullptr || n < 32) {
+    return setError(EBG_ERR_INVALID, "scene autotune needs a scene and at least 32 sample points");
+  }
+  DeviceGuard guard;
+  cudaSetDevice(s->device);
+  cudaStream_t st  = static_cast<cudaStream_t>(stream);
+  float*       out = nullptr;
+  if (cudaMallocAsync(reinterpret_cast<void**>(&out), size_t(n) * sizeof(float), st) != cudaSuccess) {
+    cudaGetLastError();
+    return setError(EBG_ERR_NO_MEMORY, "scene autotune output buffer");
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float      bestMs = INFINITY;
+  int        bestC  = 1;
+  ebg_status rc     = EBG_OK;
+  for (int c : {1, 2, 4, 8}) {
+    ebg_query_opts q{};
+    q.queue_chunk = c;
+    float ms      = INFINITY;
+    for (int rep = 0; rep < 3 && rc == EBG_OK; rep++) { // the first run warms caches and the pool
+      cudaEventRecord(e0, st);
+      rc = sceneQuery(s, sample_points_dev, out, nullptr, 0, n, &q, stream);
+      cudaEventRecord(e1, st);
+      if (rc == EBG_OK && cudaEventSynchronize(e1) != cudaSuccess) {
+        rc = setError(EBG_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+      }
+      float t = 0.f;
+      if (rc == EBG_OK && rep > 0 && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
+        ms = std::min(ms, t);
+      }
+    }
+    if (ms < bestMs) {
+      bestMs = ms;
+      bestC  = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(out, st);
+  cudaStreamSynchronize(st);
+  if (rc != EBG_OK) {
+    return rc;
+  }
+  s->tunedChunk = bestC;
+  if (best_queue_chunk) {
+    *best_queue_chunk = bestC;
+  }
+  if (best_ms) {
+    *best_ms = bestMs;
+  }
+  return EBG_OK;
+}
 
 } // extern "C"

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "cells_kernels.h"
 #include "ebg_layout.h"
 
 namespace ebg {
@@ -15,14 +16,13 @@ struct MeshQueryArgs
   const float*       points;     // caller's xyz (n x 3)
   const double*      points64;   // the caller's FP64 xyz when it passed FP64 (nullable)
   const uint32_t*    order;      // sorted position -> caller index (nullptr = identity)
-  const float4*      seed_pk;    // per packet of 32 sorted queries: centre xyz and the radius
-                                 // predicted there (nullptr = none)
   const float*       hint;       // per query (caller order): radius upper bound (nullptr = none)
   int64_t            n;
   float*             out_d;      // caller order
   double*            out_d64;    // caller order, FP64 results of the band pass (nullable)
   int                eval;       // FP64 evaluator: 0 the Triangle test (TriMeshSDF), 1 the DCEL face (MeshSDF)
   int32_t*           out_tri;    // caller order (nullable)
+  int                tri_leaf;   // 1: out_tri gets the leaf-order triangle (the device records' index)
   float              band;       // |d| <= band -> FP64 re-evaluation list
   uint32_t*          band_list;  // sorted positions needing FP64 (nullable = no band pass)
   uint32_t*          band_count;
@@ -30,8 +30,11 @@ struct MeshQueryArgs
   uint8_t*           band_flag;  // per sorted position, 1 = needs FP64 (nullable: the traversal
                                  // appends to band_list itself, in completion order)
   unsigned long long* work;      // packet counter (zeroed before the launch)
+  int                chunk;      // packets taken from the counter at a time (0, 1: one)
   int*               status;     // device status word (ST_* bits)
-  unsigned long long* stats;     // 12 counters (nullable): 6 per query, 6 per packet
+  unsigned long long* stats;     // 15 counters (nullable): 6 per query, 6 per packet, 2 of the cuts,
+                                 // [14] triangle records of the leaves the warps opened
+  SeedCellsView      cells;      // per-cell entry cuts (used when cells.count is non-null)
 };
 
 // Morton keys of the query points (30 bits) and the identity permutation.

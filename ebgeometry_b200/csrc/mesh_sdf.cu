@@ -34,7 +34,8 @@ namespace ebg {
 
 namespace {
 
-// SEED: 0 plain, 1 learned radius per packet (+ distance to the centroid), 2 per-query radius hint
+// SEED: 0 plain, 2 per-query radius hint, 3 per-cell entry cuts and anchors of an attached model
+// (cells_kernels.h)
 // OCC selects the register budget: 0 = 256-thread blocks, compiler's choice; 1..3 = 128-thread
 // blocks with 8, 10, 12 resident blocks per SM (at most 64, 51, 42 registers).
 template <int OCC>
@@ -48,18 +49,24 @@ template <bool STATS, int SEED, int OCC>
 __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMeshSdf32(const MeshQueryArgs a)
 {
   extern __shared__ float4 smem[];
+  constexpr int STACK = SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH;
   const int     lane = threadIdx.x & 31;
-  float4*       stk  = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH + 32);
-  float4*       lpts = stk + 2 * EBG_STACK_DEPTH; // the warp's 32 spread-leaf points
+  float4*       stk  = smem + (threadIdx.x >> 5) * (2 * STACK + 32);
+  float4*       lpts = stk + 2 * STACK; // the warp's 32 spread-leaf points
   const EbgMeshView& m = a.mesh;
   const uint64_t numPackets = (uint64_t(a.n) + 31) / 32;
 
+  // packets come from the work counter `chunk` at a time (the queue chunk the autotuner picks)
+  const unsigned long long chunk = a.chunk > 1 ? (unsigned long long)a.chunk : 1ull;
+  unsigned long long       pk = 0, pkEnd = 0;
   while (true) {
-    unsigned long long pk = 0;
-    if (lane == 0) {
-      pk = atomicAdd(a.work, 1ull);
+    if (pk == pkEnd) {
+      if (lane == 0) {
+        pk = atomicAdd(a.work, chunk);
+      }
+      pk    = __shfl_sync(FULL, pk, 0);
+      pkEnd = pk + chunk;
     }
-    pk = __shfl_sync(FULL, pk, 0);
     if (pk >= numPackets) {
       break;
     }
@@ -80,18 +87,71 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       const float r = __ldg(a.hint + id);
       best          = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
     }
-    if (SEED == 1) {
-      // packet radius at the packet's centre, widened by this lane's distance to that centre (the
-      // SDF is 1-Lipschitz), squared and rounded up so FP32 rounding never makes the bound too tight
-      const float4 sp = __ldg(a.seed_pk + pk);
-      const float  ex = px - sp.x, ey = py - sp.y, ez = pz - sp.z;
-      const float  r  = sp.w + sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez))) * 1.000001f;
-      best           = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
+    int startSp = 0; // entries of a cell's cut copied onto the stack (0: start at the root)
+    if (SEED == 3) {
+      // the packet's box over its valid lanes, and the cell holding the box's centre
+      const float inf = __int_as_float(0x7f800000);
+      float       mnx = valid ? px : inf, mny = valid ? py : inf, mnz = valid ? pz : inf;
+      float       mxx = valid ? px : -inf, mxy = valid ? py : -inf, mxz = valid ? pz : -inf;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        mnx = fminf(mnx, __shfl_xor_sync(FULL, mnx, o));
+        mny = fminf(mny, __shfl_xor_sync(FULL, mny, o));
+        mnz = fminf(mnz, __shfl_xor_sync(FULL, mnz, o));
+        mxx = fmaxf(mxx, __shfl_xor_sync(FULL, mxx, o));
+        mxy = fmaxf(mxy, __shfl_xor_sync(FULL, mxy, o));
+        mxz = fmaxf(mxz, __shfl_xor_sync(FULL, mxz, o));
+      }
+      const SeedCellsView& cv = a.cells;
+      const float fx = (0.5f * (mnx + mxx) - cv.lo[0]) * cv.inv[0];
+      const float fy = (0.5f * (mny + mxy) - cv.lo[1]) * cv.inv[1];
+      const float fz = (0.5f * (mnz + mxz) - cv.lo[2]) * cv.inv[2];
+      const float g  = float(cv.g);
+      // (NaN coordinates fail these comparisons and keep the packet at the root)
+      if (fx >= 0.f && fx < g && fy >= 0.f && fy < g && fz >= 0.f && fz < g) {
+        const int ix = min(int(fx), cv.g - 1), iy = min(int(fy), cv.g - 1), iz = min(int(fz), cv.g - 1);
+        // the grown cell exactly as the cut builder rounded it
+        const bool inside =
+          mnx >= __fsub_rd(__fadd_rd(cv.lo[0], float(ix) * cv.size[0]), cv.margin[0]) &&
+          mny >= __fsub_rd(__fadd_rd(cv.lo[1], float(iy) * cv.size[1]), cv.margin[1]) &&
+          mnz >= __fsub_rd(__fadd_rd(cv.lo[2], float(iz) * cv.size[2]), cv.margin[2]) &&
+          mxx <= __fadd_ru(__fadd_ru(cv.lo[0], float(ix + 1) * cv.size[0]), cv.margin[0]) &&
+          mxy <= __fadd_ru(__fadd_ru(cv.lo[1], float(iy + 1) * cv.size[1]), cv.margin[1]) &&
+          mxz <= __fadd_ru(__fadd_ru(cv.lo[2], float(iz + 1) * cv.size[2]), cv.margin[2]);
+        const int64_t cell = (int64_t(iz) * cv.g + iy) * cv.g + ix;
+        const int     ne   = inside ? int(__ldg(cv.count + cell)) : 0;
+        if (ne > 0) {
+          const float4* src = cv.entries + size_t(cell) * size_t(cv.lmax) * 2;
+          for (int i = lane; i < 2 * ne; i += 32) {
+            stk[i] = __ldg(src + i);
+          }
+          __syncwarp();
+          // start below R_C by more than the FP32 error of a triangle distance, so that whatever
+          // is found within the bound is nearer than every triangle the cut left out
+          const float R = __ldg(cv.radius + cell);
+          best          = isfinite(R) ? __fmul_rd(__fmul_rd(R, R), 0.99998f) : FLT_MAX;
+          startSp       = ne;
+          // the cell's anchor (the triangle nearest to its centre) gives every lane a real distance
+          // to start from, usually within a hair of its own nearest
+          const int anc = cv.anchor ? __ldg(cv.anchor + cell) : -1;
+          if (anc >= 0) {
+            const float4* h  = reinterpret_cast<const float4*>(m.hot + anc);
+            const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
+            float         s_, t_;
+            int           r_;
+            const float   dd = triDist2<false>(h0, h1, h2, px, py, pz, s_, t_, r_);
+            if (dd <= best) {
+              best    = dd;
+              besttri = anc;
+            }
+          }
+        }
+      }
     }
     uint32_t iters = 0;
     int      err   = 0;
     uint32_t cNode = 0, cLeaf = 0, cTri = 0, cFall = 0, cBox = 0;
-    uint32_t pPops = 0, pNode = 0, pLeaf = 0, pTri = 0, pBox = 0;
+    uint32_t pPops = 0, pNode = 0, pLeaf = 0, pTri = 0, pBox = 0, pRecs = 0;
 
 #pragma unroll 1
     for (int pass = 0; pass < (SEEDED ? 2 : 1); pass++) {
@@ -106,7 +166,12 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         }
       }
       TraversalCounters tc;
-      traverseMesh<STATS>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc);
+      if (SEED == 3 && pass == 0 && startSp > 0) {
+        traverseFrom<STATS, STACK>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc);
+      }
+      else {
+        traverseMesh<STATS, STACK>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc);
+      }
       cNode += tc.node;
       cLeaf += tc.leaf;
       cTri += tc.tri;
@@ -116,6 +181,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       pNode += tc.pnode;
       pLeaf += tc.pleaf;
       pTri += tc.ptri;
+      pRecs += tc.precs;
       if (err) {
         break;
       }
@@ -131,7 +197,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
     if (valid) {
       a.out_d[id] = dist;
       if (a.out_tri) {
-        a.out_tri[id] = besttri >= 0 ? __ldg(m.tri_id + besttri) : -1;
+        a.out_tri[id] = besttri >= 0 ? (a.tri_leaf ? besttri : __ldg(m.tri_id + besttri)) : -1;
       }
     }
     if (a.band_flag) {
@@ -172,8 +238,14 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         atomicAdd(a.stats + 8, (unsigned long long)pLeaf);
         atomicAdd(a.stats + 9, (unsigned long long)pTri);
         atomicAdd(a.stats + 11, (unsigned long long)pBox);
+        atomicAdd(a.stats + 14, (unsigned long long)pRecs);
+        if (startSp > 0) {
+          atomicAdd(a.stats + 12, 1ull);
+          atomicAdd(a.stats + 13, (unsigned long long)startSp);
+        }
       }
     }
+    pk++;
   }
 }
 
@@ -200,7 +272,7 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
     wpb = 4;
   }
   const int    threads = 32 * wpb;
-  const size_t smem    = size_t(wpb) * (2 * EBG_STACK_DEPTH + 32) * sizeof(float4);
+  const size_t smem    = size_t(wpb) * (2 * (SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH) + 32) * sizeof(float4);
   // resident blocks per SM for each block size, looked up once (the query path then issues no
   // runtime calls besides its launches, so it can be captured in a CUDA graph)
   static int cache[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -242,9 +314,15 @@ cudaError_t launchStats(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_
 template <int OCC>
 cudaError_t launchSeed(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
-  const int mode = a.seed_pk != nullptr ? 1 : (a.hint != nullptr ? 2 : 0);
-  return mode == 1 ? launchStats<1, OCC>(a, wpb, numSms, s)
-                   : (mode == 2 ? launchStats<2, OCC>(a, wpb, numSms, s) : launchStats<0, OCC>(a, wpb, numSms, s));
+  const int mode = a.cells.count != nullptr ? 3 : (a.hint != nullptr ? 2 : 0);
+  switch (mode) {
+  case 3:
+    return launchStats<3, OCC>(a, wpb, numSms, s);
+  case 2:
+    return launchStats<2, OCC>(a, wpb, numSms, s);
+  default:
+    return launchStats<0, OCC>(a, wpb, numSms, s);
+  }
 }
 
 cudaError_t launchMeshSdf32(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s, int occupancy)

@@ -137,28 +137,24 @@ struct TraversalCounters
 {
   uint32_t node = 0, leaf = 0, tri = 0, fall = 0, box = 0; // per lane: what this query needed
   uint32_t pops = 0, pnode = 0, pleaf = 0, ptri = 0, pbox = 0; // per packet: what the warp executed
+  uint32_t precs = 0;                                             // triangle records of its opened leaves
 };
 
-// One packet traversal of mesh m: each lane's best squared distance `best` (its pruning bound,
-// already seeded or FLT_MAX) and winning triangle `besttri` (leaf order) are updated.  Children are
-// ordered by their smallest distance over the packet's lanes.  `stk` is this warp's stack region
-// (2 float4 per entry, EBG_STACK_DEPTH entries); `pts` is this warp's 32-entry scratch for the
-// points of the lanes a leaf is spread over; `iters` counts loop trips against MAX_ITERS; `err`
-// receives ST_* bits.  All 32 lanes must call it together.
-template <bool STATS>
-__device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
-                                             int& besttri, float4* stk, float4* pts, uint32_t& iters, int& err,
-                                             TraversalCounters& cnt_)
+// Packet traversal of mesh m from the `sp` entries already on the warp's stack (the top entry is
+// popped first): each lane's best squared distance `best` (its pruning bound, already seeded or
+// FLT_MAX) and winning triangle `besttri` (leaf order) are updated.  Children are ordered by their
+// smallest distance over the packet's lanes.  `stk` is this warp's stack region (2 float4 per entry,
+// STACK entries); `pts` is this warp's 32-entry scratch for the points of the lanes a leaf is spread
+// over; `iters` counts loop trips against MAX_ITERS; `err` receives ST_* bits.  All 32 lanes must
+// call it together.
+template <bool STATS, int STACK>
+__device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, float py, float pz, float& best,
+                                             int& besttri, float4* stk, float4* pts, int sp, uint32_t& iters,
+                                             int& err, TraversalCounters& cnt_)
 {
   const int lane = threadIdx.x & 31;
       // a finite bound keeps empty child slots (infinite box distance) off the stack
       best = fminf(best, FLT_MAX);
-      int sp = 1;
-      if (lane == 0) {
-        stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
-        stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
-      }
-      __syncwarp();
 #pragma unroll 1
       while (sp > 0) {
         if (++iters > MAX_ITERS) {
@@ -204,6 +200,7 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           if (STATS) {
             cnt_.pleaf++;
             cnt_.ptri += passes < int(cnt) - 1 ? uint32_t(passes) : cnt;
+            cnt_.precs += cnt;
           }
           if (passes < int(cnt) - 1) {
             const int rank = __popc(needMask & ((1u << lane) - 1u));
@@ -310,7 +307,7 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
             key[k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
           }
           const int np = int(key[0] >= 0.f) + int(key[1] >= 0.f) + int(key[2] >= 0.f) + int(key[3] >= 0.f);
-          if (sp + np > EBG_STACK_DEPTH) {
+          if (sp + np > STACK) {
             err |= ST_STACK;
             break;
           }
@@ -339,6 +336,20 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
           }
         }
       }
+}
+
+// One packet traversal from the root of mesh m (see traverseFrom).
+template <bool STATS, int STACK = EBG_STACK_DEPTH>
+__device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
+                                             int& besttri, float4* stk, float4* pts, uint32_t& iters, int& err,
+                                             TraversalCounters& cnt_)
+{
+  if ((threadIdx.x & 31) == 0) {
+    stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
+    stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+  }
+  __syncwarp();
+  traverseFrom<STATS, STACK>(m, px, py, pz, best, besttri, stk, pts, 1, iters, err, cnt_);
 }
 
 } // namespace ebg

@@ -27,6 +27,13 @@ namespace {
 
 constexpr int OUTER_DEPTH = 48; // object-BVH stack entries per warp (builder checks the depth)
 
+// A batched call whose batch sizes did not add up to its point count reads no point.
+__device__ __forceinline__ bool batchesValid(const SceneQueryArgs& a)
+{
+  return a.batches == nullptr || __ldg(a.batch_start + a.num_batches) == a.n;
+}
+
+
 __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
 {
   __shared__ float4 smem[4 * (2 * (OUTER_DEPTH + EBG_STACK_DEPTH) + 32)];
@@ -36,13 +43,21 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
   float4*           lpts  = istk + 2 * EBG_STACK_DEPTH; // the warp's 32 spread-leaf points
   const SceneView&  sc    = a.scene;
   const uint64_t    numPk = (uint64_t(a.n) + 31) / 32;
+  if (!batchesValid(a)) {
+    return;
+  }
 
+  // packets come from the work counter `chunk` at a time
+  const unsigned long long chunk = a.chunk > 1 ? (unsigned long long)a.chunk : 1ull;
+  unsigned long long       pk = 0, pkEnd = 0;
   while (true) {
-    unsigned long long pk = 0;
-    if (lane == 0) {
-      pk = atomicAdd(a.work, 1ull);
+    if (pk == pkEnd) {
+      if (lane == 0) {
+        pk = atomicAdd(a.work, chunk);
+      }
+      pk    = __shfl_sync(FULL, pk, 0);
+      pkEnd = pk + chunk;
     }
-    pk = __shfl_sync(FULL, pk, 0);
     if (pk >= numPk) {
       break;
     }
@@ -50,8 +65,9 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
     const bool     valid = pos < a.n;
     const int64_t  src   = valid ? pos : a.n - 1;
     const uint32_t id    = a.order ? __ldg(a.order + src) : uint32_t(src);
-    const float px = __ldg(a.points + 3 * size_t(id)), py = __ldg(a.points + 3 * size_t(id) + 1),
-                pz = __ldg(a.points + 3 * size_t(id) + 2);
+    float*         outp  = nullptr;
+    const float*   pp    = scenePoint(a, id, &outp);
+    const float    px = __ldg(pp), py = __ldg(pp + 1), pz = __ldg(pp + 2);
     float    best  = __int_as_float(0x7f800000); // +inf, as the reference starts
     uint32_t iters = 0;
     int      err   = 0;
@@ -147,14 +163,83 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
       atomicOr(a.status, err);
     }
     if (valid) {
-      a.out[id] = best;
+      *outp = best;
+      if (a.band_flag) {
+        a.band_flag[pos] = uint8_t(fabsf(best) <= a.band);
+      }
     }
+    pk++;
   }
 }
 
 } // namespace
 
+__global__ void kSceneBatchKeys(const SceneQueryArgs a, uint64_t* __restrict__ keys, uint32_t* __restrict__ ids)
+{
+  const SceneView& v = a.scene;
+  if (!batchesValid(a)) {
+    return;
+  }
+  for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < a.n; g += int64_t(gridDim.x) * blockDim.x) {
+    float*       outp = nullptr;
+    const float* p    = scenePoint(a, uint32_t(g), &outp);
+    // the batch index (the same binary search as scenePoint) above the point's Morton code
+    int lo = 0, hi = a.num_batches - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.batch_start[mid] <= g) {
+        lo = mid;
+      }
+      else {
+        hi = mid - 1;
+      }
+    }
+    const float fx = fminf(fmaxf((p[0] - v.morton_lo[0]) * v.morton_scale[0], 0.f), 1023.f);
+    const float fy = fminf(fmaxf((p[1] - v.morton_lo[1]) * v.morton_scale[1], 0.f), 1023.f);
+    const float fz = fminf(fmaxf((p[2] - v.morton_lo[2]) * v.morton_scale[2], 0.f), 1023.f);
+    const uint32_t m = (spread10(uint32_t(fx)) << 2) | (spread10(uint32_t(fy)) << 1) | spread10(uint32_t(fz));
+    keys[g]          = (uint64_t(lo) << 30) | uint64_t(m);
+    ids[g]           = uint32_t(g);
+  }
+}
+
+// One thread: the exclusive prefix of the batch sizes (at most a few thousand batches).  A negative
+// size, or a total other than the caller's, is reported as ST_INPUT and leaves start[nb] != the
+// call's point count, which every kernel of the call checks before it reads a point.
+__global__ void kSceneBatchStarts(const SceneBatch* __restrict__ b, int32_t nb, int64_t* __restrict__ start,
+                                  int* __restrict__ status, int64_t expect)
+{
+  int64_t acc = 0;
+  bool    bad = false;
+  for (int32_t i = 0; i < nb; i++) {
+    start[i]        = acc;
+    const int64_t n = b[i].n;
+    bad             = bad || n < 0;
+    acc += n > 0 ? n : 0;
+  }
+  bad       = bad || acc != expect;
+  start[nb] = bad ? -1 : acc;
+  if (bad) {
+    atomicOr(status, ST_INPUT);
+  }
+}
+
 int sceneOuterDepth() { return OUTER_DEPTH; }
+
+cudaError_t launchSceneBatchKeys(const SceneQueryArgs& a, uint64_t* keys, uint32_t* ids, cudaStream_t s)
+{
+  int64_t blocks = (a.n + 255) / 256;
+  blocks         = blocks < 4096 ? blocks : 4096;
+  kSceneBatchKeys<<<unsigned(blocks < 1 ? 1 : blocks), 256, 0, s>>>(a, keys, ids);
+  return cudaGetLastError();
+}
+
+cudaError_t launchSceneBatchStarts(const SceneBatch* batches, int32_t nb, int64_t* start, int* status,
+                                   int64_t expectTotal, cudaStream_t s)
+{
+  kSceneBatchStarts<<<1, 1, 0, s>>>(batches, nb, start, status, expectTotal);
+  return cudaGetLastError();
+}
 
 cudaError_t launchSceneValue(const SceneQueryArgs& a, int numSms, cudaStream_t s)
 {

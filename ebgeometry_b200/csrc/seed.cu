@@ -409,38 +409,7 @@ __global__ void __launch_bounds__(WARPS * 32) kSeedTrain(const SeedTrainArgs a)
   }
 }
 
-struct PredSmem
-{
-  SmemWeights w;
-  WarpTiles   tiles[WARPS];
-};
-
-__global__ void __launch_bounds__(WARPS * 32) kSeedPredict(const SeedView v, const float* __restrict__ pts, int64_t n,
-                                                           float* __restrict__ out)
-{
-  extern __shared__ __align__(16) unsigned char smraw[];
-  PredSmem&  S    = *reinterpret_cast<PredSmem*>(smraw);
-  const int  lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  stageWeights(v.params, S.w);
-  __syncthreads();
-  WarpTiles&    tl    = S.tiles[wid];
-  const int64_t tiles = (n + 31) / 32;
-  for (int64_t tile = int64_t(blockIdx.x) * WARPS + wid; tile < tiles; tile += int64_t(gridDim.x) * WARPS) {
-    const int64_t i  = tile * 32 + lane;
-    const int64_t ii = i < n ? i : n - 1;
-    float         feat[SEED_IN];
-    encode(v, pts[3 * ii], pts[3 * ii + 1], pts[3 * ii + 2], feat);
-    storeFeatures(tl, lane, feat);
-    __syncwarp();
-    const float y = mlpForward(S.w, tl, lane);
-    if (i < n) {
-      out[i] = y;
-    }
-    __syncwarp();
-  }
-}
-
-// ---- per-packet inference with the activations in registers -----------------------------------
+// ---- inference with the activations in registers ---------------------------------------------
 //
 // The accumulator fragment of m16n8k16 (rows g, g+8; columns 2t, 2t+1 of an 8-wide n-tile) is, for
 // two neighbouring n-tiles, exactly the A fragment of a 16-wide k-chunk of the next layer, so the
@@ -448,10 +417,10 @@ __global__ void __launch_bounds__(WARPS * 32) kSeedPredict(const SeedView v, con
 
 constexpr int PK_WARPS = 8;
 
-struct PacketSmem
+struct PredSmem
 {
   SmemWeights   w;
-  __nv_bfloat16 x[PK_WARPS][32 * SEED_IN]; // encodings of the warp's 32 packet centres
+  __nv_bfloat16 x[PK_WARPS][32 * SEED_IN]; // encodings of the warp's 32 points
 };
 
 // c[nt] = bias + A x W^T restricted to n-tile nt, for one 16-row tile (W BF16 [64][K] rows in
@@ -490,114 +459,90 @@ __device__ __forceinline__ void reluToA(const float (&c)[8][4], uint32_t (&a)[4]
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
-// One inference per packet of 32 sorted queries.  Lane q of a warp takes packet 32 * group + q:
-// it averages the packet's points (positions clamped to n - 1, as the traversal clamps them), the
-// network predicts |d| there, and out[packet] = (centre, (1 + alpha) |prediction| + beta).
-__global__ void __launch_bounds__(PK_WARPS * 32, 2) kSeedPackets(const SeedView v, const float* __restrict__ pts,
-                                                              const uint32_t* __restrict__ order, int64_t n,
-                                                              float4* __restrict__ out)
+// The network on the warp's 32 encodings in xt (row q = sample q); returns row `lane`'s output.
+__device__ float mlpRegs(const SmemWeights& w, const __nv_bfloat16* xt, int lane)
+{
+  const int g = lane >> 2, t = lane & 3;
+  // y[mt][h] = this lane's share of row 16 mt + 8 h + g of the output layer, then summed over the
+  // four lanes sharing the row
+  float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll 1
+  for (int mt = 0; mt < 2; mt++) {
+    uint32_t a1[2][4];
+#pragma unroll
+    for (int kc = 0; kc < 2; kc++) {
+      const __nv_bfloat16* r0 = xt + (mt * 16 + g) * SEED_IN + kc * 16 + 2 * t;
+      a1[kc][0]               = ld32(r0);
+      a1[kc][1]               = ld32(r0 + 8 * SEED_IN);
+      a1[kc][2]               = ld32(r0 + 8);
+      a1[kc][3]               = ld32(r0 + 8 * SEED_IN + 8);
+    }
+    float    c[8][4];
+    uint32_t a[4][4];
+    denseRegs<SEED_IN>(a1, w.w1, w.b1, c, lane);
+    reluToA(c, a);
+    denseRegs<SEED_WIDTH>(a, w.w2, w.b2, c, lane);
+    reluToA(c, a);
+    denseRegs<SEED_WIDTH>(a, w.w3, w.b3, c, lane);
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+      const float w0 = __bfloat162float(w.w4[nt * 8 + 2 * t]), w1 = __bfloat162float(w.w4[nt * 8 + 2 * t + 1]);
+      y0 = fmaf(bf16r(fmaxf(c[nt][0], 0.f)), w0, fmaf(bf16r(fmaxf(c[nt][1], 0.f)), w1, y0));
+      y1 = fmaf(bf16r(fmaxf(c[nt][2], 0.f)), w0, fmaf(bf16r(fmaxf(c[nt][3], 0.f)), w1, y1));
+    }
+    if (mt == 0) {
+      y[0][0] = y0;
+      y[0][1] = y1;
+    }
+    else {
+      y[1][0] = y0;
+      y[1][1] = y1;
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      y[mt][h] += __shfl_xor_sync(FULL, y[mt][h], 1);
+      y[mt][h] += __shfl_xor_sync(FULL, y[mt][h], 2);
+    }
+  }
+  // row q = 16 mt + 8 h + g' lives on lane 4 g'; lane q takes its own row
+  const int   srcLane = (lane & 7) * 4;
+  const float r00 = __shfl_sync(FULL, y[0][0], srcLane), r01 = __shfl_sync(FULL, y[0][1], srcLane);
+  const float r10 = __shfl_sync(FULL, y[1][0], srcLane), r11 = __shfl_sync(FULL, y[1][1], srcLane);
+  const int   mtq = lane >> 4, hq = (lane >> 3) & 1;
+  return w.b4 + (mtq == 0 ? (hq == 0 ? r00 : r01) : (hq == 0 ? r10 : r11));
+}
+
+// One prediction per point: lane q of a warp encodes point 32 * tile + q (clamped to n - 1), the
+// warp runs the network on the 32 encodings.
+__global__ void __launch_bounds__(PK_WARPS * 32, 2) kSeedPredict(const SeedView v, const float* __restrict__ pts,
+                                                              int64_t n, float* __restrict__ out)
 {
   extern __shared__ __align__(16) unsigned char smraw[];
-  PacketSmem&    S    = *reinterpret_cast<PacketSmem*>(smraw);
+  PredSmem&      S    = *reinterpret_cast<PredSmem*>(smraw);
   const int      lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   stageWeights(v.params, S.w);
   __syncthreads();
-  __nv_bfloat16* xt       = S.x[wid];
-  const int64_t  nPackets = (n + 31) / 32;
-  const int64_t  groups   = (nPackets + 31) / 32;
-  const int      g = lane >> 2, t = lane & 3;
-  for (int64_t grp = int64_t(blockIdx.x) * PK_WARPS + wid; grp < groups; grp += int64_t(gridDim.x) * PK_WARPS) {
-    const int64_t pk  = grp * 32 + lane;
-    const int64_t pkc = pk < nPackets ? pk : nPackets - 1;
-    float         sx = 0.f, sy = 0.f, sz = 0.f;
-    if (pkc * 32 + 32 <= n && (reinterpret_cast<uintptr_t>(order) & 15u) == 0) {
-      // a full packet: 32 ids in eight 16-byte loads
-#pragma unroll 2
-      for (int j = 0; j < 32; j += 4) {
-        uint4 ids = order ? __ldg(reinterpret_cast<const uint4*>(order + pkc * 32 + j))
-                          : make_uint4(uint32_t(pkc * 32 + j), uint32_t(pkc * 32 + j + 1), uint32_t(pkc * 32 + j + 2),
-                                       uint32_t(pkc * 32 + j + 3));
-        const uint32_t id4[4] = {ids.x, ids.y, ids.z, ids.w};
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          sx += __ldg(pts + 3 * size_t(id4[k]));
-          sy += __ldg(pts + 3 * size_t(id4[k]) + 1);
-          sz += __ldg(pts + 3 * size_t(id4[k]) + 2);
-        }
-      }
-    }
-    else {
-      for (int j = 0; j < 32; j++) {
-        const int64_t  src = pkc * 32 + j < n ? pkc * 32 + j : n - 1;
-        const uint32_t id  = order ? __ldg(order + src) : uint32_t(src);
-        sx += __ldg(pts + 3 * size_t(id));
-        sy += __ldg(pts + 3 * size_t(id) + 1);
-        sz += __ldg(pts + 3 * size_t(id) + 2);
-      }
-    }
-    const float cx = sx * (1.f / 32.f), cy = sy * (1.f / 32.f), cz = sz * (1.f / 32.f);
-    float       feat[SEED_IN];
-    encode(v, cx, cy, cz, feat);
+  __nv_bfloat16* xt    = S.x[wid];
+  const int64_t  tiles = (n + 31) / 32;
+  for (int64_t tile = int64_t(blockIdx.x) * PK_WARPS + wid; tile < tiles; tile += int64_t(gridDim.x) * PK_WARPS) {
+    const int64_t i  = tile * 32 + lane;
+    const int64_t ii = i < n ? i : n - 1;
+    float         feat[SEED_IN];
+    encode(v, __ldg(pts + 3 * ii), __ldg(pts + 3 * ii + 1), __ldg(pts + 3 * ii + 2), feat);
 #pragma unroll
     for (int k = 0; k < SEED_IN; k += 2) {
       *reinterpret_cast<uint32_t*>(xt + lane * SEED_IN + k) = pack2(feat[k], feat[k + 1]);
     }
     __syncwarp();
-    // the network on the two 16-row tiles in turn; y[mt][h] = this lane's share of row
-    // 16 mt + 8 h + g of the output layer, then summed over the four lanes sharing the row
-    float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-#pragma unroll 1
-    for (int mt = 0; mt < 2; mt++) {
-      uint32_t a1[2][4];
-#pragma unroll
-      for (int kc = 0; kc < 2; kc++) {
-        const __nv_bfloat16* r0 = xt + (mt * 16 + g) * SEED_IN + kc * 16 + 2 * t;
-        a1[kc][0]               = ld32(r0);
-        a1[kc][1]               = ld32(r0 + 8 * SEED_IN);
-        a1[kc][2]               = ld32(r0 + 8);
-        a1[kc][3]               = ld32(r0 + 8 * SEED_IN + 8);
-      }
-      float    c[8][4];
-      uint32_t a[4][4];
-      denseRegs<SEED_IN>(a1, S.w.w1, S.w.b1, c, lane);
-      reluToA(c, a);
-      denseRegs<SEED_WIDTH>(a, S.w.w2, S.w.b2, c, lane);
-      reluToA(c, a);
-      denseRegs<SEED_WIDTH>(a, S.w.w3, S.w.b3, c, lane);
-      float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-      for (int nt = 0; nt < 8; nt++) {
-        const float w0 = __bfloat162float(S.w.w4[nt * 8 + 2 * t]), w1 = __bfloat162float(S.w.w4[nt * 8 + 2 * t + 1]);
-        y0 = fmaf(bf16r(fmaxf(c[nt][0], 0.f)), w0, fmaf(bf16r(fmaxf(c[nt][1], 0.f)), w1, y0));
-        y1 = fmaf(bf16r(fmaxf(c[nt][2], 0.f)), w0, fmaf(bf16r(fmaxf(c[nt][3], 0.f)), w1, y1));
-      }
-      if (mt == 0) {
-        y[0][0] = y0;
-        y[0][1] = y1;
-      }
-      else {
-        y[1][0] = y0;
-        y[1][1] = y1;
-      }
+    const float y = mlpRegs(S.w, xt, lane);
+    if (i < n) {
+      out[i] = y;
     }
     __syncwarp();
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        y[mt][h] += __shfl_xor_sync(FULL, y[mt][h], 1);
-        y[mt][h] += __shfl_xor_sync(FULL, y[mt][h], 2);
-      }
-    }
-    // row q = 16 mt + 8 h + g' lives on lane 4 g'; lane q takes its own row
-    const int   srcLane = (lane & 7) * 4;
-    const float r00 = __shfl_sync(FULL, y[0][0], srcLane), r01 = __shfl_sync(FULL, y[0][1], srcLane);
-    const float r10 = __shfl_sync(FULL, y[1][0], srcLane), r11 = __shfl_sync(FULL, y[1][1], srcLane);
-    const int   mtq = lane >> 4, hq = (lane >> 3) & 1;
-    const float yq  = S.w.b4 + (mtq == 0 ? (hq == 0 ? r00 : r01) : (hq == 0 ? r10 : r11));
-    if (pk < nPackets) {
-      out[pk] = make_float4(cx, cy, cz, (1.f + v.alpha) * fabsf(yq) + v.beta);
-    }
   }
 }
 
@@ -725,25 +670,10 @@ cudaError_t launchSeedPredict(const SeedView& v, const float* pts, int64_t n, fl
     return e;
   }
   const int64_t tiles  = (n + 31) / 32;
-  int64_t       blocks = (tiles + WARPS - 1) / WARPS;
-  blocks               = blocks < int64_t(numSms) * 4 ? blocks : int64_t(numSms) * 4;
-  kSeedPredict<<<unsigned(blocks), WARPS * 32, sizeof(PredSmem), s>>>(v, pts, n, out);
-  return cudaGetLastError();
-}
-
-cudaError_t launchSeedPackets(const SeedView& v, const float* pts, const uint32_t* order, int64_t n, float4* out,
-                              int numSms, cudaStream_t s)
-{
-  // the dynamic shared-memory opt-in is per device, so it is set on every launch (cheap)
-  const cudaError_t e = setSmem<PacketSmem>(reinterpret_cast<const void*>(kSeedPackets));
-  if (e != cudaSuccess) {
-    return e;
-  }
-  const int64_t groups = ((n + 31) / 32 + 31) / 32;
-  int64_t       blocks = (groups + PK_WARPS - 1) / PK_WARPS;
-  blocks               = blocks < int64_t(numSms) * 4 ? blocks : int64_t(numSms) * 4;
+  int64_t       blocks = (tiles + PK_WARPS - 1) / PK_WARPS;
+  blocks               = blocks < int64_t(numSms) * 2 ? blocks : int64_t(numSms) * 2;
   blocks               = blocks < 1 ? 1 : blocks;
-  kSeedPackets<<<unsigned(blocks), PK_WARPS * 32, sizeof(PacketSmem), s>>>(v, pts, order, n, out);
+  kSeedPredict<<<unsigned(blocks), PK_WARPS * 32, sizeof(PredSmem), s>>>(v, pts, n, out);
   return cudaGetLastError();
 }
 

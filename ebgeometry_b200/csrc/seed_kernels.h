@@ -53,10 +53,6 @@ struct SeedTrainArgs
 void        seedLevels(int baseRes, int maxRes, uint32_t log2T, SeedView& v);
 cudaError_t launchSeedTrainStep(const SeedTrainArgs& a, int numSms, cudaStream_t s);
 cudaError_t launchSeedPredict(const SeedView& v, const float* pts, int64_t n, float* out, int numSms, cudaStream_t s);
-// Per-packet radius: packet p = sorted positions [32p, 32p+32) of the queries (clamped to n-1);
-// out[p] = (centre of the packet's points, radius predicted by the network at that centre).
-cudaError_t launchSeedPackets(const SeedView& v, const float* pts, const uint32_t* order, int64_t n, float4* out,
-                              int numSms, cudaStream_t s);
 cudaError_t launchAdam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
                        int step, __nv_bfloat16* shadow, cudaStream_t s);
 cudaError_t launchInitUniform(float* p, int64_t n, float lo, float hi, uint64_t seed, cudaStream_t s);

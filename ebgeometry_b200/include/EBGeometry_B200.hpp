@@ -126,6 +126,10 @@ public:
   void signedDistancesDevice(const float* a_pointsDev, size_t a_n, float* a_distDev, void* a_stream = nullptr,
                              const SeedModel* a_seed = nullptr) const;
 
+  // Builds this mesh's per-cell entry cuts from a trained model (ebg_seed_attach); queries passing
+  // that model then start from them.  Synchronous.
+  void attachSeed(const SeedModel& a_seed, const ebg_attach_opts* a_opts = nullptr);
+
   // FP64 end to end (the reference's own precision): host points, synchronous.
   void signedDistances(const double* a_pointsHost, size_t a_n, double* a_distHost,
                        int32_t* a_closestTriangleHost = nullptr) const
@@ -274,9 +278,11 @@ protected:
 class SeedModel
 {
 public:
-  explicit SeedModel(const TriMeshSDF& a_mesh, const ebg_seed_opts* a_opts = nullptr)
+  // Trains on a_mesh and attaches the model to it with the default cells.
+  explicit SeedModel(TriMeshSDF& a_mesh, const ebg_seed_opts* a_opts = nullptr)
   {
     check(ebg_seed_train(a_mesh.handle(), a_opts, &m_seed, nullptr, nullptr));
+    a_mesh.attachSeed(*this);
   }
   explicit SeedModel(const std::string& a_checkpoint, int a_device = -1)
   {
@@ -297,6 +303,12 @@ public:
 private:
   ebg_seed* m_seed = nullptr;
 };
+
+inline void
+TriMeshSDF::attachSeed(const SeedModel& a_seed, const ebg_attach_opts* a_opts)
+{
+  check(ebg_seed_attach(m_mesh, a_seed.handle(), a_opts, nullptr, nullptr));
+}
 
 inline void
 TriMeshSDF::signedDistances(const float* a_pointsHost, size_t a_n, float* a_distHost, const SeedModel* a_seed,

@@ -99,6 +99,9 @@ typedef struct ebg_query_opts
                                          = no hint for that point.  A hint below the true |d| only
                                          costs a second traversal of that point.  Ignored when
                                          seed is set. */
+  int32_t            queue_chunk;     /* packets of 32 queries a warp takes from the device work
+                                         queue at a time (mesh and union queries); 0 = tuned
+                                         default (1) */
 } ebg_query_opts;
 
 /* Mesh summary. */
@@ -132,16 +135,14 @@ typedef struct ebg_query_stats
   int64_t packet_triangles;  /* point-triangle tests executed by the warp */
   int64_t boxes_tested;      /* oriented leaf/node boxes evaluated, per query */
   int64_t packet_boxes;      /* oriented boxes the warp evaluated */
+  int64_t cut_packets;       /* packets that started from a cell's entry cut (ebg_seed_attach) */
+  int64_t cut_entries;       /* entries those packets took from their cuts */
+  int64_t packet_triangle_records; /* triangle records (48 B each) of the leaves the warps opened */
 } ebg_query_stats;
 
 const char* ebg_last_error(void);
 const char* ebg_version(void);
 int         ebg_device_count(void);
-
-/* Read bandwidth (GB/s) of a kernel streaming a `bytes`-sized device buffer `iters` times on the
- * current device: with bytes well under the L2 size (126 MB on B200) it measures the L2 read roof
- * the traversal kernels are compared with.  No reference counterpart (measurement utility). */
-ebg_status ebg_measure_read_bandwidth(int64_t bytes, int32_t iters, double* gbs);
 
 /* ---- triangle meshes: TriMeshSDF (MeshDistanceFunctions.hpp:309-489) -------------------------
  *
@@ -355,12 +356,15 @@ ebg_status ebg_mesh_signed_distance_flat_f64_host(const ebg_mesh* mesh,
  * callers that cannot let a library allocate: AMR codes such as AMReX reserve most of the GPU's memory
  * for their own arena at start-up, so a library's cudaMalloc or stream-ordered allocation can fail
  * inside their embedded-boundary loop, and other codes forbid allocations there for latency.  The
- * per-call workspace comes from a fixed 24 MiB array compiled into the library (held on every device
- * that loads it until exit) instead of the memory pool.  Limits: n <= 524,288 points per call (larger
- * n returns EBG_ERR_TOO_LARGE); opts->timings is ignored.  The first call on a device resolves the
- * array's address there; make it before capturing a CUDA graph.  All calls on a device share the
- * array, so calls whose work overlaps on the GPU (different streams) race and must be serialised.
- * Results are those of ebg_mesh_signed_distance. */
+ * per-call workspace comes from a fixed 24 MiB array compiled into the library instead of the memory
+ * pool.  Limits: n <= 524,288 points per call (larger n returns EBG_ERR_TOO_LARGE); opts->timings is
+ * ignored.  The first call on a device (n = 0 is enough) resolves the array's address there, and
+ * with lazy module loading (the CUDA default) that is also when the 24 MiB are taken on that device,
+ * where they stay until the process exits: make that first call before reserving a memory arena and
+ * before capturing a CUDA graph.  cudaDeviceReset on the device invalidates the array; do not call
+ * this entry point on a device after resetting it.  All calls on a device share the array, so calls
+ * whose work overlaps on the GPU (different streams) race and must be serialised.  Results are those
+ * of ebg_mesh_signed_distance (the same launch shape, seed and band handling). */
 ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       mesh,
                                             const float*          points_dev,
                                             int64_t               n,
@@ -379,17 +383,21 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       mesh,
                                           void*                 stream);
 
 /* Autotuner (no reference counterpart): times the traversal's launch shapes -- register budget
- * (ebg_query_opts.occupancy 1..4) x warps per block (2, 4, 8) -- on the caller's sample points
- * (device), keeps the fastest as this mesh's default for queries that leave those options at 0, and
- * returns it (best_occupancy / best_warps_per_block, best_ms = the sample's traversal time).
- * Synchronous. */
-ebg_status ebg_mesh_autotune(ebg_mesh*    mesh,
-                             const float* sample_points_dev,
-                             int64_t      n,
-                             int32_t*     best_occupancy,
-                             int32_t*     best_warps_per_block,
-                             float*       best_ms,
-                             void*        stream);
+ * (ebg_query_opts.occupancy 1..4) x warps per block (2, 4, 8), then the work-queue chunk (1, 2, 4
+ * packets per grab) at the fastest shape -- on the caller's sample points (device), keeps the
+ * fastest as this mesh's default for queries that leave those options at 0, and returns it
+ * (best_occupancy / best_warps_per_block / best_queue_chunk, any of them nullable; best_ms = the
+ * sample's traversal time).  `seed` (nullable) times the seeded traversal of a model attached to
+ * the mesh.  Synchronous. */
+ebg_status ebg_mesh_autotune(ebg_mesh*       mesh,
+                             const float*    sample_points_dev,
+                             int64_t         n,
+                             const ebg_seed* seed,
+                             int32_t*        best_occupancy,
+                             int32_t*        best_warps_per_block,
+                             int32_t*        best_queue_chunk,
+                             float*          best_ms,
+                             void*           stream);
 
 /* ImplicitFunction<T>::value(point) for one point (ImplicitFunction.hpp:51-52): the drop-in
  * single-point call, in FP64 (ebg_mesh_signed_distance_f64_host).  Synchronous; each call is a few
@@ -524,15 +532,38 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
 ebg_status ebg_scene_destroy(ebg_scene* scene);
 int64_t    ebg_scene_num_objects(const ebg_scene* scene);
 /* BVHUnionIF::value (CSGImplem.hpp:465-501) at n device points: min over the objects, the object
- * BVH pruned with max(0, best)^2.  One persistent launch for the whole array, so many query batches
- * of uneven length go in one call when concatenated.  Asynchronous on stream; only opts->no_sort is
- * used. */
+ * BVH pruned with max(0, best)^2.  FP32 with an FP64 near-surface pass: a point whose FP32 value
+ * lies within opts->band (default 1e-4 x the scene box's diagonal) of zero is evaluated again in
+ * double as the reference does (the sphere distance, RotateIF's per-axis point map with cos / sin in
+ * double, the mesh's FP64 triangle test), over the objects that can hold the minimum.  One
+ * persistent launch for the whole array.  Asynchronous on stream; opts->no_sort, no_fp64_band and
+ * band are used. */
 ebg_status ebg_scene_value(const ebg_scene*      scene,
                            const float*          points_dev,
                            int64_t               n,
                            float*                out_dev,
                            const ebg_query_opts* opts,
                            void*                 stream);
+/* One batch of ebg_scene_eval_batches: n device points (xyz float32) and n device results. */
+typedef struct ebg_batch
+{
+  const float* points_dev;
+  int64_t      n;
+  float*       out_dev;
+} ebg_batch;
+/* Many query batches of uneven length in one call (the reference has no batch API; its callers loop
+ * over value(point)): batches_dev is a DEVICE array of num_batches descriptors whose n add up to
+ * total_points (a mismatch or a negative n computes nothing and is reported by the next status
+ * check as EBG_ERR_TRAVERSAL).  The points of all batches are ordered together along a Morton curve
+ * (batch index above the curve's bits) and served by one persistent launch with a device work
+ * queue, then the FP64 near-surface pass, as ebg_scene_value.  Only stream-ordered work, so the call
+ * can be captured in a CUDA graph. */
+ebg_status ebg_scene_eval_batches(const ebg_scene*      scene,
+                                  const ebg_batch*      batches_dev,
+                                  int32_t               num_batches,
+                                  int64_t               total_points,
+                                  const ebg_query_opts* opts,
+                                  void*                 stream);
 ebg_status ebg_scene_value_host(const ebg_scene*      scene,
                                 const float*          points_host,
                                 int64_t               n,
@@ -540,15 +571,26 @@ ebg_status ebg_scene_value_host(const ebg_scene*      scene,
                                 const ebg_query_opts* opts,
                                 void*                 stream);
 ebg_status ebg_scene_check_status(const ebg_scene* scene, void* stream);
+/* Autotuner of the union query (no reference counterpart): times the work-queue chunk (1, 2, 4, 8
+ * packets per grab) on the caller's sample points (device) and keeps the fastest as this scene's
+ * default for calls that leave ebg_query_opts.queue_chunk at 0.  best_queue_chunk and best_ms (the
+ * sample's call time) nullable.  Synchronous. */
+ebg_status ebg_scene_autotune(ebg_scene*   scene,
+                              const float* sample_points_dev,
+                              int64_t      n,
+                              int32_t*     best_queue_chunk,
+                              float*       best_ms,
+                              void*        stream);
 
 /* ---- learned pruning radius (no counterpart in the reference) --------------------------------
  *
  * A multiresolution hash-grid encoding (16 levels x 2 BF16 features, 2^log2_table entries per
  * level) feeding a 3-hidden-layer, 64-wide ReLU MLP (BF16 weights, FP32 accumulation on the tensor
- * cores) that predicts the signed distance.  Passed as ebg_query_opts.seed, it seeds each packet of
- * 32 sorted queries with the pruning radius (1 + alpha) |prediction at the packet centroid| + beta,
- * widened per query by its distance to the centroid.  Distances stay exact: the radius only prunes,
- * and a query whose radius holds no triangle is traversed again without it. */
+ * cores) that predicts the signed distance; its calibrated radius (1 + alpha) |prediction| + beta
+ * bounds |d|.  Attached to a mesh (ebg_seed_attach below), it bounds |d| over the cells of a grid,
+ * and each cell keeps the part of the mesh's tree within that bound; passed as ebg_query_opts.seed,
+ * it starts the traversal of every packet of 32 sorted queries there.  Distances stay exact: the
+ * radius only prunes, and a query whose radius holds no triangle is traversed again without it. */
 typedef struct ebg_seed_opts
 {
   int64_t  num_samples;     /* exact training samples: half uniform in the domain, half within
@@ -603,6 +645,53 @@ ebg_status ebg_seed_set_params(ebg_seed* seed, const float* table, const float* 
  * arrays (grad_table nullable). */
 ebg_status ebg_seed_gradients(ebg_seed* seed, const float* points_dev, const float* target_dev, int32_t n, float eps,
                               float* loss, float* grad_table, float* grad_params);
+
+/* Attaching a model to a mesh (no counterpart in the reference; it replaces the root-down start of
+ * PackedBVH::pruneTraverse, BVHImplem.hpp:1098-1606, for the packets it covers).
+ *
+ * A regular grid of cells_per_axis^3 cells covers the model's domain.  For every cell the model's
+ * calibrated radius at the cell centre, plus the half-diagonal of the cell grown by margin_cells
+ * cells on every side, bounds |d| over that grown cell (R_C); the mesh keeps a CUT of its BVH per
+ * cell: at most max_entries subtrees, refined nearest-first from the root, that hold every triangle
+ * within R_C of the grown cell, and the cell's ANCHOR, the triangle nearest to the cell centre
+ * (found by the mesh path itself).  A query call that passes this model (ebg_query_opts.seed)
+ * starts every packet of 32 sorted queries whose box fits a grown cell from that cell's cut, each
+ * lane's bound being the smaller of R_C and its distance to the anchor; a query that finds nothing
+ * within R_C is traversed again from the root.  Distances are exact whatever the model predicts.
+ * Queries passing a model that is not attached to the mesh are rejected (EBG_ERR_INVALID). */
+typedef struct ebg_attach_opts
+{
+  int32_t cells_per_axis; /* <= 512; 0 = 1.5 cbrt(tree leaves) rounded up to a multiple of 8,
+                             within 16..128 (96 for 1.3 M triangles) */
+  int32_t max_entries;    /* subtrees per cell, <= 112; 0 = 112 (lowered for deep trees).  Memory:
+                             cells * max_entries * 32 B (3.2 GB at 96^3 cells and 112 entries) */
+  float   margin_cells;   /* growth of each cell on every side, in cells; <= 0 -> 1.5 */
+  int32_t radius_mode;    /* 0 = the model's radius (default); 1 = no radius (cuts ordered by
+                             distance only, nothing dropped); 2 = the exact distance at the cell
+                             centres from the mesh path (for comparison with the model) */
+  int32_t no_anchors;     /* 1: no anchor triangles (the triangle nearest to each cell centre, found
+                             by the mesh path, whose distance starts every lane's bound) */
+} ebg_attach_opts;
+
+typedef struct ebg_attach_report
+{
+  int32_t cells_per_axis;
+  int32_t max_entries;
+  int64_t cells;
+  int64_t cut_entries;     /* sum over cells */
+  int64_t empty_cells;     /* cells whose cut is empty (every triangle farther than R_C) */
+  int64_t device_bytes;    /* entries + counts + radii */
+  float   build_ms;        /* device time of the cell radii and cuts */
+  float   mean_radius;     /* mean finite R_C */
+} ebg_attach_report;
+
+/* Builds the mesh's per-cell cuts from `seed` (replacing any earlier attachment; the model may be
+ * destroyed afterwards, the cuts do not refer to it).  ebg_mesh_refit drops the cuts.  Synchronous.
+ * report nullable. */
+ebg_status ebg_seed_attach(ebg_mesh* mesh, const ebg_seed* seed, const ebg_attach_opts* opts, ebg_attach_report* report,
+                           void* stream);
+/* Frees the mesh's cuts; later calls passing the model use the per-packet radius. */
+ebg_status ebg_seed_detach(ebg_mesh* mesh);
 
 #ifdef __cplusplus
 }

@@ -39,18 +39,53 @@ def _cpu_has_avx512() -> bool:
     return False
 
 
-def ref_lib_path() -> str:
+def _cpu_flags():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("flags"):
+                    return set(line.split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_lib_path(timing: bool = False) -> str:
+    """The reference oracle's library: the parity build (no fused multiply-adds), or with ``timing``
+    the -O3 -march=sapphirerapids build with fused multiply-adds, where the host supports it."""
+    if timing and {"avx512_fp16", "amx_tile", "avx512_bf16"} <= _cpu_flags():
+        fast = os.path.join(REF_DIR, "libebgref_fast.so")
+        if os.path.exists(fast):
+            return fast
     name = "libebgref_avx512.so" if _cpu_has_avx512() else "libebgref_avx2.so"
     return os.path.join(REF_DIR, name)
 
 
-def build(reference_dir: str = "/root/reference", quiet: bool = True) -> None:
-    """Builds the port and, when the reference sources are present, the reference oracle."""
+_SOURCE_NOTE = os.path.join(REF_DIR, "source_dir.txt")
+
+
+def reference_dir():
+    """Directory of the reference sources: EBG_REFERENCE_DIR, else the one the reference oracle was
+    last built from (recorded beside it); None when neither names an existing directory."""
+    d = os.environ.get("EBG_REFERENCE_DIR")
+    if not d and os.path.exists(_SOURCE_NOTE):
+        with open(_SOURCE_NOTE) as fh:
+            d = fh.read().strip()
+    return d if d and os.path.isdir(d) else None
+
+
+def build(reference_dir: str | None = None, quiet: bool = True) -> None:
+    """Builds the port and, when the reference sources are given (argument or EBG_REFERENCE_DIR)
+    and present, the reference oracle."""
+    ref = reference_dir or os.environ.get("EBG_REFERENCE_DIR")
     targets = ["port"]
-    if os.path.isdir(reference_dir):
+    if ref and os.path.isdir(ref):
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE, f"REF={reference_dir}", *targets], check=True,
+    subprocess.run(["make", "-C", HERE, *([f"REF={ref}"] if "ref" in targets else []), *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
+    if "ref" in targets:
+        with open(_SOURCE_NOTE, "w") as fh:
+            fh.write(os.path.abspath(ref) + "\n")
 
 
 def _ptr(a):
@@ -427,14 +462,24 @@ def ref_available() -> bool:
     return os.path.exists(ref_lib_path())
 
 
-def ref() -> _Ref:
-    global _ref_cache
-    if _ref_cache is None:
-        path = ref_lib_path()
+_ref_timing_cache = None
+
+
+def ref(timing: bool = False) -> _Ref:
+    """The reference oracle: the parity build, or with ``timing`` the build bench.py times (see
+    ref_lib_path); both are the unmodified reference behind the same extern "C" harness."""
+    global _ref_cache, _ref_timing_cache
+    cached = _ref_timing_cache if timing else _ref_cache
+    if cached is None:
+        path = ref_lib_path(timing)
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference sources exist")
-        _ref_cache = _Ref(path)
-    return _ref_cache
+        cached = _Ref(path)
+        if timing:
+            _ref_timing_cache = cached
+        else:
+            _ref_cache = cached
+    return cached
 
 
 def port() -> _Port:

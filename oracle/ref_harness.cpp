@@ -633,13 +633,18 @@ ref_scene_create(int64_t        ns,
     s->prims.emplace_back(std::make_shared<SphereSDF<double>>(Vec3d(sp[0], sp[1], sp[2]), sp[3]));
     bvs.emplace_back(Vec3d(sp[0] - sp[3], sp[1] - sp[3], sp[2] - sp[3]), Vec3d(sp[0] + sp[3], sp[1] + sp[3], sp[2] + sp[3]));
   }
+  // the meshes are independent objects: build them on all host threads, then add them in order
+  std::vector<std::shared_ptr<ImplicitFunction<double>>> built(size_t(nm < 0 ? 0 : nm));
+#pragma omp parallel for schedule(dynamic, 1)
   for (int64_t m = 0; m < nm; m++) {
     auto mesh = makeMesh(V + 3 * vOff[m], vCnt[m], F + 3 * fOff[m], fCnt[m]);
     std::shared_ptr<ImplicitFunction<double>> sdf = std::make_shared<TriSDF44>(mesh, BVH::Build::SAH, 4);
     const double* ps  = pose + 5 * m;
     sdf               = Rotate<double>(sdf, ps[0], size_t(ps[1]));
-    sdf               = Translate<double>(sdf, Vec3d(ps[2], ps[3], ps[4]));
-    s->prims.emplace_back(sdf);
+    built[size_t(m)]  = Translate<double>(sdf, Vec3d(ps[2], ps[3], ps[4]));
+  }
+  for (int64_t m = 0; m < nm; m++) {
+    s->prims.emplace_back(built[size_t(m)]);
     const double* b = bbox + 6 * m;
     bvs.emplace_back(Vec3d(b[0], b[1], b[2]), Vec3d(b[3], b[4], b[5]));
   }

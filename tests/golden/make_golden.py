@@ -1,6 +1,7 @@
 """Generates the committed golden fixtures of tests/golden/ from the reference itself.
 
-Run where the reference sources exist (they are read from REFERENCE, default /root/reference):
+Run where the reference sources exist (the directory is the first argument, or the
+EBG_REFERENCE_DIR environment variable):
 
     python tests/golden/make_golden.py [REFERENCE]
 
@@ -185,4 +186,7 @@ def main(reference: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EBG_REFERENCE_DIR")
+    if not ref_dir:
+        sys.exit("usage: make_golden.py REFERENCE_DIR (or set EBG_REFERENCE_DIR)")
+    main(ref_dir)

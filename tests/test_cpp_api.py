@@ -10,10 +10,12 @@ import pytest
 
 from conftest import ROOT
 
+import oracle
+
 EXAMPLE = os.path.join(ROOT, "ebgeometry_b200", "examples", "meshsdf_example.cpp")
 LIBDIR = os.path.join(ROOT, "ebgeometry_b200")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
-REFERENCE = "/root/reference"
+REFERENCE = oracle.reference_dir()
 
 
 def compile_example(out, extra=(), link=True):
@@ -27,7 +29,7 @@ def test_example_compiles_and_links(tmp_path):
     assert r.returncode == 0, r.stderr
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference sources not present on this host")
+@pytest.mark.skipif(REFERENCE is None, reason="reference sources not present on this host (EBG_REFERENCE_DIR)")
 def test_classes_derive_from_the_reference_interface(tmp_path):
     r = compile_example(str(tmp_path / "ex.o"), ["-DEBGEOMETRY_B200_WITH_REFERENCE", f"-I{REFERENCE}"], link=False)
     assert r.returncode == 0, r.stderr

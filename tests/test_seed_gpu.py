@@ -1,13 +1,15 @@
 """The learned pruning-radius model (no counterpart in the reference): gradients of the GPU
 backward kernels against the CPU restatement (oracle/seed_numpy.py), training quality, exactness of
-seeded queries (the radius only prunes), the fallback when a radius is wrong, checkpoints, what the
-trained model saves in traversal work, and the per-query radius hint (the exact distances as hint
-give the least work any radius can give)."""
+seeded queries (the model's radius only prunes: queries start from per-cell entry cuts of the tree),
+the traversal work the trained model must save, the fallback when a radius is wrong, the attach
+options (radius from the model, none or exact; anchors on or off) giving identical answers, a refit
+dropping the cuts, checkpoints, and the per-query radius hint (the exact distances as hint give the
+least work any radius can give)."""
 import numpy as np
 import pytest
 import torch
 
-from ebgeometry_b200 import SeedModel, TriMeshSDF
+from ebgeometry_b200 import EbgError, SeedModel, TriMeshSDF
 from ebgeometry_b200 import workloads as W
 from oracle import seed_numpy as SN
 
@@ -68,40 +70,84 @@ def test_training_quality(trained):
     assert np.isfinite(r["max_abs_err_far"])
 
 
+def _workload(n_grid=96, n_band=100000):
+    v, f = W.displaced_icosphere(5, 1)
+    return torch.from_numpy(np.concatenate([W.grid_points(n_grid, -1.25, 1.25), W.band_points(v, f, n_band, 4)])).cuda()
+
+
+def _packet_work(s):
+    """What a packet's warp executes, per packet: stack pops, interior nodes, oriented boxes and
+    triangle passes."""
+    pk = max(s["packets"], 1)
+    return {k: s[k] / pk for k in ("packet_pops", "packet_nodes", "packet_boxes", "packet_triangles")}
+
+
 def test_seeded_queries_are_exact_and_cheaper(trained):
     mesh, seed = trained
-    p = torch.from_numpy(np.concatenate([W.grid_points(96, -1.25, 1.25),
-                                         W.band_points(*W.displaced_icosphere(5, 1), 100000, 4)])).cuda()
+    p = _workload()
     d0, s0 = mesh.stats(p)
     d1, s1 = mesh.stats(p, seed=seed)
-    d0, d1 = d0.cpu().numpy(), d1.cpu().numpy()
-    err = np.abs(d0 - d1)
-    assert err.max() <= 1e-6 * mesh.diagonal
-    out = np.abs(d0) > 1e-4 * mesh.diagonal
-    assert np.all(np.sign(d0[out]) == np.sign(d1[out]))
-    assert np.mean(d0 == d1) > 0.999
-    # what the trained network gains over the plain traversal (printed; -s shows it): it must never
-    # cost work, and its radius must hold for almost every query
-    gain = {k: 1.0 - s1[k] / max(s0[k], 1) for k in ("nodes_visited", "leaves_visited", "triangles_tested")}
-    print("seed gain (fraction of traversal work saved):", gain, "fallbacks:", s1["seed_fallbacks"])
-    assert s1["nodes_visited"] <= 1.02 * s0["nodes_visited"], (s0, s1)
-    assert s1["triangles_tested"] <= 1.02 * s0["triangles_tested"], (s0, s1)
-    assert s1["seed_fallbacks"] < 0.02 * p.shape[0]
+    # the seeded traversal returns the plain traversal's answers, bit for bit
+    assert torch.equal(d0, d1)
+    w0, w1 = _packet_work(s0), _packet_work(s1)
+    print("packet work plain:", w0, "seeded:", w1, "cut packets:", s1["cut_packets"] / s1["packets"],
+          "fallbacks:", s1["seed_fallbacks"])
+    # what the trained model must save: most packets start from a cut, and the warps open far fewer
+    # interior nodes and test fewer boxes and triangles
+    assert s1["cut_packets"] >= 0.8 * s1["packets"]
+    assert w1["packet_nodes"] <= 0.6 * w0["packet_nodes"], (w0, w1)
+    assert w1["packet_boxes"] <= 0.9 * w0["packet_boxes"], (w0, w1)
+    assert w1["packet_triangles"] <= 0.95 * w0["packet_triangles"], (w0, w1)
+    assert s1["seed_fallbacks"] < 0.01 * p.shape[0]
 
 
 def test_wrong_radius_falls_back(trained):
     mesh, seed = trained
     bad = SeedModel.create(log2_table=12, base_resolution=4, max_resolution=32, lo=[-1.25] * 3, hi=[1.25] * 3)
     table, params = bad.get_params(16 * (1 << 12) * 2)
-    params[:] = 0.0  # predicts 0 everywhere: the radius is only the distance to the packet centroid
+    params[:] = 0.0  # predicts 0 everywhere: each cell's radius is only the cell's half-diagonal
     bad.set_params(params=params)
-    p = torch.from_numpy(W.uniform_points(20000, 5)).cuda()
-    d0 = mesh.signed_distance(p).cpu().numpy()
-    d1, st = mesh.stats(p, seed=bad)
-    d1 = d1.cpu().numpy()
-    assert np.abs(d0 - d1).max() <= 1e-6 * mesh.diagonal
-    assert np.mean(d0 == d1) > 0.999
-    assert st["seed_fallbacks"] > 10000  # most radii held no triangle and were traversed again
+    p = torch.from_numpy(W.grid_points(64, -1.25, 1.25)).cuda()  # packets compact enough to fit cells
+    d0 = mesh.signed_distance(p)
+    try:
+        mesh.attach_seed(bad, anchors=False)
+        d1, st = mesh.stats(p, seed=bad)
+        assert torch.equal(d0, d1)
+        assert st["cut_packets"] > 0
+        assert st["seed_fallbacks"] > 0  # radii that held no triangle: traversed again from the root
+    finally:
+        mesh.attach_seed(seed)
+
+
+def test_attach_options_give_identical_answers(trained):
+    mesh, seed = trained
+    p = _workload(48, 20000)
+    d0 = mesh.signed_distance(p)
+    try:
+        for mode in (0, 1, 2):
+            for anchors in (True, False):
+                rep = mesh.attach_seed(seed, cells_per_axis=24, max_entries=40, radius_mode=mode, anchors=anchors)
+                assert rep["cells"] == 24 ** 3 and rep["max_entries"] == 40
+                assert torch.equal(mesh.signed_distance(p, seed=seed), d0), (mode, anchors)
+    finally:
+        mesh.attach_seed(seed)
+
+
+def test_unattached_model_is_rejected_and_refit_drops_cuts():
+    v, f = W.displaced_icosphere(3, 2)
+    mesh = TriMeshSDF(v, f)
+    seed = SeedModel.train(mesh, num_samples=1 << 16, steps=50, batch=1 << 12, rng_seed=2, attach=False)
+    p = torch.from_numpy(W.uniform_points(5000, 3)).cuda()
+    with pytest.raises(EbgError):
+        mesh.signed_distance(p, seed=seed)
+    mesh.attach_seed(seed)
+    d = mesh.signed_distance(p, seed=seed)
+    assert torch.equal(d, mesh.signed_distance(p))
+    mesh.refit(v)  # the cuts were cut from the old boxes: a refit drops them
+    with pytest.raises(EbgError):
+        mesh.signed_distance(p, seed=seed)
+    mesh.attach_seed(seed)
+    assert torch.equal(mesh.signed_distance(p, seed=seed), d)
 
 
 def test_checkpoint_roundtrip(trained, tmp_path):
