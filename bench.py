@@ -697,14 +697,21 @@ def measure_knn(args, torch, dev, stream, cpu=True):
             ns = 200000
             for k in (1, 8):
                 t0 = time.perf_counter()
-                ri, rd = rc.knn(q[:ns], k, lex=False)
+                rc.knn(q[:ns], k, lex=False)
                 dt = time.perf_counter() - t0
-                gi, gd = cloud.knn(q[:ns], k)
                 res[f"k{k}"]["cpu_baseline"] = {
                     "value": ns / dt, "unit": UNIT, "cores": R.max_threads(), "kind": "reference",
                     "sample": f"first {ns} queries, reference PointCloudBVH<float> closestPoints (build {tb:.1f}s), "
                               "-O3 -march=sapphirerapids"}
-                res[f"k{k}"]["d2_equal_fraction"] = float(np.mean(gd == rd))
+            del rc
+            # parity against the reference's parity build (its float arithmetic without fused
+            # multiply-adds, which the timing build contracts)
+            rp = oracle.ref().cloud(pts)
+            for k in (1, 8):
+                ri, rd = rp.knn(q[:ns], k, lex=True)
+                gi, gd = cloud.knn(q[:ns], k)
+                res[f"k{k}"]["parity"] = {"queries": ns, "d2_equal_fraction": float(np.mean(gd == rd)),
+                                          "index_equal_fraction": float(np.mean(gi == ri))}
     return res
 
 

@@ -23,7 +23,7 @@ import numpy as np
 from . import _capi
 from ._capi import EbgError, check, lib
 
-__all__ = ["read_soup", "read_polygon_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PolygonMeshSDF",
+__all__ = ["sample_points", "read_soup", "read_polygon_soup", "TriMeshSDF", "MeshSDF", "FlatMeshSDF", "PolygonMeshSDF",
            "PolygonFlatMeshSDF", "polygon_normals", "PointCloudBVH", "PointCloudHashGrid",
            "BVHUnion", "SeedModel", "EbgError", "BUILD_SAH", "BUILD_MORTON", "version", "device_count"]
 
@@ -37,6 +37,14 @@ def version() -> str:
 
 def device_count() -> int:
     return int(lib.ebg_device_count())
+
+
+def sample_points(n: int, seed: int) -> np.ndarray:
+    """Random::samplePoints<double>(n, seed) (RandomImplem.hpp:27-44): the reference's seeded
+    points uniform in [0,1)^3, float64 (n,3)."""
+    out = np.empty((int(n), 3), np.float64)
+    check(lib.ebg_sample_points(int(n), C.c_uint64(int(seed)), _ptr(out)))
+    return out
 
 
 def read_soup(path):
@@ -803,8 +811,13 @@ class BVHUnion:
             if not (b.is_cuda and b.dtype == torch.float32 and b.is_contiguous()):
                 raise ValueError("batches must be contiguous float32 CUDA tensors of shape (n,3)")
             desc[i] = (b.data_ptr(), b.numel() // 3, o.data_ptr())
-        d = torch.from_numpy(desc).to(dev, non_blocking=False)
-        self._last_batches = d  # the descriptors must outlive the asynchronous call
+        # the descriptors live on the device and must outlive the asynchronous call; the same
+        # batches again reuse them (no host-to-device copy, so such a call can be graph-captured)
+        key = desc.tobytes()
+        if getattr(self, "_batch_key", None) != key:
+            self._batch_desc = torch.from_numpy(desc).to(dev, non_blocking=False)
+            self._batch_key = key
+        d = self._batch_desc
         opts = _capi.QueryOpts(0.0, 0 if sort else 1, 0 if fp64_band else 1, None, 0, 0, None)
         check(lib.ebg_scene_eval_batches(self._h, C.c_void_p(d.data_ptr()), len(batches), int(desc[:, 1].sum()),
                                          C.byref(opts), _stream_ptr(stream)))

@@ -83,6 +83,7 @@ SIGNATURES = {
     "ebg_last_error": (C.c_char_p, []),
     "ebg_version": (C.c_char_p, []),
     "ebg_device_count": (C.c_int, []),
+    "ebg_sample_points": (C.c_int, [_I64, C.c_uint64, _P]),
     "ebg_mesh_create": (C.c_int, [_P, _I64, _P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_mesh_create_with_normals": (C.c_int, [_P, _I64, _P, _I64, _P, _P, C.POINTER(BuildOpts),
                                                C.POINTER(_P)]),

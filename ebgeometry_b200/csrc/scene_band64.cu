@@ -11,7 +11,8 @@
 //   mesh instance:   TranslateIF(RotateIF(TriMeshSDF)) -- local = rot(p - t) with RotateIF's
 //                    per-axis formulas (TransformImplem.hpp:152-225) -- then the FP64 triangle test
 //                    over every triangle within |d32| + delta of the local point (band64.cuh), whose
-//                    winner is the mesh's exact value whenever the mesh can hold the minimum.
+//                    winner is the mesh's exact value whenever the mesh can hold the minimum (a
+//                    winner farther than that is left out: such a mesh cannot).
 // The union's value is the minimum over them (std::min, as the reference's evalLeaf).
 #include <cfloat>
 
@@ -116,7 +117,11 @@ __global__ void __launch_bounds__(128, 4) kSceneBand64(const SceneQueryArgs a, f
           if (err) {
             break;
           }
-          if (mbt >= 0) {
+          // The packet opens a leaf when any lane needs it and every lane tests its triangles, so a
+          // lane can end with a triangle outside its own radius.  Within mr is the mesh's exact
+          // value; beyond it the mesh cannot hold the minimum (its value is above d32 + delta, or
+          // below d32 - delta, which the minimum is not) and is left out.
+          if (mbt >= 0 && fabs(mb) <= double(mr)) {
             best = fmin(best, mb);
           }
         }

@@ -144,6 +144,11 @@ const char* ebg_last_error(void);
 const char* ebg_version(void);
 int         ebg_device_count(void);
 
+/* Random::samplePoints<double>(n, seed) (RandomImplem.hpp:27-44): the reference's seeded point sets
+ * (n points uniform in [0,1)^3, xyz interleaved into out_host), the same points as the reference
+ * compiled with GCC.  Host only. */
+ebg_status ebg_sample_points(int64_t n, uint64_t seed, double* out_host);
+
 /* ---- triangle meshes: TriMeshSDF (MeshDistanceFunctions.hpp:309-489) -------------------------
  *
  * ebg_mesh_create replaces TriMeshSDF(mesh, build, maxLeafGroups) after Soup::soupToDCEL

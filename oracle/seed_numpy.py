@@ -2,8 +2,9 @@
 
 CPU (numpy, FP64) restatement of the learned pruning-radius model of ebgeometry_b200/csrc/seed.cu:
 the 16-level hash-grid encoding and the 32-64-64-64-1 ReLU MLP, forward and backward, with the
-product's BF16 rounding points reproduced in the forward pass (table entries, encoding, weights and
-hidden activations are rounded to BF16) and everything else in FP64.  The model has no counterpart
+product's BF16 rounding points reproduced (forward: table entries, encoding, weights and hidden
+activations; backward: the layer deltas where they enter the weight- and input-gradient products as
+tensor-core operands) and everything else in FP64.  The model has no counterpart
 in the reference; this restatement is what the GPU gradients are checked against.
 """
 from __future__ import annotations
@@ -88,16 +89,18 @@ def loss_and_grads(p, d, table, params, lo, scale, res, dense, log2t, eps):
     g = np.zeros(NPARAM)
     g[W4:B4] = H3.T @ dy
     g[B4] = dy.sum()
+    # each delta is an FP32 matrix on the device, rounded to BF16 where it is an MMA operand; the
+    # bias gradients sum it unrounded
     dH3 = np.outer(dy, w4) * (H3 > 0)
-    g[W3:B3] = (dH3.T @ H2).ravel()
+    g[W3:B3] = (bf16(dH3).T @ H2).ravel()
     g[B3:W4] = dH3.sum(0)
-    dH2 = (dH3 @ w3) * (H2 > 0)
-    g[W2:B2] = (dH2.T @ H1).ravel()
+    dH2 = (bf16(dH3) @ w3) * (H2 > 0)
+    g[W2:B2] = (bf16(dH2).T @ H1).ravel()
     g[B2:W3] = dH2.sum(0)
-    dH1 = (dH2 @ w2) * (H1 > 0)
-    g[W1:B1] = (dH1.T @ Xb).ravel()
+    dH1 = (bf16(dH2) @ w2) * (H1 > 0)
+    g[W1:B1] = (bf16(dH1).T @ Xb).ravel()
     g[B1:W2] = dH1.sum(0)
-    dX = dH1 @ w1
+    dX = bf16(dH1) @ w1
     gt = np.zeros((LEVELS, T, 2))
     for l, (idx, w) in enumerate(cs):
         for f in range(2):

@@ -83,3 +83,15 @@ def test_workloads_deterministic():
     assert g.shape == (64, 3) and np.allclose(g[1] - g[0], [0.5, 0, 0])
     pc = W.point_cloud(1000, 2)
     assert pc.dtype == np.float32 and pc.min() >= 0 and pc.max() <= 1
+
+
+def test_sample_points_are_the_references():
+    """Random::samplePoints<double> (RandomImplem.hpp:27-44) through the library, against the
+    reference's own (oracle/_ref) for a few seeds and sizes."""
+    import oracle
+    from ebgeometry_b200 import sample_points
+    if not oracle.ref_available():
+        pytest.skip("reference oracle library not built (oracle/_ref)")
+    for n, seed in ((1, 0), (1000, 20260708), (4096, 99)):
+        assert np.array_equal(sample_points(n, seed), oracle.ref().sample_points(n, seed))
+    assert sample_points(0, 5).shape == (0, 3)

@@ -40,15 +40,20 @@ def test_gradients_match_cpu_oracle():
     scale = (1.0 / (hi - lo)).astype(np.float32).astype(np.float64)
     lref, gt_ref, gp_ref, _ = SN.loss_and_grads(pts.astype(np.float64), tgt.astype(np.float64), table, params,
                                                 lo.astype(np.float32).astype(np.float64), scale, res, dense, log2t, 0.05)
-    assert loss == pytest.approx(lref, rel=2e-2)
-    # BF16 operands in the backward products: agreement to ~1% of the gradient norm, per block
+    assert loss == pytest.approx(lref, rel=1e-3)
+    # The oracle rounds to BF16 where the kernels do (weights, activations, and the deltas that enter
+    # the gradient products as tensor-core operands), so what remains is FP32 accumulation order
+    # and the odd BF16 rounding that lands on the other side of a tie because the device's FP32
+    # input differs from the oracle's FP64 one in the last bits: 5e-3 of each block's norm.
     for name, a, b in (("W1", SN.W1, SN.B1), ("b1", SN.B1, SN.W2), ("W2", SN.W2, SN.B2), ("b2", SN.B2, SN.W3),
                        ("W3", SN.W3, SN.B3), ("b3", SN.B3, SN.W4), ("w4", SN.W4, SN.B4), ("b4", SN.B4, SN.NPARAM)):
         ref = gp_ref[a:b]
         rel = np.linalg.norm(gp[a:b] - ref) / max(np.linalg.norm(ref), 1e-12)
-        assert rel < 3e-2, (name, rel)
+        print(f"gradient block {name}: relative error {rel:.2e}")
+        assert rel < 5e-3, (name, rel)
     rel = np.linalg.norm(gt - gt_ref) / np.linalg.norm(gt_ref)
-    assert rel < 3e-2, ("table", rel)
+    print(f"gradient table: relative error {rel:.2e}")
+    assert rel < 5e-3, ("table", rel)
 
 
 @pytest.fixture(scope="module")
