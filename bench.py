@@ -678,12 +678,15 @@ def measure_knn(args, torch, dev, stream, cpu=True):
     qd = torch.from_numpy(q).to(dev)
     res = {"workload": f"{pts.shape[0]} points (half uniform, half in 64 anisotropic clusters), {q.shape[0]} uniform "
                        "queries; int32 indices", "unit": UNIT}
+    qh = torch.from_numpy(q).pin_memory().numpy()  # the caller's queries in pinned host memory
     for k in (1, 8):
         ms = device_timed(lambda: cloud.knn(qd, k), max(3, args.steps), 3, torch, dev, stream)
-        cloud.knn(q[:1000], k)
+        cloud.knn(qh[:1000], k)
+        reps = 3
         t0 = time.perf_counter()
-        cloud.knn(q, k)  # the host entry point: H2D, query, D2H (synchronous)
-        e2e_ms = (time.perf_counter() - t0) * 1e3
+        for _ in range(reps):
+            cloud.knn(qh, k)  # the host entry point: H2D, query, D2H (synchronous)
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / reps
         res[f"k{k}"] = {"value": q.shape[0] / (ms * 1e-3), "ms_per_step": ms,
                         "e2e": {"value": q.shape[0] / (e2e_ms * 1e-3), "ms_per_step": e2e_ms,
                                 "h2d_bytes_per_step": int(q.nbytes), "d2h_bytes_per_step": int(q.shape[0] * k * 8)}}

@@ -207,10 +207,8 @@ ebg_status ebg_cloud_create(const float* points_host, int64_t n, const ebg_build
   if (n >= int64_t(EBG_LEAF_BIT)) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-1 points");
   }
-  for (int64_t i = 0; i < 3 * n; i++) {
-    if (!std::isfinite(points_host[i])) {
-      return setError(EBG_ERR_INVALID, "non-finite point coordinate");
-    }
+  if (!allFinite(points_host, 3 * n)) {
+    return setError(EBG_ERR_INVALID, "non-finite point coordinate");
   }
   DeviceGuard guard;
   if (opts && opts->device >= 0 && cudaSetDevice(opts->device) != cudaSuccess) {
@@ -320,10 +318,8 @@ ebg_status ebg_cloud_knn_host(const ebg_cloud*      c,
   if (nq == 0) {
     return EBG_OK;
   }
-  for (int64_t i = 0; i < 3 * nq; i++) {
-    if (!std::isfinite(queries_host[i])) {
-      return setError(EBG_ERR_INVALID, "non-finite query coordinate");
-    }
+  if (!allFinite(queries_host, 3 * nq)) {
+    return setError(EBG_ERR_INVALID, "non-finite query coordinate");
   }
   DeviceGuard        guard;
   cudaSetDevice(c->device);

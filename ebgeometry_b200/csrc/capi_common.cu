@@ -1,4 +1,5 @@
 // Library-wide C ABI entry points (errors, version, devices).
+#include <cmath>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -16,6 +17,16 @@ ebg_status setError(ebg_status code, const std::string& msg)
 {
   g_lastError = msg;
   return code;
+}
+
+bool allFinite(const float* x, int64_t n)
+{
+  int64_t bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+  for (int64_t i = 0; i < n; i++) {
+    bad += std::isfinite(x[i]) ? 0 : 1;
+  }
+  return bad == 0;
 }
 
 void keepPoolMemory()

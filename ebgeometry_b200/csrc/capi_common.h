@@ -2,6 +2,7 @@
 #ifndef EBG_CAPI_COMMON_H
 #define EBG_CAPI_COMMON_H
 
+#include <cstdint>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -18,6 +19,9 @@ ebg_status setError(ebg_status code, const std::string& msg);
 // returns its memory at every synchronisation and the next call maps it again, which costs
 // milliseconds per call and varies from call to call.  Called by every create entry point.
 void keepPoolMemory();
+
+// True when every one of the n floats is finite (checked on all host threads).
+bool allFinite(const float* x, int64_t n);
 
 // Restores the caller's current CUDA device on scope exit (entry points switch to the handle's).
 struct DeviceGuard

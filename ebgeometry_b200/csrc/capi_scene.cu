@@ -119,13 +119,9 @@ ebg_status sceneQuery(const ebg_scene*      s,
     auto* iin  = static_cast<uint32_t*>(get(n * 4));
     size_t tb  = 0;
     if (batches) {
-      auto* kin  = static_cast<uint64_t*>(get(n * 8));
-      auto* kout = static_cast<uint64_t*>(get(n * 8));
-      int   bits = 30;
-      while ((int64_t(1) << (bits - 30)) < nb) {
-        bits++;
-      }
-      cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, iin, order, int(n), 0, bits, st);
+      auto* kin  = static_cast<uint32_t*>(get(n * 4));
+      auto* kout = static_cast<uint32_t*>(get(n * 4));
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, iin, order, int(n), 0, 30, st);
       void* tmp = get(tb);
       if (!ok) {
         release();
@@ -134,7 +130,7 @@ ebg_status sceneQuery(const ebg_scene*      s,
       a.batch_start = starts;
       if (launchSceneBatchStarts(batches, nb, starts, s->dStatus, n, st) != cudaSuccess ||
           launchSceneBatchKeys(a, kin, iin, st) != cudaSuccess ||
-          cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(n), 0, bits, st) != cudaSuccess) {
+          cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, iin, order, int(n), 0, 30, st) != cudaSuccess) {
         release();
         return setError(EBG_ERR_CUDA, std::string("scene batch ordering: ") + cudaGetErrorString(cudaGetLastError()));
       }
@@ -442,10 +438,8 @@ ebg_status ebg_scene_value_host(const ebg_scene*      s,
   if (n == 0) {
     return EBG_OK;
   }
-  for (int64_t i = 0; i < 3 * n; i++) {
-    if (!std::isfinite(points_host[i])) {
-      return setError(EBG_ERR_INVALID, "non-finite query coordinate");
-    }
+  if (!allFinite(points_host, 3 * n)) {
+    return setError(EBG_ERR_INVALID, "non-finite query coordinate");
   }
   DeviceGuard  guard;
   cudaSetDevice(s->device);

@@ -32,6 +32,17 @@ __device__ __forceinline__ float boxDist2(float lx, float ly, float lz, float hx
   return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
 
+// Squared distance between two axis-aligned boxes, every step rounded down (a lower bound of the
+// true distance).
+__device__ __forceinline__ float boxBoxDist2(float alx, float aly, float alz, float ahx, float ahy, float ahz, float blx,
+                                             float bly, float blz, float bhx, float bhy, float bhz)
+{
+  const float dx = fmaxf(0.f, fmaxf(__fsub_rd(blx, ahx), __fsub_rd(alx, bhx)));
+  const float dy = fmaxf(0.f, fmaxf(__fsub_rd(bly, ahy), __fsub_rd(aly, bhy)));
+  const float dz = fmaxf(0.f, fmaxf(__fsub_rd(blz, ahz), __fsub_rd(alz, bhz)));
+  return __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
+}
+
 __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
 
 // Quotients by a leaf's primitive count c (1..32) without integer division: 32 / c, and

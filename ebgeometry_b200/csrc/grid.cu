@@ -384,10 +384,8 @@ ebg_status ebg_grid_create(const float* points_host, int64_t n, double target_pe
   if (n > int64_t(INT32_MAX) - 1) {
     return setError(EBG_ERR_TOO_LARGE, "at most 2^31-2 points");
   }
-  for (int64_t i = 0; i < 3 * n; i++) {
-    if (!std::isfinite(points_host[i])) {
-      return setError(EBG_ERR_INVALID, "non-finite point coordinate");
-    }
+  if (!allFinite(points_host, 3 * n)) {
+    return setError(EBG_ERR_INVALID, "non-finite point coordinate");
   }
   DeviceGuard guard;
   if (device >= 0 && cudaSetDevice(device) != cudaSuccess) {

@@ -87,7 +87,9 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       const float r = __ldg(a.hint + id);
       best          = (r > 0.f && r < 1e18f) ? r * r * 1.000004f : FLT_MAX;
     }
-    int startSp = 0; // entries of a cell's cut copied onto the stack (0: start at the root)
+    int  startSp = 0;     // entries of a cell's cut on the stack
+    bool fromCut = false; // the packet starts from a cell's cut (else at the root)
+    int  loaded  = 0;     // entries the cut held
     if (SEED == 3) {
       // the packet's box over its valid lanes, and the cell holding the box's centre
       const float inf = __int_as_float(0x7f800000);
@@ -145,6 +147,39 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
               besttri = anc;
             }
           }
+          // Keep only the entries some lane can still need.  A lane needs an entry only if the
+          // entry's box is within its bound, and every lane lies in the packet's box, so an entry
+          // farther from that box than the largest bound is needed by none: 32 entries per step,
+          // compacted in place in their order (farthest first).
+          float bmax = best;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            bmax = fmaxf(bmax, __shfl_xor_sync(FULL, bmax, o));
+          }
+          int kept = 0;
+#pragma unroll 1
+          for (int base = 0; base < ne; base += 32) {
+            const int i    = base + lane;
+            float4    eA   = make_float4(0.f, 0.f, 0.f, 0.f), eB = eA;
+            bool      keep = false;
+            if (i < ne) {
+              eA   = stk[2 * i];
+              eB   = stk[2 * i + 1];
+              keep = boxBoxDist2(eA.x, eA.y, eA.z, eB.x, eB.y, eB.z, mnx, mny, mnz, mxx, mxy, mxz) <= bmax;
+            }
+            const unsigned km = __ballot_sync(FULL, keep);
+            __syncwarp(); // every entry of this step is read before any is overwritten
+            if (keep) {
+              const int r    = kept + __popc(km & ((1u << lane) - 1u));
+              stk[2 * r]     = eA;
+              stk[2 * r + 1] = eB;
+            }
+            kept += __popc(km);
+            __syncwarp();
+          }
+          startSp = kept;
+          fromCut = true;
+          loaded  = ne;
         }
       }
     }
@@ -166,7 +201,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         }
       }
       TraversalCounters tc;
-      if (SEED == 3 && pass == 0 && startSp > 0) {
+      if (SEED == 3 && pass == 0 && fromCut) {
         traverseFrom<STATS, STACK>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc);
       }
       else {
@@ -239,9 +274,9 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         atomicAdd(a.stats + 9, (unsigned long long)pTri);
         atomicAdd(a.stats + 11, (unsigned long long)pBox);
         atomicAdd(a.stats + 14, (unsigned long long)pRecs);
-        if (startSp > 0) {
+        if (fromCut) {
           atomicAdd(a.stats + 12, 1ull);
-          atomicAdd(a.stats + 13, (unsigned long long)startSp);
+          atomicAdd(a.stats + 13, (unsigned long long)loaded);
         }
       }
     }

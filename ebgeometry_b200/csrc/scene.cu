@@ -174,7 +174,10 @@ __global__ void __launch_bounds__(128) kSceneValue(const SceneQueryArgs a)
 
 } // namespace
 
-__global__ void kSceneBatchKeys(const SceneQueryArgs a, uint64_t* __restrict__ keys, uint32_t* __restrict__ ids)
+// Sort keys of a batched call: the 30-bit Morton code of each point of every batch, so that the
+// points of all batches are ordered together (batches that each cover the whole scene would
+// otherwise give packets of points far apart).
+__global__ void kSceneBatchKeys(const SceneQueryArgs a, uint32_t* __restrict__ keys, uint32_t* __restrict__ ids)
 {
   const SceneView& v = a.scene;
   if (!batchesValid(a)) {
@@ -183,23 +186,11 @@ __global__ void kSceneBatchKeys(const SceneQueryArgs a, uint64_t* __restrict__ k
   for (int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < a.n; g += int64_t(gridDim.x) * blockDim.x) {
     float*       outp = nullptr;
     const float* p    = scenePoint(a, uint32_t(g), &outp);
-    // the batch index (the same binary search as scenePoint) above the point's Morton code
-    int lo = 0, hi = a.num_batches - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a.batch_start[mid] <= g) {
-        lo = mid;
-      }
-      else {
-        hi = mid - 1;
-      }
-    }
-    const float fx = fminf(fmaxf((p[0] - v.morton_lo[0]) * v.morton_scale[0], 0.f), 1023.f);
-    const float fy = fminf(fmaxf((p[1] - v.morton_lo[1]) * v.morton_scale[1], 0.f), 1023.f);
-    const float fz = fminf(fmaxf((p[2] - v.morton_lo[2]) * v.morton_scale[2], 0.f), 1023.f);
-    const uint32_t m = (spread10(uint32_t(fx)) << 2) | (spread10(uint32_t(fy)) << 1) | spread10(uint32_t(fz));
-    keys[g]          = (uint64_t(lo) << 30) | uint64_t(m);
-    ids[g]           = uint32_t(g);
+    const float  fx   = fminf(fmaxf((p[0] - v.morton_lo[0]) * v.morton_scale[0], 0.f), 1023.f);
+    const float  fy   = fminf(fmaxf((p[1] - v.morton_lo[1]) * v.morton_scale[1], 0.f), 1023.f);
+    const float  fz   = fminf(fmaxf((p[2] - v.morton_lo[2]) * v.morton_scale[2], 0.f), 1023.f);
+    keys[g] = (spread10(uint32_t(fx)) << 2) | (spread10(uint32_t(fy)) << 1) | spread10(uint32_t(fz));
+    ids[g]  = uint32_t(g);
   }
 }
 
@@ -226,7 +217,7 @@ __global__ void kSceneBatchStarts(const SceneBatch* __restrict__ b, int32_t nb, 
 
 int sceneOuterDepth() { return OUTER_DEPTH; }
 
-cudaError_t launchSceneBatchKeys(const SceneQueryArgs& a, uint64_t* keys, uint32_t* ids, cudaStream_t s)
+cudaError_t launchSceneBatchKeys(const SceneQueryArgs& a, uint32_t* keys, uint32_t* ids, cudaStream_t s)
 {
   int64_t blocks = (a.n + 255) / 256;
   blocks         = blocks < 4096 ? blocks : 4096;

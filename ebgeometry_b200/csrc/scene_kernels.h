@@ -98,8 +98,9 @@ cudaError_t launchSceneValue(const SceneQueryArgs& a, int numSms, cudaStream_t s
 // FP64 re-evaluation of the band list (reads band_count on the device); delta bounds the FP32
 // error of the union's value.
 cudaError_t launchSceneBand64(const SceneQueryArgs& a, float delta, int numSms, cudaStream_t s);
-// Sort keys of a batched call: (batch << 30) | 30-bit Morton code of the point, and the identity.
-cudaError_t launchSceneBatchKeys(const SceneQueryArgs& a, uint64_t* keys, uint32_t* ids, cudaStream_t s);
+// Sort keys of a batched call: the 30-bit Morton code of every point of every batch, and the
+// identity.
+cudaError_t launchSceneBatchKeys(const SceneQueryArgs& a, uint32_t* keys, uint32_t* ids, cudaStream_t s);
 // batch_start[b] = sum of the first b batches' n, batch_start[nb] = the total (one small launch).
 cudaError_t launchSceneBatchStarts(const SceneBatch* batches, int32_t nb, int64_t* start, int* status,
                                    int64_t expectTotal, cudaStream_t s);

@@ -121,9 +121,8 @@ __device__ void encodeBackward(const SeedView& v, float px, float py, float pz, 
       const int   dx = k & 1, dy = (k >> 1) & 1, dz = k >> 2;
       const float w  = (dx ? c.fx : 1.f - c.fx) * (dy ? c.fy : 1.f - c.fy) * (dz ? c.fz : 1.f - c.fz);
       const uint32_t idx = gridIndex(v, l, c.ix + dx, c.iy + dy, c.iz + dz);
-      float*         gp  = gradTable + (size_t(l) * T + idx) * 2;
-      atomicAdd(gp, w * g0);
-      atomicAdd(gp + 1, w * g1);
+      // both features of the entry in one vector atomic (global memory, sm_90 and later)
+      atomicAdd(reinterpret_cast<float2*>(gradTable + (size_t(l) * T + idx) * 2), make_float2(w * g0, w * g1));
     }
   }
 }

@@ -39,16 +39,6 @@ __global__ void kCellRadius(const float* __restrict__ value, int64_t cells, int 
   }
 }
 
-// Squared distance between two axis-aligned boxes, rounded down (a lower bound of the true one).
-__device__ __forceinline__ float boxBoxDist2(float alx, float aly, float alz, float ahx, float ahy, float ahz, float blx,
-                                             float bly, float blz, float bhx, float bhy, float bhz)
-{
-  const float dx = fmaxf(0.f, fmaxf(__fsub_rd(blx, ahx), __fsub_rd(alx, bhx)));
-  const float dy = fmaxf(0.f, fmaxf(__fsub_rd(bly, ahy), __fsub_rd(aly, bhy)));
-  const float dz = fmaxf(0.f, fmaxf(__fsub_rd(blz, ahz), __fsub_rd(alz, bhz)));
-  return __fadd_rd(__fadd_rd(__fmul_rd(dx, dx), __fmul_rd(dy, dy)), __fmul_rd(dz, dz));
-}
-
 // One warp per cell.  The cut lives in shared memory as up to CUT_MAX_ENTRIES slots (entry, key =
 // lower bound of the squared distance from the cell centre, expandable flag); each round the warp
 // splits the expandable slot of least key into its children within R_C of the grown cell, or marks

@@ -559,9 +559,9 @@ typedef struct ebg_batch
 /* Many query batches of uneven length in one call (the reference has no batch API; its callers loop
  * over value(point)): batches_dev is a DEVICE array of num_batches descriptors whose n add up to
  * total_points (a mismatch or a negative n computes nothing and is reported by the next status
- * check as EBG_ERR_TRAVERSAL).  The points of all batches are ordered together along a Morton curve
- * (batch index above the curve's bits) and served by one persistent launch with a device work
- * queue, then the FP64 near-surface pass, as ebg_scene_value.  Only stream-ordered work, so the call
+ * check as EBG_ERR_TRAVERSAL).  The points of all batches are ordered together along one Morton
+ * curve and served by one persistent launch with a device work queue, then the FP64 near-surface
+ * pass, as ebg_scene_value.  Only stream-ordered work, so the call
  * can be captured in a CUDA graph. */
 ebg_status ebg_scene_eval_batches(const ebg_scene*      scene,
                                   const ebg_batch*      batches_dev,
