@@ -177,12 +177,13 @@ class TriMeshSDF:
 
     @staticmethod
     def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None, occupancy=None,
-              queue_chunk=None):
+              queue_chunk=None, top_nodes=None):
         return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
                                seed.handle if seed is not None else None,
                                int(warps_per_block or 0), int(occupancy or 0),
                                C.pointer(timings) if timings is not None else None,
-                               radius_hint.data_ptr() if radius_hint is not None else None, int(queue_chunk or 0))
+                               radius_hint.data_ptr() if radius_hint is not None else None, int(queue_chunk or 0),
+                               int(top_nodes or 0))
 
     # --- ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance -----------------
     def value(self, point) -> float:
@@ -197,15 +198,18 @@ class TriMeshSDF:
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
                         fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None,
-                        radius_hint=None, occupancy=None, queue_chunk=None):
+                        radius_hint=None, occupancy=None, queue_chunk=None, top_nodes=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  Float64 points (numpy or CUDA) take the FP64 entry points: every
         query is re-evaluated in FP64 and the distances come back as float64.  ``timings``: an ``_capi.PhaseTimings`` to fill with per-phase device
         times (the call then synchronises).  ``seed``: a trained :class:`SeedModel` whose predicted
         radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
-        float32 tensor of per-point upper bounds on |d| that seed the bound the same way."""
-        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy, queue_chunk)
+        float32 tensor of per-point upper bounds on |d| that seed the bound the same way.
+        ``top_nodes``: plain queries read the tree's first ``top_nodes`` nodes from a copy in each
+        block's shared memory (ebg_query_opts.top_nodes; same results)."""
+        opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy, queue_chunk,
+                          top_nodes)
         if isinstance(points, np.ndarray) and points.dtype == np.float64:
             p = np.ascontiguousarray(points).reshape(-1, 3)
             n = p.shape[0]

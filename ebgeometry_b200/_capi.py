@@ -25,7 +25,8 @@ class PhaseTimings(C.Structure):
 class QueryOpts(C.Structure):
     _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
                 ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("occupancy", C.c_int32),
-                ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p), ("queue_chunk", C.c_int32)]
+                ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p), ("queue_chunk", C.c_int32),
+                ("top_nodes", C.c_int32)]
 
 
 class SeedOpts(C.Structure):

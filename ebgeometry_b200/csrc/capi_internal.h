@@ -77,6 +77,20 @@ namespace ebg {
 // Frees a mesh's entry cuts (if any) and forgets the model they came from.
 void dropCells(ebg_mesh* m);
 
+// Nodes of the tree's top levels that each block of the FP32 traversal copies into shared memory
+// (ebg_query_opts.top_nodes, at most MAX_TOP_NODES and the tree's node count): plain queries
+// descend through them from the root; a seeded query starts below them and copies none.
+constexpr int64_t MAX_TOP_NODES = 512;
+inline uint32_t   topNodesFor(const ebg_mesh* m, const ebg_query_opts* opts, bool seeded)
+{
+  if (seeded || opts == nullptr || opts->top_nodes <= 0) {
+    return 0u;
+  }
+  int64_t t = opts->top_nodes < MAX_TOP_NODES ? opts->top_nodes : MAX_TOP_NODES;
+  t         = t < m->info.num_nodes ? t : m->info.num_nodes;
+  return uint32_t(t);
+}
+
 // The mesh query pipeline (ordering, optional seed inference, FP32 traversal, FP64 band pass) on
 // device buffers, asynchronous on s.  With pts64/out64 (the caller's FP64 points, of which pts is
 // the FP32 rounding, and an FP64 result array) every query is re-evaluated in FP64, with the

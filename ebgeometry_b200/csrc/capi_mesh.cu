@@ -612,6 +612,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   if (seed) {
     a.cells = m->cellsView;
   }
+  a.top_nodes = topNodesFor(m, opts, seed != nullptr);
   if (launchMeshSdf32(a, wpb, m->numSms, s, occ) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
   }

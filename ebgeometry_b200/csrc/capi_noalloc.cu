@@ -195,6 +195,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
   if (seed) {
     a.cells = m->cellsView; // the attached model's entry cuts live with the mesh
   }
+  a.top_nodes = topNodesFor(m, opts, seed != nullptr);
   if (launchMeshSdf32(a, wpb, m->numSms, s, occ) != cudaSuccess) {
     return cudaFailed("traversal launch");
   }

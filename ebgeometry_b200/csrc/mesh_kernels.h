@@ -35,6 +35,8 @@ struct MeshQueryArgs
   unsigned long long* stats;     // 15 counters (nullable): 6 per query, 6 per packet, 2 of the cuts,
                                  // [14] triangle records of the leaves the warps opened
   SeedCellsView      cells;      // per-cell entry cuts (used when cells.count is non-null)
+  uint32_t           top_nodes;  // nodes [0, top_nodes) and their oriented boxes are read from a copy
+                                 // in each block's shared memory (0: none)
 };
 
 // Morton keys of the query points (30 bits) and the identity permutation.

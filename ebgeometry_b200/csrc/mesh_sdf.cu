@@ -45,7 +45,8 @@ struct Bounds
   static constexpr int blocks  = OCC == 0 ? 1 : (OCC == 1 ? 8 : (OCC == 2 ? 10 : 12));
 };
 
-template <bool STATS, int SEED, int OCC>
+// TOP: each block copies the tree's first a.top_nodes nodes into shared memory (plain queries only).
+template <bool STATS, int SEED, int OCC, bool TOP = false>
 __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMeshSdf32(const MeshQueryArgs a)
 {
   extern __shared__ float4 smem[];
@@ -55,6 +56,21 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
   float4*       lpts = stk + 2 * STACK; // the warp's 32 spread-leaf points
   const EbgMeshView& m = a.mesh;
   const uint64_t numPackets = (uint64_t(a.n) + 31) / 32;
+
+  // the block's copy of the tree's first top_nodes nodes (the device build numbers nodes level by
+  // level, so these are the top levels) and their oriented boxes, after the warps' stacks
+  const uint32_t topN = TOP ? a.top_nodes : 0u;
+  float4*        top  = smem + (blockDim.x >> 5) * (2 * STACK + 32);
+  if constexpr (TOP) {
+    const float4* gn = reinterpret_cast<const float4*>(m.nodes);
+    const float4* go = reinterpret_cast<const float4*>(m.node_obb);
+    for (uint32_t i = threadIdx.x; i < topN * (TOP_NODE_BYTES / 16); i += blockDim.x) {
+      const uint32_t nI = i / (TOP_NODE_BYTES / 16), w = i - nI * (TOP_NODE_BYTES / 16);
+      top[i] = w < 8 ? __ldg(gn + 8 * nI + w) : __ldg(go + 4 * nI + (w - 8));
+    }
+    __syncthreads();
+  }
+  const uint32_t topS = uint32_t(__cvta_generic_to_shared(top));
 
   // packets come from the work counter `chunk` at a time (the queue chunk the autotuner picks)
   const unsigned long long chunk = a.chunk > 1 ? (unsigned long long)a.chunk : 1ull;
@@ -202,10 +218,10 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       }
       TraversalCounters tc;
       if (SEED == 3 && pass == 0 && fromCut) {
-        traverseFrom<STATS, STACK>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc);
+        traverseFrom<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc, topS, topN);
       }
       else {
-        traverseMesh<STATS, STACK>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc);
+        traverseMesh<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc, topS, topN);
       }
       cNode += tc.node;
       cLeaf += tc.leaf;
@@ -300,32 +316,42 @@ __global__ void kQueryKeys(const float* __restrict__ pts, int64_t n, float lx, f
   ids[i]  = uint32_t(i);
 }
 
-template <bool STATS, int SEED, int OCC>
+template <bool STATS, int SEED, int OCC, bool TOP>
 cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
   if (OCC != 0 && wpb > 4) {
     wpb = 4;
   }
   const int    threads = 32 * wpb;
-  const size_t smem    = size_t(wpb) * (2 * (SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH) + 32) * sizeof(float4);
-  // resident blocks per SM for each block size, looked up once (the query path then issues no
-  // runtime calls besides its launches, so it can be captured in a CUDA graph)
-  static int cache[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  int        perSm    = cache[wpb];
+  const size_t smem    = size_t(wpb) * (2 * (SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH) + 32) * sizeof(float4) +
+                      (TOP ? size_t(a.top_nodes) * TOP_NODE_BYTES : 0);
+  // resident blocks per SM for each block size and shared-memory size, looked up once (the query
+  // path then issues no runtime calls besides its launches, so it can be captured in a CUDA graph)
+  static int    cache[9]     = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  static size_t cacheMem[9]  = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int           perSm        = cacheMem[wpb] == smem ? cache[wpb] : 0;
   if (perSm == 0) {
+    if (smem > 48 * 1024) {
+      const cudaError_t e =
+        cudaFuncSetAttribute(kMeshSdf32<STATS, SEED, OCC, TOP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+      if (e != cudaSuccess) {
+        return e;
+      }
+    }
     const cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC>, threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC, TOP>, threads, smem);
     if (e != cudaSuccess) {
       return e;
     }
-    cache[wpb] = perSm;
+    cache[wpb]    = perSm;
+    cacheMem[wpb] = smem;
   }
   perSm               = perSm < 1 ? 1 : perSm;
   const int64_t need  = ((int64_t(a.n) + 31) / 32 + wpb - 1) / wpb;
   int64_t       grid  = int64_t(numSms) * perSm;
   grid                = grid < need ? grid : need;
   grid                = grid < 1 ? 1 : grid;
-  kMeshSdf32<STATS, SEED, OCC><<<unsigned(grid), threads, smem, s>>>(a);
+  kMeshSdf32<STATS, SEED, OCC, TOP><<<unsigned(grid), threads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -343,7 +369,12 @@ void launchQueryKeys(const float* points, int64_t n, const float* lo, const floa
 template <int SEED, int OCC>
 cudaError_t launchStats(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
-  return a.stats != nullptr ? launchOne<true, SEED, OCC>(a, wpb, numSms, s) : launchOne<false, SEED, OCC>(a, wpb, numSms, s);
+  if (SEED == 0 && a.top_nodes > 0) {
+    return a.stats != nullptr ? launchOne<true, SEED, OCC, SEED == 0>(a, wpb, numSms, s)
+                              : launchOne<false, SEED, OCC, SEED == 0>(a, wpb, numSms, s);
+  }
+  return a.stats != nullptr ? launchOne<true, SEED, OCC, false>(a, wpb, numSms, s)
+                            : launchOne<false, SEED, OCC, false>(a, wpb, numSms, s);
 }
 
 template <int OCC>

@@ -140,17 +140,38 @@ struct TraversalCounters
   uint32_t precs = 0;                                             // triangle records of its opened leaves
 };
 
+// 16- and 4-byte loads from a shared-memory address (the block's copy of the tree's top nodes).
+__device__ __forceinline__ float4 lds4(uint32_t addr)
+{
+  float4 v;
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+  return v;
+}
+
+__device__ __forceinline__ float lds1(uint32_t addr)
+{
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+
+// Bytes per node in the shared-memory copy of the top of the tree: the 128-byte node line, then
+// its 64-byte oriented box.
+constexpr uint32_t TOP_NODE_BYTES = 192;
+
 // Packet traversal of mesh m from the `sp` entries already on the warp's stack (the top entry is
 // popped first): each lane's best squared distance `best` (its pruning bound, already seeded or
 // FLT_MAX) and winning triangle `besttri` (leaf order) are updated.  Children are ordered by their
 // smallest distance over the packet's lanes.  `stk` is this warp's stack region (2 float4 per entry,
 // STACK entries); `pts` is this warp's 32-entry scratch for the points of the lanes a leaf is spread
-// over; `iters` counts loop trips against MAX_ITERS; `err` receives ST_* bits.  All 32 lanes must
-// call it together.
-template <bool STATS, int STACK>
+// over; `iters` counts loop trips against MAX_ITERS; `err` receives ST_* bits.  With TOP, nodes
+// with index below `topN` are read from the block's shared-memory copy at shared address `topS`
+// (TOP_NODE_BYTES per node).  All 32 lanes must call it together.
+template <bool STATS, int STACK, bool TOP = false>
 __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, float py, float pz, float& best,
                                              int& besttri, float4* stk, float4* pts, int sp, uint32_t& iters,
-                                             int& err, TraversalCounters& cnt_)
+                                             int& err, TraversalCounters& cnt_, uint32_t topS = 0,
+                                             uint32_t topN = 0)
 {
   const int lane = threadIdx.x & 31;
       // a finite bound keeps empty child slots (infinite box distance) off the stack
@@ -266,15 +287,30 @@ __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, flo
         }
         else {
           // the node's loads go out first; the oriented-box test below overlaps their latency
-          const float4* nd = reinterpret_cast<const float4*>(m.nodes + ref);
-          const float4  lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
-          const float4  hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+          const float4*  nd    = reinterpret_cast<const float4*>(m.nodes + ref);
+          const bool     inTop = TOP && ref < topN; // warp-uniform: the node's copy in shared memory
+          const uint32_t ts    = topS + ref * TOP_NODE_BYTES;
+          float4         lx, ly, lz, hx, hy, hz;
+          if (inTop) {
+            lx = lds4(ts), ly = lds4(ts + 16), lz = lds4(ts + 32);
+            hx = lds4(ts + 48), hy = lds4(ts + 64), hz = lds4(ts + 80);
+          }
+          else {
+            lx = __ldg(nd), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+            hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5);
+          }
           // lanes for which the node's own oriented box (all triangles below it) is within bound
           bool needN = need;
           if (cntw & EBG_NODE_HAS_OBB) {
-            const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
-            const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2), o3 = __ldg(ob + 3);
-            needN            = need && obbDist2(o0, o1, o2, o3, px, py, pz) <= best;
+            float4 o0, o1, o2, o3;
+            if (inTop) {
+              o0 = lds4(ts + 128), o1 = lds4(ts + 144), o2 = lds4(ts + 160), o3 = lds4(ts + 176);
+            }
+            else {
+              const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
+              o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2), o3 = __ldg(ob + 3);
+            }
+            needN = need && obbDist2(o0, o1, o2, o3, px, py, pz) <= best;
             if (STATS) {
               cnt_.box += need;
               cnt_.pbox++;
@@ -323,10 +359,17 @@ __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, flo
               for (int j = 0; j < 4; j++) {
                 rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
               }
-              const float* nf = reinterpret_cast<const float*>(nd) + lane;
-              float4*      e  = stk + 2 * (sp + rank);
-              e[0]            = make_float4(__ldg(nf), __ldg(nf + 4), __ldg(nf + 8), __ldg(nf + 24));
-              e[1]            = make_float4(__ldg(nf + 12), __ldg(nf + 16), __ldg(nf + 20), __ldg(nf + 28));
+              float4* e = stk + 2 * (sp + rank);
+              if (inTop) {
+                const uint32_t nf = ts + 4 * lane;
+                e[0] = make_float4(lds1(nf), lds1(nf + 16), lds1(nf + 32), lds1(nf + 96));
+                e[1] = make_float4(lds1(nf + 48), lds1(nf + 64), lds1(nf + 80), lds1(nf + 112));
+              }
+              else {
+                const float* nf = reinterpret_cast<const float*>(nd) + lane;
+                e[0]            = make_float4(__ldg(nf), __ldg(nf + 4), __ldg(nf + 8), __ldg(nf + 24));
+                e[1]            = make_float4(__ldg(nf + 12), __ldg(nf + 16), __ldg(nf + 20), __ldg(nf + 28));
+              }
             }
           }
           sp += np;
@@ -339,17 +382,17 @@ __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, flo
 }
 
 // One packet traversal from the root of mesh m (see traverseFrom).
-template <bool STATS, int STACK = EBG_STACK_DEPTH>
+template <bool STATS, int STACK = EBG_STACK_DEPTH, bool TOP = false>
 __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
                                              int& besttri, float4* stk, float4* pts, uint32_t& iters, int& err,
-                                             TraversalCounters& cnt_)
+                                             TraversalCounters& cnt_, uint32_t topS = 0, uint32_t topN = 0)
 {
   if ((threadIdx.x & 31) == 0) {
     stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
     stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
   }
   __syncwarp();
-  traverseFrom<STATS, STACK>(m, px, py, pz, best, besttri, stk, pts, 1, iters, err, cnt_);
+  traverseFrom<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, pts, 1, iters, err, cnt_, topS, topN);
 }
 
 } // namespace ebg

@@ -102,6 +102,13 @@ typedef struct ebg_query_opts
   int32_t            queue_chunk;     /* packets of 32 queries a warp takes from the device work
                                          queue at a time (mesh and union queries); 0 = tuned
                                          default (1) */
+  int32_t            top_nodes;       /* plain mesh queries: each block of the traversal copies the
+                                         tree's first top_nodes nodes (the device build numbers them
+                                         level by level: 21 = the root and two levels) with their
+                                         oriented boxes into shared memory and reads them there;
+                                         at most 512; 0 = none (the default, and the faster on the
+                                         level-8 workload).  Seeded queries start below the top
+                                         levels and ignore it. */
 } ebg_query_opts;
 
 /* Mesh summary. */

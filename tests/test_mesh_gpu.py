@@ -237,3 +237,25 @@ def test_ramped_host_call_matches_device_path():
     d_host, tri_h = m.signed_distance(p, closest_tri=np.empty(n, np.int32))
     assert np.array_equal(d_host, d_dev.cpu().numpy())
     assert np.array_equal(tri_h, tri_d.cpu().numpy())
+
+
+@pytest.mark.parametrize("on_device", [True, False])
+def test_top_nodes_in_shared_memory_change_nothing(ref, on_device):
+    """Plain queries that read the tree's top nodes from each block's shared-memory copy
+    (ebg_query_opts.top_nodes) give the results and closest triangles of the default path, for
+    the level-ordered device build and the host build, up to more nodes than the tree has."""
+    v, f = W.displaced_icosphere(6, 51)
+    m = TriMeshSDF(v, f, build="Morton", on_device=on_device)
+    p = np.concatenate([W.uniform_points(300000, 52), W.band_points(v, f, 50000, 53)])
+    pd = torch.from_numpy(p).cuda()
+    tri0 = torch.empty(p.shape[0], dtype=torch.int32, device="cuda")
+    d0, _ = m.signed_distance(pd, closest_tri=tri0)
+    for top in (1, 21, 85, 512, 100000):
+        tri = torch.empty_like(tri0)
+        d, _ = m.signed_distance(pd, closest_tri=tri, top_nodes=top)
+        torch.cuda.synchronize()
+        m.check_status()
+        assert torch.equal(d, d0), top
+        assert torch.equal(tri, tri0), top
+    d_ref = ref.mesh(v, f, kind=0, build=1, max_leaf_groups=4).sdf(p[:20000].astype(np.float64))
+    check_parity(d0[:20000].cpu().numpy(), d_ref, m.diagonal, "L6 top nodes")

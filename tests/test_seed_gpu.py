@@ -92,8 +92,10 @@ def test_seeded_queries_are_exact_and_cheaper(trained):
     p = _workload()
     d0, s0 = mesh.stats(p)
     d1, s1 = mesh.stats(p, seed=seed)
-    # the seeded traversal returns the plain traversal's answers, bit for bit
+    # the seeded traversal returns the plain traversal's answers, bit for bit (also when the plain
+    # path's option of a shared-memory top tree is passed, which seeded packets do not use)
     assert torch.equal(d0, d1)
+    assert torch.equal(mesh.signed_distance(p, seed=seed, top_nodes=21), d0)
     w0, w1 = _packet_work(s0), _packet_work(s1)
     print("packet work plain:", w0, "seeded:", w1, "cut packets:", s1["cut_packets"] / s1["packets"],
           "fallbacks:", s1["seed_fallbacks"])
