@@ -15,6 +15,7 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr int ST_STACK = 1;  // traversal stack would overflow (never for trees the builder accepts)
 constexpr int ST_ITERS = 2;  // iteration cap reached
 constexpr int ST_INPUT = 4;  // a query coordinate was NaN or infinite (its result is meaningless)
+constexpr int ST_COPY  = 8;  // an asynchronous copy did not signal completion within its wait limit
 
 // Iteration cap per packet traversal: far above any real traversal (a packet visits at most
 // every node and leaf once per pass), so hitting it means corrupt input; the kernel then stops,

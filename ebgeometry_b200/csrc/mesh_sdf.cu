@@ -34,6 +34,36 @@ namespace ebg {
 
 namespace {
 
+// Polls of the wait for a cut's bulk copy before the warp gives up: after the first 64 each
+// poll sleeps about 128 ns, so the wait ends within about a tenth of a second, far beyond the
+// microseconds a few kilobytes take.
+constexpr uint32_t COPY_WAIT_POLLS = 1u << 20;
+
+// True once the mbarrier at shared address `bar` has completed the phase with parity `phase`
+// (a non-blocking test).
+__device__ __forceinline__ bool mbarDone(uint32_t bar, uint32_t phase)
+{
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok)
+               : "r"(bar), "r"(phase)
+               : "memory");
+  return ok != 0;
+}
+
+// Every lane of the warp waits until the phase completed, at most COPY_WAIT_POLLS polls each.
+__device__ __forceinline__ bool mbarWaitWarp(uint32_t bar, uint32_t phase)
+{
+  bool done = mbarDone(bar, phase);
+  for (uint32_t t = 1; t < COPY_WAIT_POLLS && !done; t++) {
+    if (t >= 64) {
+      __nanosleep(128);
+    }
+    done = mbarDone(bar, phase);
+  }
+  return __all_sync(FULL, done);
+}
+
 // SEED: 0 plain, 2 per-query radius hint, 3 per-cell entry cuts and anchors of an attached model
 // (cells_kernels.h)
 // OCC selects the register budget: 0 = 256-thread blocks, compiler's choice; 1..3 = 128-thread
@@ -71,6 +101,19 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
     __syncthreads();
   }
   const uint32_t topS = uint32_t(__cvta_generic_to_shared(top));
+
+  // seeded packets bring their cell's cut onto the stack with one bulk copy, tracked by the warp's
+  // mbarrier (after the stacks and the top nodes' copy); `phase` is the parity of its next phase
+  uint32_t bar = 0, phase = 0;
+  if constexpr (SEED == 3) {
+    uint64_t* bars = reinterpret_cast<uint64_t*>(top + (TOP ? topN * (TOP_NODE_BYTES / 16) : 0u));
+    bar            = uint32_t(__cvta_generic_to_shared(bars + (threadIdx.x >> 5)));
+    if (lane == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+  }
 
   // packets come from the work counter `chunk` at a time (the queue chunk the autotuner picks)
   const unsigned long long chunk = a.chunk > 1 ? (unsigned long long)a.chunk : 1ull;
@@ -139,11 +182,24 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         const int64_t cell = (int64_t(iz) * cv.g + iy) * cv.g + ix;
         const int     ne   = inside ? int(__ldg(cv.count + cell)) : 0;
         if (ne > 0) {
-          const float4* src = cv.entries + size_t(cell) * size_t(cv.lmax) * 2;
-          for (int i = lane; i < 2 * ne; i += 32) {
-            stk[i] = __ldg(src + i);
-          }
+          // The cut (32 B per entry, 16-byte aligned at both ends) comes onto the stack by one
+          // asynchronous bulk copy while the lanes read the cell's radius and test its anchor.
+          // The stack's earlier reads and writes (generic proxy) are ordered before the copy's
+          // writes (async proxy) by every lane's proxy fence and the warp barrier.
+          const float4*  src   = cv.entries + size_t(cell) * size_t(cv.lmax) * 2;
+          const uint32_t bytes = uint32_t(ne) * 32u;
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
+          if (lane == 0) {
+            const uint32_t dst = uint32_t(__cvta_generic_to_shared(stk));
+            asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(bar),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                           dst),
+                         "l"(src), "r"(bytes), "r"(bar)
+                         : "memory");
+          }
           // start below R_C by more than the FP32 error of a triangle distance, so that whatever
           // is found within the bound is nearer than every triangle the cut left out
           const float R = __ldg(cv.radius + cell);
@@ -163,6 +219,17 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
               besttri = anc;
             }
           }
+          // the cut is on the stack once the copy completed the barrier's phase
+          if (!mbarWaitWarp(bar, phase)) {
+            // give up on the packet and the warp's remaining work; wait (bounded again) for the
+            // copy so that no write lands after the warp is gone
+            if (lane == 0) {
+              atomicOr(a.status, ST_COPY);
+            }
+            mbarWaitWarp(bar, phase);
+            return;
+          }
+          phase ^= 1u;
           // Keep only the entries some lane can still need.  A lane needs an entry only if the
           // entry's box is within its bound, and every lane lies in the packet's box, so an entry
           // farther from that box than the largest bound is needed by none: 32 entries per step,
@@ -324,7 +391,7 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
   }
   const int    threads = 32 * wpb;
   const size_t smem    = size_t(wpb) * (2 * (SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH) + 32) * sizeof(float4) +
-                      (TOP ? size_t(a.top_nodes) * TOP_NODE_BYTES : 0);
+                      (TOP ? size_t(a.top_nodes) * TOP_NODE_BYTES : 0) + (SEED == 3 ? size_t(wpb) * 8 : 0);
   // resident blocks per SM for each block size and shared-memory size, looked up once (the query
   // path then issues no runtime calls besides its launches, so it can be captured in a CUDA graph)
   static int    cache[9]     = {0, 0, 0, 0, 0, 0, 0, 0, 0};

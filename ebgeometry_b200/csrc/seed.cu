@@ -1,43 +1,32 @@
 // Learned pruning-radius model (no counterpart in the reference): a multiresolution hash-grid
 // encoding (16 levels x 2 BF16 features, 2^log2T entries per level) feeding a 32-64-64-64-1 ReLU
-// MLP whose matrix products run on the tensor cores as BF16 x BF16 -> FP32 warp MMAs
-// (mma.sync m16n8k16).  Forward, backward and Adam are the kernels below; the exact mesh SDF path
-// generates the training labels.
+// MLP.  The exact mesh SDF path generates the training labels.
 //
-// Per warp the MLP works on a tile of 32 samples held in shared memory:
-//   forward   H1 = relu(X W1^T + b1), H2 = relu(H1 W2^T + b2), H3 = relu(H2 W3^T + b3),
-//             y = H3 w4 + b4                      (X: 32x32 encoding, H: 32x64, BF16 tiles)
-//   backward  dH3 = dy w4^T (.) [H3>0]; dW3 += dH3^T H2; dH2 = dH3 W3 (.) [H2>0]; ...; dX = dH1 W1
-// The weight-gradient products (dW = dH^T H, K = 32 samples) and the input-gradient products
-// (dH_prev = dH W) are also m16n8k16 MMAs; weight gradients are summed per block in shared memory
-// and then added to the global FP32 gradient; encoding gradients are scattered to the FP32 table
-// gradient with atomics (several samples touch one entry).
+// Training (kSeedTrainTc) runs forward and backward on the fifth-generation tensor cores: tiles of
+// 128 samples, BF16 operands in shared memory, FP32 products in tensor memory (tcgen05.mma), the
+// weight gradients accumulated there over all of a CTA's tiles; encoding gradients are scattered
+// to the FP32 table gradient with vector atomics (several samples touch one entry).  Adam updates
+// the FP32 master copies and refreshes the BF16 table.
+//
+// Inference (kSeedPredict: the attach's one prediction per cell, and the far-field surrogate)
+// keeps a warp's 32 activations in registers between layers on m16n8k16 warp MMAs.
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
 
 #include "ebg_device.cuh"
 #include "seed_kernels.h"
+#include "tc_sm100.cuh"
 
 namespace ebg {
 
 namespace {
-
-constexpr int WARPS = 4;
 
 __device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi)
 {
   __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t*>(&h);
-}
-
-__device__ __forceinline__ uint32_t pack2b(__nv_bfloat16 lo, __nv_bfloat16 hi)
-{
-  __nv_bfloat162 h;
-  h.x = lo;
-  h.y = hi;
   return *reinterpret_cast<uint32_t*>(&h);
 }
 
@@ -49,6 +38,9 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
                : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
+
+// x rounded to BF16 (round to nearest even), as a float
+__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 __device__ __forceinline__ float clamp01(float x) { return fminf(fmaxf(x, 0.f), 1.f); }
 
@@ -138,12 +130,6 @@ struct SmemWeights
   float         b4;
 };
 
-struct WarpTiles
-{
-  __nv_bfloat16 x[32 * SEED_IN];
-  __nv_bfloat16 h1[32 * SEED_WIDTH], h2[32 * SEED_WIDTH], h3[32 * SEED_WIDTH];
-};
-
 __device__ void stageWeights(const float* __restrict__ p, SmemWeights& w)
 {
   for (int i = threadIdx.x; i < SEED_WIDTH * SEED_IN; i += blockDim.x) {
@@ -164,249 +150,356 @@ __device__ void stageWeights(const float* __restrict__ p, SmemWeights& w)
   }
 }
 
-// out[32][64] = relu(in[32][K] W^T + b), BF16 tiles, one warp.
-template <int K>
-__device__ void layerForward(const __nv_bfloat16* in, const __nv_bfloat16* W, const float* bias, __nv_bfloat16* out,
-                             int lane)
-{
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int mt = 0; mt < 2; mt++) {
-    uint32_t a[K / 16][4];
-#pragma unroll
-    for (int kc = 0; kc < K / 16; kc++) {
-      const __nv_bfloat16* r0 = in + (mt * 16 + g) * K + kc * 16 + 2 * t;
-      const __nv_bfloat16* r1 = r0 + 8 * K;
-      a[kc][0]                = ld32(r0);
-      a[kc][1]                = ld32(r1);
-      a[kc][2]                = ld32(r0 + 8);
-      a[kc][3]                = ld32(r1 + 8);
-    }
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-      const int n0   = nt * 8 + 2 * t;
-      float     c[4] = {bias[n0], bias[n0 + 1], bias[n0], bias[n0 + 1]};
-#pragma unroll
-      for (int kc = 0; kc < K / 16; kc++) {
-        const __nv_bfloat16* wr = W + (nt * 8 + g) * K + kc * 16 + 2 * t;
-        mma16816(c, a[kc], ld32(wr), ld32(wr + 8));
-      }
-      *reinterpret_cast<uint32_t*>(out + (mt * 16 + g) * SEED_WIDTH + n0)     = pack2(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
-      *reinterpret_cast<uint32_t*>(out + (mt * 16 + g + 8) * SEED_WIDTH + n0) = pack2(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
-    }
-  }
-}
+// ---- training on the fifth-generation tensor cores (tcgen05) ----------------------------------
+//
+// One CTA of 128 threads works on tiles of 128 samples: thread t owns sample t of the tile, which
+// is also row t of every MMA and lane t of tensor memory.  Per tile (all products BF16 x BF16 ->
+// FP32 in TMEM, issued by thread 0, completion through one mbarrier):
+//   forward   D = X W1^T -> H1 = relu(D + b1); D = H1 W2^T -> H2; D = H2 W3^T -> H3; y = H3 . w4 + b4
+//   backward  dH3 = dy w4 [H3 > 0]; D = dH3 W3 -> dH2 (.) [H2 > 0]; D = dH2 W2 -> dH1 (.) [H1 > 0];
+//             D = dH1 W1 -> dX -> hash-table gradient
+// The weight gradients accumulate over all of the CTA's tiles in TMEM, as two M = 128 products over
+// the tile's 128 samples (K):
+//   Gw32 += [dH3^T; dH2^T] [H2^T; H1^T; 1]^T   rows 0-63: dW3 | db3, rows 64-127: dW2 | db2
+//   Gw1  += [H3^T; dH1^T] [X^T; 1; dy]^T       rows 0-63: dW4 (column dy), rows 64-127: dW1 | db1
+// (a row of ones gives the bias gradients as sums over the samples; the off-diagonal blocks are
+// not used).  The transposed activations are written by each thread as its own column.
 
-// Forward of the 32 samples whose encodings are in tiles.x; returns sample `lane`'s output.
-__device__ float mlpForward(const SmemWeights& w, WarpTiles& tl, int lane)
-{
-  layerForward<SEED_IN>(tl.x, w.w1, w.b1, tl.h1, lane);
-  __syncwarp();
-  layerForward<SEED_WIDTH>(tl.h1, w.w2, w.b2, tl.h2, lane);
-  __syncwarp();
-  layerForward<SEED_WIDTH>(tl.h2, w.w3, w.b3, tl.h3, lane);
-  __syncwarp();
-  float y = w.b4;
-#pragma unroll 8
-  for (int n = 0; n < SEED_WIDTH; n++) {
-    y = fmaf(__bfloat162float(tl.h3[lane * SEED_WIDTH + n]), __bfloat162float(w.w4[n]), y);
-  }
-  return y;
-}
+namespace tcs {
 
-__device__ void storeFeatures(WarpTiles& tl, int lane, const float* feat)
-{
-#pragma unroll
-  for (int k = 0; k < SEED_IN; k += 2) {
-    *reinterpret_cast<uint32_t*>(tl.x + lane * SEED_IN + k) = pack2(feat[k], feat[k + 1]);
-  }
-}
+constexpr int      TILE = 128;
+constexpr uint32_t LBO  = 128;     // K-adjacent core matrices are contiguous
+constexpr uint32_t SBO32  = 4 * 128;  // R-adjacent core matrices of a K = 32 tile
+constexpr uint32_t SBO64  = 8 * 128;  // K = 64
+constexpr uint32_t SBO128 = 16 * 128; // K = 128 (the tile's samples)
+constexpr uint32_t N_W32 = 144;       // H2^T (64) + H1^T (64) + ones + 15 zero rows
+constexpr uint32_t N_W1  = 48;        // X^T (32) + ones + dy + 14 zero rows
+// TMEM columns (256 allocated): the two gradient accumulators and the per-layer product
+constexpr uint32_t TM_W32 = 0, TM_W1 = 144, TM_D = 192, TM_COLS = 256;
+constexpr uint32_t WAIT_POLLS = 1u << 22; // about a quarter second per wait before giving up
 
-// ---- backward helpers -------------------------------------------------------------------------
-
-// gW[n][k] += sum_m D[m][n] H[m][k]; D FP32 [32][64], H BF16 [32][K]; MMA with M = 64 (n),
-// N = K (k), reduction over the 32 samples.
-template <int K>
-__device__ void weightGrad(const float* D, const __nv_bfloat16* H, float* gW, int lane)
+struct alignas(128) Smem
 {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll 1
-  for (int mt = 0; mt < 4; mt++) {
-    uint32_t a[2][4];
-#pragma unroll
-    for (int kc = 0; kc < 2; kc++) {
-      const int n0 = mt * 16 + g, m0 = kc * 16 + 2 * t;
-      a[kc][0]     = pack2(D[m0 * SEED_WIDTH + n0], D[(m0 + 1) * SEED_WIDTH + n0]);
-      a[kc][1]     = pack2(D[m0 * SEED_WIDTH + n0 + 8], D[(m0 + 1) * SEED_WIDTH + n0 + 8]);
-      a[kc][2]     = pack2(D[(m0 + 8) * SEED_WIDTH + n0], D[(m0 + 9) * SEED_WIDTH + n0]);
-      a[kc][3]     = pack2(D[(m0 + 8) * SEED_WIDTH + n0 + 8], D[(m0 + 9) * SEED_WIDTH + n0 + 8]);
-    }
-#pragma unroll
-    for (int nt = 0; nt < K / 8; nt++) {
-      float     c[4] = {0.f, 0.f, 0.f, 0.f};
-      const int k0   = nt * 8 + g;
-#pragma unroll
-      for (int kc = 0; kc < 2; kc++) {
-        const int m0 = kc * 16 + 2 * t;
-        const uint32_t b0 = pack2b(H[m0 * K + k0], H[(m0 + 1) * K + k0]);
-        const uint32_t b1 = pack2b(H[(m0 + 8) * K + k0], H[(m0 + 9) * K + k0]);
-        mma16816(c, a[kc], b0, b1);
-      }
-      const int n0 = mt * 16 + g, kk = nt * 8 + 2 * t;
-      atomicAdd(gW + n0 * K + kk, c[0]);
-      atomicAdd(gW + n0 * K + kk + 1, c[1]);
-      atomicAdd(gW + (n0 + 8) * K + kk, c[2]);
-      atomicAdd(gW + (n0 + 8) * K + kk + 1, c[3]);
-    }
-  }
-}
-
-// gb[n] += sum_m D[m][n]
-__device__ void biasGrad(const float* D, float* gb, int lane)
-{
-  for (int n = lane; n < SEED_WIDTH; n += 32) {
-    float s = 0.f;
-    for (int m = 0; m < 32; m++) {
-      s += D[m * SEED_WIDTH + n];
-    }
-    atomicAdd(gb + n, s);
-  }
-}
-
-// P[m][k] = (sum_n D[m][n] W[n][k]) * [H[m][k] > 0]  (mask skipped when H is null); P FP32 with
-// row stride ldP; W BF16 [64][K].
-template <int K>
-__device__ void inputGrad(const float* D, const __nv_bfloat16* W, const __nv_bfloat16* H, float* P, int ldP, int lane)
-{
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll 1
-  for (int mt = 0; mt < 2; mt++) {
-    uint32_t a[4][4];
-#pragma unroll
-    for (int kc = 0; kc < 4; kc++) {
-      const float* r0 = D + (mt * 16 + g) * SEED_WIDTH + kc * 16 + 2 * t;
-      const float* r1 = r0 + 8 * SEED_WIDTH;
-      a[kc][0]        = pack2(r0[0], r0[1]);
-      a[kc][1]        = pack2(r1[0], r1[1]);
-      a[kc][2]        = pack2(r0[8], r0[9]);
-      a[kc][3]        = pack2(r1[8], r1[9]);
-    }
-#pragma unroll
-    for (int nt = 0; nt < K / 8; nt++) {
-      float     c[4] = {0.f, 0.f, 0.f, 0.f};
-      const int k0   = nt * 8 + g;
-#pragma unroll
-      for (int kc = 0; kc < 4; kc++) {
-        const int      n0 = kc * 16 + 2 * t;
-        const uint32_t b0 = pack2b(W[n0 * K + k0], W[(n0 + 1) * K + k0]);
-        const uint32_t b1 = pack2b(W[(n0 + 8) * K + k0], W[(n0 + 9) * K + k0]);
-        mma16816(c, a[kc], b0, b1);
-      }
-      const int r = mt * 16 + g, kk = nt * 8 + 2 * t;
-      if (H != nullptr) {
-        c[0] = __bfloat162float(H[r * K + kk]) > 0.f ? c[0] : 0.f;
-        c[1] = __bfloat162float(H[r * K + kk + 1]) > 0.f ? c[1] : 0.f;
-        c[2] = __bfloat162float(H[(r + 8) * K + kk]) > 0.f ? c[2] : 0.f;
-        c[3] = __bfloat162float(H[(r + 8) * K + kk + 1]) > 0.f ? c[3] : 0.f;
-      }
-      P[r * ldP + kk]           = c[0];
-      P[r * ldP + kk + 1]       = c[1];
-      P[(r + 8) * ldP + kk]     = c[2];
-      P[(r + 8) * ldP + kk + 1] = c[3];
-    }
-  }
-}
-
-struct TrainSmem
-{
-  SmemWeights w;
-  float       grad[SEED_NPARAM];
-  WarpTiles   tiles[WARPS];
-  float       d0[WARPS][32 * SEED_WIDTH];
-  float       d1[WARPS][32 * SEED_WIDTH];
+  unsigned char w1[64 * 32 * 2], w2[64 * 64 * 2], w3[64 * 64 * 2];     // B of the forward products
+  unsigned char w1t[32 * 64 * 2], w2t[64 * 64 * 2], w3t[64 * 64 * 2];  // B of the input gradients
+  unsigned char x[TILE * 32 * 2];                                       // A of layer 1
+  unsigned char ha[TILE * 64 * 2];                                      // H1, then dH2
+  unsigned char hb[TILE * 64 * 2];                                      // H2, then dH3, then dH1
+  unsigned char t[256 * TILE * 2];      // dH3^T, dH2^T, H3^T, dH1^T (rows), samples along K
+  unsigned char bw32[N_W32 * TILE * 2]; // H2^T, H1^T, ones, zeros
+  unsigned char bw1[N_W1 * TILE * 2];   // X^T, ones, dy, zeros
+  float         b1[64], b2[64], b3[64], w4[64];
+  float         b4;
+  uint32_t      tmemSlot;
+  uint64_t      bar;
 };
 
-__global__ void __launch_bounds__(WARPS * 32) kSeedTrain(const SeedTrainArgs a)
+__device__ __forceinline__ void st16(unsigned char* base, uint32_t off, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
 {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  TrainSmem&     S    = *reinterpret_cast<TrainSmem*>(smraw);
-  const int      lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  stageWeights(a.net.params, S.w);
-  for (int i = threadIdx.x; i < SEED_NPARAM; i += blockDim.x) {
-    S.grad[i] = 0.f;
-  }
-  __syncthreads();
-  WarpTiles& tl = S.tiles[wid];
-  float*     D0 = S.d0[wid];
-  float*     D1 = S.d1[wid];
-  const int  tiles = (a.batch + 31) / 32;
-  float      lossAcc = 0.f;
+  *reinterpret_cast<uint4*>(base + off) = make_uint4(a, b, c, d);
+}
 
-  for (int tile = blockIdx.x * WARPS + wid; tile < tiles; tile += gridDim.x * WARPS) {
-    const int     m     = tile * 32 + lane;
+__device__ __forceinline__ void stb(unsigned char* base, uint32_t off, float v)
+{
+  *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
+}
+
+// Row r of an R x K tile (K-major) from 8 consecutive values per 16-byte chunk, rounded to BF16.
+template <int K>
+__device__ __forceinline__ void storeRow(unsigned char* tile, uint32_t sbo, int r, const float* v)
+{
+#pragma unroll
+  for (int c = 0; c < K / 8; c++) {
+    st16(tile, tc::kmajorOffset(uint32_t(r), uint32_t(8 * c), LBO, sbo), pack2(v[8 * c], v[8 * c + 1]),
+         pack2(v[8 * c + 2], v[8 * c + 3]), pack2(v[8 * c + 4], v[8 * c + 5]), pack2(v[8 * c + 6], v[8 * c + 7]));
+  }
+}
+
+// Column s (a sample) of rows r0 .. r0 + n - 1 of a tile whose K is the tile's samples.
+__device__ __forceinline__ void storeCol(unsigned char* tile, int r0, int n, int s, const float* v)
+{
+  for (int i = 0; i < n; i++) {
+    stb(tile, tc::kmajorOffset(uint32_t(r0 + i), uint32_t(s), LBO, SBO128), v[i]);
+  }
+}
+
+// W [R][K] (FP32, row-major) -> BF16 K-major tile; transposed: W^T [K][R].
+__device__ void stageMatrix(const float* __restrict__ W, int R, int K, unsigned char* tile, unsigned char* tileT)
+{
+  for (int i = threadIdx.x; i < R * K; i += blockDim.x) {
+    const int r = i / K, k = i - r * K;
+    stb(tile, tc::kmajorOffset(uint32_t(r), uint32_t(k), LBO, uint32_t(K / 8) * 128u), W[i]);
+    stb(tileT, tc::kmajorOffset(uint32_t(k), uint32_t(r), LBO, uint32_t(R / 8) * 128u), W[i]);
+  }
+}
+
+// The per-layer product of this stage: operands written by every thread are made visible to the
+// tensor cores, thread 0 issues `steps` K-steps of D = A B^T into TMEM column `dcol` (K = 16 each,
+// the A and B tiles advancing 2 * LBO bytes per step), commits them, and every thread waits for
+// them.  `extra` issues further products before the commit (they complete with it).  Returns
+// false if the wait gave up.
+template <class Extra>
+__device__ __forceinline__ bool stage(uint32_t tmem, uint32_t dcol, uint32_t aAddr, uint32_t aSbo, uint32_t bAddr,
+                                     uint32_t bSbo, uint32_t n, int steps, uint32_t bar, uint32_t& phase,
+                                     Extra extra)
+{
+  tc::fenceProxyAsync();
+  tc::fenceBeforeSync();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::fenceAfterSync();
+    extra();
+    for (int k = 0; k < steps; k++) {
+      tc::mma(tmem + dcol, tc::smemDesc(aAddr + uint32_t(k) * 2u * LBO, LBO, aSbo),
+              tc::smemDesc(bAddr + uint32_t(k) * 2u * LBO, LBO, bSbo), tc::idescBf16(n), k > 0 ? 1u : 0u);
+    }
+    tc::commit(bar);
+  }
+  const bool ok = tc::mbarWait(bar, phase, WAIT_POLLS);
+  phase ^= 1u;
+  tc::fenceAfterSync();
+  return __syncthreads_and(ok) != 0;
+}
+
+struct NoExtra
+{
+  __device__ void operator()() const {}
+};
+
+// This thread's TMEM lane, columns [col, col + N) (N a multiple of 16).
+template <int N>
+__device__ __forceinline__ void loadRow(uint32_t tmem, uint32_t col, float* v)
+{
+  const uint32_t lane = (threadIdx.x & ~31u) << 16;
+#pragma unroll
+  for (int c = 0; c < N; c += 16) {
+    float r[16];
+    tc::ld16(tmem + lane + col + uint32_t(c), r);
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      v[c + i] = r[i];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
+{
+  extern __shared__ __align__(128) unsigned char smraw[];
+  Smem&     S = *reinterpret_cast<Smem*>(smraw);
+  const int t = threadIdx.x;
+
+  // weights (BF16, as the forward and backward products read them) and the constant rows
+  stageMatrix(a.net.params + SEED_W1, 64, 32, S.w1, S.w1t);
+  stageMatrix(a.net.params + SEED_W2, 64, 64, S.w2, S.w2t);
+  stageMatrix(a.net.params + SEED_W3, 64, 64, S.w3, S.w3t);
+  if (t < 64) {
+    S.b1[t] = a.net.params[SEED_B1 + t];
+    S.b2[t] = a.net.params[SEED_B2 + t];
+    S.b3[t] = a.net.params[SEED_B3 + t];
+    S.w4[t] = bf16r(a.net.params[SEED_W4 + t]);
+  }
+  if (t == 0) {
+    S.b4 = a.net.params[SEED_B4];
+  }
+  for (int r = 128; r < int(N_W32); r++) {
+    stb(S.bw32, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO, SBO128), r == 128 ? 1.f : 0.f);
+  }
+  for (int r = 32; r < int(N_W1); r++) {
+    stb(S.bw1, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO, SBO128), r == 32 ? 1.f : 0.f);
+  }
+  const uint32_t bar = tc::smemAddr(&S.bar);
+  if (t < 32) {
+    tc::tmemAlloc(tc::smemAddr(&S.tmemSlot), TM_COLS);
+  }
+  if (t == 0) {
+    tc::mbarInit(bar, 1);
+  }
+  tc::fenceBeforeSync();
+  __syncthreads();
+  tc::fenceAfterSync();
+  const uint32_t tmem  = S.tmemSlot;
+  uint32_t       phase = 0;
+  bool           ok    = true;
+
+  const uint32_t aX = tc::smemAddr(S.x), aHA = tc::smemAddr(S.ha), aHB = tc::smemAddr(S.hb);
+  const uint32_t aT = tc::smemAddr(S.t), aW32 = tc::smemAddr(S.bw32), aW1 = tc::smemAddr(S.bw1);
+  const int      tiles   = (a.batch + TILE - 1) / TILE;
+  float          lossAcc = 0.f, dyAcc = 0.f;
+  bool           first   = true;
+
+  for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const int     m     = tile * TILE + t;
     const bool    valid = m < a.batch;
     const int64_t si    = (a.offset + (valid ? m : 0)) % a.poolSize;
     const float   px = a.points[3 * si], py = a.points[3 * si + 1], pz = a.points[3 * si + 2];
     const float   target = a.target[si];
-    float         feat[SEED_IN];
-    encode(a.net, px, py, pz, feat);
-    storeFeatures(tl, lane, feat);
-    __syncwarp();
-    const float y = mlpForward(S.w, tl, lane);
+    float         v[64]; // one row of a layer (registers: only constant indices reach it)
+
+    // forward: the encoding, then three layers
+    {
+      float feat[SEED_IN];
+      encode(a.net, px, py, pz, feat);
+      storeRow<32>(S.x, SBO32, t, feat);
+      storeCol(S.bw1, 0, 32, t, feat);
+    }
+    ok = stage(tmem, TM_D, aX, SBO32, tc::smemAddr(S.w1), SBO32, 64, 2, bar, phase, NoExtra{});
+    if (!ok) {
+      break;
+    }
+    uint32_t mask1[2] = {0u, 0u}, mask2[2] = {0u, 0u};
+    loadRow<64>(tmem, TM_D, v);
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = bf16r(fmaxf(v[n] + S.b1[n], 0.f));
+      mask1[n >> 5] |= (v[n] > 0.f ? 1u : 0u) << (n & 31);
+    }
+    storeRow<64>(S.ha, SBO64, t, v);
+    storeCol(S.bw32, 64, 64, t, v);
+    ok = stage(tmem, TM_D, aHA, SBO64, tc::smemAddr(S.w2), SBO64, 64, 4, bar, phase, NoExtra{});
+    if (!ok) {
+      break;
+    }
+    loadRow<64>(tmem, TM_D, v);
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = bf16r(fmaxf(v[n] + S.b2[n], 0.f));
+      mask2[n >> 5] |= (v[n] > 0.f ? 1u : 0u) << (n & 31);
+    }
+    storeRow<64>(S.hb, SBO64, t, v);
+    storeCol(S.bw32, 0, 64, t, v);
+    ok = stage(tmem, TM_D, aHB, SBO64, tc::smemAddr(S.w3), SBO64, 64, 4, bar, phase, NoExtra{});
+    if (!ok) {
+      break;
+    }
+    loadRow<64>(tmem, TM_D, v);
+    float y = S.b4;
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = bf16r(fmaxf(v[n] + S.b3[n], 0.f));
+      y    = fmaf(v[n], S.w4[n], y);
+    }
+    storeCol(S.t, 128, 64, t, v); // H3^T
 
     // loss = mean w (y - d)^2, w = 1 / (|d| + eps)^2 (relative error away from the surface)
     const float wgt  = 1.f / ((fabsf(target) + a.eps) * (fabsf(target) + a.eps));
     const float diff = y - target;
     const float dy   = valid ? 2.f * wgt * diff / float(a.batch) : 0.f;
     lossAcc += valid ? wgt * diff * diff : 0.f;
+    dyAcc += dy;
+    stb(S.bw1, tc::kmajorOffset(33u, uint32_t(t), LBO, SBO128), dy);
 
-    // output layer: dW4[n] = sum_m H3[m][n] dy_m, db4 = sum_m dy_m, dH3 = dy w4 [H3 > 0]
-    for (int n = lane; n < SEED_WIDTH; n += 32) {
-      float s = 0.f;
-      for (int mm = 0; mm < 32; mm++) {
-        s = fmaf(__bfloat162float(tl.h3[mm * SEED_WIDTH + n]), __shfl_sync(FULL, dy, mm), s);
-      }
-      atomicAdd(S.grad + SEED_W4 + n, s);
+    // backward: dH3 = dy w4 [H3 > 0]
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = v[n] > 0.f ? dy * S.w4[n] : 0.f;
     }
+    storeRow<64>(S.hb, SBO64, t, v);
+    storeCol(S.t, 0, 64, t, v); // dH3^T
+    ok = stage(tmem, TM_D, aHB, SBO64, tc::smemAddr(S.w3t), SBO64, 64, 4, bar, phase, NoExtra{});
+    if (!ok) {
+      break;
+    }
+    loadRow<64>(tmem, TM_D, v);
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = (mask2[n >> 5] >> (n & 31)) & 1u ? v[n] : 0.f;
+    }
+    storeRow<64>(S.ha, SBO64, t, v);
+    storeCol(S.t, 64, 64, t, v); // dH2^T
+    // with dH2 = dD W2: the layer-3 and layer-2 weight gradients accumulate first
+    const uint32_t acc = first ? 0u : 1u;
+    ok = stage(tmem, TM_D, aHA, SBO64, tc::smemAddr(S.w2t), SBO64, 64, 4, bar, phase, [&] {
+      for (int k = 0; k < TILE / 16; k++) {
+        tc::mma(tmem + TM_W32, tc::smemDesc(aT + uint32_t(k) * 2u * LBO, LBO, SBO128),
+                tc::smemDesc(aW32 + uint32_t(k) * 2u * LBO, LBO, SBO128), tc::idescBf16(N_W32),
+                (k > 0 || acc) ? 1u : 0u);
+      }
+    });
+    if (!ok) {
+      break;
+    }
+    loadRow<64>(tmem, TM_D, v);
+#pragma unroll
+    for (int n = 0; n < 64; n++) {
+      v[n] = (mask1[n >> 5] >> (n & 31)) & 1u ? v[n] : 0.f;
+    }
+    storeRow<64>(S.hb, SBO64, t, v);
+    storeCol(S.t, 192, 64, t, v); // dH1^T
+    // dX = dH1 W1, after the layer-1 and output-layer weight gradients
+    ok = stage(tmem, TM_D, aHB, SBO64, tc::smemAddr(S.w1t), SBO64, 32, 4, bar, phase, [&] {
+      const uint32_t a1 = aT + 16u * SBO128; // rows 128-255 of T: H3^T, dH1^T
+      for (int k = 0; k < TILE / 16; k++) {
+        tc::mma(tmem + TM_W1, tc::smemDesc(a1 + uint32_t(k) * 2u * LBO, LBO, SBO128),
+                tc::smemDesc(aW1 + uint32_t(k) * 2u * LBO, LBO, SBO128), tc::idescBf16(N_W1),
+                (k > 0 || acc) ? 1u : 0u);
+      }
+    });
+    if (!ok) {
+      break;
+    }
+    first = false;
     {
-      const float sdy = warpSum(dy);
-      if (lane == 0) {
-        atomicAdd(S.grad + SEED_B4, sdy);
+      float dx[SEED_IN];
+      loadRow<32>(tmem, TM_D, dx);
+      if (valid) {
+        encodeBackward(a.net, px, py, pz, dx, a.gradTable);
       }
     }
-    for (int n = 0; n < SEED_WIDTH; n++) {
-      const float h = __bfloat162float(tl.h3[lane * SEED_WIDTH + n]);
-      D0[lane * SEED_WIDTH + n] = h > 0.f ? dy * __bfloat162float(S.w.w4[n]) : 0.f;
+  }
+
+  if (!ok) {
+    if (t == 0) {
+      atomicOr(a.status, ST_COPY);
     }
-    __syncwarp();
-    weightGrad<SEED_WIDTH>(D0, tl.h2, S.grad + SEED_W3, lane);
-    biasGrad(D0, S.grad + SEED_B3, lane);
-    inputGrad<SEED_WIDTH>(D0, S.w.w3, tl.h2, D1, SEED_WIDTH, lane);
-    __syncwarp();
-    weightGrad<SEED_WIDTH>(D1, tl.h1, S.grad + SEED_W2, lane);
-    biasGrad(D1, S.grad + SEED_B2, lane);
-    inputGrad<SEED_WIDTH>(D1, S.w.w2, tl.h1, D0, SEED_WIDTH, lane);
-    __syncwarp();
-    weightGrad<SEED_IN>(D0, tl.x, S.grad + SEED_W1, lane);
-    biasGrad(D0, S.grad + SEED_B1, lane);
-    inputGrad<SEED_IN>(D0, S.w.w1, nullptr, D1, SEED_IN, lane);
-    __syncwarp();
-    if (valid) {
-      encodeBackward(a.net, px, py, pz, D1 + lane * SEED_IN, a.gradTable);
+    // the products may still be running: wait once more (bounded) before the memory goes away
+    tc::mbarWait(bar, phase ^ 1u, WAIT_POLLS);
+  }
+  else if (!first) {
+    // this CTA's weight gradients, from the accumulators in TMEM
+    const int o = t & 63;
+    float     g[64];
+    if (t < 64) {
+      loadRow<64>(tmem, TM_W32, g); // dW3 row o
+      for (int k = 0; k < 64; k++) {
+        atomicAdd(a.gradParams + SEED_W3 + o * 64 + k, g[k]);
+      }
     }
-    __syncwarp();
+    else {
+      loadRow<64>(tmem, TM_W32 + 64, g); // dW2 row o
+      for (int k = 0; k < 64; k++) {
+        atomicAdd(a.gradParams + SEED_W2 + o * 64 + k, g[k]);
+      }
+    }
+    loadRow<16>(tmem, TM_W32 + 128, g); // column 128: the bias gradient of the row's layer
+    atomicAdd(a.gradParams + (t < 64 ? SEED_B3 : SEED_B2) + o, g[0]);
+    loadRow<48>(tmem, TM_W1, g);
+    if (t < 64) {
+      atomicAdd(a.gradParams + SEED_W4 + o, g[33]);
+    }
+    else {
+      for (int k = 0; k < 32; k++) {
+        atomicAdd(a.gradParams + SEED_W1 + o * 32 + k, g[k]);
+      }
+      atomicAdd(a.gradParams + SEED_B1 + o, g[32]);
+    }
+    const float sdy = warpSum(dyAcc);
+    if ((t & 31) == 0 && sdy != 0.f) {
+      atomicAdd(a.gradParams + SEED_B4, sdy);
+    }
   }
   lossAcc = warpSum(lossAcc);
-  if (lane == 0 && lossAcc != 0.f) {
+  if ((t & 31) == 0 && lossAcc != 0.f) {
     atomicAdd(a.lossSum, lossAcc);
   }
+  tc::fenceBeforeSync();
   __syncthreads();
-  for (int i = threadIdx.x; i < SEED_NPARAM; i += blockDim.x) {
-    if (S.grad[i] != 0.f) {
-      atomicAdd(a.gradParams + i, S.grad[i]);
-    }
+  if (t < 32) {
+    tc::fenceAfterSync();
+    tc::tmemDealloc(tmem, TM_COLS);
   }
 }
+
+} // namespace tcs
 
 // ---- inference with the activations in registers ---------------------------------------------
 //
@@ -456,7 +549,6 @@ __device__ __forceinline__ void reluToA(const float (&c)[8][4], uint32_t (&a)[4]
   }
 }
 
-__device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // The network on the warp's 32 encodings in xt (row q = sample q); returns row `lane`'s output.
 __device__ float mlpRegs(const SmemWeights& w, const __nv_bfloat16* xt, int lane)
@@ -650,14 +742,15 @@ void seedLevels(int baseRes, int maxRes, uint32_t log2T, SeedView& v)
 cudaError_t launchSeedTrainStep(const SeedTrainArgs& a, int numSms, cudaStream_t s)
 {
   // the dynamic shared-memory opt-in is per device, so it is set on every launch (cheap)
-  const cudaError_t e = setSmem<TrainSmem>(reinterpret_cast<const void*>(kSeedTrain));
+  const cudaError_t e = setSmem<tcs::Smem>(reinterpret_cast<const void*>(tcs::kSeedTrainTc));
   if (e != cudaSuccess) {
     return e;
   }
-  const int tiles  = (a.batch + 31) / 32;
-  int       blocks = (tiles + WARPS - 1) / WARPS;
-  blocks           = blocks < numSms ? blocks : numSms;
-  kSeedTrain<<<blocks, WARPS * 32, sizeof(TrainSmem), s>>>(a);
+  // one CTA per SM at most (its shared memory allows no second one, so its TMEM allocation never
+  // waits for another CTA's)
+  const int tiles  = (a.batch + tcs::TILE - 1) / tcs::TILE;
+  const int blocks = tiles < numSms ? tiles : numSms;
+  tcs::kSeedTrainTc<<<blocks, tcs::TILE, sizeof(tcs::Smem), s>>>(a);
   return cudaGetLastError();
 }
 

@@ -48,6 +48,7 @@ struct SeedTrainArgs
   float*        gradParams; // FP32 [NPARAM]
   float*        lossSum;    // accumulated loss (diagnostics)
   float         eps;        // loss weight floor: w = 1 / (|d| + eps)^2
+  int*          status;     // device status word: ST_COPY when a wait for the tensor cores gave up
 };
 
 void        seedLevels(int baseRes, int maxRes, uint32_t log2T, SeedView& v);

@@ -673,10 +673,10 @@ ebg_status ebg_seed_gradients(ebg_seed* seed, const float* points_dev, const flo
  * Queries passing a model that is not attached to the mesh are rejected (EBG_ERR_INVALID). */
 typedef struct ebg_attach_opts
 {
-  int32_t cells_per_axis; /* <= 512; 0 = 1.5 cbrt(tree leaves) rounded up to a multiple of 8,
-                             within 16..128 (96 for 1.3 M triangles) */
+  int32_t cells_per_axis; /* <= 512; 0 = 2 cbrt(tree leaves) rounded up to a multiple of 8,
+                             within 16..128 (128 for 1.3 M triangles) */
   int32_t max_entries;    /* subtrees per cell, <= 112; 0 = 112 (lowered for deep trees).  Memory:
-                             cells * max_entries * 32 B (3.2 GB at 96^3 cells and 112 entries) */
+                             cells * max_entries * 32 B (7.5 GB at 128^3 cells and 112 entries) */
   float   margin_cells;   /* growth of each cell on every side, in cells; <= 0 -> 1.5 */
   int32_t radius_mode;    /* 0 = the model's radius (default); 1 = no radius (cuts ordered by
                              distance only, nothing dropped); 2 = the exact distance at the cell

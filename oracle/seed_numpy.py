@@ -87,19 +87,20 @@ def loss_and_grads(p, d, table, params, lo, scale, res, dense, log2t, eps):
     loss = np.sum(wt * (y - d) ** 2) / n
     dy = 2 * wt * (y - d) / n
     g = np.zeros(NPARAM)
-    g[W4:B4] = H3.T @ dy
+    # The device forms every gradient but b4 as a tensor-core product over the samples, with BF16
+    # operands: the deltas and dy are rounded to BF16, and the bias gradients are products with a
+    # row of ones (sums of the rounded deltas).  b4's gradient sums dy in FP32.
+    g[W4:B4] = H3.T @ bf16(dy)
     g[B4] = dy.sum()
-    # each delta is an FP32 matrix on the device, rounded to BF16 where it is an MMA operand; the
-    # bias gradients sum it unrounded
     dH3 = np.outer(dy, w4) * (H3 > 0)
     g[W3:B3] = (bf16(dH3).T @ H2).ravel()
-    g[B3:W4] = dH3.sum(0)
+    g[B3:W4] = bf16(dH3).sum(0)
     dH2 = (bf16(dH3) @ w3) * (H2 > 0)
     g[W2:B2] = (bf16(dH2).T @ H1).ravel()
-    g[B2:W3] = dH2.sum(0)
+    g[B2:W3] = bf16(dH2).sum(0)
     dH1 = (bf16(dH2) @ w2) * (H1 > 0)
     g[W1:B1] = (bf16(dH1).T @ Xb).ravel()
-    g[B1:W2] = dH1.sum(0)
+    g[B1:W2] = bf16(dH1).sum(0)
     dX = bf16(dH1) @ w1
     gt = np.zeros((LEVELS, T, 2))
     for l, (idx, w) in enumerate(cs):
