@@ -171,7 +171,11 @@ constexpr int      TILE = 128;
 constexpr uint32_t LBO  = 128;     // K-adjacent core matrices are contiguous
 constexpr uint32_t SBO32  = 4 * 128;  // R-adjacent core matrices of a K = 32 tile
 constexpr uint32_t SBO64  = 8 * 128;  // K = 64
-constexpr uint32_t SBO128 = 16 * 128; // K = 128 (the tile's samples)
+// Tiles whose K is the tile's 128 samples are written a column (one sample) per thread; their
+// K-adjacent core matrices sit 144 bytes apart, so that the 2-byte stores of a warp's 32 samples
+// fall in distinct shared-memory banks.
+constexpr uint32_t LBO_S = 144;
+constexpr uint32_t SBO_S = 16 * LBO_S;
 constexpr uint32_t N_W32 = 144;       // H2^T (64) + H1^T (64) + ones + 15 zero rows
 constexpr uint32_t N_W1  = 48;        // X^T (32) + ones + dy + 14 zero rows
 // TMEM columns (256 allocated): the two gradient accumulators and the per-layer product
@@ -185,9 +189,9 @@ struct alignas(128) Smem
   unsigned char x[TILE * 32 * 2];                                       // A of layer 1
   unsigned char ha[TILE * 64 * 2];                                      // H1, then dH2
   unsigned char hb[TILE * 64 * 2];                                      // H2, then dH3, then dH1
-  unsigned char t[256 * TILE * 2];      // dH3^T, dH2^T, H3^T, dH1^T (rows), samples along K
-  unsigned char bw32[N_W32 * TILE * 2]; // H2^T, H1^T, ones, zeros
-  unsigned char bw1[N_W1 * TILE * 2];   // X^T, ones, dy, zeros
+  unsigned char t[256 / 8 * SBO_S];     // dH3^T, dH2^T, H3^T, dH1^T (rows), samples along K
+  unsigned char bw32[N_W32 / 8 * SBO_S]; // H2^T, H1^T, ones, zeros
+  unsigned char bw1[N_W1 / 8 * SBO_S];   // X^T, ones, dy, zeros
   float         b1[64], b2[64], b3[64], w4[64];
   float         b4;
   uint32_t      tmemSlot;
@@ -219,7 +223,7 @@ __device__ __forceinline__ void storeRow(unsigned char* tile, uint32_t sbo, int 
 __device__ __forceinline__ void storeCol(unsigned char* tile, int r0, int n, int s, const float* v)
 {
   for (int i = 0; i < n; i++) {
-    stb(tile, tc::kmajorOffset(uint32_t(r0 + i), uint32_t(s), LBO, SBO128), v[i]);
+    stb(tile, tc::kmajorOffset(uint32_t(r0 + i), uint32_t(s), LBO_S, SBO_S), v[i]);
   }
 }
 
@@ -302,10 +306,10 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
     S.b4 = a.net.params[SEED_B4];
   }
   for (int r = 128; r < int(N_W32); r++) {
-    stb(S.bw32, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO, SBO128), r == 128 ? 1.f : 0.f);
+    stb(S.bw32, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO_S, SBO_S), r == 128 ? 1.f : 0.f);
   }
   for (int r = 32; r < int(N_W1); r++) {
-    stb(S.bw1, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO, SBO128), r == 32 ? 1.f : 0.f);
+    stb(S.bw1, tc::kmajorOffset(uint32_t(r), uint32_t(t), LBO_S, SBO_S), r == 32 ? 1.f : 0.f);
   }
   const uint32_t bar = tc::smemAddr(&S.bar);
   if (t < 32) {
@@ -386,7 +390,7 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
     const float dy   = valid ? 2.f * wgt * diff / float(a.batch) : 0.f;
     lossAcc += valid ? wgt * diff * diff : 0.f;
     dyAcc += dy;
-    stb(S.bw1, tc::kmajorOffset(33u, uint32_t(t), LBO, SBO128), dy);
+    stb(S.bw1, tc::kmajorOffset(33u, uint32_t(t), LBO_S, SBO_S), dy);
 
     // backward: dH3 = dy w4 [H3 > 0]
 #pragma unroll
@@ -410,8 +414,8 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
     const uint32_t acc = first ? 0u : 1u;
     ok = stage(tmem, TM_D, aHA, SBO64, tc::smemAddr(S.w2t), SBO64, 64, 4, bar, phase, [&] {
       for (int k = 0; k < TILE / 16; k++) {
-        tc::mma(tmem + TM_W32, tc::smemDesc(aT + uint32_t(k) * 2u * LBO, LBO, SBO128),
-                tc::smemDesc(aW32 + uint32_t(k) * 2u * LBO, LBO, SBO128), tc::idescBf16(N_W32),
+        tc::mma(tmem + TM_W32, tc::smemDesc(aT + uint32_t(k) * 2u * LBO_S, LBO_S, SBO_S),
+                tc::smemDesc(aW32 + uint32_t(k) * 2u * LBO_S, LBO_S, SBO_S), tc::idescBf16(N_W32),
                 (k > 0 || acc) ? 1u : 0u);
       }
     });
@@ -427,10 +431,10 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
     storeCol(S.t, 192, 64, t, v); // dH1^T
     // dX = dH1 W1, after the layer-1 and output-layer weight gradients
     ok = stage(tmem, TM_D, aHB, SBO64, tc::smemAddr(S.w1t), SBO64, 32, 4, bar, phase, [&] {
-      const uint32_t a1 = aT + 16u * SBO128; // rows 128-255 of T: H3^T, dH1^T
+      const uint32_t a1 = aT + 16u * SBO_S; // rows 128-255 of T: H3^T, dH1^T
       for (int k = 0; k < TILE / 16; k++) {
-        tc::mma(tmem + TM_W1, tc::smemDesc(a1 + uint32_t(k) * 2u * LBO, LBO, SBO128),
-                tc::smemDesc(aW1 + uint32_t(k) * 2u * LBO, LBO, SBO128), tc::idescBf16(N_W1),
+        tc::mma(tmem + TM_W1, tc::smemDesc(a1 + uint32_t(k) * 2u * LBO_S, LBO_S, SBO_S),
+                tc::smemDesc(aW1 + uint32_t(k) * 2u * LBO_S, LBO_S, SBO_S), tc::idescBf16(N_W1),
                 (k > 0 || acc) ? 1u : 0u);
       }
     });
