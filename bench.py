@@ -262,8 +262,9 @@ def packet_bytes(st, n):
     """Bytes the traversal's warps load per call, counted per packet (each distinct line once per
     packet: the packet is what a warp executes): 128 B per interior node opened, 64 B per oriented
     box tested, 48 B per triangle record of an opened leaf, 32 B per entry of a cell's cut plus the
-    cell's count, radius, anchor index and anchor record; and per query its 12-B point, 4-B order
-    index, 4-B result and the winner's 96-B sign record."""
+    cell's count and radius and one anchor index and record (the lanes read those of their own
+    cells, one to eight per packet: counting one keeps this a lower bound); and per query its 12-B
+    point, 4-B order index, 4-B result and the winner's 96-B sign record."""
     return (128 * st["packet_nodes"] + 64 * st["packet_boxes"] + 48 * st["packet_triangle_records"] +
             32 * st["cut_entries"] + 60 * st["cut_packets"] + n * (12 + 4 + 4 + 96))
 

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
         const int     ne   = inside ? int(__ldg(cv.count + cell)) : 0;
         if (ne > 0) {
           // The cut (32 B per entry, 16-byte aligned at both ends) comes onto the stack by one
-          // asynchronous bulk copy while the lanes read the cell's radius and test its anchor.
+          // asynchronous bulk copy while the lanes read the cell's radius and test their anchors.
           // The stack's earlier reads and writes (generic proxy) are ordered before the copy's
           // writes (async proxy) by every lane's proxy fence and the warp barrier.
           const float4*  src   = cv.entries + size_t(cell) * size_t(cv.lmax) * 2;
@@ -205,9 +205,17 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
           const float R = __ldg(cv.radius + cell);
           best          = isfinite(R) ? __fmul_rd(__fmul_rd(R, R), 0.99998f) : FLT_MAX;
           startSp       = ne;
-          // the cell's anchor (the triangle nearest to its centre) gives every lane a real distance
-          // to start from, usually within a hair of its own nearest
-          const int anc = cv.anchor ? __ldg(cv.anchor + cell) : -1;
+          // the anchor of the lane's own cell (the triangle nearest to that cell's centre, which may
+          // be a neighbour of the packet's cell) gives the lane a real distance to start from,
+          // usually within a hair of its own nearest
+          int anc = -1;
+          if (cv.anchor) {
+            const float gm = float(cv.g - 1);
+            const int   lx = int(fminf(fmaxf((px - cv.lo[0]) * cv.inv[0], 0.f), gm));
+            const int   ly = int(fminf(fmaxf((py - cv.lo[1]) * cv.inv[1], 0.f), gm));
+            const int   lz = int(fminf(fmaxf((pz - cv.lo[2]) * cv.inv[2], 0.f), gm));
+            anc            = __ldg(cv.anchor + (int64_t(lz) * cv.g + ly) * cv.g + lx);
+          }
           if (anc >= 0) {
             const float4* h  = reinterpret_cast<const float4*>(m.hot + anc);
             const float4  h0 = __ldg(h), h1 = __ldg(h + 1), h2 = __ldg(h + 2);
