@@ -191,18 +191,22 @@ __device__ double dcelFaceUd2(const double* __restrict__ tri, const double* __re
 // (EVAL 0, TriMeshSDF) or the DCEL face (EVAL 1, MeshSDF); each winner shrinks the lane's bound.
 // Leaves and nodes are pruned by their axis-aligned and oriented boxes (padded to bound the exact
 // distance of every triangle inside from below).  All 32 lanes call it together; `stk` is the
-// warp's stack (EBG_STACK_DEPTH entries).
-template <int EVAL>
+// warp's stack (STACK entries).  The search starts from the `sp0` entries already on the stack
+// (a cell's cut, the top entry popped first), or from the root when sp0 is 0.
+template <int EVAL, int STACK = EBG_STACK_DEPTH>
 __device__ void band64Mesh(const EbgMeshView& m, D3 P, float px, float py, float pz, float shift, float& bound,
-                           double& best, int& bt, float4* stk, uint32_t& iters, int& err)
+                           double& best, int& bt, float4* stk, uint32_t& iters, int& err, int sp0 = 0)
 {
   const int lane = threadIdx.x & 31;
-  int sp = 1;
-  if (lane == 0) {
-    stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
-    stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+  int sp = sp0;
+  if (sp0 == 0) {
+    sp = 1;
+    if (lane == 0) {
+      stk[0] = make_float4(m.root_lo[0], m.root_lo[1], m.root_lo[2], __uint_as_float(m.root_ref));
+      stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
+    }
+    __syncwarp();
   }
-  __syncwarp();
   while (sp > 0) {
     if (++iters > MAX_ITERS) {
       err |= ST_ITERS;
@@ -271,7 +275,7 @@ __device__ void band64Mesh(const EbgMeshView& m, D3 P, float px, float py, float
         }
       }
       for (int i = 0; i < np; i++) {
-        if (sp >= EBG_STACK_DEPTH) {
+        if (sp >= STACK) {
           err |= ST_STACK;
           break;
         }

@@ -15,6 +15,7 @@
 #include <math_constants.h>
 
 #include "band64.cuh"
+#include "cells_kernels.h"
 #include "ebg_device.cuh"
 #include "mesh_kernels.h"
 #include "mesh_traverse.cuh"
@@ -23,15 +24,96 @@ namespace ebg {
 
 namespace {
 
+// A band packet's start from its cell's cut (queries that pass an attached model).  The packet's
+// box over its valid lanes must fit its cell grown by the margin, exactly as the FP32 kernel tests
+// it, and every lane's bound must lie below R_C by the FP32 kernel's margin: every triangle within a
+// lane's bound of its point is then under the cut.  The cut comes onto the stack and the entries
+// farther from the packet's box than the largest bound are dropped.  Returns the entries kept (0:
+// start at the root).
+__device__ int bandCutStart(const SeedCellsView& cv, bool valid, float px, float py, float pz, float bound,
+                            float4* stk)
+{
+  const int   lane = threadIdx.x & 31;
+  const float inf  = __int_as_float(0x7f800000);
+  float       mnx = valid ? px : inf, mny = valid ? py : inf, mnz = valid ? pz : inf;
+  float       mxx = valid ? px : -inf, mxy = valid ? py : -inf, mxz = valid ? pz : -inf;
+  float       bmax = bound;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx  = fminf(mnx, __shfl_xor_sync(FULL, mnx, o));
+    mny  = fminf(mny, __shfl_xor_sync(FULL, mny, o));
+    mnz  = fminf(mnz, __shfl_xor_sync(FULL, mnz, o));
+    mxx  = fmaxf(mxx, __shfl_xor_sync(FULL, mxx, o));
+    mxy  = fmaxf(mxy, __shfl_xor_sync(FULL, mxy, o));
+    mxz  = fmaxf(mxz, __shfl_xor_sync(FULL, mxz, o));
+    bmax = fmaxf(bmax, __shfl_xor_sync(FULL, bmax, o));
+  }
+  const float fx = (0.5f * (mnx + mxx) - cv.lo[0]) * cv.inv[0];
+  const float fy = (0.5f * (mny + mxy) - cv.lo[1]) * cv.inv[1];
+  const float fz = (0.5f * (mnz + mxz) - cv.lo[2]) * cv.inv[2];
+  const float g  = float(cv.g);
+  if (!(fx >= 0.f && fx < g && fy >= 0.f && fy < g && fz >= 0.f && fz < g)) {
+    return 0;
+  }
+  const int  ix = min(int(fx), cv.g - 1), iy = min(int(fy), cv.g - 1), iz = min(int(fz), cv.g - 1);
+  const bool inside =
+    mnx >= __fsub_rd(__fadd_rd(cv.lo[0], float(ix) * cv.size[0]), cv.margin[0]) &&
+    mny >= __fsub_rd(__fadd_rd(cv.lo[1], float(iy) * cv.size[1]), cv.margin[1]) &&
+    mnz >= __fsub_rd(__fadd_rd(cv.lo[2], float(iz) * cv.size[2]), cv.margin[2]) &&
+    mxx <= __fadd_ru(__fadd_ru(cv.lo[0], float(ix + 1) * cv.size[0]), cv.margin[0]) &&
+    mxy <= __fadd_ru(__fadd_ru(cv.lo[1], float(iy + 1) * cv.size[1]), cv.margin[1]) &&
+    mxz <= __fadd_ru(__fadd_ru(cv.lo[2], float(iz + 1) * cv.size[2]), cv.margin[2]);
+  if (!inside) {
+    return 0;
+  }
+  const int64_t cell = (int64_t(iz) * cv.g + iy) * cv.g + ix;
+  const int     ne   = int(__ldg(cv.count + cell));
+  const float   R    = __ldg(cv.radius + cell);
+  if (ne == 0 || !(isfinite(R) && bmax <= __fmul_rd(__fmul_rd(R, R), 0.99998f))) {
+    return 0;
+  }
+  const float4* src = cv.entries + size_t(cell) * size_t(cv.lmax) * 2;
+  __syncwarp(); // the stack's previous reads are done
+  for (int i = lane; i < 2 * ne; i += 32) {
+    stk[i] = __ldg(src + i);
+  }
+  __syncwarp();
+  int kept = 0;
+#pragma unroll 1
+  for (int base = 0; base < ne; base += 32) {
+    const int i    = base + lane;
+    float4    eA   = make_float4(0.f, 0.f, 0.f, 0.f), eB = eA;
+    bool      keep = false;
+    if (i < ne) {
+      eA   = stk[2 * i];
+      eB   = stk[2 * i + 1];
+      keep = boxBoxDist2(eA.x, eA.y, eA.z, eB.x, eB.y, eB.z, mnx, mny, mnz, mxx, mxy, mxz) <= bmax;
+    }
+    const unsigned km = __ballot_sync(FULL, keep);
+    __syncwarp(); // every entry of this step is read before any is overwritten
+    if (keep) {
+      const int r    = kept + __popc(km & ((1u << lane) - 1u));
+      stk[2 * r]     = eA;
+      stk[2 * r + 1] = eB;
+    }
+    kept += __popc(km);
+    __syncwarp();
+  }
+  return kept;
+}
+
 // Eight 128-thread blocks per SM (at most 64 registers, a few spills): the FP64 test is latency
 // bound, and the extra warps outweigh the spills (12 % faster than 90 registers and five blocks).
 // EVAL 0: the reference's Triangle/TriangleSoA test (TriMeshSDF); 1: the DCEL face (MeshSDF).
-template <int EVAL>
+// CUT: the queries passed an attached model, and packets start from their cells' cuts where they
+// can (bandCutStart).
+template <int EVAL, bool CUT>
 __global__ void __launch_bounds__(128, 8) kMeshBand64(const MeshQueryArgs a, float delta)
 {
-  __shared__ float4  smem[4 * 2 * EBG_STACK_DEPTH];
+  constexpr int      STACK = CUT ? CUT_STACK_DEPTH : EBG_STACK_DEPTH;
+  __shared__ float4  smem[4 * 2 * STACK];
   const int          lane  = threadIdx.x & 31;
-  float4*            stk   = smem + (threadIdx.x >> 5) * (2 * EBG_STACK_DEPTH);
+  float4*            stk   = smem + (threadIdx.x >> 5) * (2 * STACK);
   const EbgMeshView& m     = a.mesh;
   const uint32_t     count = *a.band_count;
   const uint32_t     numPk = (count + 31) / 32;
@@ -64,7 +146,8 @@ __global__ void __launch_bounds__(128, 8) kMeshBand64(const MeshQueryArgs a, flo
     uint32_t       iters = 0;
     int            err   = 0;
 
-    band64Mesh<EVAL>(m, P, px, py, pz, shift, bound, best, bt, stk, iters, err);
+    const int sp0 = CUT ? bandCutStart(a.cells, valid, px, py, pz, bound, stk) : 0;
+    band64Mesh<EVAL, STACK>(m, P, px, py, pz, shift, bound, best, bt, stk, iters, err, sp0);
     if (err && lane == 0) {
       atomicOr(a.status, err);
     }
@@ -163,11 +246,20 @@ void launchDoubleToFloat(const double* in, float* out, int64_t count, cudaStream
 
 cudaError_t launchMeshBand64(const MeshQueryArgs& a, float delta, int numSms, cudaStream_t s)
 {
+  const bool cut = a.cells.count != nullptr;
   if (a.eval == 1) {
-    kMeshBand64<1><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+    if (cut) {
+      kMeshBand64<1, true><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+    }
+    else {
+      kMeshBand64<1, false><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+    }
+  }
+  else if (cut) {
+    kMeshBand64<0, true><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
   }
   else {
-    kMeshBand64<0><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
+    kMeshBand64<0, false><<<unsigned(numSms * 8), 128, 0, s>>>(a, delta);
   }
   return cudaGetLastError();
 }

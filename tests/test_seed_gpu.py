@@ -108,6 +108,21 @@ def test_seeded_queries_are_exact_and_cheaper(trained):
     assert s1["seed_fallbacks"] < 0.01 * p.shape[0]
 
 
+def test_seeded_fp64_queries_equal_plain(trained):
+    """FP64 points, every query re-evaluated in FP64: with the model attached, FP64 packets whose
+    bounds lie within their cell's radius start from the cell's cut, the rest from the root; the
+    results equal the plain FP64 call's bit for bit, near the surface and far from it."""
+    mesh, seed = trained
+    v, f = W.displaced_icosphere(5, 1)
+    p = np.concatenate([W.grid_points(48, -1.25, 1.25), W.band_points(v, f, 50000, 5)]).astype(np.float64)
+    pd = torch.from_numpy(p).cuda()
+    d0 = mesh.signed_distance(pd)
+    d1 = mesh.signed_distance(pd, seed=seed)
+    torch.cuda.synchronize()
+    mesh.check_status()
+    assert d0.dtype == torch.float64 and torch.equal(d0, d1)
+
+
 def test_wrong_radius_falls_back(trained):
     mesh, seed = trained
     bad = SeedModel.create(log2_table=12, base_resolution=4, max_resolution=32, lo=[-1.25] * 3, hi=[1.25] * 3)
