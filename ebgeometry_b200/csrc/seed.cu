@@ -180,7 +180,7 @@ constexpr uint32_t N_W32 = 144;       // H2^T (64) + H1^T (64) + ones + 15 zero 
 constexpr uint32_t N_W1  = 48;        // X^T (32) + ones + dy + 14 zero rows
 // TMEM columns (256 allocated): the two gradient accumulators and the per-layer product
 constexpr uint32_t TM_W32 = 0, TM_W1 = 144, TM_D = 192, TM_COLS = 256;
-constexpr uint32_t WAIT_POLLS = 1u << 22; // about a quarter second per wait before giving up
+constexpr uint32_t WAIT_POLLS = 1u << 22; // polls of one wait (64 ns sleeps): under half a second
 
 struct alignas(128) Smem
 {
