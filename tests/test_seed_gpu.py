@@ -123,6 +123,31 @@ def test_seeded_fp64_queries_equal_plain(trained):
     assert d0.dtype == torch.float64 and torch.equal(d0, d1)
 
 
+def test_seeded_queries_in_a_cuda_graph(trained):
+    """The seeded query path (ordering, the cut-started traversal with its bulk copies, the
+    cut-started FP64 band pass) issues only stream-ordered work: captured once in a CUDA graph and
+    replayed, it gives the plain traversal's results."""
+    mesh, seed = trained
+    p = _workload(48, 20000)
+    d0 = mesh.signed_distance(p)
+    out = torch.empty_like(d0)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            mesh.signed_distance(p, out=out, seed=seed, stream=s)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        mesh.signed_distance(p, out=out, seed=seed, stream=s)
+    out.zero_()
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    mesh.check_status()
+    assert torch.equal(out, d0)
+
+
 def test_wrong_radius_falls_back(trained):
     mesh, seed = trained
     bad = SeedModel.create(log2_table=12, base_resolution=4, max_resolution=32, lo=[-1.25] * 3, hi=[1.25] * 3)
