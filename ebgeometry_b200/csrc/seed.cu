@@ -2,11 +2,12 @@
 // encoding (16 levels x 2 BF16 features, 2^log2T entries per level) feeding a 32-64-64-64-1 ReLU
 // MLP.  The exact mesh SDF path generates the training labels.
 //
-// Training (kSeedTrainTc) runs forward and backward on the fifth-generation tensor cores: tiles of
-// 128 samples, BF16 operands in shared memory, FP32 products in tensor memory (tcgen05.mma), the
-// weight gradients accumulated there over all of a CTA's tiles; encoding gradients are scattered
-// to the FP32 table gradient with vector atomics (several samples touch one entry).  Adam updates
-// the FP32 master copies and refreshes the BF16 table.
+// A training step is three kernels: kSeedEncode writes the batch's encodings (BF16); kSeedTrainTc
+// runs the MLP's forward and backward on the fifth-generation tensor cores (tiles of 128 samples,
+// BF16 operands in shared memory, FP32 products in tensor memory through tcgen05.mma, the weight
+// gradients accumulated there over all of a CTA's tiles) and writes each sample's input gradient;
+// kSeedEncodeBackward scatters those to the FP32 table gradient with vector atomics (several
+// samples touch one entry).  Adam then updates the FP32 master copies and refreshes the BF16 table.
 //
 // Inference (kSeedPredict: the attach's one prediction per cell, and the far-field surrogate)
 // keeps a warp's 32 activations in registers between layers on m16n8k16 warp MMAs.
@@ -157,7 +158,7 @@ __device__ void stageWeights(const float* __restrict__ p, SmemWeights& w)
 // FP32 in TMEM, issued by thread 0, completion through one mbarrier):
 //   forward   D = X W1^T -> H1 = relu(D + b1); D = H1 W2^T -> H2; D = H2 W3^T -> H3; y = H3 . w4 + b4
 //   backward  dH3 = dy w4 [H3 > 0]; D = dH3 W3 -> dH2 (.) [H2 > 0]; D = dH2 W2 -> dH1 (.) [H1 > 0];
-//             D = dH1 W1 -> dX -> hash-table gradient
+//             D = dH1 W1 -> dX (written out for kSeedEncodeBackward)
 // The weight gradients accumulate over all of the CTA's tiles in TMEM, as two M = 128 products over
 // the tile's 128 samples (K):
 //   Gw32 += [dH3^T; dH2^T] [H2^T; H1^T; 1]^T   rows 0-63: dW3 | db3, rows 64-127: dW2 | db2
@@ -332,19 +333,33 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
   bool           first   = true;
 
   for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
-    const int     m     = tile * TILE + t;
-    const bool    valid = m < a.batch;
-    const int64_t si    = (a.offset + (valid ? m : 0)) % a.poolSize;
-    const float   px = a.points[3 * si], py = a.points[3 * si + 1], pz = a.points[3 * si + 2];
+    const int     m      = tile * TILE + t;
+    const bool    valid  = m < a.batch;
+    const int64_t si     = (a.offset + (valid ? m : 0)) % a.poolSize;
     const float   target = a.target[si];
     float         v[64]; // one row of a layer (registers: only constant indices reach it)
 
-    // forward: the encoding, then three layers
+    // forward: the sample's encoding (BF16, from kSeedEncode; zeros past the batch), then three layers
     {
-      float feat[SEED_IN];
-      encode(a.net, px, py, pz, feat);
-      storeRow<32>(S.x, SBO32, t, feat);
-      storeCol(S.bw1, 0, 32, t, feat);
+      uint4 xr[4] = {make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u), make_uint4(0u, 0u, 0u, 0u),
+                     make_uint4(0u, 0u, 0u, 0u)};
+      if (valid) {
+        const uint4* src = reinterpret_cast<const uint4*>(a.feat + size_t(m) * SEED_IN);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          xr[c] = __ldg(src + c);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        *reinterpret_cast<uint4*>(S.x + tc::kmajorOffset(uint32_t(t), uint32_t(8 * c), LBO, SBO32)) = xr[c];
+        const uint32_t w[4] = {xr[c].x, xr[c].y, xr[c].z, xr[c].w};
+#pragma unroll
+        for (int h = 0; h < 8; h++) {
+          const unsigned short b = (unsigned short)(h & 1 ? (w[h >> 1] >> 16) : (w[h >> 1] & 0xffffu));
+          *reinterpret_cast<unsigned short*>(S.bw1 + tc::kmajorOffset(uint32_t(8 * c + h), uint32_t(t), LBO_S, SBO_S)) = b;
+        }
+      }
     }
     ok = stage(tmem, TM_D, aX, SBO32, tc::smemAddr(S.w1), SBO32, 64, 2, bar, phase, NoExtra{});
     if (!ok) {
@@ -442,11 +457,13 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
       break;
     }
     first = false;
-    {
-      float dx[SEED_IN];
-      loadRow<32>(tmem, TM_D, dx);
-      if (valid) {
-        encodeBackward(a.net, px, py, pz, dx, a.gradTable);
+    // dX, which kSeedEncodeBackward scatters to the hash tables' gradient
+    loadRow<32>(tmem, TM_D, v);
+    if (valid) {
+      float4* dst = reinterpret_cast<float4*>(a.dfeat + size_t(m) * SEED_IN);
+#pragma unroll
+      for (int c = 0; c < SEED_IN / 4; c++) {
+        dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
       }
     }
   }
@@ -500,6 +517,44 @@ __global__ void __launch_bounds__(TILE, 1) kSeedTrainTc(const SeedTrainArgs a)
   if (t < 32) {
     tc::fenceAfterSync();
     tc::tmemDealloc(tmem, TM_COLS);
+  }
+}
+
+// The encodings of a training step's samples (BF16 rows of 32, the MLP's input as the training
+// kernel reads it), one sample per thread at full occupancy: its 16 x 8 table reads are the step's
+// latency-bound part.
+__global__ void __launch_bounds__(256) kSeedEncode(const SeedTrainArgs a)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.batch; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t si = (a.offset + i) % a.poolSize;
+    float         feat[SEED_IN];
+    encode(a.net, a.points[3 * si], a.points[3 * si + 1], a.points[3 * si + 2], feat);
+    uint4* dst = reinterpret_cast<uint4*>(a.feat + size_t(i) * SEED_IN);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      dst[c] = make_uint4(pack2(feat[8 * c], feat[8 * c + 1]), pack2(feat[8 * c + 2], feat[8 * c + 3]),
+                          pack2(feat[8 * c + 4], feat[8 * c + 5]), pack2(feat[8 * c + 6], feat[8 * c + 7]));
+    }
+  }
+}
+
+// The encoding's gradient: each sample's dX (from the training kernel) scattered to the FP32
+// table gradient through its 16 x 8 corners, one sample per thread at full occupancy.
+__global__ void __launch_bounds__(256) kSeedEncodeBackward(const SeedTrainArgs a)
+{
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < a.batch; i += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t si = (a.offset + i) % a.poolSize;
+    float         dx[SEED_IN];
+    const float4* src = reinterpret_cast<const float4*>(a.dfeat + size_t(i) * SEED_IN);
+#pragma unroll
+    for (int c = 0; c < SEED_IN / 4; c++) {
+      const float4 q = __ldg(src + c);
+      dx[4 * c]      = q.x;
+      dx[4 * c + 1]  = q.y;
+      dx[4 * c + 2]  = q.z;
+      dx[4 * c + 3]  = q.w;
+    }
+    encodeBackward(a.net, a.points[3 * si], a.points[3 * si + 1], a.points[3 * si + 2], dx, a.gradTable);
   }
 }
 
@@ -750,11 +805,16 @@ cudaError_t launchSeedTrainStep(const SeedTrainArgs& a, int numSms, cudaStream_t
   if (e != cudaSuccess) {
     return e;
   }
-  // one CTA per SM at most (its shared memory allows no second one, so its TMEM allocation never
-  // waits for another CTA's)
+  // the encodings, then the MLP's forward and backward on the tensor cores (one CTA per SM at
+  // most: its shared memory allows no second one, so its TMEM allocation never waits for another
+  // CTA's), then the encodings' gradient
+  const int64_t nb   = (int64_t(a.batch) + 255) / 256;
+  const int     gEnc = int(nb < int64_t(numSms) * 8 ? nb : int64_t(numSms) * 8);
+  tcs::kSeedEncode<<<gEnc > 0 ? gEnc : 1, 256, 0, s>>>(a);
   const int tiles  = (a.batch + tcs::TILE - 1) / tcs::TILE;
   const int blocks = tiles < numSms ? tiles : numSms;
   tcs::kSeedTrainTc<<<blocks, tcs::TILE, sizeof(tcs::Smem), s>>>(a);
+  tcs::kSeedEncodeBackward<<<gEnc > 0 ? gEnc : 1, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -49,6 +49,8 @@ struct SeedTrainArgs
   float*        lossSum;    // accumulated loss (diagnostics)
   float         eps;        // loss weight floor: w = 1 / (|d| + eps)^2
   int*          status;     // device status word: ST_COPY when a wait for the tensor cores gave up
+  __nv_bfloat16* feat;      // workspace: the batch's encodings, [batch][32]
+  float*         dfeat;     // workspace: their gradients, [batch][32]
 };
 
 void        seedLevels(int baseRes, int maxRes, uint32_t log2T, SeedView& v);
