@@ -2,6 +2,7 @@
 #ifndef EBG_CAPI_INTERNAL_H
 #define EBG_CAPI_INTERNAL_H
 
+#include <cmath>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -76,6 +77,18 @@ namespace ebg {
 
 // Frees a mesh's entry cuts (if any) and forgets the model they came from.
 void dropCells(ebg_mesh* m);
+
+// The length that the FP32 pass's rounding errors scale with: the mesh's diagonal or, for a mesh
+// far from the origin, the magnitude of its coordinates (FP32 rounds coordinates relative to it).
+inline double fp32ErrorScale(const ebg_mesh* m)
+{
+  double s = m->info.diagonal;
+  for (int a = 0; a < 3; a++) {
+    s = s > std::fabs(m->info.lo[a]) ? s : std::fabs(m->info.lo[a]);
+    s = s > std::fabs(m->info.hi[a]) ? s : std::fabs(m->info.hi[a]);
+  }
+  return s;
+}
 
 // Nodes of the tree's top levels that each block of the FP32 traversal copies into shared memory
 // (ebg_query_opts.top_nodes, at most MAX_TOP_NODES and the tree's node count): plain queries

@@ -512,7 +512,7 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   const int  wpb    = (opts && opts->warps_per_block > 0) ? opts->warps_per_block
                                                           : (m->tunedWpb > 0 ? m->tunedWpb : 4);
   const int  occ    = (opts && opts->occupancy > 0) ? opts->occupancy : m->tunedOccupancy;
-  double     band   = fp64all ? double(INFINITY) : ((opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal);
+  double     band   = fp64all ? double(INFINITY) : ((opts && opts->band > 0) ? opts->band : 1e-4 * fp32ErrorScale(m));
   const ebg_seed* seed = opts ? opts->seed : nullptr;
   if (seed && seed->device != m->device) {
     return setError(EBG_ERR_INVALID, "seed model lives on another device than the mesh");
@@ -624,8 +624,9 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
                                    a.band_count, int(n), s) != cudaSuccess) {
       return setError(EBG_ERR_CUDA, "band list compaction failed");
     }
-    // delta bounds the FP32 distance error (relative 1e-6 of the box diagonal)
-    const float delta = float(2e-6 * m->info.diagonal) + 1e-30f;
+    // delta bounds the FP32 distance error: 2e-6 of the mesh's diagonal, or of its coordinates'
+    // magnitude for a mesh far from the origin (about 17 FP32 roundings of either)
+    const float delta = float(2e-6 * fp32ErrorScale(m)) + 1e-30f;
     if (launchMeshBand64(a, delta, m->numSms, s) != cudaSuccess) {
       return setError(EBG_ERR_CUDA, "band launch failed");
     }

@@ -127,7 +127,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
   const int    wpb      = (opts && opts->warps_per_block > 0) ? opts->warps_per_block
                                                               : (m->tunedWpb > 0 ? m->tunedWpb : 4);
   const int    occ      = (opts && opts->occupancy > 0) ? opts->occupancy : m->tunedOccupancy;
-  const double band     = (opts && opts->band > 0) ? opts->band : 1e-4 * m->info.diagonal;
+  const double band     = (opts && opts->band > 0) ? opts->band : 1e-4 * fp32ErrorScale(m);
 
   // carve the scratch
   const size_t u32n = align256(size_t(n) * sizeof(uint32_t));
@@ -205,7 +205,7 @@ ebg_status ebg_mesh_signed_distance_noalloc(const ebg_mesh*       m,
                                    bandCnt, int(n), s) != cudaSuccess) {
       return cudaFailed("band list compaction");
     }
-    if (launchMeshBand64(a, float(2e-6 * m->info.diagonal) + 1e-30f, m->numSms, s) != cudaSuccess) {
+    if (launchMeshBand64(a, float(2e-6 * fp32ErrorScale(m)) + 1e-30f, m->numSms, s) != cudaSuccess) {
       return cudaFailed("band launch");
     }
   }

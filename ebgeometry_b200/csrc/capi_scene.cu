@@ -31,6 +31,7 @@ struct ebg_scene
   int64_t   numObjects = 0;
   int       depth      = 0;
   double    diagonal   = 0.0; // of the scene's box
+  double    errScale   = 0.0; // what the FP32 union value's rounding errors scale with (see below)
   int       tunedChunk = 0;   // work-queue chunk chosen by ebg_scene_autotune (0 = one packet)
 };
 
@@ -110,7 +111,7 @@ ebg_status sceneQuery(const ebg_scene*      s,
   a.num_batches = nb;
   a.n           = n;
   a.status      = s->dStatus;
-  a.band        = float((opts && opts->band > 0) ? opts->band : 1e-4 * s->diagonal);
+  a.band        = float((opts && opts->band > 0) ? opts->band : 1e-4 * s->errScale);
   auto* counters = static_cast<unsigned long long*>(get(2 * sizeof(unsigned long long))); // work, band count
   int64_t* starts = batches ? static_cast<int64_t*>(get(size_t(nb + 1) * sizeof(int64_t))) : nullptr;
   uint32_t* order = nullptr;
@@ -192,7 +193,7 @@ ebg_status sceneQuery(const ebg_scene*      s,
     }
     else {
       // delta bounds the FP32 error of the union's value: the instance transform and the mesh distance
-      e = launchSceneBand64(a, float(4e-6 * s->diagonal) + 1e-30f, s->numSms, st);
+      e = launchSceneBand64(a, float(4e-6 * s->errScale) + 1e-30f, s->numSms, st);
     }
   }
   release();
@@ -363,6 +364,15 @@ ebg_status ebg_scene_create(int64_t                num_spheres,
   s->diagonal = std::sqrt((bvh.hi[0] - bvh.lo[0]) * (bvh.hi[0] - bvh.lo[0]) +
                           (bvh.hi[1] - bvh.lo[1]) * (bvh.hi[1] - bvh.lo[1]) +
                           (bvh.hi[2] - bvh.lo[2]) * (bvh.hi[2] - bvh.lo[2]));
+  // the scene's diagonal, or the magnitude of its world coordinates or of any mesh's local ones
+  // when those are larger (FP32 rounds coordinates relative to their magnitude)
+  s->errScale = s->diagonal;
+  for (int a = 0; a < 3; a++) {
+    s->errScale = std::max(s->errScale, std::max(std::fabs(bvh.lo[a]), std::fabs(bvh.hi[a])));
+  }
+  for (int64_t m = 0; m < num_meshes; m++) {
+    s->errScale = std::max(s->errScale, fp32ErrorScale(meshes[m]));
+  }
   for (int a = 0; a < 3; a++) {
     v.root_lo[a]      = roundDown(bvh.lo[a]);
     v.root_hi[a]      = roundUp(bvh.hi[a]);

@@ -82,7 +82,9 @@ typedef struct ebg_phase_timings
 /* Per-call options of the mesh signed-distance query.  Zero-initialised = defaults. */
 typedef struct ebg_query_opts
 {
-  double             band;            /* |d| below which the FP64 re-evaluation runs; <= 0 -> 1e-4 * diag */
+  double             band;            /* |d| below which the FP64 re-evaluation runs; <= 0 -> 1e-4 x the
+                                         mesh's diagonal (or x its coordinates' magnitude, for a
+                                         mesh far from the origin) */
   int32_t            no_sort;         /* 1: keep the caller's point order (no Morton reordering) */
   int32_t            no_fp64_band;    /* 1: skip the FP64 near-surface re-evaluation */
   const ebg_seed*    seed;            /* learned pruning-radius model (NULL = plain traversal) */
@@ -545,7 +547,8 @@ ebg_status ebg_scene_destroy(ebg_scene* scene);
 int64_t    ebg_scene_num_objects(const ebg_scene* scene);
 /* BVHUnionIF::value (CSGImplem.hpp:465-501) at n device points: min over the objects, the object
  * BVH pruned with max(0, best)^2.  FP32 with an FP64 near-surface pass: a point whose FP32 value
- * lies within opts->band (default 1e-4 x the scene box's diagonal) of zero is evaluated again in
+ * lies within opts->band (default 1e-4 x the scene box's diagonal, or x the magnitude of the
+ * scene's or its meshes' coordinates when larger) of zero is evaluated again in
  * double as the reference does (the sphere distance, RotateIF's per-axis point map with cos / sin in
  * double, the mesh's FP64 triangle test), over the objects that can hold the minimum.  One
  * persistent launch for the whole array.  Asynchronous on stream; opts->no_sort, no_fp64_band and

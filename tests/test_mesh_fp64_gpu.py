@@ -62,3 +62,27 @@ def test_host_entry_and_value_are_fp64(level5):
     assert tri.min() >= 0 and tri.max() < f.shape[0]
     for i in range(0, 4000, 211):
         assert m.value(p[i]) == pytest.approx(d_ref[i], abs=TOL * m.diagonal)
+
+
+def test_mesh_far_from_the_origin():
+    """A level-4 mesh moved about 60 diagonals from the origin, where FP32 rounds coordinates to
+    about 1.5e-5 (4 x 1e-6 of the diagonal).  The FP32 pass's error bounds scale with the
+    coordinates' magnitude there (fp32ErrorScale), so the FP64 entry point still returns the
+    reference's FP64 values, and the FP32 entry point stays within 1e-6 of that magnitude with the
+    reference's signs outside its band."""
+    v, f = W.displaced_icosphere(4, 61)
+    off = np.array([150.0, -120.0, 90.0])
+    v = v + off
+    rng = np.random.default_rng(62)
+    p = np.concatenate([rng.uniform(-1.5, 1.5, size=(100000, 3)) + off, W.band_points(v, f, 20000, 63)])
+    p = p.astype(np.float32).astype(np.float64)  # points the FP32 entry point can take exactly
+    ref = oracle.ref().mesh(v, f, kind=0, build=0, max_leaf_groups=4)
+    d_ref = ref.sdf(p)
+    m = TriMeshSDF(v, f, build="SAH")
+    scale = max(m.diagonal, float(np.abs(v).max()))
+    d64 = m.signed_distance(torch.from_numpy(p).cuda()).cpu().numpy()
+    check_exact(d64, d_ref, m.diagonal, "far mesh, FP64")
+    d32 = m.signed_distance(torch.from_numpy(p.astype(np.float32)).cuda()).cpu().numpy().astype(np.float64)
+    assert np.abs(d32 - d_ref).max() <= 1e-6 * scale
+    out = np.abs(d_ref) > 1e-4 * scale
+    assert np.sum(np.sign(d32[out]) != np.sign(d_ref[out])) == 0
