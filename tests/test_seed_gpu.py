@@ -123,6 +123,20 @@ def test_seeded_fp64_queries_equal_plain(trained):
     assert d0.dtype == torch.float64 and torch.equal(d0, d1)
 
 
+def test_seeded_queries_outside_the_models_domain(trained):
+    """Points outside the model's domain ([-1.25, 1.25]^3 here) and packets straddling its edge
+    have no cell: they start from the root, and every result equals the plain traversal's."""
+    mesh, seed = trained
+    rng = np.random.default_rng(71)
+    far = rng.uniform(-4.0, 4.0, size=(200000, 3)).astype(np.float32)
+    edge = rng.uniform(1.1, 1.4, size=(50000, 3)).astype(np.float32) * rng.choice([-1.0, 1.0], size=(50000, 3)).astype(np.float32)
+    p = torch.from_numpy(np.concatenate([far, edge])).cuda()
+    d0 = mesh.signed_distance(p)
+    d1, st = mesh.stats(p, seed=seed)
+    assert torch.equal(d0, d1)
+    assert st["cut_packets"] < st["packets"]  # some packets had no cell to start from
+
+
 def test_seeded_queries_in_a_cuda_graph(trained):
     """The seeded query path (ordering, the cut-started traversal with its bulk copies, the
     cut-started FP64 band pass) issues only stream-ordered work: captured once in a CUDA graph and
