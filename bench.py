@@ -91,6 +91,8 @@ def parse():
     ap.add_argument("--traffic-csv", default=None,
                     help="ncu CSV (dram__bytes_read.sum, dram__bytes_write.sum of the traversal kernel) captured "
                          "from this same command; fills roofline.traffic")
+    ap.add_argument("--no-wide", action="store_true",
+                    help="skip the plain traversal through the tree's 8-wide copy (the node-width comparison)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP64 level-5 and k-NN configurations measured beside the headline line")
     ap.add_argument("--seed-samples", type=int, default=1 << 25)
@@ -340,7 +342,8 @@ def run_reference(args, rank, world):
     return 0
 
 
-def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, dist, local_rank, hint=None):
+def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, dist, local_rank, hint=None,
+                node_width=None):
     """K steps bracketed by barrier + synchronize, CUDA events on the launching stream, clocks
     sampled meanwhile; per-phase events recorded inside each call.  Returns (ms/step max over
     ranks, phase array, clocks)."""
@@ -354,7 +357,7 @@ def timed_steps(mesh, pd, out, steps, seed, dev, world, stream, _capi, torch, di
     e0.record(stream)
     for _ in range(steps):
         tm = _capi.PhaseTimings()
-        mesh.signed_distance(pd, out=out, timings=tm, seed=seed, radius_hint=hint)
+        mesh.signed_distance(pd, out=out, timings=tm, seed=seed, radius_hint=hint, node_width=node_width)
         tms.append((tm.order_ms, tm.traverse_ms, tm.band_ms, tm.total_ms))
     e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -398,6 +401,28 @@ def run_ours(args, rank, world, local_rank):
     ms_plain, tms_plain, ck_plain = timed_steps(*tsteps, None, *tctx)
     plain_ref = out.clone() if not args.no_seed else None
     log(f"[rank {rank}] plain {ms_plain:.1f} ms/step")
+
+    # node width: the same plain traversal through the tree's 8-wide copy (same results)
+    wide = None
+    if not args.no_wide:
+        from ebgeometry_b200 import EbgError
+        try:
+            t0 = time.time()
+            winfo = mesh.widen()
+            winfo["widen_s"] = time.time() - t0
+            _, st_w = mesh.stats(pd, node_width=8)
+            wout = torch.empty_like(out)
+            for _ in range(args.warmup):
+                mesh.signed_distance(pd, out=wout, node_width=8)
+            torch.cuda.synchronize(dev)
+            ms_w, tms_w, _ = timed_steps(mesh, pd, wout, args.steps, None, *tctx, node_width=8)
+            wide = {"ms_per_step": ms_w, "value": n * world / (ms_w * 1e-3), "vs_width4": ms_plain / ms_w,
+                    "phase_ms_mean": tms_w, "per_packet": st_w, "tree": winfo,
+                    "equal_to_width4": bool(torch.equal(wout, out))}
+            del wout
+            log(f"[rank {rank}] plain, 8-wide copy {ms_w:.1f} ms/step {winfo}")
+        except EbgError as e:
+            wide = {"error": str(e)}
 
     # what ANY pruning-radius seed could save at best: the exact |d| (from the plain run) as radius
     perfect = None
@@ -559,6 +584,9 @@ def run_ours(args, rank, world, local_rank):
 
     phases = lambda t: {"order": float(t[:, 0].mean()), "traverse": float(t[:, 1].mean()),
                         "band64": float(t[:, 2].mean()), "total": float(t[:, 3].mean())}
+    if wide is not None and "error" not in wide:
+        wide["phase_ms_mean"] = phases(wide["phase_ms_mean"])
+        wide["per_packet"] = per_packet(wide["per_packet"])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -574,7 +602,8 @@ def run_ours(args, rank, world, local_rank):
                    "queries_per_step": n, "l2": "inputs larger than L2 "
                    f"({pts.nbytes / 1e9:.2f} GB of points per step)", "build_s": t_build,
                    "plain": {"value": plain_value, "ms_per_step": ms_plain, "phase_ms_mean": phases(tms_plain),
-                             "per_query": per_query(st), "per_packet": per_packet(st), "clocks": ck_plain},
+                             "per_query": per_query(st), "per_packet": per_packet(st), "clocks": ck_plain,
+                             "node_width8": wide},
                    "perfect_radius_bound": perfect,
                    "seeded": None if seed is None else {
                        "value": value, "ms_per_step": ms_seed, "speedup_vs_plain": value / plain_value,

@@ -177,13 +177,13 @@ class TriMeshSDF:
 
     @staticmethod
     def _opts(band, sort, fp64_band, warps_per_block, timings=None, seed=None, radius_hint=None, occupancy=None,
-              queue_chunk=None, top_nodes=None):
+              queue_chunk=None, top_nodes=None, node_width=None):
         return _capi.QueryOpts(float(band or 0.0), 0 if sort else 1, 0 if fp64_band else 1,
                                seed.handle if seed is not None else None,
                                int(warps_per_block or 0), int(occupancy or 0),
                                C.pointer(timings) if timings is not None else None,
                                radius_hint.data_ptr() if radius_hint is not None else None, int(queue_chunk or 0),
-                               int(top_nodes or 0))
+                               int(top_nodes or 0), int(node_width or 0))
 
     # --- ImplicitFunction<T>::value / SignedDistanceFunction<T>::signedDistance -----------------
     def value(self, point) -> float:
@@ -198,7 +198,7 @@ class TriMeshSDF:
     # --- batched ----------------------------------------------------------------------------------
     def signed_distance(self, points, out=None, closest_tri=None, band=None, sort=True,
                         fp64_band=True, warps_per_block=None, stream=None, timings=None, seed=None,
-                        radius_hint=None, occupancy=None, queue_chunk=None, top_nodes=None):
+                        radius_hint=None, occupancy=None, queue_chunk=None, top_nodes=None, node_width=None):
         """Signed distances of (n,3) float32 points.  CUDA tensors stay on the device (asynchronous
         on ``stream``, default the current torch stream); numpy arrays go through the host entry
         point (synchronous).  Float64 points (numpy or CUDA) take the FP64 entry points: every
@@ -207,9 +207,11 @@ class TriMeshSDF:
         radius seeds the traversal's pruning bound (results stay exact).  ``radius_hint``: a CUDA
         float32 tensor of per-point upper bounds on |d| that seed the bound the same way.
         ``top_nodes``: plain queries read the tree's first ``top_nodes`` nodes from a copy in each
-        block's shared memory (ebg_query_opts.top_nodes; same results)."""
+        block's shared memory (ebg_query_opts.top_nodes; same results).  ``node_width``: 8 traverses
+        the 8-wide copy of the tree made by :meth:`widen` (plain queries; same results), 4 the 4-wide
+        tree, None the mesh's tuned width."""
         opts = self._opts(band, sort, fp64_band, warps_per_block, timings, seed, radius_hint, occupancy, queue_chunk,
-                          top_nodes)
+                          top_nodes, node_width)
         if isinstance(points, np.ndarray) and points.dtype == np.float64:
             p = np.ascontiguousarray(points).reshape(-1, 3)
             n = p.shape[0]
@@ -247,13 +249,14 @@ class TriMeshSDF:
                                            C.byref(opts), _stream_ptr(stream)))
         return (d, closest_tri) if closest_tri is not None else d
 
-    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None, seed=None, radius_hint=None):
+    def stats(self, points, band=None, sort=True, fp64_band=True, stream=None, seed=None, radius_hint=None,
+              node_width=None):
         """Traversal counters summed over the points (synchronous; CUDA tensor input)."""
         import torch
         n = points.numel() // 3
         d = torch.empty(n, dtype=torch.float32, device=points.device)
         st = _capi.QueryStats()
-        opts = self._opts(band, sort, fp64_band, None, None, seed, radius_hint)
+        opts = self._opts(band, sort, fp64_band, None, None, seed, radius_hint, node_width=node_width)
         check(lib.ebg_mesh_signed_distance_stats(self._h, C.c_void_p(points.data_ptr()), n,
                                                  C.c_void_p(d.data_ptr()), C.byref(opts),
                                                  C.byref(st), _stream_ptr(stream)))
@@ -276,15 +279,24 @@ class TriMeshSDF:
     def detach_seed(self):
         check(lib.ebg_seed_detach(self._h))
 
+    def widen(self):
+        """Makes the 8-wide copy of the tree (ebg_mesh_widen) that plain queries can traverse
+        (``node_width=8``, or the autotuner's pick); returns {"num_nodes8", "depth8"}."""
+        n8, d8 = C.c_int64(), C.c_int32()
+        check(lib.ebg_mesh_widen(self._h, C.byref(n8), C.byref(d8)))
+        return {"num_nodes8": n8.value, "depth8": d8.value}
+
     def autotune(self, sample_points, seed=None, stream=None):
-        """Times the traversal launch shapes and the work-queue chunk on a CUDA tensor of sample
-        points (seeded with an attached :class:`SeedModel` if given) and keeps the fastest as this
-        mesh's default; returns {"occupancy", "warps_per_block", "queue_chunk", "ms"}."""
-        o, w, c, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
+        """Times the traversal launch shapes, the work-queue chunk and (plain queries of a mesh
+        with an 8-wide copy, :meth:`widen`) the node width on a CUDA tensor of sample points (seeded
+        with an attached :class:`SeedModel` if given) and keeps the fastest as this mesh's default;
+        returns {"occupancy", "warps_per_block", "queue_chunk", "node_width", "ms"}."""
+        o, w, c, nw, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_float()
         check(lib.ebg_mesh_autotune(self._h, C.c_void_p(sample_points.data_ptr()), sample_points.numel() // 3,
                                     seed.handle if seed is not None else None, C.byref(o), C.byref(w),
-                                    C.byref(c), C.byref(ms), _stream_ptr(stream)))
-        return {"occupancy": o.value, "warps_per_block": w.value, "queue_chunk": c.value, "ms": ms.value}
+                                    C.byref(c), C.byref(nw), C.byref(ms), _stream_ptr(stream)))
+        return {"occupancy": o.value, "warps_per_block": w.value, "queue_chunk": c.value, "node_width": nw.value,
+                "ms": ms.value}
 
 
 def _fp64_call(mesh, dev_fn, host_fn, points, closest_tri, stream, with_opts):

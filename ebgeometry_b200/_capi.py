@@ -26,7 +26,7 @@ class QueryOpts(C.Structure):
     _fields_ = [("band", C.c_double), ("no_sort", C.c_int32), ("no_fp64_band", C.c_int32),
                 ("seed", C.c_void_p), ("warps_per_block", C.c_int32), ("occupancy", C.c_int32),
                 ("timings", C.POINTER(PhaseTimings)), ("radius_hint", C.c_void_p), ("queue_chunk", C.c_int32),
-                ("top_nodes", C.c_int32)]
+                ("top_nodes", C.c_int32), ("node_width", C.c_int32)]
 
 
 class SeedOpts(C.Structure):
@@ -125,7 +125,8 @@ SIGNATURES = {
                                                  C.POINTER(QueryStats), _P]),
     "ebg_mesh_value": (C.c_int, [_P, _D, _D, _D, C.POINTER(_D)]),
     "ebg_mesh_autotune": (C.c_int, [_P, _P, _I64, _P, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_I32),
-                                    C.POINTER(C.c_float), _P]),
+                                    C.POINTER(_I32), C.POINTER(C.c_float), _P]),
+    "ebg_mesh_widen": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I32)]),
     "ebg_check_status": (C.c_int, [_P, _P]),
     "ebg_cloud_create": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P)]),
     "ebg_cloud_create_device": (C.c_int, [_P, _I64, C.POINTER(BuildOpts), C.POINTER(_P), _P]),

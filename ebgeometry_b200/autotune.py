@@ -1,8 +1,9 @@
 """Autotuner for the mesh query path (no reference counterpart).
 
 Two levels: the BVH's build method and leaf size (fixed when a mesh is built, so each candidate is
-a rebuild), and the traversal's launch shape (register budget x warps per block, chosen inside the
-library by ``ebg_mesh_autotune``).  The winner is cached in a JSON file keyed by a hash of the mesh
+a rebuild), and, inside the library (``ebg_mesh_autotune``), the traversal's launch shape (register
+budget x warps per block), the work-queue chunk and the node width (the 4-wide tree or its 8-wide
+copy, ``ebg_mesh_widen``).  The winner is cached in a JSON file keyed by a hash of the mesh
 and the sample size, so later runs build the tuned mesh directly.
 """
 from __future__ import annotations
@@ -23,12 +24,13 @@ def mesh_key(vertices, triangles, n_sample: int) -> str:
 
 
 def tune_mesh(vertices, triangles, sample_points, builds=("SAH", "Morton"), leaf_sizes=(4, 8, 12, 16),
-              cache_path=None, device=0):
-    """Returns {"build", "leaf_size", "occupancy", "warps_per_block", "ms", "candidates"}: the
-    fastest traversal of the sample (float32 (n,3) numpy array) over the candidates."""
+              cache_path=None, device=0, widths=(4, 8)):
+    """Returns {"build", "leaf_size", "occupancy", "warps_per_block", "queue_chunk", "node_width", "ms",
+    "candidates"}: the fastest plain traversal of the sample (float32 (n,3) numpy array) over the
+    candidates.  ``widths`` containing 8 lets each candidate also time its tree's 8-wide copy."""
     import torch
 
-    from . import TriMeshSDF
+    from . import EbgError, TriMeshSDF
     key = mesh_key(vertices, triangles, len(sample_points))
     cache = {}
     if cache_path and os.path.exists(cache_path):
@@ -41,6 +43,11 @@ def tune_mesh(vertices, triangles, sample_points, builds=("SAH", "Morton"), leaf
     for b in builds:
         for leaf in leaf_sizes:
             mesh = TriMeshSDF(vertices, triangles, build=b, leaf_size=leaf, device=device)
+            if 8 in widths:
+                try:
+                    mesh.widen()
+                except EbgError:
+                    pass  # a tree too deep for the 8-wide stack keeps width 4
             r = mesh.autotune(pts)
             cands.append({"build": b, "leaf_size": leaf, **r})
             del mesh
@@ -62,5 +69,7 @@ def build_tuned(vertices, triangles, sample_points, cache_path=None, device=0, *
     from . import TriMeshSDF
     best = tune_mesh(vertices, triangles, sample_points, cache_path=cache_path, device=device, **kw)
     mesh = TriMeshSDF(vertices, triangles, build=best["build"], leaf_size=best["leaf_size"], device=device)
+    if best.get("node_width") == 8:
+        mesh.widen()
     mesh.autotune(torch.from_numpy(np.ascontiguousarray(sample_points, np.float32)).to(f"cuda:{device}"))
     return mesh, best

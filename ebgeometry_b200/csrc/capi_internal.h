@@ -44,6 +44,16 @@ struct ebg_mesh
   int tunedOccupancy = 0;
   int tunedWpb       = 0;
   int tunedChunk     = 0;
+  int tunedWidth     = 0; // 8: plain queries take the 8-wide copy
+  // the optional 8-wide copy of the tree (ebg_mesh_widen; plain FP32 queries): its nodes and their
+  // oriented boxes, and the view the traversal reads them through (the 4-wide view with nodes,
+  // node_obb and root replaced); a refit drops it
+  bool        hasWide   = false;
+  void*       dNodes8   = nullptr;
+  void*       dNodeObb8 = nullptr;
+  EbgMeshView view8{};
+  int64_t     numNodes8 = 0;
+  int32_t     depth8    = 0;
   // per-cell entry cuts built by ebg_seed_attach from `cellsSeed` (queries passing that model use
   // them); a refit drops them
   const ebg_seed*    cellsSeed    = nullptr;
@@ -77,6 +87,9 @@ namespace ebg {
 
 // Frees a mesh's entry cuts (if any) and forgets the model they came from.
 void dropCells(ebg_mesh* m);
+
+// Frees a mesh's 8-wide copy of the tree (if any); plain queries go back to the 4-wide tree.
+void dropWide(ebg_mesh* m);
 
 // The length that the FP32 pass's rounding errors scale with: the mesh's diagonal or, for a mesh
 // far from the origin, the magnitude of its coordinates (FP32 rounds coordinates relative to it).

@@ -521,6 +521,15 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   if (seed && !(m->cellsSeed == seed && m->dCellCount != nullptr)) {
     return setError(EBG_ERR_INVALID, "the seed model is not attached to this mesh (ebg_seed_attach)");
   }
+  // node width of the FP32 traversal: the cuts index the 4-wide tree, so seeded queries keep it
+  const int askedWidth = (opts && opts->node_width > 0) ? opts->node_width : 0;
+  if (askedWidth != 0 && askedWidth != 4 && askedWidth != 8) {
+    return setError(EBG_ERR_INVALID, "node_width must be 0, 4 or 8");
+  }
+  if (askedWidth == 8 && !m->hasWide) {
+    return setError(EBG_ERR_INVALID, "node_width 8 needs the mesh's 8-wide copy (ebg_mesh_widen)");
+  }
+  const int width = seed ? 4 : (askedWidth ? askedWidth : (m->tunedWidth == 8 && m->hasWide ? 8 : 4));
 
   // optional per-phase events (ev[0] start, [1] after ordering, [2] after traversal, [3] end)
   ebg_phase_timings* tm = opts ? opts->timings : nullptr;
@@ -613,9 +622,17 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
     a.cells = m->cellsView;
   }
   a.top_nodes = topNodesFor(m, opts, seed != nullptr);
+  if (width == 8) {
+    // the 8-wide copy's nodes (the FP64 pass below reads the 4-wide tree again)
+    a.mesh       = m->view8;
+    a.node_width = 8;
+    a.top_nodes  = 0;
+  }
   if (launchMeshSdf32(a, wpb, m->numSms, s, occ) != cudaSuccess) {
     return setError(EBG_ERR_CUDA, std::string("traversal launch failed: ") + cudaGetErrorString(cudaGetLastError()));
   }
+  a.mesh       = m->view;
+  a.node_width = 4;
   if (tm) {
     cudaEventRecord(ev[2], s);
   }
@@ -647,6 +664,19 @@ ebg_status ebg::meshQuery(const ebg_mesh*       m,
   return EBG_OK;
 }
 
+
+void ebg::dropWide(ebg_mesh* m)
+{
+  cudaFree(m->dNodes8);
+  cudaFree(m->dNodeObb8);
+  m->dNodes8    = nullptr;
+  m->dNodeObb8  = nullptr;
+  m->hasWide    = false;
+  m->numNodes8  = 0;
+  m->depth8     = 0;
+  m->tunedWidth = 0;
+  m->view8      = EbgMeshView{};
+}
 
 extern "C" {
 
@@ -725,6 +755,7 @@ ebg_status ebg_mesh_destroy(ebg_mesh* m)
   cudaFree(m->dNodeFirst);
   cudaFree(m->dNodeEnd);
   dropCells(m);
+  dropWide(m);
   delete m;
   return EBG_OK;
 }
@@ -744,6 +775,7 @@ static ebg_status meshRefit(ebg_mesh* m, const double* vertices, bool onDevice, 
   // the entry cuts were cut from the old boxes; they would no longer hold every near triangle
   cudaStreamSynchronize(s);
   dropCells(m);
+  dropWide(m); // the copy holds the old boxes
   double       lo[3], hi[3];
   const ebg_status rc = refitMeshOnDevice(m, vertices, onDevice, nv, lo, hi, s);
   if (rc != EBG_OK) {
@@ -1195,6 +1227,7 @@ ebg_status ebg_mesh_autotune(ebg_mesh*       m,
                              int32_t*        best_occupancy,
                              int32_t*        best_warps_per_block,
                              int32_t*        best_queue_chunk,
+                             int32_t*        best_node_width,
                              float*          best_ms,
                              void*           stream)
 {
@@ -1210,12 +1243,13 @@ ebg_status ebg_mesh_autotune(ebg_mesh*       m,
     return setError(EBG_ERR_NO_MEMORY, "autotune output buffer");
   }
   // the traversal time of one candidate: the best of two timed runs after a warm-up run
-  auto timeOne = [&](int o, int w, int c, float& ms) -> ebg_status {
+  auto timeOne = [&](int o, int w, int c, float& ms, int width = 4) -> ebg_status {
     ebg_query_opts    q{};
     ebg_phase_timings t{};
     q.occupancy       = o;
     q.warps_per_block = w;
     q.queue_chunk     = c;
+    q.node_width      = width;
     q.no_fp64_band    = 1;
     q.seed            = seed;
     ms                = INFINITY;
@@ -1265,11 +1299,35 @@ ebg_status ebg_mesh_autotune(ebg_mesh*       m,
       bestC  = c;
     }
   }
+  // node width: the 8-wide copy at the launch shapes again (its node visits differ), kept when faster
+  int bestWidth = 4;
+  if (seed == nullptr && m->hasWide && !(m->view.root_ref & EBG_LEAF_BIT)) {
+    for (int o : occs) {
+      for (int w : wpbs) {
+        if (o != 4 && w > 4) {
+          continue;
+        }
+        float            ms = INFINITY;
+        const ebg_status rc = timeOne(o, w, bestC, ms, 8);
+        if (rc != EBG_OK) {
+          cudaFreeAsync(out, s);
+          return rc;
+        }
+        if (ms < bestMs) {
+          bestMs    = ms;
+          bestO     = o;
+          bestW     = w;
+          bestWidth = 8;
+        }
+      }
+    }
+  }
   cudaFreeAsync(out, s);
   cudaStreamSynchronize(s);
   m->tunedOccupancy = bestO;
   m->tunedWpb       = bestW;
   m->tunedChunk     = bestC;
+  m->tunedWidth     = bestWidth;
   if (best_occupancy) {
     *best_occupancy = bestO;
   }
@@ -1279,8 +1337,69 @@ ebg_status ebg_mesh_autotune(ebg_mesh*       m,
   if (best_queue_chunk) {
     *best_queue_chunk = bestC;
   }
+  if (best_node_width) {
+    *best_node_width = bestWidth;
+  }
   if (best_ms) {
     *best_ms = bestMs;
+  }
+  return EBG_OK;
+}
+
+ebg_status ebg_mesh_widen(ebg_mesh* m, int64_t* num_nodes8, int32_t* depth8)
+{
+  if (m == nullptr) {
+    return setError(EBG_ERR_INVALID, "null mesh");
+  }
+  DeviceGuard guard;
+  cudaSetDevice(m->device);
+  if (!m->hasWide) {
+    if (m->view.root_ref & EBG_LEAF_BIT) {
+      // a single leaf: nothing to widen, the 8-wide traversal meets the same root
+      m->view8   = m->view;
+      m->hasWide = true;
+    }
+    else {
+      const size_t          nn = size_t(m->info.num_nodes);
+      std::vector<EbgNode4> n4(nn);
+      std::vector<EbgObb>   o4(nn);
+      if (cudaMemcpy(n4.data(), m->dNodes, nn * sizeof(EbgNode4), cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(o4.data(), m->dNodeObb, nn * sizeof(EbgObb), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        return setError(EBG_ERR_CUDA, std::string("widen: reading the tree: ") + cudaGetErrorString(cudaGetLastError()));
+      }
+      std::vector<EbgNode8> n8;
+      std::vector<EbgObb>   o8;
+      int                   d8 = 0;
+      std::string           msg;
+      if (!widenBvh8(n4, o4, m->info.num_triangles, m->info.num_leaves, n8, o8, d8, msg)) {
+        return setError(msg.find("too deep") != std::string::npos ? EBG_ERR_TOO_LARGE : EBG_ERR_INVALID, msg);
+      }
+      if (cudaMalloc(&m->dNodes8, n8.size() * sizeof(EbgNode8)) != cudaSuccess ||
+          cudaMalloc(&m->dNodeObb8, o8.size() * sizeof(EbgObb)) != cudaSuccess) {
+        cudaGetLastError();
+        dropWide(m);
+        return setError(EBG_ERR_NO_MEMORY, "widen: device allocation for the 8-wide nodes");
+      }
+      if (cudaMemcpy(m->dNodes8, n8.data(), n8.size() * sizeof(EbgNode8), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(m->dNodeObb8, o8.data(), o8.size() * sizeof(EbgObb), cudaMemcpyHostToDevice) != cudaSuccess) {
+        const std::string e = cudaGetErrorString(cudaGetLastError());
+        dropWide(m);
+        return setError(EBG_ERR_CUDA, "widen: uploading the 8-wide nodes: " + e);
+      }
+      // the root keeps its box and index 0; the kernels read EbgNode8 records through these
+      m->view8          = m->view;
+      m->view8.nodes    = static_cast<const EbgNode4*>(m->dNodes8);
+      m->view8.node_obb = static_cast<const EbgObb*>(m->dNodeObb8);
+      m->numNodes8      = int64_t(n8.size());
+      m->depth8         = d8;
+      m->hasWide        = true;
+    }
+  }
+  if (num_nodes8) {
+    *num_nodes8 = m->numNodes8;
+  }
+  if (depth8) {
+    *depth8 = m->depth8;
   }
   return EBG_OK;
 }

@@ -55,6 +55,18 @@ struct alignas(128) EbgNode4
   uint32_t count[4];
 };
 
+// The optional 8-wide copy of the tree (plain FP32 queries only; mesh_wide.cpp): two 128-byte
+// lines per node, the boxes of eight children as structure-of-arrays (lo.x[8] ... hi.z[8]), then
+// child[8] and count[8] with the 4-wide node's meanings.  Leaves and child boxes are the 4-wide
+// tree's own, so results do not depend on the width.
+struct alignas(128) EbgNode8
+{
+  float    lox[8], loy[8], loz[8];
+  float    hix[8], hiy[8], hiz[8];
+  uint32_t child[8];
+  uint32_t count[8];
+};
+
 struct alignas(16) EbgTriHot
 {
   float v0x, v0y, v0z, ab2;
@@ -85,6 +97,7 @@ struct alignas(16) EbgObb
 };
 
 static_assert(sizeof(EbgNode4) == 128, "node must be one 128-byte line");
+static_assert(sizeof(EbgNode8) == 256, "8-wide node must be two 128-byte lines");
 static_assert(sizeof(EbgObb) == 64, "oriented box must be 64 bytes");
 static_assert(sizeof(EbgTriHot) == 48, "hot triangle record must be 48 bytes");
 static_assert(sizeof(EbgTriSign) == 96, "sign record must be 96 bytes");

@@ -62,6 +62,19 @@ bool buildBvh4(const std::vector<double>& boxLo,
                Bvh4&                      out,
                std::string&               msg);
 
+// The 8-wide copy of a 4-wide tree whose root is node 0 (mesh_wide.cpp): nodes in breadth-first
+// order (the root first), each with the oriented box of the 4-wide node it was made from.  depth8
+// counts the levels of the deepest path, the leaf level included.  Returns false (with msg) when a
+// reference is out of range or the tree is too deep for the traversal stack.
+bool widenBvh8(const std::vector<EbgNode4>& n4,
+               const std::vector<EbgObb>&   obb4,
+               int64_t                      numTris,
+               int64_t                      numLeaves,
+               std::vector<EbgNode8>&       n8,
+               std::vector<EbgObb>&         obb8,
+               int&                         depth8,
+               std::string&                 msg);
+
 // Outward rounding of FP64 box bounds to FP32.
 float roundDown(double x);
 float roundUp(double x);

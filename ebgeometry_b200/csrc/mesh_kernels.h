@@ -37,6 +37,8 @@ struct MeshQueryArgs
   SeedCellsView      cells;      // per-cell entry cuts (used when cells.count is non-null)
   uint32_t           top_nodes;  // nodes [0, top_nodes) and their oriented boxes are read from a copy
                                  // in each block's shared memory (0: none)
+  int                node_width; // 8: mesh.nodes / mesh.node_obb are the 8-wide copy (EbgNode8; plain
+                                 // and hinted queries, no top nodes); else the 4-wide tree
 };
 
 // Morton keys of the query points (30 bits) and the identity permutation.

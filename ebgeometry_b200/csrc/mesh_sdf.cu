@@ -76,9 +76,11 @@ struct Bounds
 };
 
 // TOP: each block copies the tree's first a.top_nodes nodes into shared memory (plain queries only).
-template <bool STATS, int SEED, int OCC, bool TOP = false>
+// W: node width of the tree a.mesh points at, 4 or 8 (the 8-wide copy: plain or hinted queries).
+template <bool STATS, int SEED, int OCC, bool TOP = false, int W = 4>
 __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMeshSdf32(const MeshQueryArgs a)
 {
+  static_assert(W == 4 || (W == 8 && SEED != 3 && !TOP), "the cuts and the top-tree copy index the 4-wide tree");
   extern __shared__ float4 smem[];
   constexpr int STACK = SEED == 3 ? CUT_STACK_DEPTH : EBG_STACK_DEPTH;
   const int     lane = threadIdx.x & 31;
@@ -293,10 +295,11 @@ __global__ void __launch_bounds__(Bounds<OCC>::threads, Bounds<OCC>::blocks) kMe
       }
       TraversalCounters tc;
       if (SEED == 3 && pass == 0 && fromCut) {
-        traverseFrom<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc, topS, topN);
+        traverseFrom<STATS, STACK, TOP, W>(m, px, py, pz, best, besttri, stk, lpts, startSp, iters, err, tc, topS,
+                                           topN);
       }
       else {
-        traverseMesh<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc, topS, topN);
+        traverseMesh<STATS, STACK, TOP, W>(m, px, py, pz, best, besttri, stk, lpts, iters, err, tc, topS, topN);
       }
       cNode += tc.node;
       cLeaf += tc.leaf;
@@ -391,7 +394,7 @@ __global__ void kQueryKeys(const float* __restrict__ pts, int64_t n, float lx, f
   ids[i]  = uint32_t(i);
 }
 
-template <bool STATS, int SEED, int OCC, bool TOP>
+template <bool STATS, int SEED, int OCC, bool TOP, int W = 4>
 cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
   if (OCC != 0 && wpb > 4) {
@@ -408,13 +411,13 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
   if (perSm == 0) {
     if (smem > 48 * 1024) {
       const cudaError_t e =
-        cudaFuncSetAttribute(kMeshSdf32<STATS, SEED, OCC, TOP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaFuncSetAttribute(kMeshSdf32<STATS, SEED, OCC, TOP, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
       if (e != cudaSuccess) {
         return e;
       }
     }
     const cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC, TOP>, threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kMeshSdf32<STATS, SEED, OCC, TOP, W>, threads, smem);
     if (e != cudaSuccess) {
       return e;
     }
@@ -426,7 +429,7 @@ cudaError_t launchOne(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t 
   int64_t       grid  = int64_t(numSms) * perSm;
   grid                = grid < need ? grid : need;
   grid                = grid < 1 ? 1 : grid;
-  kMeshSdf32<STATS, SEED, OCC, TOP><<<unsigned(grid), threads, smem, s>>>(a);
+  kMeshSdf32<STATS, SEED, OCC, TOP, W><<<unsigned(grid), threads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -444,6 +447,12 @@ void launchQueryKeys(const float* points, int64_t n, const float* lo, const floa
 template <int SEED, int OCC>
 cudaError_t launchStats(const MeshQueryArgs& a, int wpb, int numSms, cudaStream_t s)
 {
+  if constexpr (SEED != 3) {
+    if (a.node_width == 8) {
+      return a.stats != nullptr ? launchOne<true, SEED, OCC, false, 8>(a, wpb, numSms, s)
+                                : launchOne<false, SEED, OCC, false, 8>(a, wpb, numSms, s);
+    }
+  }
   if (SEED == 0 && a.top_nodes > 0) {
     return a.stats != nullptr ? launchOne<true, SEED, OCC, SEED == 0>(a, wpb, numSms, s)
                               : launchOne<false, SEED, OCC, SEED == 0>(a, wpb, numSms, s);

@@ -166,8 +166,10 @@ constexpr uint32_t TOP_NODE_BYTES = 192;
 // STACK entries); `pts` is this warp's 32-entry scratch for the points of the lanes a leaf is spread
 // over; `iters` counts loop trips against MAX_ITERS; `err` receives ST_* bits.  With TOP, nodes
 // with index below `topN` are read from the block's shared-memory copy at shared address `topS`
-// (TOP_NODE_BYTES per node).  All 32 lanes must call it together.
-template <bool STATS, int STACK, bool TOP = false>
+// (TOP_NODE_BYTES per node).  W is the tree's node width: 4 (EbgNode4, every kernel) or 8 (the
+// optional EbgNode8 copy, m.nodes and m.node_obb then point at the 8-wide arrays; no TOP).  All 32
+// lanes must call it together.
+template <bool STATS, int STACK, bool TOP = false, int W = 4>
 __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, float py, float pz, float& best,
                                              int& besttri, float4* stk, float4* pts, int sp, uint32_t& iters,
                                              int& err, TraversalCounters& cnt_, uint32_t topS = 0,
@@ -287,6 +289,85 @@ __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, flo
             }
           }
         }
+        else if constexpr (W == 8) {
+          static_assert(!TOP, "the shared-memory top tree is a 4-wide option");
+          // 16 float4 per node: lo.x[8] lo.y[8] lo.z[8] hi.x[8] hi.y[8] hi.z[8] child[8] count[8];
+          // the first half's boxes go out before the oriented-box test, which overlaps their latency
+          const float4* nd  = reinterpret_cast<const float4*>(m.nodes) + size_t(ref) * 16u;
+          float4        lx = __ldg(nd), ly = __ldg(nd + 2), lz = __ldg(nd + 4);
+          float4        hx = __ldg(nd + 6), hy = __ldg(nd + 8), hz = __ldg(nd + 10);
+          bool          needN = need;
+          if (cntw & EBG_NODE_HAS_OBB) {
+            const float4* ob = reinterpret_cast<const float4*>(m.node_obb + ref);
+            const float4  o0 = __ldg(ob), o1 = __ldg(ob + 1), o2 = __ldg(ob + 2), o3 = __ldg(ob + 3);
+            needN            = need && obbDist2(o0, o1, o2, o3, px, py, pz) <= best;
+            if (STATS) {
+              cnt_.box += need;
+              cnt_.pbox++;
+            }
+            if (!__any_sync(FULL, needN)) {
+              continue;
+            }
+          }
+          if (STATS && needN) {
+            cnt_.node++;
+          }
+          if (STATS) {
+            cnt_.pnode++;
+          }
+          float key[8];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (h == 1) {
+              lx = __ldg(nd + 1), ly = __ldg(nd + 3), lz = __ldg(nd + 5);
+              hx = __ldg(nd + 7), hy = __ldg(nd + 9), hz = __ldg(nd + 11);
+            }
+            const float clx[4] = {lx.x, lx.y, lx.z, lx.w}, cly[4] = {ly.x, ly.y, ly.z, ly.w},
+                        clz[4] = {lz.x, lz.y, lz.z, lz.w};
+            const float chx[4] = {hx.x, hx.y, hx.z, hx.w}, chy[4] = {hy.x, hy.y, hy.z, hy.w},
+                        chz[4] = {hz.x, hz.y, hz.z, hz.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const float dk = needN ? boxDist2(clx[k], cly[k], clz[k], chx[k], chy[k], chz[k], px, py, pz)
+                                     : __int_as_float(0x7f800000);
+              const bool  nk = __any_sync(FULL, dk <= best);
+              key[4 * h + k] = nk ? __uint_as_float(__reduce_min_sync(FULL, __float_as_uint(dk))) : -1.f;
+            }
+          }
+          int np = 0;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            np += int(key[k] >= 0.f);
+          }
+          if (sp + np > STACK) {
+            err |= ST_STACK;
+            break;
+          }
+          // lane k (< 8) writes child k into its slot, nearest on top, as in the 4-wide case
+          if (lane < 8) {
+            float kk = key[0];
+#pragma unroll
+            for (int j = 1; j < 8; j++) {
+              kk = lane == j ? key[j] : kk;
+            }
+            if (kk >= 0.f) {
+              int rank = 0;
+#pragma unroll
+              for (int j = 0; j < 8; j++) {
+                rank += int(key[j] >= 0.f && (key[j] > kk || (key[j] == kk && j < lane)));
+              }
+              float4*      e  = stk + 2 * (sp + rank);
+              const float* nf = reinterpret_cast<const float*>(nd) + lane;
+              e[0]            = make_float4(__ldg(nf), __ldg(nf + 8), __ldg(nf + 16), __ldg(nf + 48));
+              e[1]            = make_float4(__ldg(nf + 24), __ldg(nf + 32), __ldg(nf + 40), __ldg(nf + 56));
+            }
+          }
+          sp += np;
+          __syncwarp();
+          if (err) {
+            break;
+          }
+        }
         else {
           // the node's loads go out first; the oriented-box test below overlaps their latency
           const float4*  nd    = reinterpret_cast<const float4*>(m.nodes + ref);
@@ -384,7 +465,7 @@ __device__ __forceinline__ void traverseFrom(const EbgMeshView& m, float px, flo
 }
 
 // One packet traversal from the root of mesh m (see traverseFrom).
-template <bool STATS, int STACK = EBG_STACK_DEPTH, bool TOP = false>
+template <bool STATS, int STACK = EBG_STACK_DEPTH, bool TOP = false, int W = 4>
 __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, float py, float pz, float& best,
                                              int& besttri, float4* stk, float4* pts, uint32_t& iters, int& err,
                                              TraversalCounters& cnt_, uint32_t topS = 0, uint32_t topN = 0)
@@ -394,7 +475,7 @@ __device__ __forceinline__ void traverseMesh(const EbgMeshView& m, float px, flo
     stk[1] = make_float4(m.root_hi[0], m.root_hi[1], m.root_hi[2], __uint_as_float(m.root_count));
   }
   __syncwarp();
-  traverseFrom<STATS, STACK, TOP>(m, px, py, pz, best, besttri, stk, pts, 1, iters, err, cnt_, topS, topN);
+  traverseFrom<STATS, STACK, TOP, W>(m, px, py, pz, best, besttri, stk, pts, 1, iters, err, cnt_, topS, topN);
 }
 
 } // namespace ebg

@@ -153,6 +153,13 @@ public:
     check(ebg_mesh_refit(m_mesh, &a_vertices[0][0], int64_t(a_vertices.size()), a_stream));
   }
 
+  // The 8-wide copy of the tree (ebg_mesh_widen) for plain queries: taken when the autotuner picks
+  // width 8, or when a query's options ask for it.  Same results; a refit drops the copy.
+  void widen()
+  {
+    check(ebg_mesh_widen(m_mesh, nullptr, nullptr));
+  }
+
   ebg_mesh_info info() const
   {
     ebg_mesh_info i{};

@@ -111,6 +111,12 @@ typedef struct ebg_query_opts
                                          at most 512; 0 = none (the default, and the faster on the
                                          level-8 workload).  Seeded queries start below the top
                                          levels and ignore it. */
+  int32_t            node_width;      /* plain (and radius-hinted) FP32 traversals: 4 = the 4-wide
+                                         tree, 8 = the mesh's 8-wide copy (ebg_mesh_widen; without
+                                         one: EBG_ERR_INVALID); 0 = the mesh's tuned width (4 until
+                                         ebg_mesh_autotune picks 8).  Same results either way;
+                                         seeded queries and the FP64 pass read the 4-wide tree.
+                                         With 8, top_nodes is ignored. */
 } ebg_query_opts;
 
 /* Mesh summary. */
@@ -371,8 +377,8 @@ ebg_status ebg_mesh_signed_distance_flat_f64_host(const ebg_mesh* mesh,
  * for their own arena at start-up, so a library's cudaMalloc or stream-ordered allocation can fail
  * inside their embedded-boundary loop, and other codes forbid allocations there for latency.  The
  * per-call workspace comes from a fixed 24 MiB array compiled into the library instead of the memory
- * pool.  Limits: n <= 524,288 points per call (larger n returns EBG_ERR_TOO_LARGE); opts->timings is
- * ignored.  The first call on a device (n = 0 is enough) resolves the array's address there, and
+ * pool.  Limits: n <= 524,288 points per call (larger n returns EBG_ERR_TOO_LARGE); opts->timings and
+ * opts->node_width are ignored (the 4-wide tree is traversed).  The first call on a device (n = 0 is enough) resolves the array's address there, and
  * with lazy module loading (the CUDA default) that is also when the 24 MiB are taken on that device,
  * where they stay until the process exits: make that first call before reserving a memory arena and
  * before capturing a CUDA graph.  cudaDeviceReset on the device invalidates the array; do not call
@@ -396,13 +402,17 @@ ebg_status ebg_mesh_signed_distance_stats(const ebg_mesh*       mesh,
                                           ebg_query_stats*      stats,
                                           void*                 stream);
 
-/* Autotuner (no reference counterpart): times the traversal's launch shapes -- register budget
+/* Autotuner (no reference counterpart; the reference fixes its branching ratio and SoA width at
+ * compile time, DefaultBranchingRatio, BVH.hpp:89-111, and TriangleSoA::DefaultWidth,
+ * TriangleSoA.hpp:55-77): times the traversal's launch shapes -- register budget
  * (ebg_query_opts.occupancy 1..4) x warps per block (2, 4, 8), then the work-queue chunk (1, 2, 4
- * packets per grab) at the fastest shape -- on the caller's sample points (device), keeps the
- * fastest as this mesh's default for queries that leave those options at 0, and returns it
- * (best_occupancy / best_warps_per_block / best_queue_chunk, any of them nullable; best_ms = the
- * sample's traversal time).  `seed` (nullable) times the seeded traversal of a model attached to
- * the mesh.  Synchronous. */
+ * packets per grab) at the fastest shape, then (plain traversal of a mesh with an 8-wide copy,
+ * ebg_mesh_widen) the node width 8 against 4 at that shape, with the launch shape re-tuned for
+ * width 8 -- on the caller's sample points (device), keeps the fastest as this mesh's default for
+ * queries that leave those options at 0, and returns it (best_occupancy / best_warps_per_block /
+ * best_queue_chunk / best_node_width, any of them nullable; best_ms = the sample's traversal time).
+ * `seed` (nullable) times the seeded traversal of a model attached to the mesh (node width 4).
+ * Synchronous. */
 ebg_status ebg_mesh_autotune(ebg_mesh*       mesh,
                              const float*    sample_points_dev,
                              int64_t         n,
@@ -410,8 +420,21 @@ ebg_status ebg_mesh_autotune(ebg_mesh*       mesh,
                              int32_t*        best_occupancy,
                              int32_t*        best_warps_per_block,
                              int32_t*        best_queue_chunk,
+                             int32_t*        best_node_width,
                              float*          best_ms,
                              void*           stream);
+
+/* The 8-wide copy of the mesh's tree for plain FP32 queries (no reference counterpart: the
+ * reference's branching ratio is the compile-time K of BVH.hpp:89-111).  Made on the host from the
+ * 4-wide tree: each 8-wide node takes one 4-wide node's children and replaces the largest-area
+ * interior child by that child's own children while they fit in eight slots.  Leaves and child
+ * boxes are the 4-wide tree's, so queries through it give the same results bit for bit, with fewer
+ * levels and more boxes tested per node.  Costs 256 B + 64 B per 8-wide node on the device.
+ * num_nodes8 / depth8 (nullable) receive its node count and its levels on the deepest path (leaf
+ * level included).  A mesh whose root is a leaf needs no copy (EBG_OK, 0 nodes).  A tree too deep
+ * for the 8-wide traversal's stack: EBG_ERR_TOO_LARGE.  ebg_mesh_refit drops the copy (and a
+ * tuned width of 8).  Synchronous. */
+ebg_status ebg_mesh_widen(ebg_mesh* mesh, int64_t* num_nodes8, int32_t* depth8);
 
 /* ImplicitFunction<T>::value(point) for one point (ImplicitFunction.hpp:51-52): the drop-in
  * single-point call, in FP64 (ebg_mesh_signed_distance_f64_host).  Synchronous; each call is a few
